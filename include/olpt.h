@@ -1,0 +1,116 @@
+/*
+ * olpt.h -- C ABI of the B200-native OpenLPT hot path (libolpt_cuda.so).
+ *
+ * Plain C types only: no exceptions cross this boundary, every entry returns an
+ * olpt_status_t and olpt_last_error(ctx) holds the message of the last failure.
+ * A context owns one CUDA stream and all device-resident state of one camera
+ * rig (cameras, OTF table, current images, 2D detections, 3D objects).  Calls on
+ * one context are stream-ordered; entry points that return host data
+ * synchronise the context's stream before returning.  One context per host
+ * thread; a context must not be used from two threads at once.
+ *
+ * Each entry cites the reference (OpenLPT) interface it replaces.
+ */
+#ifndef OLPT_H
+#define OLPT_H
+
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+typedef enum olpt_status {
+  OLPT_OK = 0,
+  OLPT_ERR_INVALID_ARG = 1,
+  OLPT_ERR_OOM = 2,
+  OLPT_ERR_CUDA = 3,
+  OLPT_ERR_TIMEOUT = 4,
+  OLPT_ERR_UNSUPPORTED = 5,
+  OLPT_ERR_INTERNAL = 6
+} olpt_status_t;
+
+typedef enum olpt_dtype { OLPT_U8 = 0, OLPT_U16 = 1, OLPT_F32 = 2, OLPT_F64 = 3 } olpt_dtype_t;
+
+typedef struct olpt_ctx olpt_ctx;
+
+/* Camera parameters, as read by Camera::loadParameters (src/srcMath/Camera.cpp:19-158).
+ * type 0 = PINHOLE, 1 = POLYNOMIAL.  Polynomial coefficient tables are
+ * n_coeff x 4 row-major (coeff, x_power, y_power, z_power). */
+typedef struct olpt_camera_desc {
+  int type;
+  int n_row, n_col;
+  int is_active;
+  double cam_mtx[9];
+  int n_dist;
+  double dist[12];
+  double r_mtx[9], t_vec[3], r_inv[9], t_inv[3];
+  int ref_plane; /* 1 = REF_X, 2 = REF_Y, 3 = REF_Z */
+  double plane[2];
+  int n_coeff;
+  const double* u_coeffs;
+  const double* v_coeffs;
+} olpt_camera_desc;
+
+/* ------------------------------------------------------------------ context */
+/* (no reference counterpart: the reference is host-only) */
+olpt_status_t olpt_ctx_create(olpt_ctx** out, int device);
+void olpt_ctx_destroy(olpt_ctx* ctx);
+const char* olpt_last_error(const olpt_ctx* ctx);
+/* Synchronise the context's stream. */
+olpt_status_t olpt_sync(olpt_ctx* ctx);
+
+/* ------------------------------------------------------------------ cameras */
+/* Replaces std::vector<Camera> set-up (Camera::loadParameters, Camera.cpp:19-158;
+ * polynomial derivative tables as Camera::updatePolyDuDv, Camera.cpp:340-393). */
+olpt_status_t olpt_cameras_upload(olpt_ctx* ctx, const olpt_camera_desc* cams, int n_cam);
+/* Replaces toggling Camera::_is_active (inc/libMath/Camera.h:83; CameraUtil::setActiveSubset). */
+olpt_status_t olpt_cameras_set_active(olpt_ctx* ctx, const int* active);
+/* Camera::project (Camera.cpp:648-677) for n world points; host arrays n x 3 -> n x 2. */
+olpt_status_t olpt_camera_project(olpt_ctx* ctx, int cam, int64_t n, const double* xyz,
+                                  double* uv);
+/* Camera::lineOfSight (Camera.cpp:996-1016) for n image points; out n x 6 (pt, unit). */
+olpt_status_t olpt_camera_los(olpt_ctx* ctx, int cam, int64_t n, const double* uv,
+                              double* line6);
+/* myMATH::triangulation (src/srcMath/myMATH.cpp:357-419) for n_sets independent sets
+ * of k lines (n_sets x k x 6); out n_sets x 4 (x, y, z, err), ok[i] = 0 where the
+ * reference throws (negative squared distance). */
+olpt_status_t olpt_triangulate(olpt_ctx* ctx, int64_t n_sets, int k, const double* lines6,
+                               double* out4, int* ok);
+
+/* ------------------------------------------------------------------ OTF */
+/* OTF::loadParam(file) contents (src/srcSTB/OTF.cpp:195-243): grid sizes, boundary
+ * (xmin,xmax,ymin,ymax,zmin,zmax) and a table [4][n_cam][nx*ny*nz] of a, b, c, alpha. */
+olpt_status_t olpt_otf_upload(olpt_ctx* ctx, int nx, int ny, int nz, const double* bound6,
+                              const double* abca);
+/* OTF::getOTFParam (OTF.cpp:273-338) for n points on one camera; out n x 5
+ * (a, b, c, cos alpha, sin alpha). */
+olpt_status_t olpt_otf_param(olpt_ctx* ctx, int cam, int64_t n, const double* xyz, double* out5);
+
+/* ------------------------------------------------------------------ images */
+/* Load the current image of every camera (replaces building std::vector<Image>,
+ * inc/libMath/Matrix.h:171, from ImageIO::loadImg).  imgs[c] points to H[c] x W[c]
+ * elements of `dtype` with row pitch pitch_bytes[c] (0 = dense).  on_device != 0
+ * means the pointers are device pointers (zero host traffic). */
+olpt_status_t olpt_images_upload(olpt_ctx* ctx, int n_cam, olpt_dtype_t dtype,
+                                 const void* const* imgs, const int* H, const int* W,
+                                 const int64_t* pitch_bytes, int on_device);
+/* Copy the current image of camera `cam` to host memory as `dtype` (F32 or F64). */
+olpt_status_t olpt_image_download(olpt_ctx* ctx, int cam, olpt_dtype_t dtype, void* out);
+
+/* ------------------------------------------------------------------ 2D detection */
+/* ObjectFinder2D::findObject2D -> findTracer2D (src/srcObject/ObjectFinder.cpp:6-111) on the
+ * current image of every active camera, keeping detections on the device.
+ * counts (host, n_cam) receives the number of detections per camera. */
+olpt_status_t olpt_find_peaks(olpt_ctx* ctx, double min_obj_int, int64_t* counts);
+/* Download detections of one camera in raster order: xy (n x 2, x = col, y = row) and
+ * the integer peak pixel rc (n x 2: row, col); either may be NULL. */
+olpt_status_t olpt_get_peaks(olpt_ctx* ctx, int cam, double* xy, int32_t* rc, int64_t cap);
+/* Replace the detections of every camera with host lists (n_cam arrays of n x 2). */
+olpt_status_t olpt_detections_upload(olpt_ctx* ctx, int n_cam, const int64_t* counts,
+                                     const double* const* xy);
+
+#ifdef __cplusplus
+}
+#endif
+#endif /* OLPT_H */

@@ -1,0 +1,198 @@
+"""ctypes binding of the C ABI in include/olpt.h (libolpt_cuda.so).
+
+This is the thin Python view of the boundary: plain pointers and sizes, no torch
+types.  It fails loudly when the CUDA library has not been built.
+"""
+from __future__ import annotations
+
+import ctypes as C
+import os
+from typing import Optional, Sequence
+
+import numpy as np
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+LIB_PATH = os.path.join(HERE, "libolpt_cuda.so")
+
+OLPT_U8, OLPT_U16, OLPT_F32, OLPT_F64 = 0, 1, 2, 3
+_DTYPES = {np.dtype(np.uint8): OLPT_U8, np.dtype(np.uint16): OLPT_U16,
+           np.dtype(np.float32): OLPT_F32, np.dtype(np.float64): OLPT_F64}
+
+_dp = C.POINTER(C.c_double)
+_i64p = C.POINTER(C.c_int64)
+_i32p = C.POINTER(C.c_int32)
+
+
+class CameraDesc(C.Structure):
+    _fields_ = [
+        ("type", C.c_int), ("n_row", C.c_int), ("n_col", C.c_int), ("is_active", C.c_int),
+        ("cam_mtx", C.c_double * 9), ("n_dist", C.c_int), ("dist", C.c_double * 12),
+        ("r_mtx", C.c_double * 9), ("t_vec", C.c_double * 3), ("r_inv", C.c_double * 9),
+        ("t_inv", C.c_double * 3), ("ref_plane", C.c_int), ("plane", C.c_double * 2),
+        ("n_coeff", C.c_int), ("u_coeffs", _dp), ("v_coeffs", _dp),
+    ]
+
+
+class OlptError(RuntimeError):
+    def __init__(self, code: int, msg: str):
+        super().__init__(f"olpt status {code}: {msg}")
+        self.code = code
+
+
+_lib = None
+
+
+def lib():
+    global _lib
+    if _lib is None:
+        if not os.path.exists(LIB_PATH):
+            raise ImportError(f"{LIB_PATH} is missing: run __graft_entry__.build() "
+                              "(the CUDA extension is required; there is no CPU path)")
+        L = C.CDLL(LIB_PATH)
+        L.olpt_last_error.restype = C.c_char_p
+        L.olpt_last_error.argtypes = [C.c_void_p]
+        L.olpt_ctx_destroy.argtypes = [C.c_void_p]
+        _lib = L
+    return _lib
+
+
+def _p(a: Optional[np.ndarray], t=_dp):
+    return None if a is None else a.ctypes.data_as(t)
+
+
+def camera_desc_from_pinhole(cam, active: bool = True) -> CameraDesc:
+    d = CameraDesc()
+    d.type = 0
+    d.n_row, d.n_col, d.is_active = cam.n_row, cam.n_col, int(active)
+    K = [cam.fx, 0.0, cam.cx, 0.0, cam.fy, cam.cy, 0.0, 0.0, 1.0]
+    for i in range(9):
+        d.cam_mtx[i] = K[i]
+    dist = list(cam.dist)
+    d.n_dist = len(dist)
+    for i, v in enumerate(dist):
+        d.dist[i] = v
+    R, Ri, T, Ti = cam.R.ravel(), cam.Rinv.ravel(), cam.T, cam.Tinv
+    for i in range(9):
+        d.r_mtx[i] = R[i]
+        d.r_inv[i] = Ri[i]
+    for i in range(3):
+        d.t_vec[i] = T[i]
+        d.t_inv[i] = Ti[i]
+    return d
+
+
+class Context:
+    """One olpt_ctx (one CUDA stream + device-resident rig state)."""
+
+    def __init__(self, device: int = 0):
+        self.L = lib()
+        h = C.c_void_p()
+        self._check(self.L.olpt_ctx_create(C.byref(h), device), None)
+        self.h = h
+        self.n_cam = 0
+
+    def _check(self, rc: int, h=None):
+        if rc != 0:
+            msg = self.L.olpt_last_error(h if h is not None else self.h).decode() \
+                if (h is not None or getattr(self, "h", None)) else ""
+            raise OlptError(rc, msg)
+
+    def close(self):
+        if getattr(self, "h", None):
+            self.L.olpt_ctx_destroy(self.h)
+            self.h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    # ---------------------------------------------------------------- rig
+    def upload_cameras(self, descs: Sequence[CameraDesc]):
+        arr = (CameraDesc * len(descs))(*descs)
+        self._keep = descs
+        self._check(self.L.olpt_cameras_upload(self.h, arr, len(descs)))
+        self.n_cam = len(descs)
+
+    def set_active(self, active: Sequence[int]):
+        a = (C.c_int * self.n_cam)(*[int(x) for x in active])
+        self._check(self.L.olpt_cameras_set_active(self.h, a))
+
+    def upload_otf(self, nx: int, ny: int, nz: int, bound6, abca: np.ndarray):
+        b = np.ascontiguousarray(bound6, dtype=np.float64)
+        t = np.ascontiguousarray(abca, dtype=np.float64)
+        self._check(self.L.olpt_otf_upload(self.h, nx, ny, nz, _p(b), _p(t)))
+
+    def project(self, cam: int, xyz: np.ndarray) -> np.ndarray:
+        xyz = np.ascontiguousarray(xyz, dtype=np.float64).reshape(-1, 3)
+        uv = np.empty((len(xyz), 2))
+        self._check(self.L.olpt_camera_project(self.h, cam, C.c_int64(len(xyz)), _p(xyz), _p(uv)))
+        return uv
+
+    def los(self, cam: int, uv: np.ndarray) -> np.ndarray:
+        uv = np.ascontiguousarray(uv, dtype=np.float64).reshape(-1, 2)
+        out = np.empty((len(uv), 6))
+        self._check(self.L.olpt_camera_los(self.h, cam, C.c_int64(len(uv)), _p(uv), _p(out)))
+        return out
+
+    def triangulate(self, lines: np.ndarray):
+        """lines: (n_sets, k, 6) -> (out (n_sets, 4), ok (n_sets,))"""
+        lines = np.ascontiguousarray(lines, dtype=np.float64)
+        n, k = lines.shape[0], lines.shape[1]
+        out = np.empty((n, 4))
+        ok = np.empty(n, dtype=np.int32)
+        self._check(self.L.olpt_triangulate(self.h, C.c_int64(n), k, _p(lines), _p(out), _p(ok, _i32p)))
+        return out, ok.astype(bool)
+
+    def otf_param(self, cam: int, xyz: np.ndarray) -> np.ndarray:
+        xyz = np.ascontiguousarray(xyz, dtype=np.float64).reshape(-1, 3)
+        out = np.empty((len(xyz), 5))
+        self._check(self.L.olpt_otf_param(self.h, cam, C.c_int64(len(xyz)), _p(xyz), _p(out)))
+        return out
+
+    # ---------------------------------------------------------------- images
+    def upload_images(self, imgs: Sequence[np.ndarray]):
+        imgs = [np.ascontiguousarray(im) for im in imgs]
+        dt = _DTYPES[imgs[0].dtype]
+        ptrs = (C.c_void_p * len(imgs))(*[im.ctypes.data for im in imgs])
+        H = (C.c_int * len(imgs))(*[im.shape[0] for im in imgs])
+        W = (C.c_int * len(imgs))(*[im.shape[1] for im in imgs])
+        self._check(self.L.olpt_images_upload(self.h, len(imgs), dt, ptrs, H, W, None, 0))
+        self._imgs_keep = imgs
+
+    def upload_images_device(self, ptrs: Sequence[int], dtype: int, H, W, pitch=None):
+        n = len(ptrs)
+        p = (C.c_void_p * n)(*ptrs)
+        h = (C.c_int * n)(*H)
+        w = (C.c_int * n)(*W)
+        pt = None if pitch is None else (C.c_int64 * n)(*pitch)
+        self._check(self.L.olpt_images_upload(self.h, n, dtype, p, h, w, pt, 1))
+
+    def image(self, cam: int, dtype=np.float64) -> np.ndarray:
+        H, W = self._shape(cam)
+        out = np.empty((H, W), dtype=dtype)
+        self._check(self.L.olpt_image_download(self.h, cam, _DTYPES[np.dtype(dtype)],
+                                               out.ctypes.data_as(C.c_void_p)))
+        return out
+
+    def _shape(self, cam: int):
+        return self._imgs_keep[cam].shape
+
+    # ---------------------------------------------------------------- detections
+    def find_peaks(self, min_int: float):
+        counts = np.zeros(self.n_cam, dtype=np.int64)
+        self._check(self.L.olpt_find_peaks(self.h, C.c_double(min_int), _p(counts, _i64p)))
+        return counts
+
+    def get_peaks(self, cam: int, n: int):
+        xy = np.empty((n, 2))
+        rc = np.empty((n, 2), dtype=np.int32)
+        self._check(self.L.olpt_get_peaks(self.h, cam, _p(xy), _p(rc, _i32p), C.c_int64(n)))
+        return xy, rc
+
+    def upload_detections(self, dets: Sequence[np.ndarray]):
+        d = [np.ascontiguousarray(x, dtype=np.float64).reshape(-1, 2) for x in dets]
+        counts = np.array([len(x) for x in d], dtype=np.int64)
+        ptrs = (_dp * len(d))(*[_p(x) for x in d])
+        self._check(self.L.olpt_detections_upload(self.h, len(d), _p(counts, _i64p), ptrs))

@@ -1,0 +1,513 @@
+// C ABI entry points: context, cameras, OTF, images, geometry helpers, detections.
+// Declarations and reference citations: include/olpt.h.
+#include <cuda_runtime.h>
+
+#include <cmath>
+#include <new>
+#include <string>
+#include <vector>
+
+#include "olpt_ctx.cuh"
+#include "olpt_otf.cuh"
+
+namespace olpt {
+void find_peaks_device(olpt_ctx* ctx, double min_int, bool sync_counts);
+void ensure_det_capacity(olpt_ctx* ctx, int cam, int64_t cap);
+
+template <class F>
+olpt_status_t guard(olpt_ctx* ctx, F&& f) {
+  if (!ctx) return OLPT_ERR_INVALID_ARG;
+  try {
+    OLPT_CUDA(cudaSetDevice(ctx->device));
+    f();
+    ctx->err.clear();
+    return OLPT_OK;
+  } catch (ApiError const& e) {
+    ctx->err = e.msg;
+    return e.code;
+  } catch (CudaError const& e) {
+    ctx->err = std::string(cudaGetErrorString(e.code)) + " (" + e.where + ")";
+    return e.code == cudaErrorMemoryAllocation ? OLPT_ERR_OOM : OLPT_ERR_CUDA;
+  } catch (std::bad_alloc const&) {
+    ctx->err = "host allocation failed";
+    return OLPT_ERR_OOM;
+  } catch (std::exception const& e) {
+    ctx->err = e.what();
+    return OLPT_ERR_INTERNAL;
+  }
+}
+
+namespace {
+
+__global__ void project_kernel(const CamDev* cams, int cam, int64_t n, const double* xyz,
+                               double* uv) {
+  int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+  if (i >= n) return;
+  double u, v;
+  cam_project(cams[cam], xyz[3 * i], xyz[3 * i + 1], xyz[3 * i + 2], u, v);
+  uv[2 * i] = u;
+  uv[2 * i + 1] = v;
+}
+
+__global__ void los_kernel(const CamDev* cams, int cam, int64_t n, const double* uv,
+                           double* line6) {
+  int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+  if (i >= n) return;
+  Line3 L;
+  cam_los(cams[cam], uv[2 * i], uv[2 * i + 1], L);
+  for (int k = 0; k < 3; ++k) {
+    line6[6 * i + k] = L.p[k];
+    line6[6 * i + 3 + k] = L.u[k];
+  }
+}
+
+__global__ void triangulate_kernel(int64_t n, int k, const double* lines6, double* out4,
+                                   int* ok) {
+  int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+  if (i >= n) return;
+  Line3 Ls[OLPT_MAX_CAM];
+  const Line3* P[OLPT_MAX_CAM];
+  for (int j = 0; j < k; ++j) {
+    for (int q = 0; q < 3; ++q) {
+      Ls[j].p[q] = lines6[(i * k + j) * 6 + q];
+      Ls[j].u[q] = lines6[(i * k + j) * 6 + 3 + q];
+    }
+    P[j] = &Ls[j];
+  }
+  double X[3], err = 0;
+  bool good = triangulate<OLPT_MAX_CAM>(P, k, X, err);
+  out4[4 * i] = X[0];
+  out4[4 * i + 1] = X[1];
+  out4[4 * i + 2] = X[2];
+  out4[4 * i + 3] = err;
+  ok[i] = good ? 1 : 0;
+}
+
+template <typename T>
+__global__ void convert_plane_kernel(const unsigned char* src, int64_t pitch, int H, int W,
+                                     int src_dtype, T* dst) {
+  int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+  if (i >= (int64_t)H * W) return;
+  int r = (int)(i / W), c = (int)(i % W);
+  const unsigned char* row = src + (int64_t)r * pitch;
+  double v;
+  switch (src_dtype) {
+    case OLPT_U8: v = row[c]; break;
+    case OLPT_U16: v = reinterpret_cast<const uint16_t*>(row)[c]; break;
+    case OLPT_F32: v = reinterpret_cast<const float*>(row)[c]; break;
+    default: v = reinterpret_cast<const double*>(row)[c]; break;
+  }
+  dst[i] = (T)v;
+}
+
+int esize(int dtype) {
+  return dtype == OLPT_U8 ? 1 : dtype == OLPT_U16 ? 2 : dtype == OLPT_F32 ? 4 : 8;
+}
+
+inline int nblk(int64_t n, int t = 256) { return (int)((n + t - 1) / t); }
+
+__global__ void otf_param_kernel(OtfView o, int cam, int64_t n, const double* xyz, double* out5) {
+  int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+  if (i >= n) return;
+  double r[5];
+  otf_param(o, cam, xyz[3 * i], xyz[3 * i + 1], xyz[3 * i + 2], r);
+  for (int k = 0; k < 5; ++k) out5[5 * i + k] = r[k];
+}
+
+}  // namespace
+
+void ensure_plane(olpt_ctx* ctx, int c, int dtype, int H, int W) {
+  ImagePlane& im = ctx->img[c];
+  const int64_t pitch = ((int64_t)W * esize(dtype) + 15) / 16 * 16;
+  im.buf.ensure((size_t)pitch * H + 64, ctx->stream);
+  im.dtype = dtype;
+  im.H = H;
+  im.W = W;
+  im.pitch = pitch;
+}
+
+OtfView otf_view(olpt_ctx* ctx) {
+  OLPT_REQUIRE(ctx->otf_table.p, OLPT_ERR_INVALID_ARG, "no OTF uploaded");
+  OtfView v;
+  v.nx = ctx->otf.nx;
+  v.ny = ctx->otf.ny;
+  v.nz = ctx->otf.nz;
+  v.n_grid = ctx->otf.n_grid;
+  v.n_cam = ctx->n_cam;
+  for (int k = 0; k < 3; ++k) {
+    v.bmin[k] = ctx->otf.bmin[k];
+    v.bmax[k] = ctx->otf.bmax[k];
+    v.d[k] = ctx->otf.d[k];
+  }
+  v.table = ctx->otf_table.as<double>();
+  return v;
+}
+
+}  // namespace olpt
+
+using namespace olpt;
+
+extern "C" {
+
+olpt_status_t olpt_ctx_create(olpt_ctx** out, int device) {
+  if (!out) return OLPT_ERR_INVALID_ARG;
+  *out = nullptr;
+  olpt_ctx* ctx = new (std::nothrow) olpt_ctx();
+  if (!ctx) return OLPT_ERR_OOM;
+  ctx->device = device;
+  cudaError_t e = cudaSetDevice(device);
+  if (e == cudaSuccess) e = cudaStreamCreateWithFlags(&ctx->stream, cudaStreamNonBlocking);
+  if (e != cudaSuccess) {
+    delete ctx;
+    return OLPT_ERR_CUDA;
+  }
+  ctx->own_stream = true;
+  *out = ctx;
+  return OLPT_OK;
+}
+
+void olpt_ctx_destroy(olpt_ctx* ctx) {
+  if (!ctx) return;
+  cudaSetDevice(ctx->device);
+  cudaStreamSynchronize(ctx->stream);
+  ctx->cams_d.release(ctx->stream);
+  ctx->otf_table.release(ctx->stream);
+  for (int c = 0; c < OLPT_MAX_CAM; ++c) {
+    ctx->img[c].buf.release(ctx->stream);
+    ctx->dets[c].x.release(ctx->stream);
+    ctx->dets[c].y.release(ctx->stream);
+    ctx->dets[c].rc.release(ctx->stream);
+  }
+  ctx->det_counts.release(ctx->stream);
+  ctx->band_counts.release(ctx->stream);
+  ctx->band_offsets.release(ctx->stream);
+  ctx->lut_u8.release(ctx->stream);
+  ctx->lut_u16.release(ctx->stream);
+  ctx->scratch.release(ctx->stream);
+  cudaStreamSynchronize(ctx->stream);
+  if (ctx->own_stream) cudaStreamDestroy(ctx->stream);
+  delete ctx;
+}
+
+const char* olpt_last_error(const olpt_ctx* ctx) { return ctx ? ctx->err.c_str() : "null context"; }
+
+olpt_status_t olpt_sync(olpt_ctx* ctx) {
+  return guard(ctx, [&] { OLPT_CUDA(cudaStreamSynchronize(ctx->stream)); });
+}
+
+olpt_status_t olpt_cameras_upload(olpt_ctx* ctx, const olpt_camera_desc* cams, int n_cam) {
+  return guard(ctx, [&] {
+    OLPT_REQUIRE(cams && n_cam >= 1 && n_cam <= OLPT_MAX_CAM, OLPT_ERR_INVALID_ARG,
+                 "n_cam must be in [1, 8]");
+    std::vector<CamDev> h(n_cam);
+    for (int i = 0; i < n_cam; ++i) {
+      const olpt_camera_desc& d = cams[i];
+      CamDev& c = h[i];
+      std::memset(&c, 0, sizeof(CamDev));
+      c.type = d.type;
+      c.n_row = d.n_row;
+      c.n_col = d.n_col;
+      c.is_active = d.is_active;
+      OLPT_REQUIRE(d.type == CAM_PINHOLE || d.type == CAM_POLYNOMIAL, OLPT_ERR_UNSUPPORTED,
+                   "camera type must be PINHOLE (0) or POLYNOMIAL (1)");
+      if (d.type == CAM_PINHOLE) {
+        c.fx = d.cam_mtx[0];
+        c.fy = d.cam_mtx[4];
+        c.cx = d.cam_mtx[2];
+        c.cy = d.cam_mtx[5];
+        OLPT_REQUIRE(d.n_dist >= 0 && d.n_dist <= 12, OLPT_ERR_INVALID_ARG, "n_dist > 12");
+        // Camera.cpp:55-80: distorted iff some coefficient > SMALLNUMBER
+        bool dist = false;
+        for (int k = 0; k < d.n_dist; ++k) {
+          c.dist[k] = d.dist[k];
+          if (d.dist[k] > 1e-8) dist = true;
+        }
+        c.is_distorted = dist ? 1 : 0;
+        c.n_dist = dist ? d.n_dist : 0;
+        OLPT_REQUIRE(!dist || d.n_dist == 4 || d.n_dist == 5 || d.n_dist == 8 || d.n_dist == 12,
+                     OLPT_ERR_INVALID_ARG, "number of distortion coefficients must be 4/5/8/12");
+        for (int k = 0; k < 9; ++k) {
+          c.R[k] = d.r_mtx[k];
+          c.Rinv[k] = d.r_inv[k];
+        }
+        for (int k = 0; k < 3; ++k) {
+          c.T[k] = d.t_vec[k];
+          c.Tinv[k] = d.t_inv[k];
+        }
+      } else {
+        OLPT_REQUIRE(d.n_coeff >= 1 && d.n_coeff <= OLPT_MAX_POLY && d.u_coeffs && d.v_coeffs,
+                     OLPT_ERR_INVALID_ARG, "polynomial camera needs 1..32 coefficients");
+        OLPT_REQUIRE(d.ref_plane >= 1 && d.ref_plane <= 3, OLPT_ERR_INVALID_ARG,
+                     "reference plane must be REF_X/REF_Y/REF_Z");
+        c.ref_plane = d.ref_plane;
+        c.plane[0] = d.plane[0];
+        c.plane[1] = d.plane[1];
+        const int n = c.n_coeff = d.n_coeff;
+        for (int k = 0; k < 4 * n; ++k) {
+          c.ucoef[k] = d.u_coeffs[k];
+          c.vcoef[k] = d.v_coeffs[k];
+        }
+        // Camera::updatePolyDuDv (Camera.cpp:340-393)
+        int d0 = 1, d1 = 2;
+        if (c.ref_plane == 1) {
+          d0 = 2;
+          d1 = 3;
+        } else if (c.ref_plane == 2) {
+          d0 = 1;
+          d1 = 3;
+        }
+        const int rp = c.ref_plane;
+        for (int i2 = 0; i2 < n; ++i2) {
+          const double* U = &c.ucoef[4 * i2];
+          const double* V = &c.vcoef[4 * i2];
+          double* DU = &c.ducoef[4 * i2];
+          double* DV = &c.dvcoef[4 * i2];
+          double* DU2 = &c.ducoef[4 * (i2 + n)];
+          double* DV2 = &c.dvcoef[4 * (i2 + n)];
+          DU[0] = U[0] * U[d0];
+          DU[rp] = U[rp];
+          DU[d0] = std::max(U[d0] - 1, 0.0);
+          DU[d1] = U[d1];
+          DU2[0] = U[0] * U[d1];
+          DU2[rp] = U[rp];
+          DU2[d0] = U[d0];
+          DU2[d1] = std::max(U[d1] - 1, 0.0);
+          DV[0] = V[0] * V[d0];
+          DV[rp] = V[rp];
+          DV[d0] = std::max(V[d0] - 1, 0.0);
+          DV[d1] = V[d1];
+          DV2[0] = V[0] * V[d1];
+          DV2[rp] = V[rp];
+          DV2[d0] = V[d0];
+          DV2[d1] = std::max(V[d1] - 1, 0.0);
+        }
+      }
+    }
+    ctx->cams_h = h;
+    ctx->n_cam = n_cam;
+    ctx->cams_d.ensure(sizeof(CamDev) * OLPT_MAX_CAM, ctx->stream);
+    OLPT_CUDA(cudaMemcpyAsync(ctx->cams_d.p, h.data(), sizeof(CamDev) * n_cam,
+                              cudaMemcpyHostToDevice, ctx->stream));
+    OLPT_CUDA(cudaStreamSynchronize(ctx->stream));
+  });
+}
+
+olpt_status_t olpt_cameras_set_active(olpt_ctx* ctx, const int* active) {
+  return guard(ctx, [&] {
+    OLPT_REQUIRE(active && ctx->n_cam > 0, OLPT_ERR_INVALID_ARG, "no cameras");
+    for (int c = 0; c < ctx->n_cam; ++c) {
+      ctx->cams_h[c].is_active = active[c] ? 1 : 0;
+      OLPT_CUDA(cudaMemcpyAsync(reinterpret_cast<char*>(ctx->cams_d.p) + sizeof(CamDev) * c +
+                                    offsetof(CamDev, is_active),
+                                &ctx->cams_h[c].is_active, sizeof(int), cudaMemcpyHostToDevice,
+                                ctx->stream));
+    }
+    OLPT_CUDA(cudaStreamSynchronize(ctx->stream));
+  });
+}
+
+olpt_status_t olpt_camera_project(olpt_ctx* ctx, int cam, int64_t n, const double* xyz,
+                                  double* uv) {
+  return guard(ctx, [&] {
+    OLPT_REQUIRE(cam >= 0 && cam < ctx->n_cam && n >= 0 && (n == 0 || (xyz && uv)),
+                 OLPT_ERR_INVALID_ARG, "bad camera index or buffers");
+    if (n == 0) return;
+    ctx->scratch.ensure(n * 5 * sizeof(double), ctx->stream);
+    double* dx = ctx->scratch.as<double>();
+    double* du = dx + 3 * n;
+    OLPT_CUDA(cudaMemcpyAsync(dx, xyz, n * 3 * sizeof(double), cudaMemcpyHostToDevice, ctx->stream));
+    project_kernel<<<nblk(n), 256, 0, ctx->stream>>>(ctx->cams_d.as<CamDev>(), cam, n, dx, du);
+    OLPT_CUDA(cudaGetLastError());
+    OLPT_CUDA(cudaMemcpyAsync(uv, du, n * 2 * sizeof(double), cudaMemcpyDeviceToHost, ctx->stream));
+    OLPT_CUDA(cudaStreamSynchronize(ctx->stream));
+  });
+}
+
+olpt_status_t olpt_camera_los(olpt_ctx* ctx, int cam, int64_t n, const double* uv,
+                              double* line6) {
+  return guard(ctx, [&] {
+    OLPT_REQUIRE(cam >= 0 && cam < ctx->n_cam && n >= 0 && (n == 0 || (uv && line6)),
+                 OLPT_ERR_INVALID_ARG, "bad camera index or buffers");
+    if (n == 0) return;
+    ctx->scratch.ensure(n * 8 * sizeof(double), ctx->stream);
+    double* du = ctx->scratch.as<double>();
+    double* dl = du + 2 * n;
+    OLPT_CUDA(cudaMemcpyAsync(du, uv, n * 2 * sizeof(double), cudaMemcpyHostToDevice, ctx->stream));
+    los_kernel<<<nblk(n), 256, 0, ctx->stream>>>(ctx->cams_d.as<CamDev>(), cam, n, du, dl);
+    OLPT_CUDA(cudaGetLastError());
+    OLPT_CUDA(cudaMemcpyAsync(line6, dl, n * 6 * sizeof(double), cudaMemcpyDeviceToHost, ctx->stream));
+    OLPT_CUDA(cudaStreamSynchronize(ctx->stream));
+  });
+}
+
+olpt_status_t olpt_triangulate(olpt_ctx* ctx, int64_t n_sets, int k, const double* lines6,
+                               double* out4, int* ok) {
+  return guard(ctx, [&] {
+    OLPT_REQUIRE(k >= 2 && k <= OLPT_MAX_CAM && n_sets >= 0, OLPT_ERR_INVALID_ARG,
+                 "k must be in [2, 8]");
+    if (n_sets == 0) return;
+    OLPT_REQUIRE(lines6 && out4 && ok, OLPT_ERR_INVALID_ARG, "null buffer");
+    const size_t in_b = n_sets * k * 6 * sizeof(double), out_b = n_sets * 4 * sizeof(double);
+    ctx->scratch.ensure(in_b + out_b + n_sets * sizeof(int) + 64, ctx->stream);
+    double* dl = ctx->scratch.as<double>();
+    double* dout = dl + n_sets * k * 6;
+    int* dok = reinterpret_cast<int*>(dout + n_sets * 4);
+    OLPT_CUDA(cudaMemcpyAsync(dl, lines6, in_b, cudaMemcpyHostToDevice, ctx->stream));
+    triangulate_kernel<<<nblk(n_sets, 128), 128, 0, ctx->stream>>>(n_sets, k, dl, dout, dok);
+    OLPT_CUDA(cudaGetLastError());
+    OLPT_CUDA(cudaMemcpyAsync(out4, dout, out_b, cudaMemcpyDeviceToHost, ctx->stream));
+    OLPT_CUDA(cudaMemcpyAsync(ok, dok, n_sets * sizeof(int), cudaMemcpyDeviceToHost, ctx->stream));
+    OLPT_CUDA(cudaStreamSynchronize(ctx->stream));
+  });
+}
+
+olpt_status_t olpt_otf_upload(olpt_ctx* ctx, int nx, int ny, int nz, const double* bound6,
+                              const double* abca) {
+  return guard(ctx, [&] {
+    OLPT_REQUIRE(ctx->n_cam > 0, OLPT_ERR_INVALID_ARG, "upload cameras before the OTF");
+    OLPT_REQUIRE(bound6 && abca, OLPT_ERR_INVALID_ARG, "null OTF buffers");
+    // OTF::loadParam clamps grid sizes below 2 up to 2 (OTF.cpp:159-171)
+    nx = nx < 2 ? 2 : nx;
+    ny = ny < 2 ? 2 : ny;
+    nz = nz < 2 ? 2 : nz;
+    OtfDev& o = ctx->otf;
+    o.nx = nx;
+    o.ny = ny;
+    o.nz = nz;
+    o.n_grid = nx * ny * nz;
+    const int n[3] = {nx, ny, nz};
+    for (int k = 0; k < 3; ++k) {
+      o.bmin[k] = bound6[2 * k];
+      o.bmax[k] = bound6[2 * k + 1];
+      o.d[k] = (o.bmax[k] - o.bmin[k]) / (n[k] - 1);  // OTF::setGrid (OTF.cpp:146-157)
+    }
+    const size_t bytes = (size_t)4 * ctx->n_cam * o.n_grid * sizeof(double);
+    ctx->otf_table.ensure(bytes, ctx->stream);
+    OLPT_CUDA(cudaMemcpyAsync(ctx->otf_table.p, abca, bytes, cudaMemcpyHostToDevice, ctx->stream));
+    OLPT_CUDA(cudaStreamSynchronize(ctx->stream));
+  });
+}
+
+olpt_status_t olpt_otf_param(olpt_ctx* ctx, int cam, int64_t n, const double* xyz, double* out5) {
+  return guard(ctx, [&] {
+    OLPT_REQUIRE(cam >= 0 && cam < ctx->n_cam && n >= 0 && (n == 0 || (xyz && out5)),
+                 OLPT_ERR_INVALID_ARG, "bad camera index or buffers");
+    if (n == 0) return;
+    OtfView v = otf_view(ctx);
+    ctx->scratch.ensure(n * 8 * sizeof(double), ctx->stream);
+    double* dx = ctx->scratch.as<double>();
+    double* dout = dx + 3 * n;
+    OLPT_CUDA(cudaMemcpyAsync(dx, xyz, n * 3 * sizeof(double), cudaMemcpyHostToDevice, ctx->stream));
+    otf_param_kernel<<<nblk(n), 256, 0, ctx->stream>>>(v, cam, n, dx, dout);
+    OLPT_CUDA(cudaGetLastError());
+    OLPT_CUDA(cudaMemcpyAsync(out5, dout, n * 5 * sizeof(double), cudaMemcpyDeviceToHost, ctx->stream));
+    OLPT_CUDA(cudaStreamSynchronize(ctx->stream));
+  });
+}
+
+olpt_status_t olpt_images_upload(olpt_ctx* ctx, int n_cam, olpt_dtype_t dtype,
+                                 const void* const* imgs, const int* H, const int* W,
+                                 const int64_t* pitch_bytes, int on_device) {
+  return guard(ctx, [&] {
+    OLPT_REQUIRE(n_cam == ctx->n_cam && imgs && H && W, OLPT_ERR_INVALID_ARG,
+                 "image count must equal camera count");
+    OLPT_REQUIRE(dtype >= OLPT_U8 && dtype <= OLPT_F64, OLPT_ERR_INVALID_ARG, "bad dtype");
+    for (int c = 0; c < n_cam; ++c) {
+      OLPT_REQUIRE(imgs[c] && H[c] > 0 && W[c] > 0, OLPT_ERR_INVALID_ARG, "empty image");
+      ensure_plane(ctx, c, dtype, H[c], W[c]);
+      const int64_t row_b = (int64_t)W[c] * esize(dtype);
+      const int64_t sp = (pitch_bytes && pitch_bytes[c]) ? pitch_bytes[c] : row_b;
+      OLPT_CUDA(cudaMemcpy2DAsync(ctx->img[c].buf.p, ctx->img[c].pitch, imgs[c], sp, row_b, H[c],
+                                  on_device ? cudaMemcpyDeviceToDevice : cudaMemcpyHostToDevice,
+                                  ctx->stream));
+    }
+  });
+}
+
+olpt_status_t olpt_image_download(olpt_ctx* ctx, int cam, olpt_dtype_t dtype, void* out) {
+  return guard(ctx, [&] {
+    OLPT_REQUIRE(cam >= 0 && cam < ctx->n_cam && out, OLPT_ERR_INVALID_ARG, "bad camera/buffer");
+    OLPT_REQUIRE(dtype == OLPT_F32 || dtype == OLPT_F64, OLPT_ERR_INVALID_ARG,
+                 "download dtype must be F32 or F64");
+    ImagePlane& im = ctx->img[cam];
+    OLPT_REQUIRE(im.buf.p, OLPT_ERR_INVALID_ARG, "no image");
+    const int64_t n = (int64_t)im.H * im.W;
+    ctx->scratch.ensure(n * 8, ctx->stream);
+    if (dtype == OLPT_F32)
+      convert_plane_kernel<float><<<nblk(n), 256, 0, ctx->stream>>>(
+          im.buf.as<unsigned char>(), im.pitch, im.H, im.W, im.dtype, ctx->scratch.as<float>());
+    else
+      convert_plane_kernel<double><<<nblk(n), 256, 0, ctx->stream>>>(
+          im.buf.as<unsigned char>(), im.pitch, im.H, im.W, im.dtype, ctx->scratch.as<double>());
+    OLPT_CUDA(cudaGetLastError());
+    OLPT_CUDA(cudaMemcpyAsync(out, ctx->scratch.p, n * esize(dtype), cudaMemcpyDeviceToHost,
+                              ctx->stream));
+    OLPT_CUDA(cudaStreamSynchronize(ctx->stream));
+  });
+}
+
+olpt_status_t olpt_find_peaks(olpt_ctx* ctx, double min_obj_int, int64_t* counts) {
+  return guard(ctx, [&] {
+    find_peaks_device(ctx, min_obj_int, true);
+    if (counts)
+      for (int c = 0; c < ctx->n_cam; ++c) counts[c] = ctx->det_counts_h[c];
+  });
+}
+
+olpt_status_t olpt_get_peaks(olpt_ctx* ctx, int cam, double* xy, int32_t* rc, int64_t cap) {
+  return guard(ctx, [&] {
+    OLPT_REQUIRE(cam >= 0 && cam < ctx->n_cam, OLPT_ERR_INVALID_ARG, "bad camera index");
+    OLPT_REQUIRE((int64_t)ctx->det_counts_h.size() > cam, OLPT_ERR_INVALID_ARG, "no detections");
+    const int64_t n = std::min<int64_t>(cap, ctx->det_counts_h[cam]);
+    if (n <= 0) return;
+    Dets& d = ctx->dets[cam];
+    if (xy) {
+      std::vector<double> hx(n), hy(n);
+      OLPT_CUDA(cudaMemcpyAsync(hx.data(), d.x.p, n * 8, cudaMemcpyDeviceToHost, ctx->stream));
+      OLPT_CUDA(cudaMemcpyAsync(hy.data(), d.y.p, n * 8, cudaMemcpyDeviceToHost, ctx->stream));
+      OLPT_CUDA(cudaStreamSynchronize(ctx->stream));
+      for (int64_t i = 0; i < n; ++i) {
+        xy[2 * i] = hx[i];
+        xy[2 * i + 1] = hy[i];
+      }
+    }
+    if (rc) {
+      OLPT_CUDA(cudaMemcpyAsync(rc, d.rc.p, n * sizeof(int2), cudaMemcpyDeviceToHost, ctx->stream));
+      OLPT_CUDA(cudaStreamSynchronize(ctx->stream));
+    }
+  });
+}
+
+olpt_status_t olpt_detections_upload(olpt_ctx* ctx, int n_cam, const int64_t* counts,
+                                     const double* const* xy) {
+  return guard(ctx, [&] {
+    OLPT_REQUIRE(n_cam == ctx->n_cam && counts && xy, OLPT_ERR_INVALID_ARG,
+                 "detection lists must cover every camera");
+    ctx->det_counts_h.assign(n_cam, 0);
+    ctx->det_counts.ensure(OLPT_MAX_CAM * sizeof(int64_t), ctx->stream);
+    for (int c = 0; c < n_cam; ++c) {
+      const int64_t n = counts[c];
+      OLPT_REQUIRE(n >= 0 && (n == 0 || xy[c]), OLPT_ERR_INVALID_ARG, "bad detection list");
+      ensure_det_capacity(ctx, c, std::max<int64_t>(n, 1));
+      std::vector<double> hx(n), hy(n);
+      std::vector<int2> hrc(n);
+      for (int64_t i = 0; i < n; ++i) {
+        hx[i] = xy[c][2 * i];
+        hy[i] = xy[c][2 * i + 1];
+        hrc[i] = make_int2((int)std::floor(hy[i] + 0.5), (int)std::floor(hx[i] + 0.5));
+      }
+      if (n) {
+        OLPT_CUDA(cudaMemcpyAsync(ctx->dets[c].x.p, hx.data(), n * 8, cudaMemcpyHostToDevice, ctx->stream));
+        OLPT_CUDA(cudaMemcpyAsync(ctx->dets[c].y.p, hy.data(), n * 8, cudaMemcpyHostToDevice, ctx->stream));
+        OLPT_CUDA(cudaMemcpyAsync(ctx->dets[c].rc.p, hrc.data(), n * sizeof(int2),
+                                  cudaMemcpyHostToDevice, ctx->stream));
+      }
+      ctx->det_counts_h[c] = n;
+    }
+    OLPT_CUDA(cudaMemcpyAsync(ctx->det_counts.p, ctx->det_counts_h.data(), n_cam * sizeof(int64_t),
+                              cudaMemcpyHostToDevice, ctx->stream));
+    OLPT_CUDA(cudaStreamSynchronize(ctx->stream));
+  });
+}
+
+}  // extern "C"

@@ -1,0 +1,126 @@
+// Host-side context shared by all translation units of libolpt_cuda.so.
+#pragma once
+#include <cuda_runtime.h>
+
+#include <cstdint>
+#include <cstring>
+#include <string>
+#include <vector>
+
+#include "../../include/olpt.h"
+#include "olpt_device.cuh"
+
+namespace olpt {
+
+struct CudaError {
+  cudaError_t code;
+  std::string where;
+};
+struct ApiError {
+  olpt_status_t code;
+  std::string msg;
+};
+
+#define OLPT_CUDA(call)                                                             \
+  do {                                                                              \
+    cudaError_t _e = (call);                                                        \
+    if (_e != cudaSuccess) throw ::olpt::CudaError{_e, std::string(#call) + " @ " + \
+                                                       __FILE__ + ":" + std::to_string(__LINE__)}; \
+  } while (0)
+
+#define OLPT_REQUIRE(cond, code, msg) \
+  do {                                \
+    if (!(cond)) throw ::olpt::ApiError{(code), (msg)}; \
+  } while (0)
+
+// Grow-only device buffer (stream-ordered allocation).
+struct DevBuf {
+  void* p = nullptr;
+  size_t bytes = 0;
+  void ensure(size_t need, cudaStream_t s) {
+    if (need <= bytes) return;
+    if (p) OLPT_CUDA(cudaFreeAsync(p, s));
+    size_t nb = need + need / 4 + 256;
+    OLPT_CUDA(cudaMallocAsync(&p, nb, s));
+    bytes = nb;
+  }
+  template <class T>
+  T* as() const {
+    return static_cast<T*>(p);
+  }
+  void release(cudaStream_t s) {
+    if (p) cudaFreeAsync(p, s);
+    p = nullptr;
+    bytes = 0;
+  }
+};
+
+// Pinned host staging buffer.
+struct HostBuf {
+  void* p = nullptr;
+  size_t bytes = 0;
+  void ensure(size_t need) {
+    if (need <= bytes) return;
+    if (p) cudaFreeHost(p);
+    size_t nb = need + need / 4 + 256;
+    OLPT_CUDA(cudaMallocHost(&p, nb));
+    bytes = nb;
+  }
+  template <class T>
+  T* as() const {
+    return static_cast<T*>(p);
+  }
+  ~HostBuf() {
+    if (p) cudaFreeHost(p);
+  }
+};
+
+// One camera image plane in HBM (row pitch padded to 16 bytes for vector loads).
+struct ImagePlane {
+  DevBuf buf;
+  int dtype = OLPT_U8;
+  int H = 0, W = 0;
+  int64_t pitch = 0;  // bytes
+};
+
+struct OtfDev {
+  int nx = 2, ny = 2, nz = 2, n_grid = 8;
+  double bmin[3], bmax[3];
+  double d[3];  // grid spacing
+  double* table = nullptr;  // [4][n_cam][n_grid] a,b,c,alpha (device)
+};
+
+// Per-camera 2D detection list (SoA, FP64 like the reference's Pt2D).
+struct Dets {
+  DevBuf x, y, rc;          // rc: packed (row<<16 | col) is not enough for 2048+; store int2
+  int64_t cap = 0;
+};
+
+}  // namespace olpt
+
+struct olpt_ctx {
+  int device = 0;
+  cudaStream_t stream = nullptr;
+  bool own_stream = false;
+  std::string err;
+
+  int n_cam = 0;
+  std::vector<olpt::CamDev> cams_h;
+  olpt::DevBuf cams_d;
+
+  olpt::OtfDev otf;
+  olpt::DevBuf otf_table;
+
+  olpt::ImagePlane img[OLPT_MAX_CAM];  // current working image per camera
+
+  // detections
+  olpt::Dets dets[OLPT_MAX_CAM];
+  olpt::DevBuf det_counts;  // int64 per camera (device)
+  std::vector<int64_t> det_counts_h;
+  olpt::DevBuf band_counts, band_offsets;
+  olpt::DevBuf lut_u8, lut_u16;  // log(max(v, 1e-4)) of every integer level
+
+  // scratch
+  olpt::DevBuf scratch;
+  olpt::HostBuf pinned;
+};

@@ -1,0 +1,33 @@
+"""Shared seeded scenes and CPU oracles for the test-suite."""
+import functools
+
+import numpy as np
+
+from pyopenlpt_b200 import synth
+
+
+@functools.lru_cache(maxsize=None)
+def scene(kind: str = "small"):
+    if kind == "small":     # fast: 2,000 particles, 4 x 512^2 u8
+        return synth.make_scene(n_particles=2000, size=512, focal=2500.0, seed=7)
+    if kind == "cfg1":      # the single-frame IPR scene: 10k particles, 4 x 1024^2 u8
+        return synth.make_scene()
+    if kind == "u16":       # 12-bit images, 3 cameras, non-square
+        return synth.make_scene(n_particles=1500, n_cam=3, n_row=400, n_col=640, focal=2500.0,
+                                a=3000.0, noise=20.0, bits=12, seed=11)
+    raise KeyError(kind)
+
+
+@functools.lru_cache(maxsize=None)
+def ref_oracle(kind: str = "small", threads: int = 0):
+    from oracle.ref import RefOracle
+    return RefOracle(scene(kind), synth.IPRSettings(), threads=threads)
+
+
+def gpu_context(sc):
+    from pyopenlpt_b200 import _ffi
+    ctx = _ffi.Context(0)
+    ctx.upload_cameras([_ffi.camera_desc_from_pinhole(c) for c in sc.cams])
+    from oracle.ref import otf_table
+    ctx.upload_otf(2, 2, 2, sc.volume, otf_table(sc.n_cam, sc.otf_abc))
+    return ctx
