@@ -110,6 +110,29 @@ olpt_status_t olpt_get_peaks(olpt_ctx* ctx, int cam, double* xy, int32_t* rc, in
 olpt_status_t olpt_detections_upload(olpt_ctx* ctx, int n_cam, const int64_t* counts,
                                      const double* const* xy);
 
+/* ------------------------------------------------------------------ stereo matching */
+/* StereoMatch parameters (SMParam, inc/libSTB/Config.h:72-80): limit is the
+ * (xmin,xmax,ymin,ymax,zmin,zmax) box of accepted triangulations. */
+typedef struct olpt_sm_params {
+  int match_cam_count;
+  int idmap_cell_px;
+  double tol_2d_px;
+  double tol_3d_mm;
+  double limit[6];
+} olpt_sm_params;
+
+/* StereoMatch(cams, obj2d_list, cfg).match() (src/srcSTB/StereoMatch.cpp:20-178) on the
+ * current detections of the active cameras.  The selected, triangulated matches
+ * become the context's current 3D objects.  n_candidates: size of the checked
+ * candidate set (before the prune); n_matches: number of objects. */
+olpt_status_t olpt_stereo_match(olpt_ctx* ctx, const olpt_sm_params* p, int64_t* n_candidates,
+                                int64_t* n_matches);
+/* Candidate set of the last match in the reference's order (sorted by ids):
+ * ids n_candidates x n_cam (-1 = unused camera), e_check, triangulated xyz. */
+olpt_status_t olpt_get_candidates(olpt_ctx* ctx, int32_t* ids, double* e_check, double* xyz);
+/* Selected matches of the last match (triangulateMatch output order): ids, xyz. */
+olpt_status_t olpt_get_matches(olpt_ctx* ctx, int32_t* ids, double* xyz);
+
 #ifdef __cplusplus
 }
 #endif

@@ -33,6 +33,19 @@ class CameraDesc(C.Structure):
     ]
 
 
+class SmParams(C.Structure):
+    _fields_ = [("match_cam_count", C.c_int), ("idmap_cell_px", C.c_int),
+                ("tol_2d_px", C.c_double), ("tol_3d_mm", C.c_double), ("limit", C.c_double * 6)]
+
+
+def sm_params(settings, limit) -> SmParams:
+    p = SmParams(match_cam_count=settings.match_cam_count, idmap_cell_px=settings.idmap_cell_px,
+                 tol_2d_px=settings.tol_2d_px, tol_3d_mm=settings.tol_3d_mm)
+    for i in range(6):
+        p.limit[i] = limit[i]
+    return p
+
+
 class OlptError(RuntimeError):
     def __init__(self, code: int, msg: str):
         super().__init__(f"olpt status {code}: {msg}")
@@ -196,3 +209,23 @@ class Context:
         counts = np.array([len(x) for x in d], dtype=np.int64)
         ptrs = (_dp * len(d))(*[_p(x) for x in d])
         self._check(self.L.olpt_detections_upload(self.h, len(d), _p(counts, _i64p), ptrs))
+
+    # ---------------------------------------------------------------- stereo
+    def stereo_match(self, params: SmParams):
+        nc = C.c_int64()
+        nm = C.c_int64()
+        self._check(self.L.olpt_stereo_match(self.h, C.byref(params), C.byref(nc), C.byref(nm)))
+        return nc.value, nm.value
+
+    def candidates(self, n: int):
+        ids = np.empty((n, self.n_cam), dtype=np.int32)
+        e = np.empty(n)
+        x = np.empty((n, 3))
+        self._check(self.L.olpt_get_candidates(self.h, _p(ids, _i32p), _p(e), _p(x)))
+        return ids, e, x
+
+    def matches(self, n: int):
+        ids = np.empty((n, self.n_cam), dtype=np.int32)
+        x = np.empty((n, 3))
+        self._check(self.L.olpt_get_matches(self.h, _p(ids, _i32p), _p(x)))
+        return ids, x

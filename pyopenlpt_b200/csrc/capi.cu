@@ -184,6 +184,8 @@ void olpt_ctx_destroy(olpt_ctx* ctx) {
   ctx->lut_u8.release(ctx->stream);
   ctx->lut_u16.release(ctx->stream);
   ctx->scratch.release(ctx->stream);
+  ctx->sm.release(ctx->stream);
+  ctx->obj.release(ctx->stream);
   cudaStreamSynchronize(ctx->stream);
   if (ctx->own_stream) cudaStreamDestroy(ctx->stream);
   delete ctx;
@@ -507,6 +509,66 @@ olpt_status_t olpt_detections_upload(olpt_ctx* ctx, int n_cam, const int64_t* co
     OLPT_CUDA(cudaMemcpyAsync(ctx->det_counts.p, ctx->det_counts_h.data(), n_cam * sizeof(int64_t),
                               cudaMemcpyHostToDevice, ctx->stream));
     OLPT_CUDA(cudaStreamSynchronize(ctx->stream));
+  });
+}
+
+}  // extern "C"
+
+extern "C" {
+
+olpt_status_t olpt_stereo_match(olpt_ctx* ctx, const olpt_sm_params* p, int64_t* n_candidates,
+                                int64_t* n_matches) {
+  return guard(ctx, [&] {
+    OLPT_REQUIRE(p, OLPT_ERR_INVALID_ARG, "null params");
+    OLPT_REQUIRE((int)ctx->det_counts_h.size() == ctx->n_cam, OLPT_ERR_INVALID_ARG,
+                 "no detections: run olpt_find_peaks or olpt_detections_upload first");
+    SmParams prm;
+    prm.match_cam_count = p->match_cam_count;
+    prm.idmap_cell_px = p->idmap_cell_px;
+    prm.tol_2d_px = p->tol_2d_px;
+    prm.tol_3d_mm = p->tol_3d_mm;
+    for (int q = 0; q < 6; ++q) prm.limit[q] = p->limit[q];
+    StereoResult& r = ctx->sm_result;
+    stereo_match_device(ctx, prm, r);
+    // selected matches become the current 3D objects (triangulateMatch order)
+    const size_t M = r.e.size();
+    std::vector<double> xyz;
+    for (size_t j = 0; j < M; ++j)
+      if (r.selected[j]) xyz.insert(xyz.end(), &r.X[3 * j], &r.X[3 * j] + 3);
+    const int64_t n = (int64_t)(xyz.size() / 3);
+    ctx->obj.ensure(std::max<int64_t>(n, 1), ctx->n_cam, ctx->stream);
+    ctx->obj.n = n;
+    if (n)
+      OLPT_CUDA(cudaMemcpyAsync(ctx->obj.xyz.p, xyz.data(), xyz.size() * sizeof(double),
+                                cudaMemcpyHostToDevice, ctx->stream));
+    OLPT_CUDA(cudaStreamSynchronize(ctx->stream));
+    if (n_candidates) *n_candidates = (int64_t)M;
+    if (n_matches) *n_matches = n;
+  });
+}
+
+olpt_status_t olpt_get_candidates(olpt_ctx* ctx, int32_t* ids, double* e_check, double* xyz) {
+  return guard(ctx, [&] {
+    const StereoResult& r = ctx->sm_result;
+    const size_t M = r.e.size();
+    if (ids) std::copy(r.ids.begin(), r.ids.end(), ids);
+    if (e_check) std::copy(r.e.begin(), r.e.end(), e_check);
+    if (xyz) std::copy(r.X.begin(), r.X.end(), xyz);
+    (void)M;
+  });
+}
+
+olpt_status_t olpt_get_matches(olpt_ctx* ctx, int32_t* ids, double* xyz) {
+  return guard(ctx, [&] {
+    const StereoResult& r = ctx->sm_result;
+    const int n = r.n_cam;
+    int64_t k = 0;
+    for (size_t j = 0; j < r.e.size(); ++j) {
+      if (!r.selected[j]) continue;
+      if (ids) std::copy(&r.ids[j * n], &r.ids[j * n] + n, ids + k * n);
+      if (xyz) std::copy(&r.X[3 * j], &r.X[3 * j] + 3, xyz + 3 * k);
+      ++k;
+    }
   });
 }
 

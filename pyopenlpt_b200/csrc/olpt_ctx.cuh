@@ -9,6 +9,7 @@
 
 #include "../../include/olpt.h"
 #include "olpt_device.cuh"
+#include "olpt_stereo.h"
 
 namespace olpt {
 
@@ -96,6 +97,58 @@ struct Dets {
   int64_t cap = 0;
 };
 
+// Device workspace of stereo matching (grown on demand, reused across frames).
+struct StereoWork {
+  DevBuf cell_start[OLPT_MAX_CAM], cell_cursor[OLPT_MAX_CAM], cell_items[OLPT_MAX_CAM];
+  DevBuf cell_of[OLPT_MAX_CAM], los[OLPT_MAX_CAM];
+  DevBuf l2d[OLPT_MAX_CAM * OLPT_MAX_CAM];
+  DevBuf l2d_ptrs, active_d, counters;
+  DevBuf path_a, path_b, term;
+  DevBuf cand_ids, cand_e, cand_x;
+  void release(cudaStream_t s) {
+    for (int c = 0; c < OLPT_MAX_CAM; ++c) {
+      cell_start[c].release(s);
+      cell_cursor[c].release(s);
+      cell_items[c].release(s);
+      cell_of[c].release(s);
+      los[c].release(s);
+    }
+    for (auto& b : l2d) b.release(s);
+    l2d_ptrs.release(s);
+    active_d.release(s);
+    counters.release(s);
+    path_a.release(s);
+    path_b.release(s);
+    term.release(s);
+    cand_ids.release(s);
+    cand_e.release(s);
+    cand_x.release(s);
+  }
+};
+
+// 3D objects resident on the device (SoA).
+struct Objects {
+  DevBuf xyz;    // n x 3 double
+  DevBuf uv;     // n x n_cam x 2 double: current 2D projections
+  DevBuf flags;  // n uint8 (ObjFlag bits)
+  DevBuf score;  // n double
+  int64_t n = 0;
+  void ensure(int64_t cap, int n_cam, cudaStream_t s) {
+    xyz.ensure((cap + 1) * 3 * sizeof(double), s);
+    uv.ensure((cap + 1) * n_cam * 2 * sizeof(double), s);
+    flags.ensure(cap + 16, s);
+    score.ensure((cap + 1) * sizeof(double), s);
+  }
+  void release(cudaStream_t s) {
+    xyz.release(s);
+    uv.release(s);
+    flags.release(s);
+    score.release(s);
+  }
+};
+
+void stereo_match_device(olpt_ctx* ctx, const SmParams& prm, StereoResult& res);
+
 }  // namespace olpt
 
 struct olpt_ctx {
@@ -119,6 +172,13 @@ struct olpt_ctx {
   std::vector<int64_t> det_counts_h;
   olpt::DevBuf band_counts, band_offsets;
   olpt::DevBuf lut_u8, lut_u16;  // log(max(v, 1e-4)) of every integer level
+
+  // stereo matching
+  olpt::StereoWork sm;
+  olpt::StereoResult sm_result;
+
+  // 3D objects (stereo output / shake input and output)
+  olpt::Objects obj;
 
   // scratch
   olpt::DevBuf scratch;

@@ -1,0 +1,32 @@
+// Stereo matching: host-side types shared by the device driver (stereo.cu) and the
+// host-side candidate ordering / greedy prune (stereo_host.cpp).
+#pragma once
+#include <cstdint>
+#include <vector>
+
+namespace olpt {
+
+struct SmParams {
+  int match_cam_count;
+  int idmap_cell_px;
+  double tol_2d_px;
+  double tol_3d_mm;
+  double limit[6];
+};
+
+// Candidate set after checkMatch, sorted by ids (StereoMatch.cpp:153-156), and the
+// prune selection (StereoMatch.cpp:631-980).
+struct StereoResult {
+  int n_cam = 0;
+  int ref_cam = -1;
+  std::vector<int> ids;        // M x n_cam, -1 = camera unused
+  std::vector<double> e;       // e_check
+  std::vector<double> X;       // M x 3, triangulated position (camera order)
+  std::vector<char> selected;  // M
+};
+
+void sort_candidates(StereoResult& r);
+void prune_candidates(StereoResult& r, const std::vector<int>& det_counts,
+                      const std::vector<int>& active);
+
+}  // namespace olpt

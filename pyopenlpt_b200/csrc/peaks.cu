@@ -240,7 +240,7 @@ __global__ void band_scan_kernel(const PeakArgs a, int64_t* band_offsets, int64_
   const int cam = blockIdx.x;
   if (cam >= a.n_cam) return;
   const PeakCam& c = a.cam[cam];
-  __shared__ int64_t s_run;
+  __shared__ int64_t s_run, s_total;
   __shared__ int64_t warp_sums[32];
   if (threadIdx.x == 0) s_run = 0;
   __syncthreads();
@@ -262,12 +262,12 @@ __global__ void band_scan_kernel(const PeakArgs a, int64_t* band_offsets, int64_
         warp_sums[w] = acc;
         acc += t;
       }
-      warp_sums[31] = acc;  // stash block total (nw <= 31 here)
+      s_total = acc;
     }
     __syncthreads();
     if (b < c.n_bands) band_offsets[c.band_base + b] = s_run + warp_sums[wid] + incl - v;
     __syncthreads();
-    if (threadIdx.x == 0) s_run += warp_sums[31];
+    if (threadIdx.x == 0) s_run += s_total;
     __syncthreads();
   }
   if (threadIdx.x == 0) totals[cam] = s_run;

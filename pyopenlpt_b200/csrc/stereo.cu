@@ -1,0 +1,659 @@
+// Kernel family (b): stereo matching on the device.
+//
+// Reference: StereoMatch (src/srcSTB/StereoMatch.cpp): IDMap grid (:1413-1437),
+// strip intersection (:1471-1570), point visit (:1572-1627), DFS build (:184-444),
+// candidate enumeration (:449-498), back-projection (:1206-1227), quick
+// triangulation gate (:1083-1141), camera selection (:1307-1411), check (:504-609).
+//
+// B200 mapping.
+//  * Grid: a counting sort per camera (histogram -> scan -> scatter -> per-cell
+//    ascending pid order), i.e. the reference's bucket lists as CSR arrays.
+//  * Every detection's line of sight and its image line on every other camera are
+//    computed once (same FP64 functions the reference calls on the fly, so the
+//    values are bit-identical) and reused by every path that touches the point.
+//  * The depth-first search over build cameras is expanded breadth-first: level k
+//    holds all partial paths with k chosen cameras and the target camera of their
+//    next choice.  One warp expands one path: lanes take rows of cells, replicate the
+//    reference's per-row span arithmetic exactly, visit the cells and apply the exact
+//    point-line test, back-projection test and quick triangulation gate.  Children
+//    are appended with atomics; the final candidate list is sorted by ids on the
+//    host, so append order never shows.
+//  * The whole set of candidates (ids, e_check) is therefore identical to the
+//    reference's.  Decisions that pass through acos/sin (only when the minimum
+//    parallax is below 6 degrees) can differ by one ulp; those are the only
+//    non-bit-exact inputs.
+#include <cuda_runtime.h>
+
+#include <algorithm>
+#include <cmath>
+#include <vector>
+
+#include "olpt_ctx.cuh"
+#include "olpt_stereo.h"
+
+namespace olpt {
+
+struct SmView {
+  int n_cam, m, n_active;
+  int active[OLPT_MAX_CAM];
+  int cell;
+  int rows[OLPT_MAX_CAM], cols[OLPT_MAX_CAM];
+  double Wd[OLPT_MAX_CAM], Hd[OLPT_MAX_CAM];
+  const int* cell_start[OLPT_MAX_CAM];
+  const int* cell_items[OLPT_MAX_CAM];
+  const double* x[OLPT_MAX_CAM];
+  const double* y[OLPT_MAX_CAM];
+  int64_t n[OLPT_MAX_CAM];
+  const double* los[OLPT_MAX_CAM];                  // n x 6
+  const double* l2d[OLPT_MAX_CAM][OLPT_MAX_CAM];    // [c][t]: n[c] x 6 (pt, unit, U)
+  double tol2d, tol3d;
+  double limit[6];
+};
+
+struct Path {
+  int ids[OLPT_MAX_CAM];
+  signed char cams[OLPT_MAX_CAM];
+  int k;
+  int target;
+};
+
+namespace {
+
+inline int nblk(int64_t n, int t = 256) { return (int)((n + t - 1) / t); }
+
+// ---------------------------------------------------------------- grid
+__global__ void cell_hist_kernel(const double* x, const double* y, int64_t n, int cell, int rows,
+                                 int cols, int* cell_of, int* counts) {
+  int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+  if (i >= n) return;
+  // IDMap::rebuild (StereoMatch.cpp:1423-1437)
+  int cx = (int)floor(x[i] / (double)cell);
+  int cy = (int)floor(y[i] / (double)cell);
+  if (cx < 0 || cy < 0 || cx >= cols || cy >= rows) {
+    cell_of[i] = -1;
+    return;
+  }
+  int c = cy * cols + cx;
+  cell_of[i] = c;
+  atomicAdd(&counts[c], 1);
+}
+
+// exclusive scan of counts[0..n) -> start[0..n], one CTA
+__global__ void cell_scan_kernel(const int* counts, int n, int* start) {
+  __shared__ int warp_sums[32];
+  __shared__ int run, total;
+  if (threadIdx.x == 0) run = 0;
+  __syncthreads();
+  const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5, nw = blockDim.x >> 5;
+  for (int s = 0; s < n; s += blockDim.x) {
+    int i = s + threadIdx.x;
+    int v = i < n ? counts[i] : 0;
+    int incl = v;
+    for (int o = 1; o < 32; o <<= 1) {
+      int t = __shfl_up_sync(0xffffffffu, incl, o);
+      if (lane >= o) incl += t;
+    }
+    if (lane == 31) warp_sums[wid] = incl;
+    __syncthreads();
+    if (threadIdx.x == 0) {
+      int acc = 0;
+      for (int w = 0; w < nw; ++w) {
+        int t = warp_sums[w];
+        warp_sums[w] = acc;
+        acc += t;
+      }
+      total = acc;
+    }
+    __syncthreads();
+    if (i < n) start[i] = run + warp_sums[wid] + incl - v;
+    __syncthreads();
+    if (threadIdx.x == 0) run += total;
+    __syncthreads();
+  }
+  if (threadIdx.x == 0) start[n] = run;
+}
+
+__global__ void cell_scatter_kernel(const int* cell_of, int64_t n, const int* start, int* cursor,
+                                    int* items) {
+  int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+  if (i >= n) return;
+  int c = cell_of[i];
+  if (c < 0) return;
+  int pos = start[c] + atomicAdd(&cursor[c], 1);
+  items[pos] = (int)i;
+}
+
+// ascending pid order inside every cell (the reference pushes pids in order)
+__global__ void cell_sort_kernel(const int* start, int n_cells, int* items) {
+  int c = blockIdx.x * blockDim.x + threadIdx.x;
+  if (c >= n_cells) return;
+  int b = start[c], e = start[c + 1];
+  for (int i = b + 1; i < e; ++i) {
+    int v = items[i];
+    int j = i - 1;
+    while (j >= b && items[j] > v) {
+      items[j + 1] = items[j];
+      --j;
+    }
+    items[j + 1] = v;
+  }
+}
+
+// ---------------------------------------------------------------- per-detection lines
+__global__ void lines_kernel(const CamDev* cams, int c, const double* x, const double* y, int64_t n,
+                             int n_cam, const int* active, double* los, double* const* l2d) {
+  int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+  if (i >= n) return;
+  Line3 L;
+  cam_los(cams[c], x[i], y[i], L);
+  for (int k = 0; k < 3; ++k) {
+    los[6 * i + k] = L.p[k];
+    los[6 * i + 3 + k] = L.u[k];
+  }
+  for (int t = 0; t < n_cam; ++t) {
+    if (t == c || !active[t]) continue;
+    double o[4];
+    los_to_line2d(cams[t], L, o);
+    double* d = l2d[t] + 6 * i;
+    d[0] = o[0];
+    d[1] = o[1];
+    d[2] = o[2];
+    d[3] = o[3];
+    // IDMap::normalized (StereoMatch.cpp:1441-1451)
+    const double n2 = o[2] * o[2] + o[3] * o[3];
+    if (n2 <= 1e-24) {
+      d[4] = 1.0;
+      d[5] = 0.0;
+    } else {
+      const double inv = 1.0 / sqrt(n2);
+      d[4] = o[2] * inv;
+      d[5] = o[3] * inv;
+    }
+  }
+}
+
+__device__ __forceinline__ void load_line3(const double* p, Line3& L) {
+  L.p[0] = p[0];
+  L.p[1] = p[1];
+  L.p[2] = p[2];
+  L.u[0] = p[3];
+  L.u[1] = p[4];
+  L.u[2] = p[5];
+}
+
+// StereoMatch::selectSecondCameraByLineLength segment length (StereoMatch.cpp:1309-1357)
+__device__ double seg_len(const double* L, double W, double H) {
+  const double px = L[0], py = L[1], ux = L[2], uy = L[3];
+  double qx[4], qy[4];
+  int n = 0;
+  auto push_if = [&](double a, double b) {
+    if (a >= 0.0 && a <= W && b >= 0.0 && b <= H) {
+      qx[n] = a;
+      qy[n] = b;
+      ++n;
+    }
+  };
+  if (fabs(ux) > 1e-12) {
+    double t = (0.0 - px) / ux;
+    push_if(0.0, py + t * uy);
+    t = (W - 1 - px) / ux;
+    push_if(W - 1, py + t * uy);
+  }
+  if (fabs(uy) > 1e-12) {
+    double t = (0.0 - py) / uy;
+    push_if(px + t * ux, 0.0);
+    t = (H - 1 - py) / uy;
+    push_if(px + t * ux, H - 1);
+  }
+  double ux2[4], uy2[4];
+  int m = 0;
+  for (int i = 0; i < n; ++i) {
+    bool dup = false;
+    for (int j = 0; j < m; ++j)
+      if (fabs(ux2[j] - qx[i]) < 1e-9 && fabs(uy2[j] - qy[i]) < 1e-9) {
+        dup = true;
+        break;
+      }
+    if (!dup) {
+      ux2[m] = qx[i];
+      uy2[m] = qy[i];
+      ++m;
+    }
+  }
+  if (m < 2) return 0.0;
+  const double dx = ux2[0] - ux2[1], dy = uy2[0] - uy2[1];
+  return sqrt(dx * dx + dy * dy);
+}
+
+// seed level: one path per reference detection with its second build camera
+__global__ void seed_kernel(const SmView v, int ref, Path* out, int* out_count, int cap) {
+  int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+  if (i >= v.n[ref]) return;
+  int best = -1;
+  double best_len = __longlong_as_double(0x7ff0000000000000LL);
+  for (int cam = 0; cam < v.n_cam; ++cam) {
+    if (!v.active[cam] || cam == ref) continue;
+    const double L = seg_len(v.l2d[ref][cam] + 6 * i, v.Wd[cam], v.Hd[cam]);
+    if (L < best_len - 1e-9) {
+      best_len = L;
+      best = cam;
+    }
+  }
+  if (best < 0) return;
+  int slot = atomicAdd(out_count, 1);
+  if (slot >= cap) return;
+  Path p;
+  p.ids[0] = (int)i;
+  p.cams[0] = (signed char)ref;
+  p.k = 1;
+  p.target = best;
+  out[slot] = p;
+}
+
+// StereoMatch::computeMinParallaxDeg + calTriangulateTol (StereoMatch.cpp:1083-1126)
+__device__ double quick_tol(const Line3* const* L, int k, int m, double tol3d) {
+  double min_deg = 180.0;
+  for (int i = 0; i < k; ++i)
+    for (int j = i + 1; j < k; ++j) {
+      double dot = L[i]->u[0] * L[j]->u[0] + L[i]->u[1] * L[j]->u[1] + L[i]->u[2] * L[j]->u[2];
+      dot = fmax(-1.0, fmin(1.0, dot));
+      const double deg = acos(dot) * 180.0 / M_PI;
+      if (deg < min_deg) min_deg = deg;
+    }
+  const int kk = k > 2 ? k : 2;
+  const int mm = m > 2 ? m : 2;
+  const double alpha_depth = sqrt(double(mm) / double(kk));
+  const double th = fmax(min_deg, 1.0);
+  const double num = sin(6.0 * M_PI / 180.0);
+  const double den = fmax(1e-6, sin(th * M_PI / 180.0));
+  const double alpha_angle = fmax(1.0, fmin(2.0, num / den));
+  return tol3d * alpha_depth * alpha_angle;
+}
+
+// Expand one level: each warp takes one path and enumerates candidates on its target.
+__global__ void __launch_bounds__(256) level_kernel(const SmView v, const Path* in, int n_in,
+                                                    Path* out, int* out_count, int out_cap,
+                                                    Path* term, int* term_count, int term_cap) {
+  const int warp = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+  const int lane = threadIdx.x & 31;
+  if (warp >= n_in) return;
+  const Path P = in[warp];
+  const int k = P.k, t = P.target;
+  // image lines of the chosen points on the target camera
+  double lp[OLPT_MAX_CAM][2], lU[OLPT_MAX_CAM][2];
+  double cpt[OLPT_MAX_CAM][2];
+  for (int i = 0; i < k; ++i) {
+    const int c = P.cams[i];
+    const double* L = v.l2d[c][t] + 6 * (int64_t)P.ids[i];
+    lp[i][0] = L[0];
+    lp[i][1] = L[1];
+    lU[i][0] = L[4];
+    lU[i][1] = L[5];
+    cpt[i][0] = v.x[c][P.ids[i]];
+    cpt[i][1] = v.y[c][P.ids[i]];
+  }
+  const int rows = v.rows[t], cols = v.cols[t];
+  const double cellp = (double)v.cell;
+  const double hw = 0.5 * v.cell, hh = 0.5 * v.cell;
+  const double to_index = 1.0 / v.cell;
+  const double tol_grow = v.tol2d + 1e-6;
+  const double tol2 = v.tol2d * v.tol2d;
+  const int* cstart = v.cell_start[t];
+  const int* citems = v.cell_items[t];
+  const double* tx = v.x[t];
+  const double* ty = v.y[t];
+
+  for (int cy = lane; cy < rows; cy += 32) {
+    // IDMap::computeStripIntersection, one row
+    int xmin = 0, xmax = cols - 1;
+    for (int i = 0; i < k && xmin <= xmax; ++i) {
+      const double n0 = -lU[i][1], n1 = lU[i][0];
+      const double d = -(n0 * lp[i][0] + n1 * lp[i][1]);
+      const double y_c = (cy + 0.5) * cellp;
+      const double C = n1 * y_c + d;
+      const double proj_extent = fabs(n0) * hw + fabs(n1) * hh;
+      const double T = tol_grow + proj_extent;
+      int a = 0, b = cols - 1;
+      if (fabs(n0) < 1e-12) {
+        if (fabs(C) > T) {
+          xmin = 1;
+          xmax = 0;
+          break;
+        }
+      } else {
+        double xl = (-T - C) / n0;
+        double xr = (T - C) / n0;
+        if (xl > xr) {
+          double s = xl;
+          xl = xr;
+          xr = s;
+        }
+        a = (int)ceil(xl * to_index - 0.5 - 1e-9);
+        b = (int)floor(xr * to_index - 0.5 + 1e-9);
+        a = a > 0 ? a : 0;
+        b = b < cols - 1 ? b : cols - 1;
+        if (a > b) {
+          xmin = 1;
+          xmax = 0;
+          break;
+        }
+      }
+      xmin = xmin > a ? xmin : a;
+      xmax = xmax < b ? xmax : b;
+    }
+    if (xmin > xmax) continue;
+    for (int cx = xmin; cx <= xmax; ++cx) {
+      const int c = cy * cols + cx;
+      for (int q = cstart[c]; q < cstart[c + 1]; ++q) {
+        const int pid = citems[q];
+        const double qx = tx[pid], qy = ty[pid];
+        bool ok = true;
+        // IDMap::visitPointsInRowSpans precise test
+        for (int i = 0; i < k; ++i) {
+          const double dx = qx - lp[i][0], dy = qy - lp[i][1];
+          const double z = dy * lU[i][0] - dx * lU[i][1];
+          if (z * z > tol2) {
+            ok = false;
+            break;
+          }
+        }
+        if (!ok) continue;
+        // checkBackProjection (StereoMatch.cpp:1206-1227)
+        for (int i = 0; i < k; ++i) {
+          const double* L = v.l2d[t][P.cams[i]] + 6 * (int64_t)pid;
+          const double d0 = cpt[i][0] - L[0], d1 = cpt[i][1] - L[1];
+          const double z = d1 * L[2] - d0 * L[3];
+          if (z * z > tol2) {
+            ok = false;
+            break;
+          }
+        }
+        if (!ok) continue;
+        // extend the path; quick triangulation gate
+        Line3 Ls[OLPT_MAX_CAM];
+        const Line3* Lp[OLPT_MAX_CAM];
+        for (int i = 0; i < k; ++i) {
+          load_line3(v.los[P.cams[i]] + 6 * (int64_t)P.ids[i], Ls[i]);
+          Lp[i] = &Ls[i];
+        }
+        load_line3(v.los[t] + 6 * (int64_t)pid, Ls[k]);
+        Lp[k] = &Ls[k];
+        const int k1 = k + 1;
+        const double tq = quick_tol(Lp, k1, v.m, v.tol3d);
+        double X[3], err;
+        if (!triangulate<OLPT_MAX_CAM>(Lp, k1, X, err)) continue;
+        if (!(err <= tq)) continue;
+        Path ch = P;
+        ch.ids[k] = pid;
+        ch.cams[k] = (signed char)t;
+        ch.k = k1;
+        if (k1 == v.m) {
+          ch.target = -1;
+          int slot = atomicAdd(term_count, 1);
+          if (slot < term_cap) term[slot] = ch;
+          continue;
+        }
+        // StereoMatch::selectNextCameraByMaxPairAngle (StereoMatch.cpp:1375-1411)
+        int best = -1;
+        double best_score = -1.0;
+        for (int cam = 0; cam < v.n_cam; ++cam) {
+          if (!v.active[cam]) continue;
+          bool used = false;
+          for (int i = 0; i < k1; ++i) used |= (ch.cams[i] == cam);
+          if (used) continue;
+          double ux[OLPT_MAX_CAM], uy[OLPT_MAX_CAM];
+          for (int i = 0; i < k1; ++i) {
+            const double* L = v.l2d[ch.cams[i]][cam] + 6 * (int64_t)ch.ids[i];
+            ux[i] = L[2];
+            uy[i] = L[3];
+          }
+          double score = 0.0;
+          if (k1 >= 2) {
+            for (int i = 0; i < k1; ++i) {
+              for (int j = i + 1; j < k1; ++j) {
+                const double s = fabs(ux[i] * uy[j] - uy[i] * ux[j]);
+                if (s > score) score = s;
+                if (score >= 1.0 - 1e-12) break;
+              }
+              if (score >= 1.0 - 1e-12) break;
+            }
+          }
+          if (score > best_score) {
+            best_score = score;
+            best = cam;
+          }
+        }
+        if (best < 0) continue;
+        ch.target = best;
+        int slot = atomicAdd(out_count, 1);
+        if (slot < out_cap) out[slot] = ch;
+      }
+    }
+  }
+}
+
+// StereoMatch::checkMatch, case "every active camera was used to build"
+// (StereoMatch.cpp:520-540): triangulate in camera order, gate on tol_3d and limit.
+__global__ void check_kernel(const SmView v, const Path* term, int n_term, int* cand_ids,
+                             double* cand_e, double* cand_x, int* cand_count, int cap) {
+  int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= n_term) return;
+  const Path P = term[i];
+  int ids[OLPT_MAX_CAM];
+  for (int c = 0; c < v.n_cam; ++c) ids[c] = -1;
+  for (int j = 0; j < P.k; ++j) ids[P.cams[j]] = P.ids[j];
+  Line3 Ls[OLPT_MAX_CAM];
+  const Line3* Lp[OLPT_MAX_CAM];
+  int n = 0;
+  for (int c = 0; c < v.n_cam; ++c) {
+    if (ids[c] < 0) continue;
+    load_line3(v.los[c] + 6 * (int64_t)ids[c], Ls[n]);
+    Lp[n] = &Ls[n];
+    ++n;
+  }
+  double X[3], err;
+  if (!triangulate<OLPT_MAX_CAM>(Lp, n, X, err)) return;  // the reference throws here
+  if (err > v.tol3d) return;
+  if (X[0] > v.limit[1] || X[0] < v.limit[0] || X[1] > v.limit[3] || X[1] < v.limit[2] ||
+      X[2] > v.limit[5] || X[2] < v.limit[4])
+    return;
+  int slot = atomicAdd(cand_count, 1);
+  if (slot >= cap) return;
+  for (int c = 0; c < v.n_cam; ++c) cand_ids[(int64_t)slot * v.n_cam + c] = ids[c];
+  cand_e[slot] = err;
+  cand_x[3 * slot] = X[0];
+  cand_x[3 * slot + 1] = X[1];
+  cand_x[3 * slot + 2] = X[2];
+}
+
+}  // namespace
+
+// ---------------------------------------------------------------- host driver
+void stereo_match_device(olpt_ctx* ctx, const SmParams& prm, StereoResult& res) {
+  cudaStream_t s = ctx->stream;
+  const int n_cam = ctx->n_cam;
+  SmView v{};
+  v.n_cam = n_cam;
+  int n_active = 0;
+  for (int c = 0; c < n_cam; ++c) {
+    v.active[c] = ctx->cams_h[c].is_active;
+    n_active += v.active[c];
+  }
+  OLPT_REQUIRE(n_active >= 2, OLPT_ERR_INVALID_ARG, "preCheck: need at least 2 active cameras.");
+  OLPT_REQUIRE(prm.match_cam_count >= 2 && prm.match_cam_count <= n_active, OLPT_ERR_INVALID_ARG,
+               "preCheck: match_cam_count must be within [2," + std::to_string(n_active) + "].");
+  v.n_active = n_active;
+  v.m = std::min(std::max(2, prm.match_cam_count), n_active);
+  OLPT_REQUIRE(v.m == n_active, OLPT_ERR_UNSUPPORTED,
+               "match_cam_count below the number of active cameras: the reference aborts on this "
+               "path (checkMatch leaves e_check NaN, StereoMatch.cpp:561-600 vs :129)");
+  v.cell = std::max(1, prm.idmap_cell_px);
+  v.tol2d = prm.tol_2d_px;
+  v.tol3d = prm.tol_3d_mm;
+  for (int q = 0; q < 6; ++q) v.limit[q] = prm.limit[q];
+
+  StereoWork& W = ctx->sm;
+  // reference camera: fewest detections among active (StereoMatch.cpp:70-85)
+  int ref = -1;
+  int64_t best = INT64_MAX;
+  for (int c = 0; c < n_cam; ++c) {
+    if (!v.active[c]) continue;
+    if (ctx->det_counts_h[c] < best) {
+      best = ctx->det_counts_h[c];
+      ref = c;
+    }
+  }
+  res.ref_cam = ref;
+
+  // grids and lines
+  for (int c = 0; c < n_cam; ++c) {
+    const CamDev& cm = ctx->cams_h[c];
+    const int64_t n = v.active[c] ? ctx->det_counts_h[c] : 0;
+    v.n[c] = n;
+    v.x[c] = ctx->dets[c].x.as<double>();
+    v.y[c] = ctx->dets[c].y.as<double>();
+    v.Wd[c] = (double)cm.n_col;
+    v.Hd[c] = (double)cm.n_row;
+    const int rows = std::max(1, cm.n_row / v.cell + (cm.n_row % v.cell ? 1 : 0));
+    const int cols = std::max(1, cm.n_col / v.cell + (cm.n_col % v.cell ? 1 : 0));
+    v.rows[c] = rows;
+    v.cols[c] = cols;
+    if (!v.active[c]) continue;
+    const int ncell = rows * cols;
+    W.cell_start[c].ensure((ncell + 1) * sizeof(int), s);
+    W.cell_cursor[c].ensure(ncell * sizeof(int), s);
+    W.cell_items[c].ensure((n + 1) * sizeof(int), s);
+    W.cell_of[c].ensure((n + 1) * sizeof(int), s);
+    W.los[c].ensure((n + 1) * 6 * sizeof(double), s);
+    OLPT_CUDA(cudaMemsetAsync(W.cell_cursor[c].p, 0, ncell * sizeof(int), s));
+    if (n > 0) {
+      cell_hist_kernel<<<nblk(n), 256, 0, s>>>(v.x[c], v.y[c], n, v.cell, rows, cols,
+                                                W.cell_of[c].as<int>(), W.cell_cursor[c].as<int>());
+    }
+    cell_scan_kernel<<<1, 1024, 0, s>>>(W.cell_cursor[c].as<int>(), ncell, W.cell_start[c].as<int>());
+    OLPT_CUDA(cudaMemsetAsync(W.cell_cursor[c].p, 0, ncell * sizeof(int), s));
+    if (n > 0) {
+      cell_scatter_kernel<<<nblk(n), 256, 0, s>>>(W.cell_of[c].as<int>(), n, W.cell_start[c].as<int>(),
+                                                   W.cell_cursor[c].as<int>(), W.cell_items[c].as<int>());
+      cell_sort_kernel<<<nblk(ncell), 256, 0, s>>>(W.cell_start[c].as<int>(), ncell,
+                                                    W.cell_items[c].as<int>());
+    }
+    OLPT_CUDA(cudaGetLastError());
+    v.cell_start[c] = W.cell_start[c].as<int>();
+    v.cell_items[c] = W.cell_items[c].as<int>();
+    v.los[c] = W.los[c].as<double>();
+  }
+  // image lines of every detection on every other active camera
+  {
+    W.l2d_ptrs.ensure(OLPT_MAX_CAM * OLPT_MAX_CAM * sizeof(double*), s);
+    W.active_d.ensure(OLPT_MAX_CAM * sizeof(int), s);
+    std::vector<double*> ptrs(OLPT_MAX_CAM * OLPT_MAX_CAM, nullptr);
+    for (int c = 0; c < n_cam; ++c) {
+      if (!v.active[c]) continue;
+      for (int t = 0; t < n_cam; ++t) {
+        if (t == c || !v.active[t]) continue;
+        DevBuf& b = W.l2d[c * OLPT_MAX_CAM + t];
+        b.ensure((v.n[c] + 1) * 6 * sizeof(double), s);
+        ptrs[c * OLPT_MAX_CAM + t] = b.as<double>();
+        v.l2d[c][t] = b.as<double>();
+      }
+    }
+    OLPT_CUDA(cudaMemcpyAsync(W.l2d_ptrs.p, ptrs.data(), ptrs.size() * sizeof(double*),
+                              cudaMemcpyHostToDevice, s));
+    OLPT_CUDA(cudaMemcpyAsync(W.active_d.p, v.active, OLPT_MAX_CAM * sizeof(int),
+                              cudaMemcpyHostToDevice, s));
+    for (int c = 0; c < n_cam; ++c) {
+      if (!v.active[c] || v.n[c] == 0) continue;
+      lines_kernel<<<nblk(v.n[c], 128), 128, 0, s>>>(
+          ctx->cams_d.as<CamDev>(), c, v.x[c], v.y[c], v.n[c], n_cam, W.active_d.as<int>(),
+          W.los[c].as<double>(), W.l2d_ptrs.as<double*>() + c * OLPT_MAX_CAM);
+      OLPT_CUDA(cudaGetLastError());
+    }
+  }
+
+  // breadth-first expansion of the build DFS
+  W.counters.ensure(4 * sizeof(int), s);
+  int* cnt = W.counters.as<int>();
+  auto read_count = [&](int idx) {
+    int h = 0;
+    OLPT_CUDA(cudaMemcpyAsync(&h, cnt + idx, sizeof(int), cudaMemcpyDeviceToHost, s));
+    OLPT_CUDA(cudaStreamSynchronize(s));
+    return h;
+  };
+  int64_t n_ref = v.n[ref];
+  int cap_a = (int)std::max<int64_t>(n_ref, 1024);
+  W.path_a.ensure(cap_a * sizeof(Path), s);
+  OLPT_CUDA(cudaMemsetAsync(cnt, 0, 4 * sizeof(int), s));
+  if (n_ref > 0) seed_kernel<<<nblk(n_ref), 256, 0, s>>>(v, ref, W.path_a.as<Path>(), cnt, cap_a);
+  OLPT_CUDA(cudaGetLastError());
+  int n_in = read_count(0);
+  int term_cap = (int)std::max<int64_t>(4 * n_ref, 4096);
+  W.term.ensure(term_cap * sizeof(Path), s);
+  int n_term = 0;
+  DevBuf* in_buf = &W.path_a;
+  DevBuf* out_buf = &W.path_b;
+  int out_cap = (int)std::max<int64_t>(16 * (int64_t)n_in, 4096);
+  for (int level = 1; level < v.m && n_in > 0; ++level) {
+    for (;;) {
+      out_buf->ensure((size_t)out_cap * sizeof(Path), s);
+      W.term.ensure((size_t)term_cap * sizeof(Path), s);
+      // counters: [1] = children, [2] = terminals (terminals accumulate across levels)
+      OLPT_CUDA(cudaMemsetAsync(cnt + 1, 0, sizeof(int), s));
+      OLPT_CUDA(cudaMemcpyAsync(cnt + 2, &n_term, sizeof(int), cudaMemcpyHostToDevice, s));
+      const int64_t threads = (int64_t)n_in * 32;
+      level_kernel<<<nblk(threads), 256, 0, s>>>(v, in_buf->as<Path>(), n_in, out_buf->as<Path>(),
+                                                 cnt + 1, out_cap, W.term.as<Path>(), cnt + 2,
+                                                 term_cap);
+      OLPT_CUDA(cudaGetLastError());
+      int h[2];
+      OLPT_CUDA(cudaMemcpyAsync(h, cnt + 1, 2 * sizeof(int), cudaMemcpyDeviceToHost, s));
+      OLPT_CUDA(cudaStreamSynchronize(s));
+      if (h[0] > out_cap || h[1] > term_cap) {  // grow and redo this level
+        out_cap = std::max(out_cap, h[0] + h[0] / 4 + 1024);
+        term_cap = std::max(term_cap, h[1] + h[1] / 4 + 1024);
+        continue;
+      }
+      n_in = h[0];
+      n_term = h[1];
+      break;
+    }
+    std::swap(in_buf, out_buf);
+    out_cap = (int)std::max<int64_t>(4 * (int64_t)n_in, 4096);
+  }
+
+  // check + candidate list
+  int cap_c = std::max(n_term, 1);
+  W.cand_ids.ensure((size_t)cap_c * n_cam * sizeof(int), s);
+  W.cand_e.ensure((size_t)cap_c * sizeof(double), s);
+  W.cand_x.ensure((size_t)cap_c * 3 * sizeof(double), s);
+  OLPT_CUDA(cudaMemsetAsync(cnt + 3, 0, sizeof(int), s));
+  if (n_term > 0)
+    check_kernel<<<nblk(n_term, 128), 128, 0, s>>>(v, W.term.as<Path>(), n_term, W.cand_ids.as<int>(),
+                                              W.cand_e.as<double>(), W.cand_x.as<double>(), cnt + 3,
+                                              cap_c);
+  OLPT_CUDA(cudaGetLastError());
+  const int M = read_count(3);
+  res.ids.resize((size_t)M * n_cam);
+  res.e.resize(M);
+  res.X.resize((size_t)M * 3);
+  if (M > 0) {
+    OLPT_CUDA(cudaMemcpyAsync(res.ids.data(), W.cand_ids.p, (size_t)M * n_cam * sizeof(int),
+                              cudaMemcpyDeviceToHost, s));
+    OLPT_CUDA(cudaMemcpyAsync(res.e.data(), W.cand_e.p, (size_t)M * sizeof(double),
+                              cudaMemcpyDeviceToHost, s));
+    OLPT_CUDA(cudaMemcpyAsync(res.X.data(), W.cand_x.p, (size_t)M * 3 * sizeof(double),
+                              cudaMemcpyDeviceToHost, s));
+    OLPT_CUDA(cudaStreamSynchronize(s));
+  }
+  res.n_cam = n_cam;
+  sort_candidates(res);
+  std::vector<int> counts(n_cam);
+  std::vector<int> active(n_cam);
+  for (int c = 0; c < n_cam; ++c) {
+    counts[c] = (int)ctx->det_counts_h[c];
+    active[c] = v.active[c];
+  }
+  prune_candidates(res, counts, active);
+}
+
+}  // namespace olpt

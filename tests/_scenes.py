@@ -18,10 +18,18 @@ def scene(kind: str = "small"):
     raise KeyError(kind)
 
 
+def settings(kind: str = "small") -> synth.IPRSettings:
+    """IPR knobs; match_cam_count capped at n_cam as readCommonConfig does
+    (src/srcSTB/Config.cpp:222-224)."""
+    s = synth.IPRSettings()
+    s.match_cam_count = min(s.match_cam_count, scene(kind).n_cam)
+    return s
+
+
 @functools.lru_cache(maxsize=None)
 def ref_oracle(kind: str = "small", threads: int = 0):
     from oracle.ref import RefOracle
-    return RefOracle(scene(kind), synth.IPRSettings(), threads=threads)
+    return RefOracle(scene(kind), settings(kind), threads=threads)
 
 
 def gpu_context(sc):
