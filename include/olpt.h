@@ -133,6 +133,43 @@ olpt_status_t olpt_get_candidates(olpt_ctx* ctx, int32_t* ids, double* e_check, 
 /* Selected matches of the last match (triangulateMatch output order): ids, xyz. */
 olpt_status_t olpt_get_matches(olpt_ctx* ctx, int32_t* ids, double* xyz);
 
+/* ------------------------------------------------------------------ 3D objects */
+/* Replace the context's 3D objects with n tracers at xyz (n x 3); their 2D
+ * projections are computed on the device (Object3D::projectObject2D,
+ * src/srcObject/ObjectInfo.cpp:32-47) by the next shake or residual call. */
+olpt_status_t olpt_objects_upload(olpt_ctx* ctx, int64_t n, const double* xyz);
+olpt_status_t olpt_objects_count(olpt_ctx* ctx, int64_t* n);
+/* Download objects: xyz (n x 3), 2D projections uv (n x n_cam x 2), flags (ObjFlag bits:
+ * 1 = Ghost, 2 = Repeated, inc/libSTB/Shake.h:19) and shake scores; any may be NULL. */
+olpt_status_t olpt_objects_download(olpt_ctx* ctx, double* xyz, double* uv, uint8_t* flags,
+                                    double* score);
+
+/* ------------------------------------------------------------------ shake */
+/* ShakeParam + tracer radius + tol_3d (inc/libSTB/Config.h:82-89, 190-200).
+ * precision: 0 = FP32 residual / OTF Gaussian / squared-error sums (production),
+ * 1 = FP64 throughout (parity with the reference's double arithmetic). */
+typedef struct olpt_shake_params {
+  double shake_width;
+  double shakewidth_min;
+  int n_shake_loop;
+  double thred_ghost;
+  int ratio_augimg;
+  double radius_obj;
+  double tol_3d_mm;
+  int precision;
+} olpt_shake_params;
+
+/* Shake(cams, cfg).runShake(objs, images) (src/srcSTB/Shake.cpp:36-163) on the context's
+ * objects and current images: objects are moved in place; flags and scores are set. */
+olpt_status_t olpt_shake(olpt_ctx* ctx, const olpt_shake_params* p);
+/* Shake::calResidualImage(objs, images, flags) (Shake.h:41-48, Shake.cpp:165-244 with
+ * output_ipr): every camera, clamped at 0; objects with non-zero flags are skipped
+ * when use_flags.  make_current != 0 replaces the current images with the residual. */
+olpt_status_t olpt_residual(olpt_ctx* ctx, const olpt_shake_params* p, int use_flags,
+                            int make_current);
+/* Copy the last residual plane of camera `cam` to host memory as F32 or F64. */
+olpt_status_t olpt_residual_download(olpt_ctx* ctx, int cam, olpt_dtype_t dtype, void* out);
+
 #ifdef __cplusplus
 }
 #endif

@@ -46,6 +46,19 @@ def sm_params(settings, limit) -> SmParams:
     return p
 
 
+class ShakeParams(C.Structure):
+    _fields_ = [("shake_width", C.c_double), ("shakewidth_min", C.c_double),
+                ("n_shake_loop", C.c_int), ("thred_ghost", C.c_double), ("ratio_augimg", C.c_int),
+                ("radius_obj", C.c_double), ("tol_3d_mm", C.c_double), ("precision", C.c_int)]
+
+
+def shake_params(settings, precision: int = 0) -> ShakeParams:
+    return ShakeParams(shake_width=settings.shake_width, shakewidth_min=settings.shakewidth_min,
+                       n_shake_loop=settings.n_shake_loop, thred_ghost=settings.thred_ghost,
+                       ratio_augimg=settings.ratio_augimg, radius_obj=settings.radius_obj,
+                       tol_3d_mm=settings.tol_3d_mm, precision=precision)
+
+
 class OlptError(RuntimeError):
     def __init__(self, code: int, msg: str):
         super().__init__(f"olpt status {code}: {msg}")
@@ -229,3 +242,35 @@ class Context:
         x = np.empty((n, 3))
         self._check(self.L.olpt_get_matches(self.h, _p(ids, _i32p), _p(x)))
         return ids, x
+
+    # ---------------------------------------------------------------- objects / shake
+    def upload_objects(self, xyz: np.ndarray):
+        xyz = np.ascontiguousarray(xyz, dtype=np.float64).reshape(-1, 3)
+        self._check(self.L.olpt_objects_upload(self.h, C.c_int64(len(xyz)), _p(xyz)))
+
+    def n_objects(self) -> int:
+        n = C.c_int64()
+        self._check(self.L.olpt_objects_count(self.h, C.byref(n)))
+        return n.value
+
+    def objects(self):
+        n = self.n_objects()
+        xyz = np.empty((n, 3))
+        uv = np.empty((n, self.n_cam, 2))
+        fl = np.empty(n, dtype=np.uint8)
+        sc = np.empty(n)
+        self._check(self.L.olpt_objects_download(self.h, _p(xyz), _p(uv),
+                                                 fl.ctypes.data_as(C.POINTER(C.c_uint8)), _p(sc)))
+        return {"xyz": xyz, "uv": uv, "flags": fl.astype(np.int64), "score": sc}
+
+    def shake(self, params: ShakeParams):
+        self._check(self.L.olpt_shake(self.h, C.byref(params)))
+
+    def residual(self, params: ShakeParams, use_flags: bool = False, make_current: bool = False):
+        self._check(self.L.olpt_residual(self.h, C.byref(params), int(use_flags), int(make_current)))
+
+    def residual_image(self, cam: int, shape, dtype=np.float64) -> np.ndarray:
+        out = np.empty(shape, dtype=dtype)
+        self._check(self.L.olpt_residual_download(self.h, cam, _DTYPES[np.dtype(dtype)],
+                                                  out.ctypes.data_as(C.c_void_p)))
+        return out

@@ -186,6 +186,8 @@ void olpt_ctx_destroy(olpt_ctx* ctx) {
   ctx->scratch.release(ctx->stream);
   ctx->sm.release(ctx->stream);
   ctx->obj.release(ctx->stream);
+  ctx->shk.release(ctx->stream);
+  for (int c = 0; c < OLPT_MAX_CAM; ++c) ctx->resid[c].buf.release(ctx->stream);
   cudaStreamSynchronize(ctx->stream);
   if (ctx->own_stream) cudaStreamDestroy(ctx->stream);
   delete ctx;
@@ -569,6 +571,117 @@ olpt_status_t olpt_get_matches(olpt_ctx* ctx, int32_t* ids, double* xyz) {
       if (xyz) std::copy(&r.X[3 * j], &r.X[3 * j] + 3, xyz + 3 * k);
       ++k;
     }
+  });
+}
+
+}  // extern "C"
+
+// ---------------------------------------------------------------- objects / shake
+#include "olpt_shake.h"
+
+namespace olpt {
+namespace {
+olpt::ShakeParams to_shake_params(const olpt_shake_params* p) {
+  olpt::ShakeParams s;
+  s.shake_width = p->shake_width;
+  s.shakewidth_min = p->shakewidth_min;
+  s.n_shake_loop = p->n_shake_loop;
+  s.thred_ghost = p->thred_ghost;
+  s.ratio_augimg = p->ratio_augimg;
+  s.radius_obj = p->radius_obj;
+  s.tol_3d_mm = p->tol_3d_mm;
+  s.precision = p->precision;
+  return s;
+}
+
+__global__ void init_objects_kernel(uint8_t* flags, double* score, int64_t n) {
+  int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+  if (i >= n) return;
+  flags[i] = 0;
+  score[i] = 1.0;
+}
+}  // namespace
+}  // namespace olpt
+
+extern "C" {
+
+olpt_status_t olpt_objects_upload(olpt_ctx* ctx, int64_t n, const double* xyz) {
+  return guard(ctx, [&] {
+    OLPT_REQUIRE(ctx->n_cam > 0, OLPT_ERR_INVALID_ARG, "upload cameras first");
+    OLPT_REQUIRE(n >= 0 && (n == 0 || xyz), OLPT_ERR_INVALID_ARG, "bad object buffer");
+    ctx->obj.ensure(std::max<int64_t>(n, 1), ctx->n_cam, ctx->stream);
+    ctx->obj.n = n;
+    if (n > 0) {
+      OLPT_CUDA(cudaMemcpyAsync(ctx->obj.xyz.p, xyz, n * 3 * sizeof(double), cudaMemcpyHostToDevice,
+                                ctx->stream));
+      init_objects_kernel<<<nblk(n), 256, 0, ctx->stream>>>(ctx->obj.flags.as<uint8_t>(),
+                                                             ctx->obj.score.as<double>(), n);
+      OLPT_CUDA(cudaGetLastError());
+    }
+    OLPT_CUDA(cudaStreamSynchronize(ctx->stream));
+  });
+}
+
+olpt_status_t olpt_objects_count(olpt_ctx* ctx, int64_t* n) {
+  return guard(ctx, [&] {
+    OLPT_REQUIRE(n, OLPT_ERR_INVALID_ARG, "null output");
+    *n = ctx->obj.n;
+  });
+}
+
+olpt_status_t olpt_objects_download(olpt_ctx* ctx, double* xyz, double* uv, uint8_t* flags,
+                                    double* score) {
+  return guard(ctx, [&] {
+    const int64_t n = ctx->obj.n;
+    if (n <= 0) return;
+    cudaStream_t s = ctx->stream;
+    if (xyz) OLPT_CUDA(cudaMemcpyAsync(xyz, ctx->obj.xyz.p, n * 3 * 8, cudaMemcpyDeviceToHost, s));
+    if (uv)
+      OLPT_CUDA(cudaMemcpyAsync(uv, ctx->obj.uv.p, n * ctx->n_cam * 2 * 8, cudaMemcpyDeviceToHost, s));
+    if (flags) OLPT_CUDA(cudaMemcpyAsync(flags, ctx->obj.flags.p, n, cudaMemcpyDeviceToHost, s));
+    if (score) OLPT_CUDA(cudaMemcpyAsync(score, ctx->obj.score.p, n * 8, cudaMemcpyDeviceToHost, s));
+    OLPT_CUDA(cudaStreamSynchronize(s));
+  });
+}
+
+olpt_status_t olpt_shake(olpt_ctx* ctx, const olpt_shake_params* p) {
+  return guard(ctx, [&] {
+    OLPT_REQUIRE(p, OLPT_ERR_INVALID_ARG, "null params");
+    OLPT_REQUIRE(p->precision == 0 || p->precision == 1, OLPT_ERR_INVALID_ARG,
+                 "precision must be 0 (FP32) or 1 (FP64)");
+    shake_device(ctx, to_shake_params(p));
+    OLPT_CUDA(cudaStreamSynchronize(ctx->stream));
+  });
+}
+
+olpt_status_t olpt_residual(olpt_ctx* ctx, const olpt_shake_params* p, int use_flags,
+                            int make_current) {
+  return guard(ctx, [&] {
+    OLPT_REQUIRE(p, OLPT_ERR_INVALID_ARG, "null params");
+    residual_device(ctx, to_shake_params(p), use_flags != 0, make_current != 0);
+    OLPT_CUDA(cudaStreamSynchronize(ctx->stream));
+  });
+}
+
+olpt_status_t olpt_residual_download(olpt_ctx* ctx, int cam, olpt_dtype_t dtype, void* out) {
+  return guard(ctx, [&] {
+    OLPT_REQUIRE(cam >= 0 && cam < ctx->n_cam && out, OLPT_ERR_INVALID_ARG, "bad camera/buffer");
+    OLPT_REQUIRE(dtype == OLPT_F32 || dtype == OLPT_F64, OLPT_ERR_INVALID_ARG,
+                 "download dtype must be F32 or F64");
+    ImagePlane& im = ctx->resid[cam];
+    OLPT_REQUIRE(im.buf.p, OLPT_ERR_INVALID_ARG, "no residual computed");
+    const int64_t n = (int64_t)im.H * im.W;
+    ctx->scratch.ensure(n * 8, ctx->stream);
+    if (dtype == OLPT_F32)
+      convert_plane_kernel<float><<<nblk(n), 256, 0, ctx->stream>>>(
+          im.buf.as<unsigned char>(), im.pitch, im.H, im.W, im.dtype, ctx->scratch.as<float>());
+    else
+      convert_plane_kernel<double><<<nblk(n), 256, 0, ctx->stream>>>(
+          im.buf.as<unsigned char>(), im.pitch, im.H, im.W, im.dtype, ctx->scratch.as<double>());
+    OLPT_CUDA(cudaGetLastError());
+    OLPT_CUDA(cudaMemcpyAsync(out, ctx->scratch.p, n * esize(dtype), cudaMemcpyDeviceToHost,
+                              ctx->stream));
+    OLPT_CUDA(cudaStreamSynchronize(ctx->stream));
   });
 }
 

@@ -97,6 +97,37 @@ struct Dets {
   int64_t cap = 0;
 };
 
+// CSR (start[n_buckets + 1], items[n]) from per-item bucket keys (key < 0: dropped);
+// built by count -> exclusive scan -> scatter -> per-bucket ascending order (scan.cu).
+struct Csr {
+  DevBuf start, items, cursor, tmp;
+  void build(const int* key, int n, int n_buckets, cudaStream_t s);
+  void release(cudaStream_t s) {
+    start.release(s);
+    items.release(s);
+    cursor.release(s);
+    tmp.release(s);
+  }
+};
+
+// Device workspace of the shake (grown on demand).
+struct ShakeWork {
+  DevBuf otfp;      // n x n_cam x 5 OTF parameters at the object centres
+  DevBuf pair_key;  // n x n_cam tile keys
+  Csr bins;         // (object, camera) pairs per image tile
+  DevBuf rep, hkey, has_nb;
+  Csr hash;         // 3D hash grid of object centres
+  void release(cudaStream_t s) {
+    otfp.release(s);
+    pair_key.release(s);
+    bins.release(s);
+    rep.release(s);
+    hkey.release(s);
+    has_nb.release(s);
+    hash.release(s);
+  }
+};
+
 // Device workspace of stereo matching (grown on demand, reused across frames).
 struct StereoWork {
   DevBuf cell_start[OLPT_MAX_CAM], cell_cursor[OLPT_MAX_CAM], cell_items[OLPT_MAX_CAM];
@@ -148,6 +179,11 @@ struct Objects {
 };
 
 void stereo_match_device(olpt_ctx* ctx, const SmParams& prm, StereoResult& res);
+struct OtfView;
+struct ShakeParams;
+OtfView otf_view(olpt_ctx* ctx);
+void shake_device(olpt_ctx* ctx, const ShakeParams& sp);
+void residual_device(olpt_ctx* ctx, const ShakeParams& sp, bool use_flags, bool make_current);
 
 }  // namespace olpt
 
@@ -179,6 +215,10 @@ struct olpt_ctx {
 
   // 3D objects (stereo output / shake input and output)
   olpt::Objects obj;
+
+  // shake: residual planes (FP32 or FP64) and workspace
+  olpt::ImagePlane resid[OLPT_MAX_CAM];
+  olpt::ShakeWork shk;
 
   // scratch
   olpt::DevBuf scratch;
