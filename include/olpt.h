@@ -59,6 +59,17 @@ void olpt_ctx_destroy(olpt_ctx* ctx);
 const char* olpt_last_error(const olpt_ctx* ctx);
 /* Synchronise the context's stream. */
 olpt_status_t olpt_sync(olpt_ctx* ctx);
+/* The context's CUDA stream (a cudaStream_t), for callers that record their own events. */
+olpt_status_t olpt_stream(olpt_ctx* ctx, void** stream);
+/* Per-kernel event timing (no reference counterpart; the reference prints clock()
+ * CPU time per stage).  kernel: 0 = detection, 1 = stereo level expansion,
+ * 2 = residual image, 3 = shake.  read returns the summed duration, the number of
+ * timed launches and their algorithmic bytes since the last read. */
+olpt_status_t olpt_profile(olpt_ctx* ctx, int enable);
+/* Total number of kernel launches issued by this library in this process. */
+int64_t olpt_launch_count(void);
+olpt_status_t olpt_profile_read(olpt_ctx* ctx, int kernel, double* total_ms, int64_t* launches,
+                                double* bytes);
 
 /* ------------------------------------------------------------------ cameras */
 /* Replaces std::vector<Camera> set-up (Camera::loadParameters, Camera.cpp:19-158;
@@ -169,6 +180,28 @@ olpt_status_t olpt_residual(olpt_ctx* ctx, const olpt_shake_params* p, int use_f
                             int make_current);
 /* Copy the last residual plane of camera `cam` to host memory as F32 or F64. */
 olpt_status_t olpt_residual_download(olpt_ctx* ctx, int cam, olpt_dtype_t dtype, void* out);
+
+/* ------------------------------------------------------------------ IPR */
+/* ObjectConfig knobs used by IPR::runIPR (IPRParam, SMParam, ShakeParam and the
+ * tracer's _min_obj_int / _radius_obj; inc/libSTB/Config.h:37-44, 72-89, 190-195). */
+typedef struct olpt_ipr_params {
+  double min_obj_int;
+  olpt_sm_params sm;
+  olpt_shake_params shake;
+  int n_cam_reduced;
+  int n_loop_ipr;
+  int n_loop_ipr_reduced;
+  int64_t n_obj2d_process_max;
+} olpt_ipr_params;
+
+/* IPR(cams).runIPR(cfg, images) (src/srcSTB/IPR.cpp:195-305) on the current images:
+ * full camera set, then reduced subsets, each for its loop count, with the 2D
+ * tolerance growing x1.5 per loop.  The current images end as the final residual.
+ * n_objects receives the number of reconstructed objects. */
+olpt_status_t olpt_ipr_run(olpt_ctx* ctx, const olpt_ipr_params* p, int64_t* n_objects);
+/* Objects of the last olpt_ipr_run in the reference's output order: xyz (n x 3) and
+ * their 2D projections uv (n x n_cam x 2); either may be NULL. */
+olpt_status_t olpt_ipr_result(olpt_ctx* ctx, double* xyz, double* uv);
 
 #ifdef __cplusplus
 }

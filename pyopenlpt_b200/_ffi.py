@@ -82,6 +82,13 @@ def lib():
     return _lib
 
 
+def launch_count() -> int:
+    """Kernel launches issued by libolpt_cuda.so in this process."""
+    L = lib()
+    L.olpt_launch_count.restype = C.c_int64
+    return int(L.olpt_launch_count())
+
+
 def _p(a: Optional[np.ndarray], t=_dp):
     return None if a is None else a.ctypes.data_as(t)
 
@@ -274,3 +281,47 @@ class Context:
         self._check(self.L.olpt_residual_download(self.h, cam, _DTYPES[np.dtype(dtype)],
                                                   out.ctypes.data_as(C.c_void_p)))
         return out
+
+    # ---------------------------------------------------------------- IPR
+    def ipr_run(self, params: "IprParams") -> int:
+        n = C.c_int64()
+        self._check(self.L.olpt_ipr_run(self.h, C.byref(params), C.byref(n)))
+        return n.value
+
+    def ipr_result(self, n: int):
+        xyz = np.empty((n, 3))
+        uv = np.empty((n, self.n_cam, 2))
+        self._check(self.L.olpt_ipr_result(self.h, _p(xyz), _p(uv)))
+        return xyz, uv
+
+    # ---------------------------------------------------------------- profiling
+    def stream(self) -> int:
+        s = C.c_void_p()
+        self._check(self.L.olpt_stream(self.h, C.byref(s)))
+        return s.value or 0
+
+    def profile(self, enable: bool):
+        self._check(self.L.olpt_profile(self.h, int(enable)))
+
+    def profile_read(self, kernel: int):
+        ms = C.c_double()
+        n = C.c_int64()
+        b = C.c_double()
+        self._check(self.L.olpt_profile_read(self.h, kernel, C.byref(ms), C.byref(n), C.byref(b)))
+        return ms.value, n.value, b.value
+
+
+PROF_PEAKS, PROF_STEREO, PROF_RESIDUAL, PROF_SHAKE = 0, 1, 2, 3
+
+
+class IprParams(C.Structure):
+    _fields_ = [("min_obj_int", C.c_double), ("sm", SmParams), ("shake", ShakeParams),
+                ("n_cam_reduced", C.c_int), ("n_loop_ipr", C.c_int),
+                ("n_loop_ipr_reduced", C.c_int), ("n_obj2d_process_max", C.c_int64)]
+
+
+def ipr_params(settings, limit, precision: int = 0) -> IprParams:
+    return IprParams(min_obj_int=float(settings.min_obj_int), sm=sm_params(settings, limit),
+                     shake=shake_params(settings, precision), n_cam_reduced=settings.n_cam_reduced,
+                     n_loop_ipr=settings.n_loop_ipr, n_loop_ipr_reduced=settings.n_loop_ipr_reduced,
+                     n_obj2d_process_max=settings.n_obj2d_process_max)

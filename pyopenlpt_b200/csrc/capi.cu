@@ -11,6 +11,7 @@
 #include "olpt_otf.cuh"
 
 namespace olpt {
+std::atomic<long long> g_launches{0};
 void find_peaks_device(olpt_ctx* ctx, double min_int, bool sync_counts);
 void ensure_det_capacity(olpt_ctx* ctx, int cam, int64_t cap);
 
@@ -187,7 +188,9 @@ void olpt_ctx_destroy(olpt_ctx* ctx) {
   ctx->sm.release(ctx->stream);
   ctx->obj.release(ctx->stream);
   ctx->shk.release(ctx->stream);
+  ctx->ipr.release(ctx->stream);
   for (int c = 0; c < OLPT_MAX_CAM; ++c) ctx->resid[c].buf.release(ctx->stream);
+  ctx->prof.release();
   cudaStreamSynchronize(ctx->stream);
   if (ctx->own_stream) cudaStreamDestroy(ctx->stream);
   delete ctx;
@@ -197,6 +200,32 @@ const char* olpt_last_error(const olpt_ctx* ctx) { return ctx ? ctx->err.c_str()
 
 olpt_status_t olpt_sync(olpt_ctx* ctx) {
   return guard(ctx, [&] { OLPT_CUDA(cudaStreamSynchronize(ctx->stream)); });
+}
+
+olpt_status_t olpt_stream(olpt_ctx* ctx, void** stream) {
+  return guard(ctx, [&] {
+    OLPT_REQUIRE(stream, OLPT_ERR_INVALID_ARG, "null output");
+    *stream = (void*)ctx->stream;
+  });
+}
+
+int64_t olpt_launch_count(void) { return (int64_t)g_launches.load(); }
+
+olpt_status_t olpt_profile(olpt_ctx* ctx, int enable) {
+  return guard(ctx, [&] { ctx->prof.on = enable != 0; });
+}
+
+olpt_status_t olpt_profile_read(olpt_ctx* ctx, int kernel, double* total_ms, int64_t* launches,
+                                double* bytes) {
+  return guard(ctx, [&] {
+    OLPT_REQUIRE(kernel >= 0 && kernel < PROF_N, OLPT_ERR_INVALID_ARG, "bad kernel id");
+    double ms, b;
+    long long n;
+    ctx->prof.read(kernel, ms, n, b);
+    if (total_ms) *total_ms = ms;
+    if (launches) *launches = n;
+    if (bytes) *bytes = b;
+  });
 }
 
 olpt_status_t olpt_cameras_upload(olpt_ctx* ctx, const olpt_camera_desc* cams, int n_cam) {
@@ -320,7 +349,7 @@ olpt_status_t olpt_camera_project(olpt_ctx* ctx, int cam, int64_t n, const doubl
     double* dx = ctx->scratch.as<double>();
     double* du = dx + 3 * n;
     OLPT_CUDA(cudaMemcpyAsync(dx, xyz, n * 3 * sizeof(double), cudaMemcpyHostToDevice, ctx->stream));
-    project_kernel<<<nblk(n), 256, 0, ctx->stream>>>(ctx->cams_d.as<CamDev>(), cam, n, dx, du);
+    project_kernel<<<OLPT_G(nblk(n)), 256, 0, ctx->stream>>>(ctx->cams_d.as<CamDev>(), cam, n, dx, du);
     OLPT_CUDA(cudaGetLastError());
     OLPT_CUDA(cudaMemcpyAsync(uv, du, n * 2 * sizeof(double), cudaMemcpyDeviceToHost, ctx->stream));
     OLPT_CUDA(cudaStreamSynchronize(ctx->stream));
@@ -337,7 +366,7 @@ olpt_status_t olpt_camera_los(olpt_ctx* ctx, int cam, int64_t n, const double* u
     double* du = ctx->scratch.as<double>();
     double* dl = du + 2 * n;
     OLPT_CUDA(cudaMemcpyAsync(du, uv, n * 2 * sizeof(double), cudaMemcpyHostToDevice, ctx->stream));
-    los_kernel<<<nblk(n), 256, 0, ctx->stream>>>(ctx->cams_d.as<CamDev>(), cam, n, du, dl);
+    los_kernel<<<OLPT_G(nblk(n)), 256, 0, ctx->stream>>>(ctx->cams_d.as<CamDev>(), cam, n, du, dl);
     OLPT_CUDA(cudaGetLastError());
     OLPT_CUDA(cudaMemcpyAsync(line6, dl, n * 6 * sizeof(double), cudaMemcpyDeviceToHost, ctx->stream));
     OLPT_CUDA(cudaStreamSynchronize(ctx->stream));
@@ -357,7 +386,7 @@ olpt_status_t olpt_triangulate(olpt_ctx* ctx, int64_t n_sets, int k, const doubl
     double* dout = dl + n_sets * k * 6;
     int* dok = reinterpret_cast<int*>(dout + n_sets * 4);
     OLPT_CUDA(cudaMemcpyAsync(dl, lines6, in_b, cudaMemcpyHostToDevice, ctx->stream));
-    triangulate_kernel<<<nblk(n_sets, 128), 128, 0, ctx->stream>>>(n_sets, k, dl, dout, dok);
+    triangulate_kernel<<<OLPT_G(nblk(n_sets, 128)), 128, 0, ctx->stream>>>(n_sets, k, dl, dout, dok);
     OLPT_CUDA(cudaGetLastError());
     OLPT_CUDA(cudaMemcpyAsync(out4, dout, out_b, cudaMemcpyDeviceToHost, ctx->stream));
     OLPT_CUDA(cudaMemcpyAsync(ok, dok, n_sets * sizeof(int), cudaMemcpyDeviceToHost, ctx->stream));
@@ -402,7 +431,7 @@ olpt_status_t olpt_otf_param(olpt_ctx* ctx, int cam, int64_t n, const double* xy
     double* dx = ctx->scratch.as<double>();
     double* dout = dx + 3 * n;
     OLPT_CUDA(cudaMemcpyAsync(dx, xyz, n * 3 * sizeof(double), cudaMemcpyHostToDevice, ctx->stream));
-    otf_param_kernel<<<nblk(n), 256, 0, ctx->stream>>>(v, cam, n, dx, dout);
+    otf_param_kernel<<<OLPT_G(nblk(n)), 256, 0, ctx->stream>>>(v, cam, n, dx, dout);
     OLPT_CUDA(cudaGetLastError());
     OLPT_CUDA(cudaMemcpyAsync(out5, dout, n * 5 * sizeof(double), cudaMemcpyDeviceToHost, ctx->stream));
     OLPT_CUDA(cudaStreamSynchronize(ctx->stream));
@@ -438,10 +467,10 @@ olpt_status_t olpt_image_download(olpt_ctx* ctx, int cam, olpt_dtype_t dtype, vo
     const int64_t n = (int64_t)im.H * im.W;
     ctx->scratch.ensure(n * 8, ctx->stream);
     if (dtype == OLPT_F32)
-      convert_plane_kernel<float><<<nblk(n), 256, 0, ctx->stream>>>(
+      convert_plane_kernel<float><<<OLPT_G(nblk(n)), 256, 0, ctx->stream>>>(
           im.buf.as<unsigned char>(), im.pitch, im.H, im.W, im.dtype, ctx->scratch.as<float>());
     else
-      convert_plane_kernel<double><<<nblk(n), 256, 0, ctx->stream>>>(
+      convert_plane_kernel<double><<<OLPT_G(nblk(n)), 256, 0, ctx->stream>>>(
           im.buf.as<unsigned char>(), im.pitch, im.H, im.W, im.dtype, ctx->scratch.as<double>());
     OLPT_CUDA(cudaGetLastError());
     OLPT_CUDA(cudaMemcpyAsync(out, ctx->scratch.p, n * esize(dtype), cudaMemcpyDeviceToHost,
@@ -614,7 +643,7 @@ olpt_status_t olpt_objects_upload(olpt_ctx* ctx, int64_t n, const double* xyz) {
     if (n > 0) {
       OLPT_CUDA(cudaMemcpyAsync(ctx->obj.xyz.p, xyz, n * 3 * sizeof(double), cudaMemcpyHostToDevice,
                                 ctx->stream));
-      init_objects_kernel<<<nblk(n), 256, 0, ctx->stream>>>(ctx->obj.flags.as<uint8_t>(),
+      init_objects_kernel<<<OLPT_G(nblk(n)), 256, 0, ctx->stream>>>(ctx->obj.flags.as<uint8_t>(),
                                                              ctx->obj.score.as<double>(), n);
       OLPT_CUDA(cudaGetLastError());
     }
@@ -663,6 +692,42 @@ olpt_status_t olpt_residual(olpt_ctx* ctx, const olpt_shake_params* p, int use_f
   });
 }
 
+olpt_status_t olpt_ipr_run(olpt_ctx* ctx, const olpt_ipr_params* p, int64_t* n_objects) {
+  return guard(ctx, [&] {
+    OLPT_REQUIRE(p, OLPT_ERR_INVALID_ARG, "null params");
+    OLPT_REQUIRE(p->shake.precision == 0 || p->shake.precision == 1, OLPT_ERR_INVALID_ARG,
+                 "precision must be 0 (FP32) or 1 (FP64)");
+    IprParams ip;
+    ip.min_obj_int = p->min_obj_int;
+    ip.sm.match_cam_count = p->sm.match_cam_count;
+    ip.sm.idmap_cell_px = p->sm.idmap_cell_px;
+    ip.sm.tol_2d_px = p->sm.tol_2d_px;
+    ip.sm.tol_3d_mm = p->sm.tol_3d_mm;
+    for (int q = 0; q < 6; ++q) ip.sm.limit[q] = p->sm.limit[q];
+    ip.shake = to_shake_params(&p->shake);
+    ip.n_cam_reduced = p->n_cam_reduced;
+    ip.n_loop_ipr = p->n_loop_ipr;
+    ip.n_loop_ipr_reduced = p->n_loop_ipr_reduced;
+    ip.n_obj2d_process_max = p->n_obj2d_process_max;
+    ipr_device(ctx, ip);
+    if (n_objects) *n_objects = ctx->ipr.n_out;
+  });
+}
+
+olpt_status_t olpt_ipr_result(olpt_ctx* ctx, double* xyz, double* uv) {
+  return guard(ctx, [&] {
+    const int64_t n = ctx->ipr.n_out;
+    if (n <= 0) return;
+    if (xyz)
+      OLPT_CUDA(cudaMemcpyAsync(xyz, ctx->ipr.out_xyz.p, n * 3 * sizeof(double),
+                                cudaMemcpyDeviceToHost, ctx->stream));
+    if (uv)
+      OLPT_CUDA(cudaMemcpyAsync(uv, ctx->ipr.out_uv.p, n * ctx->n_cam * 2 * sizeof(double),
+                                cudaMemcpyDeviceToHost, ctx->stream));
+    OLPT_CUDA(cudaStreamSynchronize(ctx->stream));
+  });
+}
+
 olpt_status_t olpt_residual_download(olpt_ctx* ctx, int cam, olpt_dtype_t dtype, void* out) {
   return guard(ctx, [&] {
     OLPT_REQUIRE(cam >= 0 && cam < ctx->n_cam && out, OLPT_ERR_INVALID_ARG, "bad camera/buffer");
@@ -673,10 +738,10 @@ olpt_status_t olpt_residual_download(olpt_ctx* ctx, int cam, olpt_dtype_t dtype,
     const int64_t n = (int64_t)im.H * im.W;
     ctx->scratch.ensure(n * 8, ctx->stream);
     if (dtype == OLPT_F32)
-      convert_plane_kernel<float><<<nblk(n), 256, 0, ctx->stream>>>(
+      convert_plane_kernel<float><<<OLPT_G(nblk(n)), 256, 0, ctx->stream>>>(
           im.buf.as<unsigned char>(), im.pitch, im.H, im.W, im.dtype, ctx->scratch.as<float>());
     else
-      convert_plane_kernel<double><<<nblk(n), 256, 0, ctx->stream>>>(
+      convert_plane_kernel<double><<<OLPT_G(nblk(n)), 256, 0, ctx->stream>>>(
           im.buf.as<unsigned char>(), im.pitch, im.H, im.W, im.dtype, ctx->scratch.as<double>());
     OLPT_CUDA(cudaGetLastError());
     OLPT_CUDA(cudaMemcpyAsync(out, ctx->scratch.p, n * esize(dtype), cudaMemcpyDeviceToHost,

@@ -2,6 +2,7 @@
 #pragma once
 #include <cuda_runtime.h>
 
+#include <atomic>
 #include <cstdint>
 #include <cstring>
 #include <string>
@@ -9,9 +10,16 @@
 
 #include "../../include/olpt.h"
 #include "olpt_device.cuh"
+#include "olpt_prof.h"
+#include "olpt_shake.h"
 #include "olpt_stereo.h"
 
 namespace olpt {
+
+// Number of kernel launches issued by this library (every launch site wraps its
+// grid expression in OLPT_G, which is evaluated exactly once per launch).
+extern std::atomic<long long> g_launches;
+#define OLPT_G(grid) (::olpt::g_launches.fetch_add(1, std::memory_order_relaxed), (grid))
 
 struct CudaError {
   cudaError_t code;
@@ -178,9 +186,36 @@ struct Objects {
   }
 };
 
+// IPR knobs (IPRParam + tracer threshold, inc/libSTB/Config.h:37-44, 190-195).
+struct IprParams {
+  double min_obj_int;
+  SmParams sm;
+  ShakeParams shake;
+  int n_cam_reduced, n_loop_ipr, n_loop_ipr_reduced;
+  int64_t n_obj2d_process_max;
+};
+
+// IPR workspace and the accumulated output objects of the last run.
+struct IprWork {
+  DevBuf perm, tx, ty, trc, keep, pos, scan_tmp;
+  DevBuf out_xyz, out_uv;
+  int64_t n_out = 0, cap_out = 0;
+  void release(cudaStream_t s) {
+    perm.release(s);
+    tx.release(s);
+    ty.release(s);
+    trc.release(s);
+    keep.release(s);
+    pos.release(s);
+    scan_tmp.release(s);
+    out_xyz.release(s);
+    out_uv.release(s);
+    n_out = cap_out = 0;
+  }
+};
+
 void stereo_match_device(olpt_ctx* ctx, const SmParams& prm, StereoResult& res);
-struct OtfView;
-struct ShakeParams;
+void ipr_device(olpt_ctx* ctx, const IprParams& p);
 OtfView otf_view(olpt_ctx* ctx);
 void shake_device(olpt_ctx* ctx, const ShakeParams& sp);
 void residual_device(olpt_ctx* ctx, const ShakeParams& sp, bool use_flags, bool make_current);
@@ -219,6 +254,12 @@ struct olpt_ctx {
   // shake: residual planes (FP32 or FP64) and workspace
   olpt::ImagePlane resid[OLPT_MAX_CAM];
   olpt::ShakeWork shk;
+
+  // IPR workspace and output
+  olpt::IprWork ipr;
+
+  // optional per-kernel event timing
+  olpt::Prof prof;
 
   // scratch
   olpt::DevBuf scratch;

@@ -1,0 +1,80 @@
+// Optional per-kernel timing: when enabled, launches of the named kernel classes are
+// bracketed by CUDA events recorded on the context's stream (no extra
+// synchronisation); olpt_profile_read sums the durations after a sync.  The
+// algorithmic bytes of every timed launch are accumulated alongside.
+#pragma once
+#include <cuda_runtime.h>
+
+#include <vector>
+
+namespace olpt {
+
+enum ProfKernel : int {
+  PROF_PEAKS = 0,     // detection, count + emit passes
+  PROF_STEREO = 1,    // stereo level expansion (all levels)
+  PROF_RESIDUAL = 2,  // tile-owned residual image
+  PROF_SHAKE = 3,     // warp-per-particle shake
+  PROF_N = 4
+};
+
+struct Prof {
+  bool on = false;
+  struct Rec {
+    cudaEvent_t a, b;
+    double bytes;
+  };
+  std::vector<Rec> open[PROF_N];
+  std::vector<cudaEvent_t> pool;
+
+  cudaEvent_t get() {
+    if (!pool.empty()) {
+      cudaEvent_t e = pool.back();
+      pool.pop_back();
+      return e;
+    }
+    cudaEvent_t e;
+    cudaEventCreate(&e);
+    return e;
+  }
+  // begin/end bracket one launch (or one group of launches) on stream s
+  int begin(int k, cudaStream_t s) {
+    if (!on) return -1;
+    Rec r{get(), get(), 0.0};
+    cudaEventRecord(r.a, s);
+    open[k].push_back(r);
+    return (int)open[k].size() - 1;
+  }
+  void end(int k, int id, cudaStream_t s, double bytes) {
+    if (id < 0) return;
+    open[k][id].bytes = bytes;
+    cudaEventRecord(open[k][id].b, s);
+  }
+  // sum of durations (ms), launches and bytes; recycles the events
+  void read(int k, double& ms, long long& n, double& bytes) {
+    ms = 0;
+    n = 0;
+    bytes = 0;
+    for (auto& r : open[k]) {
+      float t = 0;
+      cudaEventSynchronize(r.b);
+      cudaEventElapsedTime(&t, r.a, r.b);
+      ms += t;
+      bytes += r.bytes;
+      ++n;
+      pool.push_back(r.a);
+      pool.push_back(r.b);
+    }
+    open[k].clear();
+  }
+  void release() {
+    for (auto& v : open)
+      for (auto& r : v) {
+        cudaEventDestroy(r.a);
+        cudaEventDestroy(r.b);
+      }
+    for (auto e : pool) cudaEventDestroy(e);
+    pool.clear();
+  }
+};
+
+}  // namespace olpt

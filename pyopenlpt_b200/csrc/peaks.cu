@@ -276,13 +276,13 @@ __global__ void band_scan_kernel(const PeakArgs a, int64_t* band_offsets, int64_
 template <typename T>
 void launch_peaks(const PeakArgs& a, int n_blocks, int64_t* band_offsets, int64_t* totals,
                   cudaStream_t s) {
-  peaks_kernel<T, false><<<n_blocks, kPeakThreads, 0, s>>>(a);
+  peaks_kernel<T, false><<<OLPT_G(n_blocks), kPeakThreads, 0, s>>>(a);
   OLPT_CUDA(cudaGetLastError());
-  band_scan_kernel<<<a.n_cam, 256, 0, s>>>(a, band_offsets, totals);
+  band_scan_kernel<<<OLPT_G(a.n_cam), 256, 0, s>>>(a, band_offsets, totals);
   OLPT_CUDA(cudaGetLastError());
   PeakArgs b = a;
   b.band_offsets = band_offsets;
-  peaks_kernel<T, true><<<n_blocks, kPeakThreads, 0, s>>>(b);
+  peaks_kernel<T, true><<<OLPT_G(n_blocks), kPeakThreads, 0, s>>>(b);
   OLPT_CUDA(cudaGetLastError());
 }
 
@@ -354,6 +354,12 @@ void find_peaks_device(olpt_ctx* ctx, double min_int, bool sync_counts) {
   a.band_counts = ctx->band_counts.as<int>();
   int64_t* offs = ctx->band_offsets.as<int64_t>();
   int64_t* tot = ctx->det_counts.as<int64_t>();
+  double img_bytes = 0;
+  for (int c = 0; c < ctx->n_cam; ++c)
+    if (a.cam[c].active)
+      img_bytes += (double)a.cam[c].H * a.cam[c].W *
+                   (dtype == OLPT_U8 ? 1 : dtype == OLPT_U16 ? 2 : dtype == OLPT_F32 ? 4 : 8);
+  const int pid = ctx->prof.begin(PROF_PEAKS, ctx->stream);
   switch (dtype) {
     case OLPT_U8:
       a.lut = ctx->lut_u8.as<double>();
@@ -370,6 +376,7 @@ void find_peaks_device(olpt_ctx* ctx, double min_int, bool sync_counts) {
       launch_peaks<double>(a, blocks, offs, tot, ctx->stream);
       break;
   }
+  ctx->prof.end(PROF_PEAKS, pid, ctx->stream, img_bytes);
   ctx->det_counts_h.assign(ctx->n_cam, 0);
   if (sync_counts) {
     OLPT_CUDA(cudaMemcpyAsync(ctx->det_counts_h.data(), tot, ctx->n_cam * sizeof(int64_t),

@@ -82,9 +82,9 @@ void exclusive_scan(const int* in, int n, int* out, DevBuf& tmp, cudaStream_t s)
   OLPT_REQUIRE(n_tiles <= kScanTile, OLPT_ERR_UNSUPPORTED, "scan longer than 16M entries");
   tmp.ensure((n_tiles + 1) * sizeof(int), s);
   if (n > 0) {
-    scan_tiles_kernel<<<n_tiles, kScanThreads, 0, s>>>(in, n, out, tmp.as<int>());
-    scan_sums_kernel<<<1, 1024, 0, s>>>(tmp.as<int>(), n_tiles);
-    scan_add_kernel<<<(n + 255) / 256, 256, 0, s>>>(out, n, tmp.as<int>(), n_tiles);
+    scan_tiles_kernel<<<OLPT_G(n_tiles), kScanThreads, 0, s>>>(in, n, out, tmp.as<int>());
+    scan_sums_kernel<<<OLPT_G(1), 1024, 0, s>>>(tmp.as<int>(), n_tiles);
+    scan_add_kernel<<<OLPT_G((n + 255) / 256), 256, 0, s>>>(out, n, tmp.as<int>(), n_tiles);
   } else {
     OLPT_CUDA(cudaMemsetAsync(out, 0, sizeof(int), s));
   }
@@ -133,13 +133,13 @@ void Csr::build(const int* key, int n, int n_buckets, cudaStream_t s) {
     cursor.ensure((n_buckets + 1) * sizeof(int), s);
     items.ensure((n + 1) * sizeof(int), s);
     OLPT_CUDA(cudaMemsetAsync(cursor.p, 0, n_buckets * sizeof(int), s));
-    if (n > 0) csr_count_kernel<<<(n + 255) / 256, 256, 0, s>>>(key, n, cursor.as<int>());
+    if (n > 0) csr_count_kernel<<<OLPT_G((n + 255) / 256), 256, 0, s>>>(key, n, cursor.as<int>());
     exclusive_scan(cursor.as<int>(), n_buckets, start.as<int>(), tmp, s);
     OLPT_CUDA(cudaMemsetAsync(cursor.p, 0, n_buckets * sizeof(int), s));
     if (n > 0) {
-      csr_scatter_kernel<<<(n + 255) / 256, 256, 0, s>>>(key, n, start.as<int>(), cursor.as<int>(),
+      csr_scatter_kernel<<<OLPT_G((n + 255) / 256), 256, 0, s>>>(key, n, start.as<int>(), cursor.as<int>(),
                                                          items.as<int>());
-      csr_sort_kernel<<<(n_buckets + 255) / 256, 256, 0, s>>>(start.as<int>(), n_buckets,
+      csr_sort_kernel<<<OLPT_G((n_buckets + 255) / 256), 256, 0, s>>>(start.as<int>(), n_buckets,
                                                               items.as<int>());
     }
     OLPT_CUDA(cudaGetLastError());

@@ -771,14 +771,24 @@ static void residual_pass(olpt_ctx* ctx, ShakeView& v, const uint8_t* flags, int
   W.otfp.ensure((n * C + 1) * 5 * sizeof(Real), s);
   W.pair_key.ensure((n * C + 1) * sizeof(int), s);
   if (n > 0)
-    prep_kernel<Real><<<nblk(n, 128), 128, 0, s>>>(v, ctx->obj.xyz.as<double>(), n,
+    prep_kernel<Real><<<OLPT_G(nblk(n, 128)), 128, 0, s>>>(v, ctx->obj.xyz.as<double>(), n,
                                                    ctx->obj.uv.as<double>(), W.otfp.as<Real>(),
                                                    W.pair_key.as<int>(), flags, all_cams);
   OLPT_CUDA(cudaGetLastError());
   W.bins.build(W.pair_key.as<int>(), (int)(n * C), v.n_tiles, s);
-  residual_kernel<Real><<<v.n_tiles, 256, 0, s>>>(v, ctx->obj.uv.as<double>(), W.otfp.as<Real>(),
+  // algorithmic bytes: read the image, write the residual, for every computed camera
+  double bytes = 0;
+  for (int c = 0; c < C; ++c) {
+    if (!(all_cams || ctx->cams_h[c].is_active)) continue;
+    const int d = v.orig[c].dtype;
+    const int esz = d == OLPT_U8 ? 1 : d == OLPT_U16 ? 2 : d == OLPT_F32 ? 4 : 8;
+    bytes += (double)v.orig[c].H * v.orig[c].W * (esz + sizeof(Real));
+  }
+  const int pid = ctx->prof.begin(PROF_RESIDUAL, s);
+  residual_kernel<Real><<<OLPT_G(v.n_tiles), 256, 0, s>>>(v, ctx->obj.uv.as<double>(), W.otfp.as<Real>(),
                                                   W.bins.start.as<int>(), W.bins.items.as<int>(),
                                                   clamp, all_cams);
+  ctx->prof.end(PROF_RESIDUAL, pid, s, bytes);
   OLPT_CUDA(cudaGetLastError());
 }
 
@@ -792,7 +802,7 @@ static void shake_impl(olpt_ctx* ctx, const ShakeParams& sp) {
   const int C = ctx->n_cam;
   ShakeWork& W = ctx->shk;
   ctx->obj.ensure(std::max<int64_t>(n, 1), C, s);
-  if (n > 0) fill_kernel<<<nblk(n), 256, 0, s>>>(ctx->obj.score.as<double>(), n, 1.0);
+  if (n > 0) fill_kernel<<<OLPT_G(nblk(n)), 256, 0, s>>>(ctx->obj.score.as<double>(), n, 1.0);
   double delta = sp.shake_width;
   double dmin = sp.shakewidth_min;
   dmin = (dmin > 0) ? dmin : delta / 20;
@@ -802,10 +812,18 @@ static void shake_impl(olpt_ctx* ctx, const ShakeParams& sp) {
                                  (int)smem));
   for (int it = 0; it < sp.n_shake_loop; ++it) {
     residual_pass<Real>(ctx, v, nullptr, 0, 0);
+    // algorithmic bytes: the augmented ROI of every active camera plus the object
+    // state (xyz, projections, OTF parameters, score) read and written once
+    int n_act = 0;
+    for (int c = 0; c < C; ++c) n_act += ctx->cams_h[c].is_active;
+    const double bytes = (double)n * (n_act * v.roi_area * (double)sizeof(Real) +
+                                      2.0 * (3 * 8 + C * 2 * 8 + 8) + C * 5.0 * sizeof(Real));
+    const int pid = ctx->prof.begin(PROF_SHAKE, s);
     if (n > 0)
-      shake_kernel<Real><<<nblk(n, warps_per_blk), 32 * warps_per_blk, smem, s>>>(
+      shake_kernel<Real><<<OLPT_G(nblk(n, warps_per_blk)), 32 * warps_per_blk, smem, s>>>(
           v, n, ctx->obj.xyz.as<double>(), ctx->obj.uv.as<double>(), W.otfp.as<Real>(),
           ctx->obj.score.as<double>(), delta);
+    ctx->prof.end(PROF_SHAKE, pid, s, bytes);
     OLPT_CUDA(cudaGetLastError());
     delta *= 0.5;
     if (delta < dmin) delta = dmin;
@@ -818,17 +836,17 @@ static void shake_impl(olpt_ctx* ctx, const ShakeParams& sp) {
     const int nb = (int)std::max<int64_t>(1024, 2 * n);
     W.hkey.ensure((n + 1) * sizeof(int), s);
     W.has_nb.ensure((n + 1) * sizeof(int), s);
-    hash_key_kernel<<<nblk(n), 256, 0, s>>>(ctx->obj.xyz.as<double>(), (int)n, cell, nb,
+    hash_key_kernel<<<OLPT_G(nblk(n)), 256, 0, s>>>(ctx->obj.xyz.as<double>(), (int)n, cell, nb,
                                              W.hkey.as<int>());
     W.hash.build(W.hkey.as<int>(), (int)n, nb, s);
     const double r2 = sp.tol_3d_mm * sp.tol_3d_mm;
-    neighbour_kernel<<<nblk(n), 256, 0, s>>>(ctx->obj.xyz.as<double>(), (int)n, cell, nb,
+    neighbour_kernel<<<OLPT_G(nblk(n)), 256, 0, s>>>(ctx->obj.xyz.as<double>(), (int)n, cell, nb,
                                               W.hash.start.as<int>(), W.hash.items.as<int>(), r2,
                                               W.has_nb.as<int>());
-    repeat_greedy_kernel<<<1, 32, 0, s>>>(ctx->obj.xyz.as<double>(), (int)n, cell, nb,
+    repeat_greedy_kernel<<<OLPT_G(1), 32, 0, s>>>(ctx->obj.xyz.as<double>(), (int)n, cell, nb,
                                           W.hash.start.as<int>(), W.hash.items.as<int>(), r2,
                                           W.has_nb.as<int>(), W.rep.as<uint8_t>());
-    ghost_kernel<<<1, 1024, 0, s>>>(ctx->obj.score.as<double>(), W.rep.as<uint8_t>(), (int)n,
+    ghost_kernel<<<OLPT_G(1), 1024, 0, s>>>(ctx->obj.score.as<double>(), W.rep.as<uint8_t>(), (int)n,
                                     sp.thred_ghost, ctx->obj.flags.as<uint8_t>());
     OLPT_CUDA(cudaGetLastError());
   }

@@ -527,15 +527,15 @@ void stereo_match_device(olpt_ctx* ctx, const SmParams& prm, StereoResult& res) 
     W.los[c].ensure((n + 1) * 6 * sizeof(double), s);
     OLPT_CUDA(cudaMemsetAsync(W.cell_cursor[c].p, 0, ncell * sizeof(int), s));
     if (n > 0) {
-      cell_hist_kernel<<<nblk(n), 256, 0, s>>>(v.x[c], v.y[c], n, v.cell, rows, cols,
+      cell_hist_kernel<<<OLPT_G(nblk(n)), 256, 0, s>>>(v.x[c], v.y[c], n, v.cell, rows, cols,
                                                 W.cell_of[c].as<int>(), W.cell_cursor[c].as<int>());
     }
-    cell_scan_kernel<<<1, 1024, 0, s>>>(W.cell_cursor[c].as<int>(), ncell, W.cell_start[c].as<int>());
+    cell_scan_kernel<<<OLPT_G(1), 1024, 0, s>>>(W.cell_cursor[c].as<int>(), ncell, W.cell_start[c].as<int>());
     OLPT_CUDA(cudaMemsetAsync(W.cell_cursor[c].p, 0, ncell * sizeof(int), s));
     if (n > 0) {
-      cell_scatter_kernel<<<nblk(n), 256, 0, s>>>(W.cell_of[c].as<int>(), n, W.cell_start[c].as<int>(),
+      cell_scatter_kernel<<<OLPT_G(nblk(n)), 256, 0, s>>>(W.cell_of[c].as<int>(), n, W.cell_start[c].as<int>(),
                                                    W.cell_cursor[c].as<int>(), W.cell_items[c].as<int>());
-      cell_sort_kernel<<<nblk(ncell), 256, 0, s>>>(W.cell_start[c].as<int>(), ncell,
+      cell_sort_kernel<<<OLPT_G(nblk(ncell)), 256, 0, s>>>(W.cell_start[c].as<int>(), ncell,
                                                     W.cell_items[c].as<int>());
     }
     OLPT_CUDA(cudaGetLastError());
@@ -564,7 +564,7 @@ void stereo_match_device(olpt_ctx* ctx, const SmParams& prm, StereoResult& res) 
                               cudaMemcpyHostToDevice, s));
     for (int c = 0; c < n_cam; ++c) {
       if (!v.active[c] || v.n[c] == 0) continue;
-      lines_kernel<<<nblk(v.n[c], 128), 128, 0, s>>>(
+      lines_kernel<<<OLPT_G(nblk(v.n[c], 128)), 128, 0, s>>>(
           ctx->cams_d.as<CamDev>(), c, v.x[c], v.y[c], v.n[c], n_cam, W.active_d.as<int>(),
           W.los[c].as<double>(), W.l2d_ptrs.as<double*>() + c * OLPT_MAX_CAM);
       OLPT_CUDA(cudaGetLastError());
@@ -584,7 +584,7 @@ void stereo_match_device(olpt_ctx* ctx, const SmParams& prm, StereoResult& res) 
   int cap_a = (int)std::max<int64_t>(n_ref, 1024);
   W.path_a.ensure(cap_a * sizeof(Path), s);
   OLPT_CUDA(cudaMemsetAsync(cnt, 0, 4 * sizeof(int), s));
-  if (n_ref > 0) seed_kernel<<<nblk(n_ref), 256, 0, s>>>(v, ref, W.path_a.as<Path>(), cnt, cap_a);
+  if (n_ref > 0) seed_kernel<<<OLPT_G(nblk(n_ref)), 256, 0, s>>>(v, ref, W.path_a.as<Path>(), cnt, cap_a);
   OLPT_CUDA(cudaGetLastError());
   int n_in = read_count(0);
   int term_cap = (int)std::max<int64_t>(4 * n_ref, 4096);
@@ -601,9 +601,11 @@ void stereo_match_device(olpt_ctx* ctx, const SmParams& prm, StereoResult& res) 
       OLPT_CUDA(cudaMemsetAsync(cnt + 1, 0, sizeof(int), s));
       OLPT_CUDA(cudaMemcpyAsync(cnt + 2, &n_term, sizeof(int), cudaMemcpyHostToDevice, s));
       const int64_t threads = (int64_t)n_in * 32;
-      level_kernel<<<nblk(threads), 256, 0, s>>>(v, in_buf->as<Path>(), n_in, out_buf->as<Path>(),
+      const int pid = ctx->prof.begin(PROF_STEREO, s);
+      level_kernel<<<OLPT_G(nblk(threads)), 256, 0, s>>>(v, in_buf->as<Path>(), n_in, out_buf->as<Path>(),
                                                  cnt + 1, out_cap, W.term.as<Path>(), cnt + 2,
                                                  term_cap);
+      ctx->prof.end(PROF_STEREO, pid, s, 0.0);
       OLPT_CUDA(cudaGetLastError());
       int h[2];
       OLPT_CUDA(cudaMemcpyAsync(h, cnt + 1, 2 * sizeof(int), cudaMemcpyDeviceToHost, s));
@@ -628,7 +630,7 @@ void stereo_match_device(olpt_ctx* ctx, const SmParams& prm, StereoResult& res) 
   W.cand_x.ensure((size_t)cap_c * 3 * sizeof(double), s);
   OLPT_CUDA(cudaMemsetAsync(cnt + 3, 0, sizeof(int), s));
   if (n_term > 0)
-    check_kernel<<<nblk(n_term, 128), 128, 0, s>>>(v, W.term.as<Path>(), n_term, W.cand_ids.as<int>(),
+    check_kernel<<<OLPT_G(nblk(n_term, 128)), 128, 0, s>>>(v, W.term.as<Path>(), n_term, W.cand_ids.as<int>(),
                                               W.cand_e.as<double>(), W.cand_x.as<double>(), cnt + 3,
                                               cap_c);
   OLPT_CUDA(cudaGetLastError());

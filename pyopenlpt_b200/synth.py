@@ -152,6 +152,14 @@ def make_scene(n_particles: int = 10000, n_cam: int = 4, size: int = 1024, focal
     return Scene(cams, xyz, images, tuple(volume), (a, b, c), max_val)
 
 
+def otf_table_array(n_cam: int, abc, alpha: float = 0.0, n=(2, 2, 2)) -> np.ndarray:
+    """Uniform OTF table [4][n_cam][nx*ny*nz] (a, b, c, alpha planes)."""
+    ng = n[0] * n[1] * n[2]
+    t = np.empty((4, n_cam, ng), dtype=np.float64)
+    t[0], t[1], t[2], t[3] = abc[0], abc[1], abc[2], alpha
+    return t
+
+
 def otf_text(n_cam: int, volume, a: float, b: float, c: float, alpha: float = 0.0,
              nx: int = 2, ny: int = 2, nz: int = 2) -> str:
     """Uniform OTF table in the reference's OTF file layout."""
