@@ -250,16 +250,29 @@ __global__ void seed_kernel(const SmView v, int ref, Path* out, int* out_count, 
   out[slot] = p;
 }
 
-// StereoMatch::computeMinParallaxDeg + calTriangulateTol (StereoMatch.cpp:1083-1126)
-__device__ double quick_tol(const Line3* const* L, int k, int m, double tol3d) {
-  double min_deg = 180.0;
-  for (int i = 0; i < k; ++i)
-    for (int j = i + 1; j < k; ++j) {
-      double dot = L[i]->u[0] * L[j]->u[0] + L[i]->u[1] * L[j]->u[1] + L[i]->u[2] * L[j]->u[2];
-      dot = fmax(-1.0, fmin(1.0, dot));
-      const double deg = acos(dot) * 180.0 / M_PI;
-      if (deg < min_deg) min_deg = deg;
-    }
+// (I - n n^T) of one line of sight, in myMATH::triangulation's element order.
+__device__ __forceinline__ void normal_terms(const double u[3], double t[9]) {
+  const double nx = u[0], ny = u[1], nz = u[2];
+  t[0] = 1 - nx * nx;
+  t[1] = -nx * ny;
+  t[2] = -nx * nz;
+  t[3] = -nx * ny;
+  t[4] = 1 - ny * ny;
+  t[5] = -ny * nz;
+  t[6] = -nx * nz;
+  t[7] = -ny * nz;
+  t[8] = 1 - nz * nz;
+}
+
+// Angle in degrees between two unit directions (StereoMatch.cpp:1077-1083).
+__device__ __forceinline__ double pair_deg(const double a[3], const double b[3]) {
+  double dot = a[0] * b[0] + a[1] * b[1] + a[2] * b[2];
+  dot = fmax(-1.0, fmin(1.0, dot));
+  return acos(dot) * 180.0 / M_PI;
+}
+
+// StereoMatch::calTriangulateTol (StereoMatch.cpp:1103-1126) from the min parallax.
+__device__ __forceinline__ double quick_tol_from_deg(double min_deg, int k, int m, double tol3d) {
   const int kk = k > 2 ? k : 2;
   const int mm = m > 2 ? m : 2;
   const double alpha_depth = sqrt(double(mm) / double(kk));
@@ -270,7 +283,28 @@ __device__ double quick_tol(const Line3* const* L, int k, int m, double tol3d) {
   return tol3d * alpha_depth * alpha_angle;
 }
 
-// Expand one level: each warp takes one path and enumerates candidates on its target.
+// One line's contribution to the triangulation error (myMATH.cpp:396-418);
+// false where the reference throws (squared distance below -1e-8).
+__device__ __forceinline__ bool line_error_term(const double X[3], const double p[3],
+                                                const double u[3], double& e) {
+  const double d0 = X[0] - p[0], d1 = X[1] - p[1], d2 = X[2] - p[2];
+  const double nrm = sqrt(d0 * d0 + d1 * d1 + d2 * d2);
+  const double dt = d0 * u[0] + d1 * u[1] + d2 * u[2];
+  double h = nrm * nrm - dt * dt;
+  if (h < 0.0 && h >= -1e-8) {
+    h = 0.0;
+  } else if (h < -1e-8) {
+    return false;
+  } else {
+    h = sqrt(h);
+  }
+  e += h * h;
+  return true;
+}
+
+// Expand one level: each warp takes one path with K chosen cameras and enumerates
+// candidates on its target camera.
+template <int K>
 __global__ void __launch_bounds__(256) level_kernel(const SmView v, const Path* in, int n_in,
                                                     Path* out, int* out_count, int out_cap,
                                                     Path* term, int* term_count, int term_cap) {
@@ -278,11 +312,13 @@ __global__ void __launch_bounds__(256) level_kernel(const SmView v, const Path* 
   const int lane = threadIdx.x & 31;
   if (warp >= n_in) return;
   const Path P = in[warp];
-  const int k = P.k, t = P.target;
+  const int t = P.target;
   // image lines of the chosen points on the target camera
-  double lp[OLPT_MAX_CAM][2], lU[OLPT_MAX_CAM][2];
-  double cpt[OLPT_MAX_CAM][2];
-  for (int i = 0; i < k; ++i) {
+  double lp[K][2], lU[K][2];
+  double cpt[K][2];
+  double cp[K][3], cu[K][3];  // chosen lines of sight (build order)
+#pragma unroll
+  for (int i = 0; i < K; ++i) {
     const int c = P.cams[i];
     const double* L = v.l2d[c][t] + 6 * (int64_t)P.ids[i];
     lp[i][0] = L[0];
@@ -291,7 +327,37 @@ __global__ void __launch_bounds__(256) level_kernel(const SmView v, const Path* 
     lU[i][1] = L[5];
     cpt[i][0] = v.x[c][P.ids[i]];
     cpt[i][1] = v.y[c][P.ids[i]];
+    const double* S = v.los[c] + 6 * (int64_t)P.ids[i];
+#pragma unroll
+    for (int q = 0; q < 3; ++q) {
+      cp[i][q] = S[q];
+      cu[i][q] = S[3 + q];
+    }
   }
+  // Normal equations of the chosen lines, summed in build order: the candidate's
+  // term is added last, which is the reference's summation order
+  // (myMATH::triangulation sums lines in list order, myMATH.cpp:376-391).
+  double Mc[9], bc[3];
+#pragma unroll
+  for (int q = 0; q < 9; ++q) Mc[q] = 0.0;
+  bc[0] = bc[1] = bc[2] = 0.0;
+#pragma unroll
+  for (int i = 0; i < K; ++i) {
+    double tt[9];
+    normal_terms(cu[i], tt);
+#pragma unroll
+    for (int r = 0; r < 3; ++r)
+      bc[r] = bc[r] + (tt[3 * r] * cp[i][0] + tt[3 * r + 1] * cp[i][1] + tt[3 * r + 2] * cp[i][2]);
+#pragma unroll
+    for (int q = 0; q < 9; ++q) Mc[q] = Mc[q] + tt[q];
+  }
+  // minimum parallax among the chosen pairs (min is order-free)
+  double min_deg_c = 180.0;
+#pragma unroll
+  for (int i = 0; i < K; ++i)
+#pragma unroll
+    for (int j = i + 1; j < K; ++j) min_deg_c = fmin(min_deg_c, pair_deg(cu[i], cu[j]));
+
   const int rows = v.rows[t], cols = v.cols[t];
   const double cellp = (double)v.cell;
   const double hw = 0.5 * v.cell, hh = 0.5 * v.cell;
@@ -303,10 +369,42 @@ __global__ void __launch_bounds__(256) level_kernel(const SmView v, const Path* 
   const double* tx = v.x[t];
   const double* ty = v.y[t];
 
-  for (int cy = lane; cy < rows; cy += 32) {
+  // Rows that can hold a non-empty span: with two or more strips, the cell-centre rows
+  // inside the y-extent of the first two strips' intersection parallelogram (plus one
+  // row each side).  Rows outside it have an empty exact span, so skipping them leaves
+  // the visited set unchanged.
+  int row_lo = 0, row_hi = rows - 1;
+  if (K >= 2) {
+    const double n00 = -lU[0][1], n01 = lU[0][0], n10 = -lU[1][1], n11 = lU[1][0];
+    const double d0 = -(n00 * lp[0][0] + n01 * lp[0][1]);
+    const double d1 = -(n10 * lp[1][0] + n11 * lp[1][1]);
+    const double T0 = tol_grow + fabs(n00) * hw + fabs(n01) * hh;
+    const double T1 = tol_grow + fabs(n10) * hw + fabs(n11) * hh;
+    const double det = n00 * n11 - n01 * n10;
+    if (fabs(det) > 1e-9) {
+      double ymin = 1e300, ymax = -1e300;
+#pragma unroll
+      for (int s0 = -1; s0 <= 1; s0 += 2)
+#pragma unroll
+        for (int s1 = -1; s1 <= 1; s1 += 2) {
+          const double y = (n00 * (s1 * T1 - d1) - n10 * (s0 * T0 - d0)) / det;
+          ymin = fmin(ymin, y);
+          ymax = fmax(ymax, y);
+        }
+      if (isfinite(ymin) && isfinite(ymax)) {
+        const double lo = floor(ymin / cellp - 0.5) - 1.0, hi = ceil(ymax / cellp - 0.5) + 1.0;
+        row_lo = (int)fmax(0.0, fmin((double)(rows - 1), lo));
+        row_hi = (int)fmax(-1.0, fmin((double)(rows - 1), hi));
+      }
+    }
+  }
+
+  for (int cy = row_lo + lane; cy <= row_hi; cy += 32) {
     // IDMap::computeStripIntersection, one row
     int xmin = 0, xmax = cols - 1;
-    for (int i = 0; i < k && xmin <= xmax; ++i) {
+#pragma unroll
+    for (int i = 0; i < K; ++i) {
+      if (xmin > xmax) break;
       const double n0 = -lU[i][1], n1 = lU[i][0];
       const double d = -(n0 * lp[i][0] + n1 * lp[i][1]);
       const double y_c = (cy + 0.5) * cellp;
@@ -349,43 +447,68 @@ __global__ void __launch_bounds__(256) level_kernel(const SmView v, const Path* 
         const double qx = tx[pid], qy = ty[pid];
         bool ok = true;
         // IDMap::visitPointsInRowSpans precise test
-        for (int i = 0; i < k; ++i) {
+#pragma unroll
+        for (int i = 0; i < K; ++i) {
           const double dx = qx - lp[i][0], dy = qy - lp[i][1];
           const double z = dy * lU[i][0] - dx * lU[i][1];
-          if (z * z > tol2) {
-            ok = false;
-            break;
-          }
+          ok = ok && !(z * z > tol2);
         }
         if (!ok) continue;
         // checkBackProjection (StereoMatch.cpp:1206-1227)
-        for (int i = 0; i < k; ++i) {
+#pragma unroll
+        for (int i = 0; i < K; ++i) {
+          if (!ok) break;
           const double* L = v.l2d[t][P.cams[i]] + 6 * (int64_t)pid;
           const double d0 = cpt[i][0] - L[0], d1 = cpt[i][1] - L[1];
           const double z = d1 * L[2] - d0 * L[3];
-          if (z * z > tol2) {
-            ok = false;
-            break;
-          }
+          ok = !(z * z > tol2);
         }
         if (!ok) continue;
-        // extend the path; quick triangulation gate
-        Line3 Ls[OLPT_MAX_CAM];
-        const Line3* Lp[OLPT_MAX_CAM];
-        for (int i = 0; i < k; ++i) {
-          load_line3(v.los[P.cams[i]] + 6 * (int64_t)P.ids[i], Ls[i]);
-          Lp[i] = &Ls[i];
+        // extend the path; quick triangulation gate (computeMinParallaxDeg,
+        // calTriangulateTol, TriangulationCheckWithTol: StereoMatch.cpp:1072-1141)
+        double qp[3], qu[3];
+        {
+          const double* S = v.los[t] + 6 * (int64_t)pid;
+          qp[0] = S[0];
+          qp[1] = S[1];
+          qp[2] = S[2];
+          qu[0] = S[3];
+          qu[1] = S[4];
+          qu[2] = S[5];
         }
-        load_line3(v.los[t] + 6 * (int64_t)pid, Ls[k]);
-        Lp[k] = &Ls[k];
-        const int k1 = k + 1;
-        const double tq = quick_tol(Lp, k1, v.m, v.tol3d);
-        double X[3], err;
-        if (!triangulate<OLPT_MAX_CAM>(Lp, k1, X, err)) continue;
+        constexpr int k1 = K + 1;
+        double min_deg = min_deg_c;
+#pragma unroll
+        for (int i = 0; i < K; ++i) min_deg = fmin(min_deg, pair_deg(cu[i], qu));
+        const double tq = quick_tol_from_deg(min_deg, k1, v.m, v.tol3d);
+        double M[9], b[3];
+        {
+          double tt[9];
+          normal_terms(qu, tt);
+#pragma unroll
+          for (int r = 0; r < 3; ++r)
+            b[r] = bc[r] + (tt[3 * r] * qp[0] + tt[3 * r + 1] * qp[1] + tt[3 * r + 2] * qp[2]);
+#pragma unroll
+          for (int q2 = 0; q2 < 9; ++q2) M[q2] = Mc[q2] + tt[q2];
+        }
+        double Mi[9], X[3];
+        gauss_inverse3(M, Mi);
+#pragma unroll
+        for (int r = 0; r < 3; ++r) X[r] = Mi[3 * r] * b[0] + Mi[3 * r + 1] * b[1] + Mi[3 * r + 2] * b[2];
+        double e = 0.0;
+        bool thrown = false;
+#pragma unroll
+        for (int i = 0; i < k1; ++i) {
+          const double* pp = (i < K) ? cp[i] : qp;
+          const double* uu = (i < K) ? cu[i] : qu;
+          thrown |= !line_error_term(X, pp, uu, e);
+        }
+        if (thrown) continue;  // the reference's triangulation throws; the check fails
+        const double err = sqrt(e / k1);
         if (!(err <= tq)) continue;
         Path ch = P;
-        ch.ids[k] = pid;
-        ch.cams[k] = (signed char)t;
+        ch.ids[K] = pid;
+        ch.cams[K] = (signed char)t;
         ch.k = k1;
         if (k1 == v.m) {
           ch.target = -1;
@@ -393,6 +516,7 @@ __global__ void __launch_bounds__(256) level_kernel(const SmView v, const Path* 
           if (slot < term_cap) term[slot] = ch;
           continue;
         }
+        if (k1 >= OLPT_MAX_CAM) continue;
         // StereoMatch::selectNextCameraByMaxPairAngle (StereoMatch.cpp:1375-1411)
         int best = -1;
         double best_score = -1.0;
@@ -602,7 +726,17 @@ void stereo_match_device(olpt_ctx* ctx, const SmParams& prm, StereoResult& res) 
       OLPT_CUDA(cudaMemcpyAsync(cnt + 2, &n_term, sizeof(int), cudaMemcpyHostToDevice, s));
       const int64_t threads = (int64_t)n_in * 32;
       const int pid = ctx->prof.begin(PROF_STEREO, s);
-      level_kernel<<<OLPT_G(nblk(threads)), 256, 0, s>>>(v, in_buf->as<Path>(), n_in, out_buf->as<Path>(),
+      auto kern = level_kernel<1>;
+      switch (level) {
+        case 1: kern = level_kernel<1>; break;
+        case 2: kern = level_kernel<2>; break;
+        case 3: kern = level_kernel<3>; break;
+        case 4: kern = level_kernel<4>; break;
+        case 5: kern = level_kernel<5>; break;
+        case 6: kern = level_kernel<6>; break;
+        default: kern = level_kernel<7>; break;
+      }
+      kern<<<OLPT_G(nblk(threads)), 256, 0, s>>>(v, in_buf->as<Path>(), n_in, out_buf->as<Path>(),
                                                  cnt + 1, out_cap, W.term.as<Path>(), cnt + 2,
                                                  term_cap);
       ctx->prof.end(PROF_STEREO, pid, s, 0.0);
