@@ -63,8 +63,11 @@ olpt_status_t olpt_sync(olpt_ctx* ctx);
 olpt_status_t olpt_stream(olpt_ctx* ctx, void** stream);
 /* Per-kernel event timing (no reference counterpart; the reference prints clock()
  * CPU time per stage).  kernel: 0 = detection, 1 = stereo level expansion,
- * 2 = residual image, 3 = shake.  read returns the summed duration, the number of
- * timed launches and their algorithmic bytes since the last read. */
+ * 2 = residual image, 3 = shake (device time from CUDA events); 4..8 = host
+ * wall-clock phases of olpt_ipr_run (detection, stereo matching, candidate sort +
+ * prune, shake, output compaction + residual).  read returns the summed duration,
+ * the number of timed launches/phases and their algorithmic bytes since the last
+ * read. */
 olpt_status_t olpt_profile(olpt_ctx* ctx, int enable);
 /* Total number of kernel launches issued by this library in this process. */
 int64_t olpt_launch_count(void);
@@ -143,6 +146,11 @@ olpt_status_t olpt_stereo_match(olpt_ctx* ctx, const olpt_sm_params* p, int64_t*
 olpt_status_t olpt_get_candidates(olpt_ctx* ctx, int32_t* ids, double* e_check, double* xyz);
 /* Selected matches of the last match (triangulateMatch output order): ids, xyz. */
 olpt_status_t olpt_get_matches(olpt_ctx* ctx, int32_t* ids, double* xyz);
+/* StereoMatch::pruneMatch (src/srcSTB/StereoMatch.cpp:631-980) on a host candidate list
+ * already in the reference's order (sorted by ids): ids M x n_cam, e_check M,
+ * det_counts/active per camera; selected[j] = 1 for kept candidates.  Host only. */
+olpt_status_t olpt_prune_matches(int n_cam, int64_t M, const int32_t* ids, const double* e_check,
+                                 const int64_t* det_counts, const int* active, uint8_t* selected);
 
 /* ------------------------------------------------------------------ 3D objects */
 /* Replace the context's 3D objects with n tracers at xyz (n x 3); their 2D

@@ -218,10 +218,13 @@ olpt_status_t olpt_profile(olpt_ctx* ctx, int enable) {
 olpt_status_t olpt_profile_read(olpt_ctx* ctx, int kernel, double* total_ms, int64_t* launches,
                                 double* bytes) {
   return guard(ctx, [&] {
-    OLPT_REQUIRE(kernel >= 0 && kernel < PROF_N, OLPT_ERR_INVALID_ARG, "bad kernel id");
-    double ms, b;
+    OLPT_REQUIRE(kernel >= 0 && kernel < PROF_N + PH_N, OLPT_ERR_INVALID_ARG, "bad kernel id");
+    double ms, b = 0;
     long long n;
-    ctx->prof.read(kernel, ms, n, b);
+    if (kernel < PROF_N)
+      ctx->prof.read(kernel, ms, n, b);
+    else
+      ctx->prof.read_phase(kernel - PROF_N, ms, n);
     if (total_ms) *total_ms = ms;
     if (launches) *launches = n;
     if (bytes) *bytes = b;
@@ -587,6 +590,30 @@ olpt_status_t olpt_get_candidates(olpt_ctx* ctx, int32_t* ids, double* e_check, 
     if (xyz) std::copy(r.X.begin(), r.X.end(), xyz);
     (void)M;
   });
+}
+
+olpt_status_t olpt_prune_matches(int n_cam, int64_t M, const int32_t* ids, const double* e_check,
+                                 const int64_t* det_counts, const int* active, uint8_t* selected) {
+  if (n_cam < 1 || n_cam > OLPT_MAX_CAM || M < 0 || (M > 0 && (!ids || !e_check || !selected)) ||
+      !det_counts || !active)
+    return OLPT_ERR_INVALID_ARG;
+  try {
+    StereoResult r;
+    r.n_cam = n_cam;
+    r.ids.assign(ids, ids + M * n_cam);
+    r.e.assign(e_check, e_check + M);
+    r.X.assign(3 * M, 0.0);
+    std::vector<int> counts(n_cam), act(n_cam);
+    for (int c = 0; c < n_cam; ++c) {
+      counts[c] = (int)det_counts[c];
+      act[c] = active[c];
+    }
+    prune_candidates(r, counts, act);
+    for (int64_t j = 0; j < M; ++j) selected[j] = (uint8_t)r.selected[j];
+    return OLPT_OK;
+  } catch (...) {
+    return OLPT_ERR_INTERNAL;
+  }
 }
 
 olpt_status_t olpt_get_matches(olpt_ctx* ctx, int32_t* ids, double* xyz) {

@@ -159,10 +159,16 @@ void append_result(olpt_ctx* ctx) {
 
 // runSingleIPRIteration (IPR.cpp:69-192)
 void single_iteration(olpt_ctx* ctx, const IprParams& p, const SmParams& sm) {
-  find_peaks_device(ctx, p.min_obj_int, true);
-  limit_detections(ctx, p.n_obj2d_process_max);
+  {
+    PhaseTimer pt(ctx->prof, PH_DETECT);
+    find_peaks_device(ctx, p.min_obj_int, true);
+    limit_detections(ctx, p.n_obj2d_process_max);
+  }
   StereoResult& r = ctx->sm_result;
-  stereo_match_device(ctx, sm, r);
+  {
+    PhaseTimer pt(ctx->prof, PH_STEREO);
+    stereo_match_device(ctx, sm, r);
+  }
   std::vector<double> xyz;
   for (size_t j = 0; j < r.e.size(); ++j)
     if (r.selected[j]) xyz.insert(xyz.end(), &r.X[3 * j], &r.X[3 * j] + 3);
@@ -172,9 +178,15 @@ void single_iteration(olpt_ctx* ctx, const IprParams& p, const SmParams& sm) {
   if (n == 0) return;
   OLPT_CUDA(cudaMemcpyAsync(ctx->obj.xyz.p, xyz.data(), xyz.size() * sizeof(double),
                             cudaMemcpyHostToDevice, ctx->stream));
-  shake_device(ctx, p.shake);
+  {
+    PhaseTimer pt(ctx->prof, PH_SHAKE);
+    shake_device(ctx, p.shake);
+    if (ctx->prof.on) OLPT_CUDA(cudaStreamSynchronize(ctx->stream));
+  }
+  PhaseTimer pt(ctx->prof, PH_OUTPUT);
   append_result(ctx);
   residual_device(ctx, p.shake, true, true);  // filtered objects only; becomes the image
+  if (ctx->prof.on) OLPT_CUDA(cudaStreamSynchronize(ctx->stream));
 }
 
 }  // namespace

@@ -109,7 +109,8 @@ struct Dets {
 // built by count -> exclusive scan -> scatter -> per-bucket ascending order (scan.cu).
 struct Csr {
   DevBuf start, items, cursor, tmp;
-  void build(const int* key, int n, int n_buckets, cudaStream_t s);
+  // sort_buckets: ascending item order inside each bucket (only where order matters)
+  void build(const int* key, int n, int n_buckets, cudaStream_t s, bool sort_buckets = false);
   void release(cudaStream_t s) {
     start.release(s);
     items.release(s);
@@ -123,9 +124,12 @@ struct ShakeWork {
   DevBuf otfp;      // n x n_cam x 5 OTF parameters at the object centres
   DevBuf pair_key;  // n x n_cam tile keys
   Csr bins;         // (object, camera) pairs per image tile
-  DevBuf rep, hkey, has_nb;
+  DevBuf rep, hkey, has_nb, nb_pos, nb_list, scan_tmp;
   Csr hash;         // 3D hash grid of object centres
   void release(cudaStream_t s) {
+    nb_pos.release(s);
+    nb_list.release(s);
+    scan_tmp.release(s);
     otfp.release(s);
     pair_key.release(s);
     bins.release(s);
@@ -141,7 +145,7 @@ struct StereoWork {
   DevBuf cell_start[OLPT_MAX_CAM], cell_cursor[OLPT_MAX_CAM], cell_items[OLPT_MAX_CAM];
   DevBuf cell_of[OLPT_MAX_CAM], los[OLPT_MAX_CAM];
   DevBuf l2d[OLPT_MAX_CAM * OLPT_MAX_CAM];
-  DevBuf l2d_ptrs, active_d, counters;
+  DevBuf l2d_ptrs, active_d, counters, scan_tmp;
   DevBuf path_a, path_b, term;
   DevBuf cand_ids, cand_e, cand_x;
   void release(cudaStream_t s) {

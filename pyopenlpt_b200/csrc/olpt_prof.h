@@ -5,6 +5,7 @@
 #pragma once
 #include <cuda_runtime.h>
 
+#include <chrono>
 #include <vector>
 
 namespace olpt {
@@ -17,8 +18,20 @@ enum ProfKernel : int {
   PROF_N = 4
 };
 
+// Host wall-clock phases (ids PROF_N + phase in olpt_profile_read).
+enum ProfPhase : int {
+  PH_DETECT = 0,   // detection incl. count read-back
+  PH_STEREO = 1,   // whole stereo match (device + host)
+  PH_PRUNE = 2,    // host candidate sort + prune
+  PH_SHAKE = 3,    // whole shake (all iterations + flags)
+  PH_OUTPUT = 4,   // compaction of kept objects + final residual
+  PH_N = 5
+};
+
 struct Prof {
   bool on = false;
+  double phase_ms[PH_N] = {0, 0, 0, 0, 0};
+  long long phase_n[PH_N] = {0, 0, 0, 0, 0};
   struct Rec {
     cudaEvent_t a, b;
     double bytes;
@@ -66,6 +79,17 @@ struct Prof {
     }
     open[k].clear();
   }
+  void add_phase(int p, double ms) {
+    if (!on) return;
+    phase_ms[p] += ms;
+    phase_n[p] += 1;
+  }
+  void read_phase(int p, double& ms, long long& n) {
+    ms = phase_ms[p];
+    n = phase_n[p];
+    phase_ms[p] = 0;
+    phase_n[p] = 0;
+  }
   void release() {
     for (auto& v : open)
       for (auto& r : v) {
@@ -74,6 +98,18 @@ struct Prof {
       }
     for (auto e : pool) cudaEventDestroy(e);
     pool.clear();
+  }
+};
+
+// Scope timer for a host phase (wall clock, includes the stream waits it contains).
+struct PhaseTimer {
+  Prof& p;
+  int id;
+  std::chrono::steady_clock::time_point t0;
+  PhaseTimer(Prof& pr, int i) : p(pr), id(i), t0(std::chrono::steady_clock::now()) {}
+  ~PhaseTimer() {
+    p.add_phase(id, std::chrono::duration<double, std::milli>(std::chrono::steady_clock::now() - t0)
+                        .count());
   }
 };
 

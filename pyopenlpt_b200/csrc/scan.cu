@@ -128,7 +128,7 @@ __global__ void csr_count_kernel(const int* key, int n, int* counts) {
 
 }  // namespace
 
-void Csr::build(const int* key, int n, int n_buckets, cudaStream_t s) {
+void Csr::build(const int* key, int n, int n_buckets, cudaStream_t s, bool sort_buckets) {
     start.ensure((n_buckets + 1) * sizeof(int), s);
     cursor.ensure((n_buckets + 1) * sizeof(int), s);
     items.ensure((n + 1) * sizeof(int), s);
@@ -139,8 +139,9 @@ void Csr::build(const int* key, int n, int n_buckets, cudaStream_t s) {
     if (n > 0) {
       csr_scatter_kernel<<<OLPT_G((n + 255) / 256), 256, 0, s>>>(key, n, start.as<int>(), cursor.as<int>(),
                                                          items.as<int>());
-      csr_sort_kernel<<<OLPT_G((n_buckets + 255) / 256), 256, 0, s>>>(start.as<int>(), n_buckets,
-                                                              items.as<int>());
+      if (sort_buckets)
+        csr_sort_kernel<<<OLPT_G((n_buckets + 255) / 256), 256, 0, s>>>(start.as<int>(), n_buckets,
+                                                                items.as<int>());
     }
     OLPT_CUDA(cudaGetLastError());
 }

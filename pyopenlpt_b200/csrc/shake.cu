@@ -639,17 +639,22 @@ __global__ void neighbour_kernel(const double* xyz, int n, double cell, int n_bu
           if (d2 < r2) ++cnt;
         }
       }
-  has_nb[i] = cnt;
+  has_nb[i] = cnt > 0 ? 1 : 0;
 }
 
 // Greedy in index order (Shake.cpp:802-822): an object that is not itself marked
 // marks every neighbour within the radius.  Only objects with neighbours do work.
+// `list` holds, in ascending order, the objects that have any neighbour (list_n[0]
+// of them); objects without neighbours mark nothing, so skipping them keeps the
+// greedy identical.
 __global__ void repeat_greedy_kernel(const double* xyz, int n, double cell, int n_buckets,
                                      const int* start, const int* items, double r2,
-                                     const int* has_nb, uint8_t* rep) {
+                                     const int* list, const int* list_n, uint8_t* rep) {
   if (threadIdx.x != 0 || blockIdx.x != 0) return;
-  for (int i = 0; i < n - 1; ++i) {
-    if (rep[i] || has_nb[i] == 0) continue;
+  const int m = list_n[0];
+  for (int q0 = 0; q0 < m; ++q0) {
+    const int i = list[q0];
+    if (i >= n - 1 || rep[i]) continue;
     const double X = xyz[3 * i], Y = xyz[3 * i + 1], Z = xyz[3 * i + 2];
     const long long cx = (long long)floor(X / cell), cy = (long long)floor(Y / cell),
                     cz = (long long)floor(Z / cell);
@@ -675,15 +680,24 @@ __global__ void repeat_greedy_kernel(const double* xyz, int n, double cell, int 
 __global__ void ghost_kernel(const double* score, const uint8_t* rep, int n, double thred,
                              uint8_t* flags) {
   __shared__ double s_mean;
-  if (threadIdx.x == 0) {
+  if (threadIdx.x < 32) {
+    // warp 0 streams the scores in; lane 0 adds them strictly in index order
+    const int lane = threadIdx.x;
     double sum = 0.0;
     long long cnt = 0;
-    for (int i = 0; i < n; ++i) {
-      if (rep[i]) continue;
-      sum += score[i];
-      ++cnt;
+    for (int base = 0; base < n; base += 32) {
+      const int i = base + lane;
+      const bool valid = i < n && !rep[i];
+      const double x = valid ? score[i] : 0.0;
+      const unsigned ball = __ballot_sync(0xffffffffu, valid);
+#pragma unroll 4
+      for (int j = 0; j < 32; ++j) {
+        const double y = __shfl_sync(0xffffffffu, x, j);
+        if (lane == 0 && (ball >> j) & 1u) sum += y;
+      }
+      cnt += __popc(ball);
     }
-    s_mean = cnt ? sum / (double)cnt : 0.0;
+    if (lane == 0) s_mean = cnt ? sum / (double)cnt : 0.0;
   }
   __syncthreads();
   const double m = s_mean;
@@ -692,6 +706,12 @@ __global__ void ghost_kernel(const double* score, const uint8_t* rep, int n, dou
     if (score[i] < m * thred || score[i] == 0.0) f |= 1;
     flags[i] = f;
   }
+}
+
+// has_nb[i] is 0 or 1 after neighbour_kernel; pos = exclusive scan of it
+__global__ void compact_kernel(const int* flag, const int* pos, int n, int* list) {
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i < n && flag[i]) list[pos[i]] = i;
 }
 
 __global__ void fill_kernel(double* p, int64_t n, double v) {
@@ -843,9 +863,16 @@ static void shake_impl(olpt_ctx* ctx, const ShakeParams& sp) {
     neighbour_kernel<<<OLPT_G(nblk(n)), 256, 0, s>>>(ctx->obj.xyz.as<double>(), (int)n, cell, nb,
                                               W.hash.start.as<int>(), W.hash.items.as<int>(), r2,
                                               W.has_nb.as<int>());
+    // ascending list of the objects that have neighbours (order-preserving compaction)
+    W.nb_pos.ensure((n + 1) * sizeof(int), s);
+    W.nb_list.ensure((n + 1) * sizeof(int), s);
+    exclusive_scan(W.has_nb.as<int>(), (int)n, W.nb_pos.as<int>(), W.scan_tmp, s);
+    compact_kernel<<<OLPT_G(nblk(n)), 256, 0, s>>>(W.has_nb.as<int>(), W.nb_pos.as<int>(), (int)n,
+                                                  W.nb_list.as<int>());
     repeat_greedy_kernel<<<OLPT_G(1), 32, 0, s>>>(ctx->obj.xyz.as<double>(), (int)n, cell, nb,
                                           W.hash.start.as<int>(), W.hash.items.as<int>(), r2,
-                                          W.has_nb.as<int>(), W.rep.as<uint8_t>());
+                                          W.nb_list.as<int>(), W.nb_pos.as<int>() + n,
+                                          W.rep.as<uint8_t>());
     ghost_kernel<<<OLPT_G(1), 1024, 0, s>>>(ctx->obj.score.as<double>(), W.rep.as<uint8_t>(), (int)n,
                                     sp.thred_ghost, ctx->obj.flags.as<uint8_t>());
     OLPT_CUDA(cudaGetLastError());

@@ -29,6 +29,7 @@
 #include <vector>
 
 #include "olpt_ctx.cuh"
+#include "olpt_scan.cuh"
 #include "olpt_stereo.h"
 
 namespace olpt {
@@ -76,41 +77,6 @@ __global__ void cell_hist_kernel(const double* x, const double* y, int64_t n, in
   int c = cy * cols + cx;
   cell_of[i] = c;
   atomicAdd(&counts[c], 1);
-}
-
-// exclusive scan of counts[0..n) -> start[0..n], one CTA
-__global__ void cell_scan_kernel(const int* counts, int n, int* start) {
-  __shared__ int warp_sums[32];
-  __shared__ int run, total;
-  if (threadIdx.x == 0) run = 0;
-  __syncthreads();
-  const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5, nw = blockDim.x >> 5;
-  for (int s = 0; s < n; s += blockDim.x) {
-    int i = s + threadIdx.x;
-    int v = i < n ? counts[i] : 0;
-    int incl = v;
-    for (int o = 1; o < 32; o <<= 1) {
-      int t = __shfl_up_sync(0xffffffffu, incl, o);
-      if (lane >= o) incl += t;
-    }
-    if (lane == 31) warp_sums[wid] = incl;
-    __syncthreads();
-    if (threadIdx.x == 0) {
-      int acc = 0;
-      for (int w = 0; w < nw; ++w) {
-        int t = warp_sums[w];
-        warp_sums[w] = acc;
-        acc += t;
-      }
-      total = acc;
-    }
-    __syncthreads();
-    if (i < n) start[i] = run + warp_sums[wid] + incl - v;
-    __syncthreads();
-    if (threadIdx.x == 0) run += total;
-    __syncthreads();
-  }
-  if (threadIdx.x == 0) start[n] = run;
 }
 
 __global__ void cell_scatter_kernel(const int* cell_of, int64_t n, const int* start, int* cursor,
@@ -302,16 +268,29 @@ __device__ __forceinline__ bool line_error_term(const double X[3], const double 
   return true;
 }
 
-// Expand one level: each warp takes one path with K chosen cameras and enumerates
-// candidates on its target camera.
-template <int K>
+__device__ __forceinline__ double clamped_dot(const double a[3], const double b[3]) {
+  const double dot = a[0] * b[0] + a[1] * b[1] + a[2] * b[2];
+  return fmax(-1.0, fmin(1.0, dot));
+}
+
+// cos(6 deg): the quick-gate angle factor of calTriangulateTol is exactly 1 whenever
+// the smallest pairwise parallax lies inside (6, 174) degrees.
+constexpr double kCos6 = 0.99452189536827329;
+
+// Expand one level: each path has K chosen cameras; its candidates on the target
+// camera are enumerated over rows of cells.  WARP: one warp per path, lanes take rows
+// (the single long strip of K = 1); otherwise one thread per path (K >= 2, where the
+// strips intersect in a few rows).
+template <int K, bool WARP>
 __global__ void __launch_bounds__(256) level_kernel(const SmView v, const Path* in, int n_in,
                                                     Path* out, int* out_count, int out_cap,
                                                     Path* term, int* term_count, int term_cap) {
-  const int warp = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
-  const int lane = threadIdx.x & 31;
-  if (warp >= n_in) return;
-  const Path P = in[warp];
+  const int gtid = blockIdx.x * blockDim.x + threadIdx.x;
+  const int pidx = WARP ? (gtid >> 5) : gtid;
+  const int r0 = WARP ? (threadIdx.x & 31) : 0;
+  const int rstep = WARP ? 32 : 1;
+  if (pidx >= n_in) return;
+  const Path P = in[pidx];
   const int t = P.target;
   // image lines of the chosen points on the target camera
   double lp[K][2], lU[K][2];
@@ -351,12 +330,12 @@ __global__ void __launch_bounds__(256) level_kernel(const SmView v, const Path* 
 #pragma unroll
     for (int q = 0; q < 9; ++q) Mc[q] = Mc[q] + tt[q];
   }
-  // minimum parallax among the chosen pairs (min is order-free)
-  double min_deg_c = 180.0;
+  // largest pairwise dot (smallest parallax) among the chosen lines
+  double maxdot_c = -2.0;
 #pragma unroll
   for (int i = 0; i < K; ++i)
 #pragma unroll
-    for (int j = i + 1; j < K; ++j) min_deg_c = fmin(min_deg_c, pair_deg(cu[i], cu[j]));
+    for (int j = i + 1; j < K; ++j) maxdot_c = fmax(maxdot_c, clamped_dot(cu[i], cu[j]));
 
   const int rows = v.rows[t], cols = v.cols[t];
   const double cellp = (double)v.cell;
@@ -399,7 +378,7 @@ __global__ void __launch_bounds__(256) level_kernel(const SmView v, const Path* 
     }
   }
 
-  for (int cy = row_lo + lane; cy <= row_hi; cy += 32) {
+  for (int cy = row_lo + r0; cy <= row_hi; cy += rstep) {
     // IDMap::computeStripIntersection, one row
     int xmin = 0, xmax = cols - 1;
 #pragma unroll
@@ -477,10 +456,23 @@ __global__ void __launch_bounds__(256) level_kernel(const SmView v, const Path* 
           qu[2] = S[5];
         }
         constexpr int k1 = K + 1;
-        double min_deg = min_deg_c;
+        double maxdot = maxdot_c;
 #pragma unroll
-        for (int i = 0; i < K; ++i) min_deg = fmin(min_deg, pair_deg(cu[i], qu));
-        const double tq = quick_tol_from_deg(min_deg, k1, v.m, v.tol3d);
+        for (int i = 0; i < K; ++i) maxdot = fmax(maxdot, clamped_dot(cu[i], qu));
+        double tq;
+        if (maxdot <= kCos6 - 1e-9 && maxdot >= -kCos6 + 1e-9) {
+          // min parallax in (6 + 5e-7, 174 - 5e-7) deg: the angle factor is exactly 1
+          tq = v.tol3d * sqrt(double(v.m > 2 ? v.m : 2) / double(k1)) * 1.0;
+        } else {
+          // near the 6-degree knee or beyond: the reference's acos/sin path
+          double min_deg = 180.0;
+#pragma unroll
+          for (int i = 0; i < k1; ++i)
+#pragma unroll
+            for (int j = i + 1; j < k1; ++j)
+              min_deg = fmin(min_deg, pair_deg(i < K ? cu[i] : qu, j < K ? cu[j] : qu));
+          tq = quick_tol_from_deg(min_deg, k1, v.m, v.tol3d);
+        }
         double M[9], b[3];
         {
           double tt[9];
@@ -654,7 +646,7 @@ void stereo_match_device(olpt_ctx* ctx, const SmParams& prm, StereoResult& res) 
       cell_hist_kernel<<<OLPT_G(nblk(n)), 256, 0, s>>>(v.x[c], v.y[c], n, v.cell, rows, cols,
                                                 W.cell_of[c].as<int>(), W.cell_cursor[c].as<int>());
     }
-    cell_scan_kernel<<<OLPT_G(1), 1024, 0, s>>>(W.cell_cursor[c].as<int>(), ncell, W.cell_start[c].as<int>());
+    exclusive_scan(W.cell_cursor[c].as<int>(), ncell, W.cell_start[c].as<int>(), W.scan_tmp, s);
     OLPT_CUDA(cudaMemsetAsync(W.cell_cursor[c].p, 0, ncell * sizeof(int), s));
     if (n > 0) {
       cell_scatter_kernel<<<OLPT_G(nblk(n)), 256, 0, s>>>(W.cell_of[c].as<int>(), n, W.cell_start[c].as<int>(),
@@ -726,17 +718,18 @@ void stereo_match_device(olpt_ctx* ctx, const SmParams& prm, StereoResult& res) 
       OLPT_CUDA(cudaMemcpyAsync(cnt + 2, &n_term, sizeof(int), cudaMemcpyHostToDevice, s));
       const int64_t threads = (int64_t)n_in * 32;
       const int pid = ctx->prof.begin(PROF_STEREO, s);
-      auto kern = level_kernel<1>;
+      auto kern = level_kernel<1, true>;
       switch (level) {
-        case 1: kern = level_kernel<1>; break;
-        case 2: kern = level_kernel<2>; break;
-        case 3: kern = level_kernel<3>; break;
-        case 4: kern = level_kernel<4>; break;
-        case 5: kern = level_kernel<5>; break;
-        case 6: kern = level_kernel<6>; break;
-        default: kern = level_kernel<7>; break;
+        case 1: kern = level_kernel<1, true>; break;
+        case 2: kern = level_kernel<2, false>; break;
+        case 3: kern = level_kernel<3, false>; break;
+        case 4: kern = level_kernel<4, false>; break;
+        case 5: kern = level_kernel<5, false>; break;
+        case 6: kern = level_kernel<6, false>; break;
+        default: kern = level_kernel<7, false>; break;
       }
-      kern<<<OLPT_G(nblk(threads)), 256, 0, s>>>(v, in_buf->as<Path>(), n_in, out_buf->as<Path>(),
+      const int64_t work = level == 1 ? threads : (int64_t)n_in;
+      kern<<<OLPT_G(nblk(work)), 256, 0, s>>>(v, in_buf->as<Path>(), n_in, out_buf->as<Path>(),
                                                  cnt + 1, out_cap, W.term.as<Path>(), cnt + 2,
                                                  term_cap);
       ctx->prof.end(PROF_STEREO, pid, s, 0.0);
@@ -782,6 +775,7 @@ void stereo_match_device(olpt_ctx* ctx, const SmParams& prm, StereoResult& res) 
     OLPT_CUDA(cudaStreamSynchronize(s));
   }
   res.n_cam = n_cam;
+  PhaseTimer pt(ctx->prof, PH_PRUNE);
   sort_candidates(res);
   std::vector<int> counts(n_cam);
   std::vector<int> active(n_cam);

@@ -3,13 +3,19 @@
 // StereoMatch::pruneMatch (src/srcSTB/StereoMatch.cpp:631-980) is an
 // order-dependent greedy whose comparators use a relative tolerance and are not a
 // strict weak ordering; the ranks it produces depend on the exact merge sequence of
-// libstdc++'s std::stable_sort.  It is a short serial pass over an already small
-// candidate list, so it runs here, with the same std::stable_sort over the same
-// comparators, which keeps the selection identical to the reference's.  All
-// numerical work (detection, lines of sight, strip search, triangulation) stays on
-// the device.
+// libstdc++'s std::stable_sort.  It therefore runs here, calling the same
+// std::stable_sort with the same comparators, which keeps the selection identical
+// to the reference's.  The data layout is flat (CSR point -> candidate lists), and
+// the per-point percentile pass runs on all host threads: every point writes its own
+// slots, and each candidate then sums its slots in ascending point order -- the
+// order in which the reference accumulates pct_sum -- so the floating-point sums are
+// unchanged.  All numerical geometry (detection, lines of sight, strip search,
+// triangulation) stays on the device.
+#include <omp.h>
+
 #include <algorithm>
 #include <cmath>
+#include <cstdint>
 #include <limits>
 #include <numeric>
 #include <utility>
@@ -23,11 +29,28 @@ void sort_candidates(StereoResult& r) {
   const int n = r.n_cam;
   const size_t M = r.e.size();
   std::vector<size_t> ord(M);
-  std::iota(ord.begin(), ord.end(), 0);
   const int* ids = r.ids.data();
-  std::sort(ord.begin(), ord.end(), [&](size_t a, size_t b) {
-    return std::lexicographical_compare(ids + a * n, ids + a * n + n, ids + b * n, ids + b * n + n);
-  });
+  // ids are compared lexicographically (camera 0 first, -1 < any id); with
+  // 21 bits per camera the key of up to 6 cameras fits in 128 bits.
+  int max_id = 0;
+  for (size_t q = 0; q < r.ids.size(); ++q) max_id = std::max(max_id, ids[q]);
+  if (n <= 6 && max_id < (1 << 21) - 2) {
+    std::vector<std::pair<unsigned __int128, uint32_t>> key(M);
+    for (size_t j = 0; j < M; ++j) {
+      unsigned __int128 k = 0;
+      for (int c = 0; c < n; ++c) k = (k << 21) | (unsigned __int128)(ids[j * n + c] + 1);
+      key[j] = {k, (uint32_t)j};
+    }
+    std::sort(key.begin(), key.end(),
+              [](const auto& a, const auto& b) { return a.first < b.first; });
+    for (size_t i = 0; i < M; ++i) ord[i] = key[i].second;
+  } else {
+    std::iota(ord.begin(), ord.end(), 0);
+    std::sort(ord.begin(), ord.end(), [&](size_t a, size_t b) {
+      return std::lexicographical_compare(ids + a * n, ids + a * n + n, ids + b * n,
+                                          ids + b * n + n);
+    });
+  }
   std::vector<int> ids2(r.ids.size());
   std::vector<double> e2(M), X2(3 * M);
   for (size_t i = 0; i < M; ++i) {
@@ -61,59 +84,97 @@ void prune_candidates(StereoResult& r, const std::vector<int>& det_counts,
   for (int c = 0; c < n_cams; ++c) cam_offsets[c + 1] = cam_offsets[c] + det_counts[c];
   const size_t total_points = cam_offsets.back();
 
-  // Step 1: flat 2D point indices per candidate
-  std::vector<std::vector<size_t>> flats(M);
+  // Step 1: flat 2D point indices per candidate (ascending: camera order)
+  std::vector<int> foff(M + 1, 0);
+  std::vector<int64_t> flat;
+  flat.reserve(M * n_cams);
   for (size_t j = 0; j < M; ++j) {
-    auto& lf = flats[j];
     for (int c = 0; c < n_cams; ++c) {
       if (!active[c]) continue;
       const int pid = r.ids[j * n_cams + c];
       if (pid < 0 || pid >= det_counts[c]) continue;
-      lf.push_back(cam_offsets[c] + (size_t)pid);
+      flat.push_back((int64_t)(cam_offsets[c] + (size_t)pid));
     }
+    foff[j + 1] = (int)flat.size();
   }
-  // Step 2: reverse index
-  std::vector<std::vector<int>> p2c(total_points);
-  for (size_t j = 0; j < M; ++j)
-    for (size_t f : flats[j]) p2c[f].push_back((int)j);
-  // Step 3: percentile scores
-  std::vector<double> pct_sum(M, 0.0);
-  std::vector<int> pct_count(M, 0);
-  for (size_t f = 0; f < total_points; ++f) {
-    const auto& idxs = p2c[f];
-    if (idxs.empty()) continue;
-    std::vector<std::pair<double, int>> pool;
-    pool.reserve(idxs.size());
-    for (int j : idxs)
-      if (std::isfinite(e_checks[j])) pool.emplace_back(e_checks[j], j);
-    const int n = (int)pool.size();
-    if (n == 0) continue;
-    if (n == 1) {
-      pct_sum[pool[0].second] += 0.0;
-      pct_count[pool[0].second] += 1;
-      continue;
-    }
-    std::stable_sort(pool.begin(), pool.end(), [&](const auto& A, const auto& B) {
-      if (!eq_eps(A.first, B.first)) return A.first < B.first;
-      return A.second < B.second;
-    });
-    int k = 0;
-    while (k < n) {
-      int k0 = k, k1 = k + 1;
-      while (k1 < n && eq_eps(pool[k1].first, pool[k0].first)) ++k1;
-      const double avg_rank = 0.5 * (double)(k0 + (k1 - 1));
-      const double denom = (double)(n - 1);
-      const double pct = (denom > 0.0) ? (avg_rank / denom) : 0.0;
-      for (int t = k0; t < k1; ++t) {
-        pct_sum[pool[t].second] += pct;
-        pct_count[pool[t].second] += 1;
+  // Step 2: point -> candidates (ascending j), with the slot of the point in the candidate
+  std::vector<int> poff(total_points + 1, 0);
+  for (int64_t f : flat) ++poff[f + 1];
+  for (size_t f = 0; f < total_points; ++f) poff[f + 1] += poff[f];
+  std::vector<int> pc_j(flat.size()), pc_slot(flat.size());
+  {
+    std::vector<int> cur(poff.begin(), poff.end() - 1);
+    for (size_t j = 0; j < M; ++j)
+      for (int q = foff[j]; q < foff[j + 1]; ++q) {
+        const int64_t f = flat[q];
+        pc_j[cur[f]] = (int)j;
+        pc_slot[cur[f]] = q;
+        ++cur[f];
       }
-      k = k1;
+  }
+  // Step 3: percentile of every (point, candidate) pair, written to the candidate's slot
+  std::vector<double> slot_pct(flat.size(), 0.0);
+  std::vector<char> slot_used(flat.size(), 0);
+#pragma omp parallel
+  {
+    std::vector<std::pair<double, int>> pool;
+    std::vector<int> pool_slot;
+#pragma omp for schedule(dynamic, 256)
+    for (int64_t f = 0; f < (int64_t)total_points; ++f) {
+      const int b = poff[f], e = poff[f + 1];
+      if (b == e) continue;
+      pool.clear();
+      for (int q = b; q < e; ++q) {
+        const int j = pc_j[q];
+        const double ej = e_checks[j];
+        if (std::isfinite(ej)) pool.emplace_back(ej, j);
+      }
+      const int n = (int)pool.size();
+      if (n == 0) continue;
+      auto slot_of = [&](int j) {
+        for (int q = b; q < e; ++q)
+          if (pc_j[q] == j) return pc_slot[q];
+        return -1;
+      };
+      if (n == 1) {
+        const int s = slot_of(pool[0].second);
+        slot_pct[s] = 0.0;
+        slot_used[s] = 1;
+        continue;
+      }
+      std::stable_sort(pool.begin(), pool.end(), [&](const auto& A, const auto& B) {
+        if (!eq_eps(A.first, B.first)) return A.first < B.first;
+        return A.second < B.second;
+      });
+      int k = 0;
+      while (k < n) {
+        int k0 = k, k1 = k + 1;
+        while (k1 < n && eq_eps(pool[k1].first, pool[k0].first)) ++k1;
+        const double avg_rank = 0.5 * (double)(k0 + (k1 - 1));
+        const double denom = (double)(n - 1);
+        const double pct = (denom > 0.0) ? (avg_rank / denom) : 0.0;
+        for (int t = k0; t < k1; ++t) {
+          const int s = slot_of(pool[t].second);
+          slot_pct[s] = pct;
+          slot_used[s] = 1;
+        }
+        k = k1;
+      }
     }
   }
+  // per candidate: sum over its points in ascending point order (the reference's order)
   std::vector<double> pct_score(M, std::numeric_limits<double>::infinity());
-  for (size_t j = 0; j < M; ++j)
-    if (pct_count[j] > 0) pct_score[j] = pct_sum[j] / (double)pct_count[j];
+#pragma omp parallel for schedule(static)
+  for (int64_t j = 0; j < (int64_t)M; ++j) {
+    double sum = 0.0;
+    int cnt = 0;
+    for (int q = foff[j]; q < foff[j + 1]; ++q)
+      if (slot_used[q]) {
+        sum += slot_pct[q];
+        ++cnt;
+      }
+    if (cnt > 0) pct_score[j] = sum / (double)cnt;
+  }
   // Step 4: order by (pct, e_check, index)
   std::vector<int> order(M);
   std::iota(order.begin(), order.end(), 0);
@@ -142,21 +203,21 @@ void prune_candidates(StereoResult& r, const std::vector<int>& det_counts,
   std::vector<int> owner(total_points, -1);
   std::vector<char>& selected = r.selected;
   auto place = [&](int cand) {
-    for (size_t f : flats[cand]) owner[f] = cand;
+    for (int q = foff[cand]; q < foff[cand + 1]; ++q) owner[flat[q]] = cand;
     selected[cand] = 1;
   };
   auto clear_owner_of = [&](int cand) {
-    for (size_t f : flats[cand])
-      if (owner[f] == cand) owner[f] = -1;
+    for (int q = foff[cand]; q < foff[cand + 1]; ++q)
+      if (owner[flat[q]] == cand) owner[flat[q]] = -1;
     selected[cand] = 0;
   };
+  std::vector<int> S;
   for (int j : order) {
     if (!std::isfinite(pct_score[j]) || !std::isfinite(e_checks[j])) continue;
-    const auto& fl = flats[j];
-    if (fl.empty()) continue;
+    if (foff[j] == foff[j + 1]) continue;
     bool conflict = false;
-    for (size_t f : fl)
-      if (owner[f] != -1) {
+    for (int q = foff[j]; q < foff[j + 1]; ++q)
+      if (owner[flat[q]] != -1) {
         conflict = true;
         break;
       }
@@ -164,9 +225,9 @@ void prune_candidates(StereoResult& r, const std::vector<int>& det_counts,
       place(j);
       continue;
     }
-    std::vector<int> S;
-    for (size_t f : fl) {
-      const int o = owner[f];
+    S.clear();
+    for (int q = foff[j]; q < foff[j + 1]; ++q) {
+      const int o = owner[flat[q]];
       if (o == -1) continue;
       if (std::find(S.begin(), S.end(), o) == S.end()) S.push_back(o);
     }
