@@ -124,6 +124,33 @@ olpt_status_t olpt_get_peaks(olpt_ctx* ctx, int cam, double* xy, int32_t* rc, in
 olpt_status_t olpt_detections_upload(olpt_ctx* ctx, int n_cam, const int64_t* counts,
                                      const double* const* xy);
 
+/* Allocation-free tracer detection on one camera image.  No counterpart in the
+ * reference (which is host-only): it exists for callers that cannot allocate device
+ * memory -- code that runs inside another framework's memory arena or caching
+ * allocator, or a plug-in host that budgets the device memory itself -- so it needs
+ * no context and calls no cudaMalloc/cudaFree or allocating library routine.  Same
+ * kernels and results as olpt_find_peaks; its scratch (per-band counts and offsets)
+ * and the log table live in library-owned static device arrays that every GPU
+ * loading this library holds until exit.
+ *   d_img       device image, H x W elements of `dtype`, rows pitch_bytes apart
+ *               (pitch and pointer 16-byte aligned); H, W at most 16384
+ *   d_x, d_y    device outputs (capacity doubles each), d_rc device output
+ *               (capacity x 2 int32: row, col), raster order
+ *   capacity    at least (H * W + 1) / 2
+ *   d_count     device int64 receiving the number of detections
+ *   stream      cudaStream_t to launch on (NULL = default stream); the call returns
+ *               without synchronising.
+ * The first call on a device does a one-time, synchronous set-up (resolving the
+ * static arrays' device addresses and filling the log table), so make it before
+ * any stream capture.  All calls share the static scratch: calls that overlap on
+ * the GPU (different streams, host threads) race; serialise them.  Error text:
+ * olpt_find_peaks_noalloc_error(). */
+olpt_status_t olpt_find_peaks_noalloc(const void* d_img, olpt_dtype_t dtype, int H, int W,
+                                      int64_t pitch_bytes, double min_obj_int, double* d_x,
+                                      double* d_y, int32_t* d_rc, int64_t capacity,
+                                      int64_t* d_count, void* stream);
+const char* olpt_find_peaks_noalloc_error(void);
+
 /* ------------------------------------------------------------------ stereo matching */
 /* StereoMatch parameters (SMParam, inc/libSTB/Config.h:72-80): limit is the
  * (xmin,xmax,ymin,ymax,zmin,zmax) box of accepted triangulations. */

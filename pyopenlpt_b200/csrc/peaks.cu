@@ -19,6 +19,8 @@
 #include <cuda_runtime.h>
 
 #include <cmath>
+#include <mutex>
+#include <string>
 #include <vector>
 
 #include "olpt_ctx.cuh"
@@ -385,4 +387,146 @@ void find_peaks_device(olpt_ctx* ctx, double min_int, bool sync_counts) {
   }
 }
 
+// ---------------------------------------------------------------------------
+// Allocation-free detection for callers that cannot allocate device memory:
+// code running inside a host-side memory arena or pool that forbids outside
+// allocations, code that must not perturb another framework's caching allocator,
+// or plug-in hosts whose device memory is budgeted by someone else.  Their scratch
+// (the per-band counts and offsets of the two-pass raster compaction) and the
+// log table for integer images live in these file-scope device arrays, which every
+// GPU that loads this library holds until the process exits.
+constexpr int kNoAllocMaxBands = 16384;  // one band per row at most: images up to 16384 rows
+constexpr int kNoAllocMaxCols = 16384;
+
+static __device__ __align__(256) unsigned char g_noalloc_scratch[kNoAllocMaxBands * (4 + 8) + 256];
+static __device__ __align__(256) double g_noalloc_log_lut[65536];
+
+namespace {
+struct NoAllocDevice {
+  bool ready = false;
+  unsigned char* scratch = nullptr;  // device address of g_noalloc_scratch
+  double* lut = nullptr;             // device address of g_noalloc_log_lut
+};
+std::mutex g_noalloc_mu;
+NoAllocDevice g_noalloc_dev[64];
+}  // namespace
+
+// Once per device, with that device current: resolve the arrays' device addresses
+// (in host code their names are host-side stand-ins, not device addresses) and fill
+// the log table.  Synchronous; must run before any stream capture.
+static olpt_status_t noalloc_setup(int dev, NoAllocDevice*& out, std::string& err) {
+  std::lock_guard<std::mutex> lk(g_noalloc_mu);
+  if (dev < 0 || dev >= 64) {
+    err = "device ordinal out of range";
+    return OLPT_ERR_INVALID_ARG;
+  }
+  NoAllocDevice& d = g_noalloc_dev[dev];
+  if (!d.ready) {
+    cudaError_t e = cudaGetSymbolAddress((void**)&d.scratch, g_noalloc_scratch);
+    if (e == cudaSuccess) e = cudaGetSymbolAddress((void**)&d.lut, g_noalloc_log_lut);
+    if (e != cudaSuccess) {
+      err = std::string("cudaGetSymbolAddress failed: ") + cudaGetErrorString(e);
+      return OLPT_ERR_CUDA;
+    }
+    std::vector<double> t(65536);
+    for (int v = 0; v < 65536; ++v) {
+      const double x = (double)v;
+      t[v] = std::log(x < 1e-4 ? 1e-4 : x);
+    }
+    e = cudaMemcpy(d.lut, t.data(), sizeof(double) * 65536, cudaMemcpyHostToDevice);
+    if (e != cudaSuccess) {
+      err = std::string("log table upload failed: ") + cudaGetErrorString(e);
+      return OLPT_ERR_CUDA;
+    }
+    d.ready = true;
+  }
+  out = &d;
+  return OLPT_OK;
+}
+
+thread_local std::string g_noalloc_err;
+
 }  // namespace olpt
+
+extern "C" {
+
+const char* olpt_find_peaks_noalloc_error(void) { return olpt::g_noalloc_err.c_str(); }
+
+olpt_status_t olpt_find_peaks_noalloc(const void* d_img, olpt_dtype_t dtype, int H, int W,
+                                      int64_t pitch_bytes, double min_obj_int, double* d_x,
+                                      double* d_y, int32_t* d_rc, int64_t capacity,
+                                      int64_t* d_count, void* stream) {
+  using namespace olpt;
+  std::string& err = g_noalloc_err;
+  err.clear();
+  if (!d_img || !d_x || !d_y || !d_rc || !d_count) {
+    err = "null buffer";
+    return OLPT_ERR_INVALID_ARG;
+  }
+  if (dtype < OLPT_U8 || dtype > OLPT_F64) {
+    err = "bad dtype";
+    return OLPT_ERR_INVALID_ARG;
+  }
+  const int esz = dtype == OLPT_U8 ? 1 : dtype == OLPT_U16 ? 2 : dtype == OLPT_F32 ? 4 : 8;
+  if (H < 1 || W < 1 || H > kNoAllocMaxBands || W > kNoAllocMaxCols) {
+    err = "image must be 1..16384 rows and 1..16384 columns for the allocation-free detector";
+    return OLPT_ERR_INVALID_ARG;
+  }
+  if (pitch_bytes < (int64_t)W * esz || pitch_bytes % 16 != 0 ||
+      reinterpret_cast<uintptr_t>(d_img) % 16 != 0) {
+    err = "image rows must start on 16-byte boundaries (pitch a multiple of 16, >= W * elem)";
+    return OLPT_ERR_INVALID_ARG;
+  }
+  if (capacity < ((int64_t)H * W + 1) / 2) {
+    err = "capacity must be at least (H * W + 1) / 2 (the most 4-neighbour maxima an image can hold)";
+    return OLPT_ERR_INVALID_ARG;
+  }
+  int dev = 0;
+  cudaError_t ce = cudaGetDevice(&dev);
+  if (ce != cudaSuccess) {
+    err = cudaGetErrorString(ce);
+    return OLPT_ERR_CUDA;
+  }
+  NoAllocDevice* nd = nullptr;
+  olpt_status_t st = noalloc_setup(dev, nd, err);
+  if (st != OLPT_OK) return st;
+  try {
+    const int N = 16 / esz;
+    const int cpr = (W + N - 1) / N;
+    int band_rows = (2048 + cpr - 1) / cpr;
+    if (band_rows < 1) band_rows = 1;
+    PeakArgs a{};
+    a.n_cam = 1;
+    a.min_int = min_obj_int;
+    PeakCam& pc = a.cam[0];
+    pc.img = static_cast<const unsigned char*>(d_img);
+    pc.pitch = pitch_bytes;
+    pc.H = H;
+    pc.W = W;
+    pc.band_rows = band_rows;
+    pc.n_bands = (H + band_rows - 1) / band_rows;
+    pc.band_base = 0;
+    pc.active = 1;
+    pc.x = d_x;
+    pc.y = d_y;
+    pc.rc = reinterpret_cast<int2*>(d_rc);
+    // scratch layout: band offsets (int64) then band counts (int); every band count
+    // that the scan reads is written by this call's count pass first.
+    int64_t* offs = reinterpret_cast<int64_t*>(nd->scratch);
+    a.band_counts = reinterpret_cast<int*>(nd->scratch + sizeof(int64_t) * kNoAllocMaxBands);
+    a.lut = nd->lut;
+    cudaStream_t s = static_cast<cudaStream_t>(stream);
+    switch (dtype) {
+      case OLPT_U8: launch_peaks<uint8_t>(a, pc.n_bands, offs, d_count, s); break;
+      case OLPT_U16: launch_peaks<uint16_t>(a, pc.n_bands, offs, d_count, s); break;
+      case OLPT_F32: launch_peaks<float>(a, pc.n_bands, offs, d_count, s); break;
+      default: launch_peaks<double>(a, pc.n_bands, offs, d_count, s); break;
+    }
+  } catch (CudaError const& e) {
+    err = std::string(cudaGetErrorString(e.code)) + " (" + e.where + ")";
+    return OLPT_ERR_CUDA;
+  }
+  return OLPT_OK;
+}
+
+}  // extern "C"
