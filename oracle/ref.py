@@ -220,3 +220,53 @@ class RefOracle:
             self.close()
         except Exception:
             pass
+
+
+class RefSTB:
+    """The reference STB (processFrame) on a synthetic sequence, built from
+    reference-format config files written by synth.write_stb_config."""
+
+    def __init__(self, seq, ipr_settings, stb_settings, workdir: Optional[str] = None,
+                 threads: int = 0, n_frames: Optional[int] = None):
+        from pyopenlpt_b200.synth import write_stb_config
+        self.lib = lib = C.CDLL(REF_SO)
+        lib.oref_stb_new.restype = C.c_void_p
+        lib.oref_stb_tracks.restype = C.c_void_p
+        lib.oref_res_len.restype = C.c_longlong
+        lib.oref_res_len.argtypes = [C.c_void_p, C.c_char_p]
+        lib.oref_res_copy.argtypes = [C.c_void_p, C.c_char_p, _dp]
+        lib.oref_res_free.argtypes = [C.c_void_p]
+        lib.oref_last_error.restype = C.c_char_p
+        lib.oref_set_threads(int(threads))
+        self.seq = seq
+        self._tmp = workdir or tempfile.mkdtemp(prefix="oref_stb_")
+        main = write_stb_config(seq, self._tmp, ipr_settings, stb_settings, n_frames=n_frames)
+        self.h = lib.oref_stb_new(main.encode(), os.path.join(self._tmp, "otf.txt").encode())
+        if not self.h:
+            raise RuntimeError(lib.oref_last_error().decode())
+
+    def frame(self, t: int, imgs=None):
+        imgs = imgs if imgs is not None else self.seq.frames[t]
+        d = [np.ascontiguousarray(im, dtype=np.float64) for im in imgs]
+        H = (C.c_int * len(d))(*[im.shape[0] for im in d])
+        W = (C.c_int * len(d))(*[im.shape[1] for im in d])
+        rc = self.lib.oref_stb_frame(C.c_void_p(self.h), t, len(d), _ptr_array(d), H, W)
+        if rc != 0:
+            raise RuntimeError(self.lib.oref_last_error().decode())
+
+    def tracks(self):
+        h = C.c_void_p(self.lib.oref_stb_tracks(C.c_void_p(self.h)))
+        out = {}
+        for name in ("long_active", "short_active", "long_inactive", "exit"):
+            n = self.lib.oref_res_len(h, name.encode())
+            a = np.empty(max(n, 0))
+            if n > 0:
+                self.lib.oref_res_copy(h, name.encode(), _as_dp(a))
+            out[name] = a.reshape(-1, 5)
+        self.lib.oref_res_free(h)
+        return out
+
+    def close(self):
+        if getattr(self, "h", None):
+            self.lib.oref_stb_free(C.c_void_p(self.h))
+            self.h = None

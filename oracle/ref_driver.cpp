@@ -459,3 +459,84 @@ int oref_otf_param(void* cfg_h, int cam, long long n, const double* xyz, double*
   return 0;
 }
 }  // extern "C"
+
+// ---------------------------------------------------------------- STB
+// STB::processFrame (src/srcSTB/STB.cpp:40-89) on in-memory frames.  The STB is
+// built from reference-format config files (BasicSetting::readConfig and the
+// STB constructor, which estimates an OTF from the first frames); the OTF is then
+// replaced by the scene's exact table so that the device run sees the same one.
+struct DebugAccess_STB {
+  static ObjectConfig& cfg(STB& s) { return *s._obj_config; }
+};
+
+namespace {
+struct RefStb {
+  BasicSetting bs;
+  std::unique_ptr<STB> stb;
+};
+
+void put_tracks(Result* r, const char* name, const std::deque<Track>& tracks) {
+  auto& v = r->arrays[name];
+  for (size_t i = 0; i < tracks.size(); ++i) {
+    const Track& tr = tracks[i];
+    for (size_t k = 0; k < tr._obj3d_list.size(); ++k) {
+      v.push_back((double)i);
+      v.push_back((double)tr._t_list[k]);
+      for (int d = 0; d < 3; ++d) v.push_back(tr._obj3d_list[k]->_pt_center[d]);
+    }
+  }
+}
+}  // namespace
+
+extern "C" {
+
+void* oref_stb_new(const char* main_cfg, const char* otf_file) {
+  try {
+    auto* r = new RefStb();
+    if (!r->bs.readConfig(main_cfg)) {
+      g_last_error = "BasicSetting::readConfig failed";
+      delete r;
+      return nullptr;
+    }
+    r->stb = std::make_unique<STB>(r->bs, "Tracer", r->bs._object_config_paths.at(0));
+    auto& tc = static_cast<TracerConfig&>(DebugAccess_STB::cfg(*r->stb));
+    tc._otf.loadParam(std::string(otf_file));
+    return r;
+  } catch (std::exception const& e) {
+    g_last_error = e.what();
+  } catch (...) {
+    g_last_error = "STB construction failed";
+  }
+  return nullptr;
+}
+
+void oref_stb_free(void* h) { delete static_cast<RefStb*>(h); }
+
+int oref_stb_frame(void* h, int frame, int n_cam, const double* const* imgs, const int* H,
+                   const int* W) {
+  auto* r = static_cast<RefStb*>(h);
+  try {
+    auto images = make_images(n_cam, imgs, H, W);
+    r->stb->processFrame(frame, images);
+  } catch (std::exception const& e) {
+    g_last_error = e.what();
+    return -1;
+  } catch (...) {
+    g_last_error = "processFrame failed";
+    return -1;
+  }
+  return 0;
+}
+
+// tracks of the four lists: rows of (track index, frame, x, y, z)
+void* oref_stb_tracks(void* h) {
+  auto* r = static_cast<RefStb*>(h);
+  auto* res = new Result();
+  put_tracks(res, "long_active", r->stb->_long_track_active);
+  put_tracks(res, "short_active", r->stb->_short_track_active);
+  put_tracks(res, "long_inactive", r->stb->_long_track_inactive);
+  put_tracks(res, "exit", r->stb->_exit_track);
+  return res;
+}
+
+}  // extern "C"

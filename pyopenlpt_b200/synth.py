@@ -152,6 +152,88 @@ def make_scene(n_particles: int = 10000, n_cam: int = 4, size: int = 1024, focal
     return Scene(cams, xyz, images, tuple(volume), (a, b, c), max_val)
 
 
+def burgers_velocity(xyz: np.ndarray, center, gamma: float = 2e4, r_core: float = 8.0,
+                     strain: float = 2.0, drift=(0.0, 0.0, 0.0)) -> np.ndarray:
+    """Burgers vortex along z through `center` (circulation gamma mm^2/s, core radius
+    r_core mm, axial strain 1/s) plus a uniform drift; mm/s."""
+    d = xyz - np.asarray(center)
+    x, y, z = d[:, 0], d[:, 1], d[:, 2]
+    r2 = x * x + y * y
+    r2s = np.maximum(r2, 1e-12)
+    ut_over_r = gamma / (2 * np.pi * r2s) * (1.0 - np.exp(-r2s / (r_core * r_core)))
+    u = -ut_over_r * y - 0.5 * strain * x + drift[0]
+    v = ut_over_r * x - 0.5 * strain * y + drift[1]
+    w = strain * z + drift[2]
+    return np.stack([u, v, w], axis=1)
+
+
+def rk4(f, xyz: np.ndarray, dt: float) -> np.ndarray:
+    k1 = f(xyz)
+    k2 = f(xyz + 0.5 * dt * k1)
+    k3 = f(xyz + 0.5 * dt * k2)
+    k4 = f(xyz + dt * k3)
+    return xyz + dt / 6.0 * (k1 + 2 * k2 + 2 * k3 + k4)
+
+
+@dataclasses.dataclass
+class Sequence_:
+    cams: List[PinholeCam]
+    frames: List[List[np.ndarray]]   # frames[t][cam] images
+    truth: List[np.ndarray]          # truth[t] (N,3) positions
+    ids: List[np.ndarray]            # truth[t] particle ids (re-seeded particles get new ids)
+    volume: tuple
+    otf_abc: tuple
+    max_val: int
+    dt: float
+
+    @property
+    def n_cam(self) -> int:
+        return len(self.cams)
+
+
+def make_sequence(n_particles: int = 51000, n_frames: int = 50, n_cam: int = 4,
+                  n_row: int = 800, n_col: int = 1280, focal: float = 5000.0,
+                  volume=(-30.0, 30.0, -20.0, 20.0, -15.0, 15.0), a: float = 3000.0,
+                  b: float = 0.5, c: float = 0.5, noise: float = 20.0, bits: int = 12,
+                  max_px_per_frame: float = 3.0, gamma: float = 2e4, r_core: float = 8.0,
+                  strain: float = 2.0, drift=(20.0, 0.0, 0.0), seed: int = 1234,
+                  with_images: bool = True) -> Sequence_:
+    """Particles advected by a Burgers vortex plus drift (RK4, FP64); the time step
+    gives at most `max_px_per_frame` pixels of image motion per frame; particles that
+    leave the volume are re-seeded uniformly.  Defaults: the BASELINE STB sequence
+    (51,000 particles, 4 x 1280x800 12-bit, 60x40x30 mm, 50 frames)."""
+    rng = np.random.default_rng(seed)
+    cams = ring_rig(n_cam, n_row, n_col, focal)
+    lo = np.array(volume[0::2])
+    hi = np.array(volume[1::2])
+    center = 0.5 * (lo + hi)
+    vel = lambda p: burgers_velocity(p, center, gamma, r_core, strain, drift)  # noqa: E731
+    xyz = lo + (hi - lo) * rng.random((n_particles, 3))
+    ids = np.arange(n_particles)
+    next_id = n_particles
+    # time step from the fastest image motion over a probe cloud
+    probe = lo + (hi - lo) * rng.random((200000, 3))
+    vmax = float(np.max(np.linalg.norm(vel(probe), axis=1)))
+    mm_per_px = 500.0 / focal
+    dt = max_px_per_frame * mm_per_px / max(vmax, 1e-9)
+    max_val = (1 << bits) - 1
+    dtype = np.uint8 if bits <= 8 else np.uint16
+    frames, truth, idl = [], [], []
+    for t in range(n_frames):
+        truth.append(xyz.copy())
+        idl.append(ids.copy())
+        if with_images:
+            frames.append([render(cm, xyz, a, b, c, noise, max_val, dtype, rng) for cm in cams])
+        xyz = rk4(vel, xyz, dt)
+        out = np.any((xyz < lo) | (xyz > hi), axis=1)
+        k = int(out.sum())
+        if k:
+            xyz[out] = lo + (hi - lo) * rng.random((k, 3))
+            ids[out] = np.arange(next_id, next_id + k)
+            next_id += k
+    return Sequence_(cams, frames, truth, idl, tuple(volume), (a, b, c), max_val, dt)
+
+
 def otf_table_array(n_cam: int, abc, alpha: float = 0.0, n=(2, 2, 2)) -> np.ndarray:
     """Uniform OTF table [4][n_cam][nx*ny*nz] (a, b, c, alpha planes)."""
     ng = n[0] * n[1] * n[2]
@@ -195,6 +277,72 @@ class IPRSettings:
     @property
     def shakewidth_min(self) -> float:
         return self.shake_width / 20
+
+
+@dataclasses.dataclass
+class STBSettings:
+    """STB / predictive-field knobs of the reference's object config
+    (src/srcSTB/Config.cpp:199-214); lengths in mm (voxel_to_mm = 1)."""
+    radius_search_obj: float = 1.0
+    n_initial_frames: int = 4
+    radius_search_track: float = 1.0
+    pf_nx: int = 11
+    pf_ny: int = 11
+    pf_nz: int = 6
+    pf_r: float = 3.0
+
+
+def write_raw_frame(path: str, img: np.ndarray):
+    """The oracle's raw frame format: b"ORIM", int32 rows, int32 cols, int32 dtype."""
+    code = {np.dtype(np.uint8): 0, np.dtype(np.uint16): 1, np.dtype(np.float64): 3}[img.dtype]
+    with open(path, "wb") as f:
+        f.write(b"ORIM")
+        f.write(np.array([img.shape[0], img.shape[1], code], dtype=np.int32).tobytes())
+        f.write(np.ascontiguousarray(img).tobytes())
+
+
+def write_stb_config(seq, folder: str, ipr: "IPRSettings", stb: STBSettings,
+                     n_frames: Optional[int] = None) -> str:
+    """Reference-format main config (BasicSetting::readConfig, Config.cpp:49-135), tracer
+    config (readCommonConfig + TracerConfig::readConfig, Config.cpp:163-286), camera
+    files, image lists with raw frames, and the OTF file.  Returns the main config path."""
+    os.makedirs(folder, exist_ok=True)
+    n_frames = n_frames or len(seq.frames)
+    cam_paths = []
+    for i, cm in enumerate(seq.cams):
+        p = os.path.join(folder, f"cam{i + 1}.txt")
+        with open(p, "w") as f:
+            f.write(cm.to_text())
+        cam_paths.append(p)
+    lists = []
+    for i in range(seq.n_cam):
+        names = []
+        for t in range(n_frames):
+            nm = f"cam{i + 1}_{t:05d}.raw"
+            write_raw_frame(os.path.join(folder, nm), seq.frames[t][i])
+            names.append(os.path.join(folder, nm))
+        lp = f"cam{i + 1}ImageNames.txt"
+        with open(os.path.join(folder, lp), "w") as f:
+            f.write("\n".join(names) + "\n")
+        lists.append(os.path.join(folder, lp))
+    with open(os.path.join(folder, "otf.txt"), "w") as f:
+        f.write(otf_text(seq.n_cam, seq.volume, *seq.otf_abc))
+    tracer = os.path.join(folder, "tracerConfig.txt")
+    with open(tracer, "w") as f:
+        f.write("\n".join(str(v) for v in [
+            stb.radius_search_obj, stb.n_initial_frames, stb.radius_search_track, ipr.shake_width,
+            stb.pf_nx, stb.pf_ny, stb.pf_nz, stb.pf_r, ipr.n_loop_ipr, ipr.n_shake_loop,
+            ipr.thred_ghost, ipr.tol_2d_px, ipr.tol_3d_mm, ipr.n_cam_reduced,
+            ipr.n_loop_ipr_reduced, ipr.min_obj_int, ipr.radius_obj]) + "\n")
+    main = os.path.join(folder, "config.txt")
+    out_dir = os.path.join(folder, "out") + "/"
+    lines = [f"0,{n_frames - 1}", "1", "0", str(seq.n_cam)]
+    lines += [f"{p},{seq.max_val}" for p in cam_paths]
+    lines += lists
+    lines += [",".join(repr(float(v)) for v in seq.volume), "1.0", out_dir, "Tracer", tracer, "0"]
+    with open(main, "w") as f:
+        f.write("\n".join(lines) + "\n")
+    return main
 
 
 def write_scene_files(scene: Scene, folder: str) -> List[str]:
