@@ -238,6 +238,62 @@ olpt_status_t olpt_ipr_run(olpt_ctx* ctx, const olpt_ipr_params* p, int64_t* n_o
  * their 2D projections uv (n x n_cam x 2); either may be NULL. */
 olpt_status_t olpt_ipr_result(olpt_ctx* ctx, double* xyz, double* uv);
 
+/* ------------------------------------------------------------------ STB */
+/* STB configuration: the tracer's IPR knobs plus STBParam and PFParam
+ * (inc/libSTB/Config.h:17-69) and BasicSetting's frame range and axis limit; all
+ * lengths in mm (the reference multiplies its config values by voxel_to_mm,
+ * src/srcSTB/Config.cpp:195-230).  Replaces STB::STB(setting, "Tracer", cfg_path)
+ * (inc/libSTB/STB.h:38-40) once the config files are read. */
+typedef struct olpt_stb_params {
+  olpt_ipr_params ipr;
+  int frame_start;
+  int frame_end;
+  int n_initial_frames;           /* >= 4 */
+  double radius_search_obj_mm;    /* initial-phase link radius */
+  double radius_search_track_mm;  /* convergence-phase link radius */
+  double limit[6];                /* axis limit: x_min, x_max, y_min, y_max, z_min, z_max */
+  int pf_n[3];                    /* predictive-field grid nodes (>= 2 each) */
+  double pf_r_mm;                 /* predictive-field search half-width */
+  int pf_nbin[3];                 /* displacement PDF bins (reference default 11) */
+  int pf_smooth;                  /* smooth the field (reference default 1) */
+  double pf_sigma[3];             /* smoothing sigma per component (default 1) */
+  const char* output_path;        /* NULL / "": no files; else the reference's outputs
+                                     (InitialTrack/, ConvergeTrack/, PredField_*.csv) */
+} olpt_stb_params;
+
+enum {
+  OLPT_TRACK_LONG_ACTIVE = 0,   /* STB::_long_track_active */
+  OLPT_TRACK_SHORT_ACTIVE = 1,  /* STB::_short_track_active */
+  OLPT_TRACK_LONG_INACTIVE = 2, /* STB::_long_track_inactive */
+  OLPT_TRACK_EXIT = 3           /* STB::_exit_track */
+};
+
+/* Reset the tracker and set its parameters. */
+olpt_status_t olpt_stb_configure(olpt_ctx* ctx, const olpt_stb_params* p);
+/* STB::processFrame(frame_id, img_list) (src/srcSTB/STB.cpp:40-89) on the current
+ * images (olpt_images_upload).  Initial phase: IPR, and at the last initial frame the
+ * predictive-field linking; convergence phase: predict, shake, IPR on the residual,
+ * repeat check, short-track linking, linear-fit pruning.  The current images end as
+ * residuals. */
+olpt_status_t olpt_stb_process_frame(olpt_ctx* ctx, int frame);
+/* Sizes of the four track lists (indexed by OLPT_TRACK_*), and the particles of the
+ * last frame: predictions extended and new IPR objects (either pointer may be NULL). */
+olpt_status_t olpt_stb_counts(olpt_ctx* ctx, int64_t counts[4], int64_t* n_extended,
+                              int64_t* n_new);
+/* Number of tracks and of points (rows) in one list. */
+olpt_status_t olpt_stb_track_rows(olpt_ctx* ctx, int which, int64_t* n_tracks, int64_t* n_rows);
+/* The rows of one list in the order of STB::saveTracks: track id (= position in the
+ * list), frame id, x, y, z. capacity_rows bounds the output. */
+olpt_status_t olpt_stb_get_tracks(olpt_ctx* ctx, int which, int32_t* track_id, int32_t* frame,
+                                  double* xyz, int64_t capacity_rows);
+/* Replace one list by rows (track ids index the list, as in STB::loadTracks). */
+olpt_status_t olpt_stb_set_tracks(olpt_ctx* ctx, int which, const int32_t* track_id,
+                                  const int32_t* frame, const double* xyz, int64_t n_rows);
+/* STB::saveTracks / loadTracks (src/srcSTB/STB.cpp:967-1047) for one list, in the
+ * reference's CSV format. */
+olpt_status_t olpt_stb_save_tracks(olpt_ctx* ctx, int which, const char* path);
+olpt_status_t olpt_stb_load_tracks(olpt_ctx* ctx, int which, const char* path);
+
 #ifdef __cplusplus
 }
 #endif

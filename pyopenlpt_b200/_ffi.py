@@ -294,6 +294,49 @@ class Context:
         self._check(self.L.olpt_ipr_result(self.h, _p(xyz), _p(uv)))
         return xyz, uv
 
+    # ---------------------------------------------------------------- STB
+    def stb_configure(self, params: "StbParams"):
+        self._stb_params = params  # keeps output_path alive
+        self._check(self.L.olpt_stb_configure(self.h, C.byref(params)))
+
+    def stb_process_frame(self, frame: int):
+        self._check(self.L.olpt_stb_process_frame(self.h, int(frame)))
+
+    def stb_counts(self):
+        """(sizes of long_active, short_active, long_inactive, exit), n_extended, n_new"""
+        c = (C.c_int64 * 4)()
+        ne = C.c_int64()
+        nn = C.c_int64()
+        self._check(self.L.olpt_stb_counts(self.h, c, C.byref(ne), C.byref(nn)))
+        return tuple(c), ne.value, nn.value
+
+    def stb_tracks(self, which: int):
+        """Rows of one track list: (track_id int32, frame int32, xyz (n, 3))."""
+        nt = C.c_int64()
+        nr = C.c_int64()
+        self._check(self.L.olpt_stb_track_rows(self.h, which, C.byref(nt), C.byref(nr)))
+        n = nr.value
+        tid = np.empty(n, np.int32)
+        fr = np.empty(n, np.int32)
+        xyz = np.empty((n, 3))
+        self._check(self.L.olpt_stb_get_tracks(self.h, which, tid.ctypes.data_as(C.c_void_p),
+                                               fr.ctypes.data_as(C.c_void_p), _p(xyz), C.c_int64(n)))
+        return tid, fr, xyz
+
+    def stb_set_tracks(self, which: int, tid, frame, xyz):
+        tid = np.ascontiguousarray(tid, dtype=np.int32)
+        frame = np.ascontiguousarray(frame, dtype=np.int32)
+        xyz = np.ascontiguousarray(xyz, dtype=np.float64).reshape(-1, 3)
+        self._check(self.L.olpt_stb_set_tracks(self.h, which, tid.ctypes.data_as(C.c_void_p),
+                                               frame.ctypes.data_as(C.c_void_p), _p(xyz),
+                                               C.c_int64(len(tid))))
+
+    def stb_save_tracks(self, which: int, path: str):
+        self._check(self.L.olpt_stb_save_tracks(self.h, which, str(path).encode()))
+
+    def stb_load_tracks(self, which: int, path: str):
+        self._check(self.L.olpt_stb_load_tracks(self.h, which, str(path).encode()))
+
     # ---------------------------------------------------------------- profiling
     def stream(self) -> int:
         s = C.c_void_p()
@@ -311,7 +354,10 @@ class Context:
         return ms.value, n.value, b.value
 
 
-PROF_PEAKS, PROF_STEREO, PROF_RESIDUAL, PROF_SHAKE = 0, 1, 2, 3
+PROF_PEAKS, PROF_STEREO, PROF_RESIDUAL, PROF_SHAKE, PROF_PF = 0, 1, 2, 3, 4
+# host phases (wall clock): id = PROF_N + phase
+PROF_N = 5
+PH_DETECT, PH_STEREO, PH_PRUNE, PH_SHAKE, PH_OUTPUT, PH_TRACK = range(PROF_N, PROF_N + 6)
 
 
 class IprParams(C.Structure):
@@ -325,3 +371,34 @@ def ipr_params(settings, limit, precision: int = 0) -> IprParams:
                      shake=shake_params(settings, precision), n_cam_reduced=settings.n_cam_reduced,
                      n_loop_ipr=settings.n_loop_ipr, n_loop_ipr_reduced=settings.n_loop_ipr_reduced,
                      n_obj2d_process_max=settings.n_obj2d_process_max)
+
+
+TRACK_LONG_ACTIVE, TRACK_SHORT_ACTIVE, TRACK_LONG_INACTIVE, TRACK_EXIT = 0, 1, 2, 3
+TRACK_LISTS = ("long_active", "short_active", "long_inactive", "exit")
+
+
+class StbParams(C.Structure):
+    _fields_ = [("ipr", IprParams), ("frame_start", C.c_int), ("frame_end", C.c_int),
+                ("n_initial_frames", C.c_int), ("radius_search_obj_mm", C.c_double),
+                ("radius_search_track_mm", C.c_double), ("limit", C.c_double * 6),
+                ("pf_n", C.c_int * 3), ("pf_r_mm", C.c_double), ("pf_nbin", C.c_int * 3),
+                ("pf_smooth", C.c_int), ("pf_sigma", C.c_double * 3),
+                ("output_path", C.c_char_p)]
+
+
+def stb_params(ipr_settings, stb_settings, limit, frame_start: int, frame_end: int,
+               precision: int = 0, output_path: Optional[str] = None) -> StbParams:
+    """STB parameters from IPR/STB knobs in mm (voxel_to_mm already applied)."""
+    p = StbParams(ipr=ipr_params(ipr_settings, limit, precision), frame_start=frame_start,
+                  frame_end=frame_end, n_initial_frames=stb_settings.n_initial_frames,
+                  radius_search_obj_mm=stb_settings.radius_search_obj,
+                  radius_search_track_mm=stb_settings.radius_search_track,
+                  pf_r_mm=stb_settings.pf_r, pf_smooth=1,
+                  output_path=None if output_path is None else str(output_path).encode())
+    for i in range(6):
+        p.limit[i] = limit[i]
+    p.pf_n[0], p.pf_n[1], p.pf_n[2] = stb_settings.pf_nx, stb_settings.pf_ny, stb_settings.pf_nz
+    for i in range(3):
+        p.pf_nbin[i] = 11
+        p.pf_sigma[i] = 1.0
+    return p

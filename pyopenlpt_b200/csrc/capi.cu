@@ -719,24 +719,38 @@ olpt_status_t olpt_residual(olpt_ctx* ctx, const olpt_shake_params* p, int use_f
   });
 }
 
+}  // extern "C"
+
+namespace olpt {
+namespace {
+IprParams to_ipr_params(const olpt_ipr_params* p) {
+  OLPT_REQUIRE(p->shake.precision == 0 || p->shake.precision == 1, OLPT_ERR_INVALID_ARG,
+               "precision must be 0 (FP32) or 1 (FP64)");
+  IprParams ip;
+  ip.min_obj_int = p->min_obj_int;
+  ip.sm.match_cam_count = p->sm.match_cam_count;
+  ip.sm.idmap_cell_px = p->sm.idmap_cell_px;
+  ip.sm.tol_2d_px = p->sm.tol_2d_px;
+  ip.sm.tol_3d_mm = p->sm.tol_3d_mm;
+  for (int q = 0; q < 6; ++q) ip.sm.limit[q] = p->sm.limit[q];
+  ip.shake = to_shake_params(&p->shake);
+  ip.n_cam_reduced = p->n_cam_reduced;
+  ip.n_loop_ipr = p->n_loop_ipr;
+  ip.n_loop_ipr_reduced = p->n_loop_ipr_reduced;
+  ip.n_obj2d_process_max = p->n_obj2d_process_max;
+  return ip;
+}
+}  // namespace
+}  // namespace olpt
+
+extern "C" {
+
 olpt_status_t olpt_ipr_run(olpt_ctx* ctx, const olpt_ipr_params* p, int64_t* n_objects) {
   return guard(ctx, [&] {
     OLPT_REQUIRE(p, OLPT_ERR_INVALID_ARG, "null params");
     OLPT_REQUIRE(p->shake.precision == 0 || p->shake.precision == 1, OLPT_ERR_INVALID_ARG,
                  "precision must be 0 (FP32) or 1 (FP64)");
-    IprParams ip;
-    ip.min_obj_int = p->min_obj_int;
-    ip.sm.match_cam_count = p->sm.match_cam_count;
-    ip.sm.idmap_cell_px = p->sm.idmap_cell_px;
-    ip.sm.tol_2d_px = p->sm.tol_2d_px;
-    ip.sm.tol_3d_mm = p->sm.tol_3d_mm;
-    for (int q = 0; q < 6; ++q) ip.sm.limit[q] = p->sm.limit[q];
-    ip.shake = to_shake_params(&p->shake);
-    ip.n_cam_reduced = p->n_cam_reduced;
-    ip.n_loop_ipr = p->n_loop_ipr;
-    ip.n_loop_ipr_reduced = p->n_loop_ipr_reduced;
-    ip.n_obj2d_process_max = p->n_obj2d_process_max;
-    ipr_device(ctx, ip);
+    ipr_device(ctx, to_ipr_params(p));
     if (n_objects) *n_objects = ctx->ipr.n_out;
   });
 }
@@ -774,6 +788,100 @@ olpt_status_t olpt_residual_download(olpt_ctx* ctx, int cam, olpt_dtype_t dtype,
     OLPT_CUDA(cudaMemcpyAsync(out, ctx->scratch.p, n * esize(dtype), cudaMemcpyDeviceToHost,
                               ctx->stream));
     OLPT_CUDA(cudaStreamSynchronize(ctx->stream));
+  });
+}
+
+olpt_status_t olpt_stb_configure(olpt_ctx* ctx, const olpt_stb_params* p) {
+  return guard(ctx, [&] {
+    OLPT_REQUIRE(p, OLPT_ERR_INVALID_ARG, "null params");
+    OLPT_REQUIRE(ctx->n_cam >= 2, OLPT_ERR_INVALID_ARG, "upload at least 2 cameras first");
+    StbParams sp;
+    sp.frame_start = p->frame_start;
+    sp.frame_end = p->frame_end;
+    sp.n_initial_frames = p->n_initial_frames;
+    sp.radius_search_obj = p->radius_search_obj_mm;
+    sp.radius_search_track = p->radius_search_track_mm;
+    for (int q = 0; q < 6; ++q) sp.limit[q] = p->limit[q];
+    for (int k = 0; k < 3; ++k) {
+      sp.pf_n[k] = p->pf_n[k];
+      sp.pf_nbin[k] = p->pf_nbin[k];
+      sp.pf_sigma[k] = p->pf_sigma[k];
+    }
+    sp.pf_r = p->pf_r_mm;
+    sp.pf_smooth = p->pf_smooth;
+    sp.output_path = p->output_path ? p->output_path : "";
+    stb_configure(ctx, sp, to_ipr_params(&p->ipr));
+  });
+}
+
+olpt_status_t olpt_stb_process_frame(olpt_ctx* ctx, int frame) {
+  return guard(ctx, [&] { stb_process_frame(ctx, frame); });
+}
+
+olpt_status_t olpt_stb_counts(olpt_ctx* ctx, int64_t counts[4], int64_t* n_extended,
+                              int64_t* n_new) {
+  return guard(ctx, [&] {
+    if (counts)
+      for (int w = 0; w < 4; ++w) counts[w] = (int64_t)stb_list(ctx, w).size();
+    if (n_extended) *n_extended = ctx->stb.last_extended;
+    if (n_new) *n_new = ctx->stb.last_new;
+  });
+}
+
+olpt_status_t olpt_stb_track_rows(olpt_ctx* ctx, int which, int64_t* n_tracks, int64_t* n_rows) {
+  return guard(ctx, [&] {
+    const auto& L = stb_list(ctx, which);
+    int64_t r = 0;
+    for (const auto& t : L) r += (int64_t)t.size();
+    if (n_tracks) *n_tracks = (int64_t)L.size();
+    if (n_rows) *n_rows = r;
+  });
+}
+
+olpt_status_t olpt_stb_get_tracks(olpt_ctx* ctx, int which, int32_t* track_id, int32_t* frame,
+                                  double* xyz, int64_t capacity_rows) {
+  return guard(ctx, [&] {
+    const auto& L = stb_list(ctx, which);
+    int64_t r = 0;
+    for (size_t i = 0; i < L.size(); ++i)
+      for (size_t k = 0; k < L[i].size(); ++k, ++r) {
+        OLPT_REQUIRE(r < capacity_rows, OLPT_ERR_INVALID_ARG, "output capacity too small");
+        if (track_id) track_id[r] = (int32_t)i;
+        if (frame) frame[r] = L[i].t[k];
+        if (xyz)
+          for (int d = 0; d < 3; ++d) xyz[3 * r + d] = L[i].xyz[3 * k + d];
+      }
+  });
+}
+
+olpt_status_t olpt_stb_set_tracks(olpt_ctx* ctx, int which, const int32_t* track_id,
+                                  const int32_t* frame, const double* xyz, int64_t n_rows) {
+  return guard(ctx, [&] {
+    OLPT_REQUIRE(n_rows >= 0 && (n_rows == 0 || (track_id && frame && xyz)), OLPT_ERR_INVALID_ARG,
+                 "bad track rows");
+    auto& L = stb_list(ctx, which);
+    L.clear();
+    for (int64_t r = 0; r < n_rows; ++r) {
+      OLPT_REQUIRE(track_id[r] >= 0, OLPT_ERR_INVALID_ARG, "negative track id");
+      while ((int64_t)L.size() <= track_id[r]) L.emplace_back();
+      TrackH& t = L[track_id[r]];
+      t.xyz.insert(t.xyz.end(), xyz + 3 * r, xyz + 3 * r + 3);
+      t.t.push_back(frame[r]);
+    }
+  });
+}
+
+olpt_status_t olpt_stb_save_tracks(olpt_ctx* ctx, int which, const char* path) {
+  return guard(ctx, [&] {
+    OLPT_REQUIRE(path, OLPT_ERR_INVALID_ARG, "null path");
+    stb_save_tracks(ctx, which, path);
+  });
+}
+
+olpt_status_t olpt_stb_load_tracks(olpt_ctx* ctx, int which, const char* path) {
+  return guard(ctx, [&] {
+    OLPT_REQUIRE(path, OLPT_ERR_INVALID_ARG, "null path");
+    stb_load_tracks(ctx, which, path);
   });
 }
 

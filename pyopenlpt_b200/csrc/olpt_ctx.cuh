@@ -12,6 +12,7 @@
 #include "olpt_device.cuh"
 #include "olpt_prof.h"
 #include "olpt_shake.h"
+#include "olpt_stb.h"
 #include "olpt_stereo.h"
 
 namespace olpt {
@@ -224,6 +225,38 @@ OtfView otf_view(olpt_ctx* ctx);
 void shake_device(olpt_ctx* ctx, const ShakeParams& sp);
 void residual_device(olpt_ctx* ctx, const ShakeParams& sp, bool use_flags, bool make_current);
 
+// Device workspace of the STB frame loop (grown on demand, reused across frames).
+struct StbWork {
+  DevBuf a, b, c, d, ia, link, flag, field, field2, kern, k1, k2;
+  Csr g1, g2;
+  void release(cudaStream_t s) {
+    for (DevBuf* x : {&a, &b, &c, &d, &ia, &link, &flag, &field, &field2, &kern, &k1, &k2})
+      x->release(s);
+    g1.release(s);
+    g2.release(s);
+  }
+};
+
+// STB state (STB members, inc/libSTB/STB.h:58-70): the four track lists and the
+// initial-phase IPR results.
+struct StbState {
+  StbParams p;
+  IprParams ipr;
+  bool configured = false;
+  std::deque<TrackH> short_active, long_active, long_inactive, exited;
+  std::vector<std::vector<double>> ipr_xyz;   // initial phase, per frame
+  std::vector<std::vector<char>> ipr_tracked;
+  std::vector<double> linfit_kernel;          // 2 x n_pts
+  int64_t last_new = 0, last_extended = 0;
+  StbWork w;
+};
+
+void stb_configure(olpt_ctx* ctx, const StbParams& p, const IprParams& ipr);
+void stb_process_frame(olpt_ctx* ctx, int frame);
+std::deque<TrackH>& stb_list(olpt_ctx* ctx, int which);
+void stb_save_tracks(olpt_ctx* ctx, int which, const std::string& path);
+void stb_load_tracks(olpt_ctx* ctx, int which, const std::string& path);
+
 }  // namespace olpt
 
 struct olpt_ctx {
@@ -261,6 +294,9 @@ struct olpt_ctx {
 
   // IPR workspace and output
   olpt::IprWork ipr;
+
+  // Shake-the-Box frame loop
+  olpt::StbState stb;
 
   // optional per-kernel event timing
   olpt::Prof prof;

@@ -15,7 +15,8 @@ enum ProfKernel : int {
   PROF_STEREO = 1,    // stereo level expansion (all levels)
   PROF_RESIDUAL = 2,  // tile-owned residual image
   PROF_SHAKE = 3,     // warp-per-particle shake
-  PROF_N = 4
+  PROF_PF = 4,        // predictive-field nodes (STB initial phase)
+  PROF_N = 5
 };
 
 // Host wall-clock phases (ids PROF_N + phase in olpt_profile_read).
@@ -25,13 +26,14 @@ enum ProfPhase : int {
   PH_PRUNE = 2,    // host candidate sort + prune
   PH_SHAKE = 3,    // whole shake (all iterations + flags)
   PH_OUTPUT = 4,   // compaction of kept objects + final residual
-  PH_N = 5
+  PH_TRACK = 5,    // STB track bookkeeping, prediction, linking and pruning
+  PH_N = 6
 };
 
 struct Prof {
   bool on = false;
-  double phase_ms[PH_N] = {0, 0, 0, 0, 0};
-  long long phase_n[PH_N] = {0, 0, 0, 0, 0};
+  double phase_ms[PH_N] = {};
+  long long phase_n[PH_N] = {};
   struct Rec {
     cudaEvent_t a, b;
     double bytes;

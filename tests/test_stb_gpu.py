@@ -1,0 +1,173 @@
+"""STB frame-loop parity (STB::processFrame, src/srcSTB/STB.cpp:40-696): the four
+track lists against the reference after every frame of a seeded Burgers-vortex
+sequence, with the FP64 and the FP32 shake; the predictive field and the track
+files the reference writes (PredField_*.csv, InitialTrack/, ConvergeTrack/);
+saveTracks -> loadTracks round trip."""
+import functools
+import os
+import tempfile
+
+import numpy as np
+import pytest
+from scipy.spatial import cKDTree
+
+from pyopenlpt_b200 import _ffi, synth
+
+pytestmark = pytest.mark.gpu
+
+N_FRAMES = 8
+
+
+@functools.lru_cache(maxsize=None)
+def _seq():
+    return synth.make_sequence(n_particles=2000, n_frames=N_FRAMES, n_row=512, n_col=512,
+                               focal=2500.0, volume=(-20, 20, -20, 20, -10, 10), a=200.0,
+                               noise=2.0, bits=8, gamma=4e3, r_core=6.0, drift=(5.0, 0.0, 0.0),
+                               seed=3)
+
+
+def _settings(seq):
+    ipr = synth.IPRSettings(n_loop_ipr=2, n_shake_loop=2)
+    ipr.match_cam_count = min(ipr.match_cam_count, seq.n_cam)
+    stb = synth.STBSettings(radius_search_obj=1.0, radius_search_track=1.0, pf_nx=9, pf_ny=9,
+                            pf_nz=5, pf_r=3.0)
+    return ipr, stb
+
+
+@functools.lru_cache(maxsize=None)
+def _ref_run():
+    from oracle.ref import RefSTB
+    seq = _seq()
+    ipr, stb = _settings(seq)
+    r = RefSTB(seq, ipr, stb, threads=0)
+    out = []
+    for t in range(N_FRAMES):
+        r.frame(t)
+        out.append(r.tracks())
+    r.close()
+    return out, os.path.join(r._tmp, "out")
+
+
+def _gpu_run(precision, out_dir=None):
+    from oracle.ref import otf_table
+    seq = _seq()
+    ipr, stb = _settings(seq)
+    ctx = _ffi.Context(0)
+    ctx.upload_cameras([_ffi.camera_desc_from_pinhole(c) for c in seq.cams])
+    ctx.upload_otf(2, 2, 2, seq.volume, otf_table(seq.n_cam, seq.otf_abc))
+    ctx.stb_configure(_ffi.stb_params(ipr, stb, seq.volume, 0, N_FRAMES - 1, precision,
+                                      None if out_dir is None else out_dir + "/"))
+    out = []
+    for t in range(N_FRAMES):
+        ctx.upload_images(seq.frames[t])
+        ctx.stb_process_frame(t)
+        lists = {}
+        for w, name in enumerate(_ffi.TRACK_LISTS):
+            tid, fr, xyz = ctx.stb_tracks(w)
+            lists[name] = np.column_stack([tid, fr, xyz]).astype(np.float64).reshape(-1, 5)
+        out.append(lists)
+    return ctx, out
+
+
+def _tracks(rows):
+    """rows (n, 5): track id, frame, x, y, z -> list of (frames, xyz) per track."""
+    if len(rows) == 0:
+        return []
+    ids = rows[:, 0].astype(np.int64)
+    cut = np.flatnonzero(np.diff(ids)) + 1
+    return [(g[:, 1].astype(np.int64), g[:, 2:5]) for g in np.split(rows, cut)]
+
+
+def _reproduced(ref_rows, gpu_rows, tol):
+    """Fraction of reference tracks found among the GPU tracks with the same frames
+    and every point within tol (matched on the first point)."""
+    rt, gt = _tracks(ref_rows), _tracks(gpu_rows)
+    if not rt:
+        return 1.0 if not gt else 0.0
+    if not gt:
+        return 0.0
+    tree = cKDTree(np.array([g[1][0] for g in gt]))
+    hit = 0
+    for fr, xyz in rt:
+        for j in tree.query_ball_point(xyz[0], tol):
+            gf, gx = gt[j]
+            if len(gf) == len(fr) and np.array_equal(gf, fr) and np.max(np.abs(gx - xyz)) <= tol:
+                hit += 1
+                break
+    return hit / len(rt)
+
+
+def test_stb_fp64_tracks_match_reference():
+    ref, _ = _ref_run()
+    _, gpu = _gpu_run(1)
+    for t in range(N_FRAMES):
+        for name in _ffi.TRACK_LISTS:
+            a, b = ref[t][name], gpu[t][name]
+            na = len(_tracks(a))
+            nb = len(_tracks(b))
+            frac = _reproduced(a, b, 1e-6)
+            print(f"frame {t} {name:13s}: ref {na:5d} tracks gpu {nb:5d} reproduced {frac:.4f}")
+            assert abs(na - nb) <= max(2, 0.01 * na), (t, name, na, nb)
+            assert frac >= 0.98, (t, name, frac)
+
+
+def test_stb_fp32_track_counts_close():
+    ref, _ = _ref_run()
+    _, gpu = _gpu_run(0)
+    t = N_FRAMES - 1
+    for name in ("long_active", "short_active"):
+        na = len(_tracks(ref[t][name]))
+        nb = len(_tracks(gpu[t][name]))
+        frac = _reproduced(ref[t][name], gpu[t][name], 1e-4)
+        print(f"fp32 frame {t} {name}: ref {na} gpu {nb} reproduced within 1e-4 mm {frac:.4f}")
+        assert abs(na - nb) <= max(5, 0.03 * na)
+        assert frac >= 0.9
+
+
+def _read_csv(path):
+    with open(path) as f:
+        lines = f.read().splitlines()
+    return lines[0], lines[1:]
+
+
+def test_stb_output_files_match_reference():
+    _, ref_dir = _ref_run()
+    with tempfile.TemporaryDirectory() as d:
+        _gpu_run(1, out_dir=d)
+        # predictive fields of the initial phase
+        pf = sorted(f for f in os.listdir(ref_dir) if f.startswith("PredField_"))
+        assert pf and pf == sorted(f for f in os.listdir(d) if f.startswith("PredField_"))
+        for f in pf:
+            a = np.loadtxt(os.path.join(ref_dir, f), delimiter=",")
+            b = np.loadtxt(os.path.join(d, f), delimiter=",")
+            print(f"{f}: max |diff| {np.max(np.abs(a - b)):.3e} mm, nonzero nodes "
+                  f"{np.count_nonzero(np.any(a != 0, axis=1))}")
+            assert a.shape == b.shape and np.allclose(a, b, rtol=0, atol=1e-9)
+        for sub in ("InitialTrack", "ConvergeTrack"):
+            names = sorted(os.listdir(os.path.join(ref_dir, sub)))
+            assert names == sorted(os.listdir(os.path.join(d, sub))), sub
+            for f in names:
+                ha, ra = _read_csv(os.path.join(ref_dir, sub, f))
+                hb, rb = _read_csv(os.path.join(d, sub, f))
+                assert ha == hb
+                same = sum(x == y for x, y in zip(ra, rb)) / max(1, len(ra))
+                print(f"{sub}/{f}: {len(ra)} rows ref, {len(rb)} gpu, identical lines {same:.4f}")
+                assert abs(len(ra) - len(rb)) <= max(8, 0.01 * len(ra))
+                assert same >= 0.95 or len(ra) == 0
+
+
+def test_stb_save_load_round_trip():
+    ctx, gpu = _gpu_run(1)
+    with tempfile.TemporaryDirectory() as d:
+        p = os.path.join(d, "long.csv")
+        ctx.stb_save_tracks(_ffi.TRACK_LONG_ACTIVE, p)
+        tid, fr, xyz = ctx.stb_tracks(_ffi.TRACK_LONG_ACTIVE)
+        ctx.stb_load_tracks(_ffi.TRACK_SHORT_ACTIVE, p)
+        tid2, fr2, xyz2 = ctx.stb_tracks(_ffi.TRACK_SHORT_ACTIVE)
+        assert np.array_equal(tid, tid2) and np.array_equal(fr, fr2)
+        assert np.max(np.abs(xyz - xyz2)) <= 5e-7  # six decimals in the file
+        # the file's 2D columns are the projections of the stored points
+        rows = np.loadtxt(p, delimiter=",", skiprows=1).reshape(-1, 5 + 2 * ctx.n_cam)
+        for c in range(ctx.n_cam):
+            uv = ctx.project(c, xyz)
+            assert np.max(np.abs(rows[:, 5 + 2 * c:7 + 2 * c] - uv)) <= 5e-7
