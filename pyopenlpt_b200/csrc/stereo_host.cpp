@@ -1,21 +1,33 @@
 // Host half of stereo matching: canonical candidate order and the greedy prune.
 //
 // StereoMatch::pruneMatch (src/srcSTB/StereoMatch.cpp:631-980) is an
-// order-dependent greedy whose comparators use a relative tolerance and are not a
-// strict weak ordering; the ranks it produces depend on the exact merge sequence of
-// libstdc++'s std::stable_sort.  It therefore runs here, calling the same
-// std::stable_sort with the same comparators, which keeps the selection identical
-// to the reference's.  The data layout is flat (CSR point -> candidate lists), and
-// the per-point percentile pass runs on all host threads: every point writes its own
-// slots, and each candidate then sums its slots in ascending point order -- the
-// order in which the reference accumulates pct_sum -- so the floating-point sums are
-// unchanged.  All numerical geometry (detection, lines of sight, strip search,
-// triangulation) stays on the device.
+// order-dependent greedy whose comparators use a relative tolerance; such a
+// comparator is not a strict weak ordering in general, and then the ranks depend on
+// the exact merge sequence of libstdc++'s std::stable_sort.  The reference's result
+// is kept bit-for-bit as follows:
+//  * per 2D point, the candidate pools are small: they are sorted with the same
+//    std::stable_sort and comparator as the reference, from the same input order;
+//  * the global order of the candidates by (percentile, e_check, index) is only
+//    needed for the candidates the greedy can take (finite percentile and e_check).
+//    The values are grouped into tolerance classes (runs of neighbours within the
+//    tolerance in sorted order).  When every class is within the tolerance end to
+//    end, the tolerance relation is an equivalence on the data, the comparator is a
+//    strict weak ordering made total by the index, and stable_sort's output is the
+//    unique sorted order by (class, class, index): that order is produced here by
+//    parallel sorts.  Otherwise the reference's std::stable_sort runs as is.
+// Point -> candidate lists are built in parallel; every per-point pool is put into
+// ascending candidate order, the order in which the reference appends to it, and
+// each candidate sums its per-point percentiles in ascending point order, as the
+// reference accumulates pct_sum.  All numerical geometry (detection, lines of sight,
+// strip search, triangulation) stays on the device.
 #include <omp.h>
+#include <parallel/algorithm>
 
 #include <algorithm>
+#include <atomic>
 #include <cmath>
 #include <cstdint>
+#include <cstring>
 #include <limits>
 #include <numeric>
 #include <utility>
@@ -24,36 +36,52 @@
 #include "olpt_stereo.h"
 
 namespace olpt {
+namespace {
+
+// Sorts by a strict total order on all host threads (libstdc++ parallel mode).
+template <class It, class Cmp>
+void par_sort(It b, It e, Cmp cmp) {
+  __gnu_parallel::sort(b, e, cmp);
+}
+
+}  // namespace
 
 void sort_candidates(StereoResult& r) {
   const int n = r.n_cam;
   const size_t M = r.e.size();
-  std::vector<size_t> ord(M);
   const int* ids = r.ids.data();
   // ids are compared lexicographically (camera 0 first, -1 < any id); with
-  // 21 bits per camera the key of up to 6 cameras fits in 128 bits.
+  // 21 bits per camera the key of up to 6 cameras fits in 128 bits.  Candidate id
+  // sets are unique, so the order is total.
   int max_id = 0;
   for (size_t q = 0; q < r.ids.size(); ++q) max_id = std::max(max_id, ids[q]);
+  std::vector<int> ord(M);
   if (n <= 6 && max_id < (1 << 21) - 2) {
-    std::vector<std::pair<unsigned __int128, uint32_t>> key(M);
-    for (size_t j = 0; j < M; ++j) {
+    std::vector<std::pair<unsigned __int128, int>> key(M);
+#pragma omp parallel for schedule(static)
+    for (int64_t j = 0; j < (int64_t)M; ++j) {
       unsigned __int128 k = 0;
       for (int c = 0; c < n; ++c) k = (k << 21) | (unsigned __int128)(ids[j * n + c] + 1);
-      key[j] = {k, (uint32_t)j};
+      key[j] = {k, (int)j};
     }
-    std::sort(key.begin(), key.end(),
-              [](const auto& a, const auto& b) { return a.first < b.first; });
+    par_sort(key.begin(), key.end(), [](const auto& a, const auto& b) {
+      return a.first < b.first || (a.first == b.first && a.second < b.second);
+    });
     for (size_t i = 0; i < M; ++i) ord[i] = key[i].second;
   } else {
     std::iota(ord.begin(), ord.end(), 0);
-    std::sort(ord.begin(), ord.end(), [&](size_t a, size_t b) {
-      return std::lexicographical_compare(ids + a * n, ids + a * n + n, ids + b * n,
-                                          ids + b * n + n);
+    par_sort(ord.begin(), ord.end(), [&](int a, int b) {
+      const bool lt = std::lexicographical_compare(ids + (size_t)a * n, ids + (size_t)a * n + n,
+                                                   ids + (size_t)b * n, ids + (size_t)b * n + n);
+      const bool gt = std::lexicographical_compare(ids + (size_t)b * n, ids + (size_t)b * n + n,
+                                                   ids + (size_t)a * n, ids + (size_t)a * n + n);
+      return lt || (!gt && a < b);
     });
   }
   std::vector<int> ids2(r.ids.size());
   std::vector<double> e2(M), X2(3 * M);
-  for (size_t i = 0; i < M; ++i) {
+#pragma omp parallel for schedule(static)
+  for (int64_t i = 0; i < (int64_t)M; ++i) {
     const size_t j = ord[i];
     std::copy(ids + j * n, ids + j * n + n, ids2.begin() + i * n);
     e2[i] = r.e[j];
@@ -69,7 +97,7 @@ void sort_candidates(StereoResult& r) {
 void prune_candidates(StereoResult& r, const std::vector<int>& det_counts,
                       const std::vector<int>& active) {
   const size_t M = r.e.size();
-  const int n_cams = r.n_cam;
+  const int n = r.n_cam;
   r.selected.assign(M, 0);
   if (M == 0) return;
   const double rtol = 1e-9, atol = 1e-12;
@@ -80,182 +108,242 @@ void prune_candidates(StereoResult& r, const std::vector<int>& det_counts,
   const double swap_pct_margin = 1e-12, swap_err_margin = 1e-12;
   const std::vector<double>& e_checks = r.e;
 
-  std::vector<size_t> cam_offsets(n_cams + 1, 0);
-  for (int c = 0; c < n_cams; ++c) cam_offsets[c + 1] = cam_offsets[c] + det_counts[c];
-  const size_t total_points = cam_offsets.back();
+  std::vector<int64_t> cam_offsets(n + 1, 0);
+  for (int c = 0; c < n; ++c) cam_offsets[c + 1] = cam_offsets[c] + det_counts[c];
+  const int64_t total_points = cam_offsets.back();
 
-  // Step 1: flat 2D point indices per candidate (ascending: camera order)
-  std::vector<int> foff(M + 1, 0);
-  std::vector<int64_t> flat;
-  flat.reserve(M * n_cams);
-  for (size_t j = 0; j < M; ++j) {
-    for (int c = 0; c < n_cams; ++c) {
+  // Step 1: the candidate's 2D points (global point index, ascending = camera order),
+  // fixed width n; slot j*n+k
+  std::vector<int> fl(M * n, -1);
+  std::vector<uint8_t> fcnt(M);
+#pragma omp parallel for schedule(static)
+  for (int64_t j = 0; j < (int64_t)M; ++j) {
+    int k = 0;
+    for (int c = 0; c < n; ++c) {
       if (!active[c]) continue;
-      const int pid = r.ids[j * n_cams + c];
+      const int pid = r.ids[j * n + c];
       if (pid < 0 || pid >= det_counts[c]) continue;
-      flat.push_back((int64_t)(cam_offsets[c] + (size_t)pid));
+      fl[j * n + k++] = (int)(cam_offsets[c] + pid);
     }
-    foff[j + 1] = (int)flat.size();
+    fcnt[j] = (uint8_t)k;
   }
-  // Step 2: point -> candidates (ascending j), with the slot of the point in the candidate
+  // Step 2: point -> (candidate, slot) lists
+  std::vector<std::atomic<int>> pcount(total_points + 1);
+  for (auto& a : pcount) a.store(0, std::memory_order_relaxed);
+#pragma omp parallel for schedule(static)
+  for (int64_t j = 0; j < (int64_t)M; ++j)
+    for (int k = 0; k < fcnt[j]; ++k) pcount[fl[j * n + k] + 1].fetch_add(1, std::memory_order_relaxed);
   std::vector<int> poff(total_points + 1, 0);
-  for (int64_t f : flat) ++poff[f + 1];
-  for (size_t f = 0; f < total_points; ++f) poff[f + 1] += poff[f];
-  std::vector<int> pc_j(flat.size()), pc_slot(flat.size());
-  {
-    std::vector<int> cur(poff.begin(), poff.end() - 1);
-    for (size_t j = 0; j < M; ++j)
-      for (int q = foff[j]; q < foff[j + 1]; ++q) {
-        const int64_t f = flat[q];
-        pc_j[cur[f]] = (int)j;
-        pc_slot[cur[f]] = q;
-        ++cur[f];
-      }
-  }
-  // Step 3: percentile of every (point, candidate) pair, written to the candidate's slot
-  std::vector<double> slot_pct(flat.size(), 0.0);
-  std::vector<char> slot_used(flat.size(), 0);
+  for (int64_t f = 0; f < total_points; ++f) poff[f + 1] = poff[f] + pcount[f + 1].load();
+  for (int64_t f = 0; f < total_points; ++f) pcount[f].store(poff[f], std::memory_order_relaxed);
+  std::vector<int> pc_slot(poff[total_points]);
+#pragma omp parallel for schedule(static)
+  for (int64_t j = 0; j < (int64_t)M; ++j)
+    for (int k = 0; k < fcnt[j]; ++k) {
+      const int pos = pcount[fl[j * n + k]].fetch_add(1, std::memory_order_relaxed);
+      pc_slot[pos] = (int)(j * n + k);
+    }
+  // Step 3: percentile of every (point, candidate) pair, written to the slot
+  std::vector<double> slot_pct(M * n, 0.0);
+  std::vector<char> slot_used(M * n, 0);
 #pragma omp parallel
   {
-    std::vector<std::pair<double, int>> pool;
-    std::vector<int> pool_slot;
+    struct Item {
+      double e;
+      int j, slot;
+    };
+    std::vector<Item> pool;
 #pragma omp for schedule(dynamic, 256)
-    for (int64_t f = 0; f < (int64_t)total_points; ++f) {
+    for (int64_t f = 0; f < total_points; ++f) {
       const int b = poff[f], e = poff[f + 1];
       if (b == e) continue;
+      // the reference appends candidates to the point's pool in ascending j
+      std::sort(pc_slot.begin() + b, pc_slot.begin() + e);
       pool.clear();
       for (int q = b; q < e; ++q) {
-        const int j = pc_j[q];
+        const int slot = pc_slot[q];
+        const int j = slot / n;
         const double ej = e_checks[j];
-        if (std::isfinite(ej)) pool.emplace_back(ej, j);
+        if (std::isfinite(ej)) pool.push_back({ej, j, slot});
       }
-      const int n = (int)pool.size();
-      if (n == 0) continue;
-      auto slot_of = [&](int j) {
-        for (int q = b; q < e; ++q)
-          if (pc_j[q] == j) return pc_slot[q];
-        return -1;
-      };
-      if (n == 1) {
-        const int s = slot_of(pool[0].second);
-        slot_pct[s] = 0.0;
-        slot_used[s] = 1;
+      const int np = (int)pool.size();
+      if (np == 0) continue;
+      if (np == 1) {
+        slot_pct[pool[0].slot] = 0.0;
+        slot_used[pool[0].slot] = 1;
         continue;
       }
-      std::stable_sort(pool.begin(), pool.end(), [&](const auto& A, const auto& B) {
-        if (!eq_eps(A.first, B.first)) return A.first < B.first;
-        return A.second < B.second;
+      std::stable_sort(pool.begin(), pool.end(), [&](const Item& A, const Item& B) {
+        if (!eq_eps(A.e, B.e)) return A.e < B.e;
+        return A.j < B.j;
       });
       int k = 0;
-      while (k < n) {
+      while (k < np) {
         int k0 = k, k1 = k + 1;
-        while (k1 < n && eq_eps(pool[k1].first, pool[k0].first)) ++k1;
+        while (k1 < np && eq_eps(pool[k1].e, pool[k0].e)) ++k1;
         const double avg_rank = 0.5 * (double)(k0 + (k1 - 1));
-        const double denom = (double)(n - 1);
+        const double denom = (double)(np - 1);
         const double pct = (denom > 0.0) ? (avg_rank / denom) : 0.0;
         for (int t = k0; t < k1; ++t) {
-          const int s = slot_of(pool[t].second);
-          slot_pct[s] = pct;
-          slot_used[s] = 1;
+          slot_pct[pool[t].slot] = pct;
+          slot_used[pool[t].slot] = 1;
         }
         k = k1;
       }
     }
   }
-  // per candidate: sum over its points in ascending point order (the reference's order)
+  // per candidate: sum over its points in ascending point order
   std::vector<double> pct_score(M, std::numeric_limits<double>::infinity());
 #pragma omp parallel for schedule(static)
   for (int64_t j = 0; j < (int64_t)M; ++j) {
     double sum = 0.0;
     int cnt = 0;
-    for (int q = foff[j]; q < foff[j + 1]; ++q)
-      if (slot_used[q]) {
-        sum += slot_pct[q];
+    for (int k = 0; k < fcnt[j]; ++k)
+      if (slot_used[j * n + k]) {
+        sum += slot_pct[j * n + k];
         ++cnt;
       }
     if (cnt > 0) pct_score[j] = sum / (double)cnt;
   }
-  // Step 4: order by (pct, e_check, index)
-  std::vector<int> order(M);
-  std::iota(order.begin(), order.end(), 0);
-  std::stable_sort(order.begin(), order.end(), [&](int aj, int bj) {
-    const double pa = pct_score[aj], pb = pct_score[bj];
-    const bool af = std::isfinite(pa), bf = std::isfinite(pb);
-    if (af && bf) {
-      if (!eq_eps(pa, pb)) return pa < pb;
-    } else if (af) {
-      return true;
-    } else if (bf) {
-      return false;
-    }
-    const double ea = e_checks[aj], eb = e_checks[bj];
-    const bool aef = std::isfinite(ea), bef = std::isfinite(eb);
-    if (aef && bef) {
-      if (!eq_eps(ea, eb)) return ea < eb;
-    } else if (aef) {
-      return true;
-    } else if (bef) {
-      return false;
-    }
-    return aj < bj;
-  });
-  // Step 5: greedy exclusive ownership with local replacement
-  std::vector<int> owner(total_points, -1);
-  std::vector<char>& selected = r.selected;
-  auto place = [&](int cand) {
-    for (int q = foff[cand]; q < foff[cand + 1]; ++q) owner[flat[q]] = cand;
-    selected[cand] = 1;
-  };
-  auto clear_owner_of = [&](int cand) {
-    for (int q = foff[cand]; q < foff[cand + 1]; ++q)
-      if (owner[flat[q]] == cand) owner[flat[q]] = -1;
-    selected[cand] = 0;
-  };
-  std::vector<int> S;
-  for (int j : order) {
-    if (!std::isfinite(pct_score[j]) || !std::isfinite(e_checks[j])) continue;
-    if (foff[j] == foff[j + 1]) continue;
-    bool conflict = false;
-    for (int q = foff[j]; q < foff[j + 1]; ++q)
-      if (owner[flat[q]] != -1) {
-        conflict = true;
-        break;
+
+  // Step 4: the greedy order of the candidates it can take, by (pct, e_check, index)
+  std::vector<int> order;
+  {
+    // tolerance classes of the finite values; false when a class is wider than the
+    // tolerance end to end
+    auto classes = [&](const std::vector<int>& items, const std::vector<double>& val,
+                       std::vector<int>& cls) -> int {
+      std::vector<std::pair<double, int>> v(items.size());
+      for (size_t i = 0; i < items.size(); ++i) v[i] = {val[items[i]], items[i]};
+      par_sort(v.begin(), v.end(), [](const auto& a, const auto& b) {
+        return a.first < b.first || (a.first == b.first && a.second < b.second);
+      });
+      int c = -1;
+      double first = 0.0, prev = 0.0;
+      for (size_t i = 0; i < v.size(); ++i) {
+        const double x = v[i].first;
+        if (i == 0 || !eq_eps(prev, x)) {
+          ++c;
+          first = x;
+        } else if (!eq_eps(first, x)) {
+          return -1;
+        }
+        cls[v[i].second] = c;
+        prev = x;
       }
-    if (!conflict) {
-      place(j);
-      continue;
+      return c + 1;
+    };
+    std::vector<int> fin_pct;  // finite percentile (the comparator's consistent part)
+    for (size_t j = 0; j < M; ++j)
+      if (std::isfinite(pct_score[j])) fin_pct.push_back((int)j);
+    std::vector<int> fin_both;
+    for (int j : fin_pct)
+      if (std::isfinite(e_checks[j])) fin_both.push_back(j);
+    std::vector<int> pcls(M, 0), ecls(M, 0);
+    const int n_pc = classes(fin_pct, pct_score, pcls);
+    const int n_ec = n_pc < 0 ? -1 : classes(fin_both, e_checks, ecls);
+    if (n_pc >= 0 && n_ec >= 0) {
+      std::vector<std::pair<uint64_t, int>> key(fin_both.size());
+      for (size_t i = 0; i < fin_both.size(); ++i) {
+        const int j = fin_both[i];
+        key[i] = {((uint64_t)pcls[j] << 32) | (uint64_t)ecls[j], j};
+      }
+      par_sort(key.begin(), key.end(), [](const auto& a, const auto& b) {
+        return a.first < b.first || (a.first == b.first && a.second < b.second);
+      });
+      order.resize(key.size());
+      for (size_t i = 0; i < key.size(); ++i) order[i] = key[i].second;
+    } else {
+      // the reference's sort, verbatim in its comparator
+      std::vector<int> all(M);
+      std::iota(all.begin(), all.end(), 0);
+      std::stable_sort(all.begin(), all.end(), [&](int aj, int bj) {
+        const double pa = pct_score[aj], pb = pct_score[bj];
+        const bool af = std::isfinite(pa), bf = std::isfinite(pb);
+        if (af && bf) {
+          if (!eq_eps(pa, pb)) return pa < pb;
+        } else if (af) {
+          return true;
+        } else if (bf) {
+          return false;
+        }
+        const double ea = e_checks[aj], eb = e_checks[bj];
+        const bool aef = std::isfinite(ea), bef = std::isfinite(eb);
+        if (aef && bef) {
+          if (!eq_eps(ea, eb)) return ea < eb;
+        } else if (aef) {
+          return true;
+        } else if (bef) {
+          return false;
+        }
+        return aj < bj;
+      });
+      for (int j : all)
+        if (std::isfinite(pct_score[j]) && std::isfinite(e_checks[j])) order.push_back(j);
     }
-    S.clear();
-    for (int q = foff[j]; q < foff[j + 1]; ++q) {
-      const int o = owner[flat[q]];
+  }
+
+  // Step 5: greedy exclusive ownership with local replacement, over the candidates
+  // gathered in greedy order (owner holds the position in that order)
+  const int64_t G = (int64_t)order.size();
+  std::vector<int> g_pts((size_t)G * n);
+  std::vector<uint8_t> g_cnt(G);
+  std::vector<double> g_pct(G), g_e(G);
+#pragma omp parallel for schedule(static)
+  for (int64_t i = 0; i < G; ++i) {
+    const int j = order[i];
+    g_cnt[i] = fcnt[j];
+    for (int k = 0; k < n; ++k) g_pts[i * n + k] = fl[(size_t)j * n + k];
+    g_pct[i] = pct_score[j];
+    g_e[i] = e_checks[j];
+  }
+  std::vector<int> owner(total_points, -1);
+  std::vector<char> sel(G, 0);
+  auto place = [&](int64_t i) {
+    for (int k = 0; k < g_cnt[i]; ++k) owner[g_pts[i * n + k]] = (int)i;
+    sel[i] = 1;
+  };
+  auto clear_owner_of = [&](int o) {
+    for (int k = 0; k < g_cnt[o]; ++k)
+      if (owner[g_pts[(int64_t)o * n + k]] == o) owner[g_pts[(int64_t)o * n + k]] = -1;
+    sel[o] = 0;
+  };
+  std::vector<int> S_buf(std::max(n, 1));
+  int* S = S_buf.data();
+  for (int64_t i = 0; i < G; ++i) {
+    const int cnt_i = g_cnt[i];
+    if (cnt_i == 0) continue;
+    const int* P = &g_pts[i * n];
+    int ns = 0;
+    for (int k = 0; k < cnt_i; ++k) {
+      const int o = owner[P[k]];
       if (o == -1) continue;
-      if (std::find(S.begin(), S.end(), o) == S.end()) S.push_back(o);
+      bool seen = false;
+      for (int t = 0; t < ns; ++t) seen |= (S[t] == o);
+      if (!seen) S[ns++] = o;
     }
-    if (S.empty()) {
-      place(j);
+    if (ns == 0) {
+      place(i);
       continue;
     }
     double avg_pct = 0.0, avg_err = 0.0;
-    int cnt = 0;
-    for (int o : S) {
-      const double po = pct_score[o], eo = e_checks[o];
-      if (!std::isfinite(po) || !std::isfinite(eo)) continue;
-      avg_pct += po;
-      avg_err += eo;
-      ++cnt;
+    for (int t = 0; t < ns; ++t) {  // owners are always finite in both
+      avg_pct += g_pct[S[t]];
+      avg_err += g_e[S[t]];
     }
-    if (cnt == 0) continue;
-    avg_pct /= (double)cnt;
-    avg_err /= (double)cnt;
-    const double pj = pct_score[j], ej = e_checks[j];
+    avg_pct /= (double)ns;
+    avg_err /= (double)ns;
+    const double pj = g_pct[i], ej = g_e[i];
     const bool better_pct = (!eq_eps(pj, avg_pct)) && ((pj + swap_pct_margin) < avg_pct);
     const bool tie_better = eq_eps(pj, avg_pct) && (!eq_eps(ej, avg_err)) &&
                             ((ej + swap_err_margin) < avg_err);
     if (better_pct || tie_better) {
-      for (int o : S) clear_owner_of(o);
-      place(j);
+      for (int t = 0; t < ns; ++t) clear_owner_of(S[t]);
+      place(i);
     }
   }
+  for (int64_t i = 0; i < G; ++i)
+    if (sel[i]) r.selected[order[i]] = 1;
 }
 
 }  // namespace olpt
