@@ -1,16 +1,22 @@
 #!/usr/bin/env python
-"""Throughput of the OpenLPT IPR hot path (detection -> stereo matching -> shake ->
-residual, looped) on B200, against the reference CPU implementation.
+"""Throughput of the OpenLPT hot path on B200 against the reference CPU implementation.
 
-Metric: particles/s (IPR+shake) = 3D particles reconstructed per second of
-IPR::runIPR on one synthetic frame.  One step = one full IPR run (all outer loops,
-all shake iterations) over the frame's camera images.
+Metric: particles/s (IPR+shake).
+
+* stb_1280x800_u16_51k (default): the Shake-the-Box sequence -- 4 pinhole cameras
+  (f = 5000 px, 45 deg ring of radius 500 mm, 30 deg tilt), 1280x800 12-bit images,
+  51,000 particles in 60x40x30 mm advected by a Burgers vortex plus drift.  After the
+  4-frame initial phase, one step = one convergence-phase STB::processFrame (predict,
+  shake the predictions, IPR on the residual, repeat check, link, linear-fit prune).
+  Particles per step = track points the frame adds over the four track lists.
+* ipr_1024_u8_10k: one step = IPR::runIPR on one 4 x 1024^2 uint8 frame of 10,000
+  particles; particles per step = reconstructed objects.
 
   python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
 
-With N > 1 (torchrun) every rank runs an independent replica of the workload on
-its own GPU ("replicas only": the frame loop has no cross-GPU exchange); value is
-the particles of all ranks divided by the slowest rank's time.
+With N > 1 (torchrun) every rank runs an independent replica of the workload on its
+own GPU ("replicas only": the frame loop has no cross-GPU exchange); value is the
+particles of all ranks divided by the slowest rank's time.
 """
 from __future__ import annotations
 
@@ -31,24 +37,40 @@ sys.path.insert(0, ROOT)
 from pyopenlpt_b200 import synth  # noqa: E402
 
 METRIC = "particles/s (IPR+shake)"
+N_INIT = 4  # STB initial-phase frames
 
 WORKLOADS = {
-    # The single-frame IPR scene: 4 pinhole cameras (f = 5000 px, 45 deg ring, 30 deg
-    # tilt), 1024^2 uint8, 10,000 particles in 40x40x20 mm, a=200, b=c=0.5, sigma=2;
+    # 4 x 1280x800 12-bit (a=3000, b=c=0.5, noise 20), 51,000 particles, Burgers vortex
+    # (circulation 2e4 mm^2/s, core 8 mm, strain 2/s) + 20 mm/s drift, <= 3 px/frame.
+    # IPR: threshold 300, shake width 0.025 mm (0.25 px), 4 loops x 4 shakes, tol_2d 1 px,
+    # tol_3d 0.06 mm; STB: 4 initial frames, link radii 1 mm, field 11x11x6, r 3 mm.
+    "stb_1280x800_u16_51k": dict(kind="stb", seq=dict(), settings=dict(min_obj_int=300,
+                                                                       shake_width=0.025),
+                                 stb=dict()),
+    # 4 x 1024^2 uint8 (a=200, b=c=0.5, noise 2), 10,000 particles in 40x40x20 mm;
     # 4 IPR loops x 4 shake iterations, shake width 0.25 mm, threshold 30, tol_2d 1 px.
-    "ipr_1024_u8_10k": dict(scene=dict(n_particles=10000, n_cam=4, size=1024, focal=5000.0,
-                                       a=200.0, b=0.5, c=0.5, noise=2.0, bits=8),
+    "ipr_1024_u8_10k": dict(kind="ipr", scene=dict(n_particles=10000, n_cam=4, size=1024,
+                                                   focal=5000.0, a=200.0, b=0.5, c=0.5,
+                                                   noise=2.0, bits=8),
                             settings=dict()),
 }
-DEFAULT_WORKLOAD = "ipr_1024_u8_10k"
+DEFAULT_WORKLOAD = "stb_1280x800_u16_51k"
+
+
+def ipr_settings(name: str, n_cam: int):
+    s = synth.IPRSettings(**WORKLOADS[name]["settings"])
+    s.match_cam_count = min(s.match_cam_count, n_cam)
+    return s
 
 
 def build_scene(name: str, seed: int):
-    w = WORKLOADS[name]
-    sc = synth.make_scene(seed=seed, **w["scene"])
-    s = synth.IPRSettings(**w["settings"])
-    s.match_cam_count = min(s.match_cam_count, sc.n_cam)
-    return sc, s
+    sc = synth.make_scene(seed=seed, **WORKLOADS[name]["scene"])
+    return sc, ipr_settings(name, sc.n_cam)
+
+
+def build_sequence(name: str, seed: int, n_frames: int):
+    seq = synth.make_sequence(n_frames=n_frames, seed=seed, **WORKLOADS[name]["seq"])
+    return seq, ipr_settings(name, seq.n_cam), synth.STBSettings(**WORKLOADS[name]["stb"])
 
 
 # ----------------------------------------------------------------------------- clocks
@@ -135,11 +157,11 @@ class _MuteStdout:
         return False
 
 
-def reference_ipr_time(sc, s, threads: int):
+def reference_ipr_time(sc, s, threads: int, images=None):
     """Wall time of the reference IPR::runIPR on this host (compiled from source)."""
     from oracle.ref import RefOracle
     ref = RefOracle(sc, s, threads=threads)
-    imgs = [im.astype(np.float64) for im in sc.images]
+    imgs = [im.astype(np.float64) for im in (images if images is not None else sc.images)]
     with _MuteStdout():
         t = time.perf_counter()
         out = ref.ipr(imgs)
@@ -148,28 +170,57 @@ def reference_ipr_time(sc, s, threads: int):
     return len(out["xyz"]), dt
 
 
+REF_STB_BUDGET_S = 240.0  # convergence frames of the reference arm stop after this
+
+
 def run_reference(args):
     rank = int(os.environ.get("RANK", "0"))
     if rank != 0:
         return 0
-    sc, s = build_scene(args.workload, 1234)
     threads = os.cpu_count() or 1
+    kind = WORKLOADS[args.workload]["kind"]
     times, counts = [], []
-    for i in range(args.warmup + args.steps):
-        n, dt = reference_ipr_time(sc, s, threads)
-        if i >= args.warmup:
-            times.append(dt)
-            counts.append(n)
+    if kind == "ipr":
+        sc, s = build_scene(args.workload, 1234)
+        for i in range(args.warmup + args.steps):
+            n, dt = reference_ipr_time(sc, s, threads)
+            if i >= args.warmup:
+                times.append(dt)
+                counts.append(n)
+        cfg = workload_config(args.workload, s, sc=sc)
+        sample = "whole frame per step (IPR::runIPR, OpenMP, all host threads)"
+    else:
+        from oracle.ref import RefSTB
+        nf = N_INIT + args.steps
+        seq, s, st = build_sequence(args.workload, 1234, nf)
+        with _MuteStdout():
+            ref = RefSTB(seq, s, st, threads=threads)
+            t_start = time.perf_counter()
+            for t in range(nf):
+                a = time.perf_counter()
+                ref.frame(t)
+                dt = time.perf_counter() - a
+                if t >= N_INIT:
+                    rows = ref.tracks()
+                    times.append(dt)
+                    counts.append(sum(int(np.count_nonzero(v[:, 1] == t)) for v in rows.values()
+                                      if len(v)))
+                    if time.perf_counter() - t_start > REF_STB_BUDGET_S:
+                        break
+            ref.close()
+        cfg = workload_config(args.workload, s, seq=seq, st=st)
+        sample = (f"STB::processFrame: {N_INIT} initial-phase frames untimed, then "
+                  f"{len(times)} convergence-phase frames timed (stops after "
+                  f"{REF_STB_BUDGET_S:.0f} s); OpenMP, all host threads")
     value = sum(counts) / sum(times)
     line = {
         "impl": "reference", "metric": METRIC, "value": value, "unit": "particles/s",
-        "n_gpus": args.gpus, "steps": args.steps, "warmup": args.warmup,
+        "n_gpus": args.gpus, "steps": len(times), "warmup": args.warmup,
         "ms_per_step": 1e3 * sum(times) / len(times), "higher_is_better": True,
         "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
-        "config": workload_config(args.workload, sc, s),
+        "config": cfg,
         "cpu_baseline": {"value": value, "unit": "particles/s", "cores": threads,
-                         "kind": "reference",
-                         "sample": "whole frame per step (IPR::runIPR, OpenMP, all host threads)"},
+                         "kind": "reference", "sample": sample},
         "e2e": {"value": value, "unit": "particles/s", "h2d_bytes_per_step": 0,
                 "d2h_bytes_per_step": 0},
     }
@@ -177,43 +228,118 @@ def run_reference(args):
     return 0
 
 
-def workload_config(name, sc, s):
-    H, W = sc.images[0].shape
-    return {"workload": name, "particles": int(len(sc.xyz)), "cameras": sc.n_cam,
-            "image": f"{H}x{W} {sc.images[0].dtype}", "ipr_loops": s.n_loop_ipr,
-            "shake_loops": s.n_shake_loop, "shake_width_mm": s.shake_width,
+def workload_config(name, s, sc=None, seq=None, st=None):
+    base = {"workload": name, "ipr_loops": s.n_loop_ipr, "shake_loops": s.n_shake_loop,
+            "shake_width_mm": s.shake_width, "threshold": s.min_obj_int,
             "tol_2d_px": s.tol_2d_px, "tol_3d_mm": s.tol_3d_mm, "parallelism": "replicas",
-            "l2": "flushed (256 MiB write) between timed steps"}
+            "l2": "flushed (256 MiB write) before every timed step"}
+    if sc is not None:
+        H, W = sc.images[0].shape
+        base.update(particles=int(len(sc.xyz)), cameras=sc.n_cam,
+                    image=f"{H}x{W} {sc.images[0].dtype}")
+    else:
+        H, W = seq.frames[0][0].shape
+        base.update(particles=int(len(seq.truth[0])), cameras=seq.n_cam,
+                    image=f"{H}x{W} {seq.frames[0][0].dtype} ({int(seq.max_val).bit_length()}-bit)",
+                    initial_frames=N_INIT, link_radius_mm=st.radius_search_track,
+                    pred_field=f"{st.pf_nx}x{st.pf_ny}x{st.pf_nz} r {st.pf_r} mm",
+                    step="one convergence-phase frame")
+    return base
 
 
 # ----------------------------------------------------------------------------- our arm
-def run_ours(args):
-    import torch
-    import torch.distributed as dist
+PROF_NAMES = {0: "peak detection", 1: "stereo level expansion", 2: "residual image",
+              3: "shake (warp per particle)", 4: "predictive field"}
+
+
+class Ours:
+    """One rank of our arm: device set-up, rank reduction and the JSON line."""
+
+    def __init__(self, args):
+        import torch
+        import torch.distributed as dist
+        self.torch, self.dist, self.args = torch, dist, args
+        self.rank = int(os.environ.get("RANK", "0"))
+        self.world = int(os.environ.get("WORLD_SIZE", "1"))
+        self.local = int(os.environ.get("LOCAL_RANK", "0"))
+        torch.cuda.set_device(self.local)
+        if self.world > 1:
+            import datetime
+            dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120),
+                                    device_id=torch.device("cuda", self.local))
+        self.prec = 1 if args.precision == "fp64" else 0
+        self.flush = torch.empty(256 * 1024 * 1024, dtype=torch.uint8, device="cuda")
+
+    def barrier(self):
+        if self.world > 1:
+            self.dist.barrier()
+
+    def context(self, cams, volume, otf_abc):
+        from pyopenlpt_b200 import _ffi
+        ctx = _ffi.Context(self.local)
+        ctx.upload_cameras([_ffi.camera_desc_from_pinhole(c) for c in cams])
+        ctx.upload_otf(2, 2, 2, volume, synth.otf_table_array(len(cams), otf_abc))
+        return ctx
+
+    def reduce(self, dev_ms, parts, e2e_s, e2e_parts):
+        torch, dist = self.torch, self.dist
+        vals = torch.tensor([dev_ms, float(parts), e2e_s, float(e2e_parts)], dtype=torch.float64,
+                            device="cuda")
+        if self.world == 1:
+            return dev_ms, float(parts), e2e_s, float(e2e_parts)
+        tmax = vals.clone()
+        dist.all_reduce(tmax, op=dist.ReduceOp.MAX)
+        tsum = vals.clone()
+        dist.all_reduce(tsum, op=dist.ReduceOp.SUM)
+        return tmax[0].item(), tsum[1].item(), tmax[2].item(), tsum[3].item()
+
+    def line(self, prof, dev_ms, parts, e2e_s, e2e_parts, bi, bo, launches, clk, cfg, cpu,
+             extra):
+        args = self.args
+        peak, peak_kind = measured_peak_hbm()
+        # dominant HBM-bound kernel: the largest share of device time among the
+        # streaming kernels (detection, residual, shake)
+        cand = {k: prof[k] for k in (0, 2, 3) if prof[k][1] > 0}
+        dom = max(cand, key=lambda k: cand[k][0]) if cand else 2
+        ms, nl, by = prof[dom]
+        achieved = (by / nl) / ((ms / nl) * 1e-3) / 1e9 if nl and ms > 0 else 0.0
+        kernel_ms = {PROF_NAMES[k]: round(prof[k][0] / args.steps, 4) for k in PROF_NAMES}
+        line = {
+            "metric": METRIC, "value": parts / (dev_ms * 1e-3), "unit": "particles/s",
+            "n_gpus": self.world, "steps": args.steps, "warmup": args.warmup,
+            "ms_per_step": dev_ms / args.steps, "higher_is_better": True,
+            "scaling": "weak", "vs_baseline": None,
+            "dtype": "f32" if self.prec == 0 else "f64", "data": "synthetic",
+            "config": dict(cfg, precision="fp32 residual/shake, fp64 geometry"
+                           if self.prec == 0 else "fp64"),
+            "frames_per_s": self.world * args.steps / (dev_ms * 1e-3),
+            "e2e": {"value": e2e_parts / e2e_s, "unit": "particles/s",
+                    "h2d_bytes_per_step": bi, "d2h_bytes_per_step": bo},
+            "gpu_launches": int(launches),
+            "kernel_ms_per_step": kernel_ms,
+            "roofline": {"bound": "hbm", "kernel": PROF_NAMES[dom], "achieved": achieved,
+                         "peak": peak, "unit": "GB/s", "frac": achieved / peak,
+                         "peak_source": peak_kind,
+                         "bytes_per_launch": by / nl if nl else 0.0,
+                         "launch_ms": ms / nl if nl else 0.0, "traffic": None},
+            "cpu_baseline": cpu,
+            "clocks": clk,
+        }
+        line.update(extra)
+        print(json.dumps(line), flush=True)
+
+
+def run_ours_ipr(args, o: Ours):
     from pyopenlpt_b200 import _ffi
-
-    rank = int(os.environ.get("RANK", "0"))
-    world = int(os.environ.get("WORLD_SIZE", "1"))
-    local = int(os.environ.get("LOCAL_RANK", "0"))
-    torch.cuda.set_device(local)
-    if world > 1:
-        import datetime
-        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120),
-                                device_id=torch.device("cuda", local))
-
-    sc, s = build_scene(args.workload, 1234 + rank)
-    prec = 1 if args.precision == "fp64" else 0
-    ctx = _ffi.Context(local)
-    ctx.upload_cameras([_ffi.camera_desc_from_pinhole(c) for c in sc.cams])
-    from pyopenlpt_b200.synth import otf_table_array
-    ctx.upload_otf(2, 2, 2, sc.volume, otf_table_array(sc.n_cam, sc.otf_abc))
-    params = _ffi.ipr_params(s, sc.volume, prec)
+    torch = o.torch
+    sc, s = build_scene(args.workload, 1234 + o.rank)
+    ctx = o.context(sc.cams, sc.volume, sc.otf_abc)
+    params = _ffi.ipr_params(s, sc.volume, o.prec)
     H, W = sc.images[0].shape
     dtype = _ffi._DTYPES[sc.images[0].dtype]
     dev_imgs = [torch.from_numpy(im).cuda() for im in sc.images]
     host_imgs = [torch.from_numpy(im).pin_memory() for im in sc.images]
     stream = torch.cuda.ExternalStream(ctx.stream())
-    flush = torch.empty(256 * 1024 * 1024, dtype=torch.uint8, device="cuda")
     torch.cuda.synchronize()
 
     def step_device():
@@ -221,33 +347,19 @@ def run_ours(args):
                                  [W] * sc.n_cam)
         return ctx.ipr_run(params)
 
-    def step_e2e():
-        ctx.upload_images([t.numpy() for t in host_imgs])
-        n = ctx.ipr_run(params)
-        xyz, uv = ctx.ipr_result(n)
-        return n, xyz, uv
-
-    def barrier():
-        if world > 1:
-            dist.barrier()
-
     for _ in range(args.warmup):
         step_device()
     torch.cuda.synchronize()
-
-    # ---- device-resident timed region
-    clocks = ClockSampler(local)
+    clocks = ClockSampler(o.local)
     clocks.start()
     ctx.profile(True)
-    barrier()
+    o.barrier()
     torch.cuda.synchronize()
     launches0 = _ffi.launch_count()
-    t_wall = time.perf_counter()
-    dev_ms = 0.0
-    parts = 0
+    dev_ms, parts = 0.0, 0
     for _ in range(args.steps):
         with torch.cuda.stream(stream):
-            flush.zero_()
+            o.flush.zero_()
             e0 = torch.cuda.Event(enable_timing=True)
             e1 = torch.cuda.Event(enable_timing=True)
             e0.record(stream)
@@ -257,87 +369,158 @@ def run_ours(args):
         dev_ms += e0.elapsed_time(e1)
         parts += n
     torch.cuda.synchronize()
-    barrier()
-    wall = time.perf_counter() - t_wall
+    o.barrier()
     launches = _ffi.launch_count() - launches0
-    prof = {k: ctx.profile_read(k) for k in range(4)}
+    prof = {k: ctx.profile_read(k) for k in PROF_NAMES}
     ctx.profile(False)
     clk = clocks.stop()
 
-    # ---- end-to-end through the C ABI with host buffers
-    barrier()
-    torch.cuda.synchronize()
-    e2e_t = 0.0
-    e2e_parts = 0
-    bo = 0
+    # end to end through the C ABI with host buffers
+    o.barrier()
+    e2e_s, e2e_parts, bo = 0.0, 0, 0
     for _ in range(args.steps):
         with torch.cuda.stream(stream):
-            flush.zero_()
+            o.flush.zero_()
         torch.cuda.synchronize()
         t0 = time.perf_counter()
-        n, xyz, uv = step_e2e()
-        e2e_t += time.perf_counter() - t0
+        ctx.upload_images([t.numpy() for t in host_imgs])
+        n = ctx.ipr_run(params)
+        xyz, uv = ctx.ipr_result(n)
+        e2e_s += time.perf_counter() - t0
         e2e_parts += n
         bo += xyz.nbytes + uv.nbytes
-    barrier()
+    o.barrier()
     bi = sum(im.nbytes for im in sc.images)
-
-    # ---- max over ranks
-    vals = torch.tensor([dev_ms, float(parts), e2e_t, float(e2e_parts)], dtype=torch.float64,
-                        device="cuda")
-    if world > 1:
-        tmax = vals.clone()
-        dist.all_reduce(tmax, op=dist.ReduceOp.MAX)
-        tsum = vals.clone()
-        dist.all_reduce(tsum, op=dist.ReduceOp.SUM)
-        dev_ms_max, e2e_max = tmax[0].item(), tmax[2].item()
-        parts_all, e2e_parts_all = tsum[1].item(), tsum[3].item()
-    else:
-        dev_ms_max, e2e_max = dev_ms, e2e_t
-        parts_all, e2e_parts_all = float(parts), float(e2e_parts)
-
-    if rank == 0:
-        peak, peak_kind = measured_peak_hbm()
-        names = {0: "peak detection", 1: "stereo level expansion", 2: "residual image",
-                 3: "shake (warp per particle)"}
-        # dominant HBM-bound kernel: the one with the largest share of device time
-        cand = {k: prof[k] for k in (0, 2, 3) if prof[k][1] > 0}
-        dom = max(cand, key=lambda k: cand[k][0]) if cand else 2
-        ms, nl, by = prof[dom]
-        achieved = (by / nl) / ((ms / nl) * 1e-3) / 1e9 if nl and ms > 0 else 0.0
-        kernel_ms = {names[k]: round(prof[k][0] / args.steps, 4) for k in range(4)}
+    dev_ms, parts, e2e_s, e2e_parts = o.reduce(dev_ms, parts, e2e_s, e2e_parts)
+    if o.rank == 0:
         cpu = None
-        if world == 1 and not args.no_cpu_baseline:
+        if o.world == 1 and not args.no_cpu_baseline:
             threads = os.cpu_count() or 1
             ncpu, tcpu = reference_ipr_time(sc, s, threads)
             cpu = {"value": ncpu / tcpu, "unit": "particles/s", "cores": threads,
                    "kind": "reference",
                    "sample": "one whole frame of the same workload (IPR::runIPR compiled "
                              "from the reference sources, OpenMP)"}
-        line = {
-            "metric": METRIC, "value": parts_all / (dev_ms_max * 1e-3), "unit": "particles/s",
-            "n_gpus": world, "steps": args.steps, "warmup": args.warmup,
-            "ms_per_step": dev_ms_max / args.steps, "higher_is_better": True,
-            "scaling": "weak", "vs_baseline": None,
-            "dtype": "f32" if prec == 0 else "f64", "data": "synthetic",
-            "config": dict(workload_config(args.workload, sc, s),
-                           precision="fp32 residual/shake, fp64 geometry" if prec == 0 else "fp64"),
-            "frames_per_s": world * args.steps / (dev_ms_max * 1e-3),
-            "wall_s": wall,
-            "e2e": {"value": e2e_parts_all / e2e_max, "unit": "particles/s",
-                    "h2d_bytes_per_step": bi, "d2h_bytes_per_step": bo // max(1, args.steps)},
-            "gpu_launches": int(launches),
-            "kernel_ms_per_step": kernel_ms,
-            "roofline": {"bound": "hbm", "kernel": names[dom], "achieved": achieved,
-                         "peak": peak, "unit": "GB/s", "frac": achieved / peak,
-                         "peak_source": peak_kind, "traffic": None},
-            "cpu_baseline": cpu,
-            "clocks": clk,
-        }
-        print(json.dumps(line), flush=True)
+        o.line(prof, dev_ms, parts, e2e_s, e2e_parts, bi, bo // max(1, args.steps), launches,
+               clk, workload_config(args.workload, s, sc=sc), cpu, {})
     ctx.close()
-    if world > 1:
-        dist.destroy_process_group()
+
+
+def run_ours_stb(args, o: Ours):
+    from pyopenlpt_b200 import _ffi
+    torch = o.torch
+    nf = N_INIT + args.warmup + args.steps
+    seq, s, st = build_sequence(args.workload, 1234 + o.rank, nf)
+    H, W = seq.frames[0][0].shape
+    C = seq.n_cam
+    dtype = _ffi._DTYPES[seq.frames[0][0].dtype]
+    dev_frames = [torch.from_numpy(np.stack(f)).cuda() for f in seq.frames]
+    host_frames = [torch.from_numpy(np.stack(f)).pin_memory() for f in seq.frames]
+    params = _ffi.stb_params(s, st, seq.volume, 0, nf - 1, o.prec)
+
+    def new_ctx():
+        ctx = o.context(seq.cams, seq.volume, seq.otf_abc)
+        ctx.stb_configure(params)
+        return ctx
+
+    ctx = new_ctx()
+    stream = torch.cuda.ExternalStream(ctx.stream())
+    torch.cuda.synchronize()
+
+    def frame_device(t):
+        ctx.upload_images_device([dev_frames[t][c].data_ptr() for c in range(C)], dtype,
+                                 [H] * C, [W] * C)
+        ctx.stb_process_frame(t)
+
+    init_ms = []
+    for t in range(N_INIT):
+        a = time.perf_counter()
+        frame_device(t)
+        init_ms.append(1e3 * (time.perf_counter() - a))
+    for t in range(N_INIT, N_INIT + args.warmup):
+        frame_device(t)
+    torch.cuda.synchronize()
+
+    clocks = ClockSampler(o.local)
+    clocks.start()
+    ctx.profile(True)
+    o.barrier()
+    torch.cuda.synchronize()
+    launches0 = _ffi.launch_count()
+    dev_ms, parts, ext_new = 0.0, 0, 0
+    t0_frame = N_INIT + args.warmup
+    for t in range(t0_frame, nf):
+        with torch.cuda.stream(stream):
+            o.flush.zero_()
+            e0 = torch.cuda.Event(enable_timing=True)
+            e1 = torch.cuda.Event(enable_timing=True)
+            e0.record(stream)
+        frame_device(t)
+        e1.record(stream)
+        e1.synchronize()
+        dev_ms += e0.elapsed_time(e1)
+        parts += ctx.stb_frame_points(t)
+        _, ne, nn = ctx.stb_counts()
+        ext_new += ne + nn
+    torch.cuda.synchronize()
+    o.barrier()
+    launches = _ffi.launch_count() - launches0
+    prof = {k: ctx.profile_read(k) for k in PROF_NAMES}
+    ctx.profile(False)
+    clk = clocks.stop()
+    lists, _, _ = ctx.stb_counts()
+    ctx.close()
+
+    # end to end through the C ABI with host (pinned) images: a second tracker over the
+    # same frames; each timed step uploads the frame, processes it and reads back the
+    # frame's particles
+    ctx = new_ctx()
+    stream = torch.cuda.ExternalStream(ctx.stream())
+    for t in range(t0_frame):
+        ctx.upload_images(list(host_frames[t].numpy()))
+        ctx.stb_process_frame(t)
+    o.barrier()
+    e2e_s, e2e_parts, bo = 0.0, 0, 0
+    for t in range(t0_frame, nf):
+        with torch.cuda.stream(stream):
+            o.flush.zero_()
+        torch.cuda.synchronize()
+        a = time.perf_counter()
+        ctx.upload_images(list(host_frames[t].numpy()))
+        ctx.stb_process_frame(t)
+        xyz = ctx.stb_frame_objects()
+        e2e_s += time.perf_counter() - a
+        e2e_parts += ctx.stb_frame_points(t)
+        bo += xyz.nbytes
+    o.barrier()
+    ctx.close()
+    bi = C * H * W * seq.frames[0][0].itemsize
+    dev_ms, parts, e2e_s, e2e_parts = o.reduce(dev_ms, parts, e2e_s, e2e_parts)
+    if o.rank == 0:
+        cpu = None
+        if o.world == 1 and not args.no_cpu_baseline:
+            threads = os.cpu_count() or 1
+            ncpu, tcpu = reference_ipr_time(seq, s, threads, images=seq.frames[0])
+            cpu = {"value": ncpu / tcpu, "unit": "particles/s", "cores": threads,
+                   "kind": "reference",
+                   "sample": "IPR::runIPR on frame 0 of the same sequence (the work of an "
+                             "initial-phase STB::processFrame), compiled from the reference "
+                             "sources, OpenMP"}
+        extra = {"initial_phase_ms_per_frame": [round(x, 1) for x in init_ms],
+                 "extended_plus_new_per_step": ext_new / args.steps,
+                 "track_lists_after": dict(zip(_ffi.TRACK_LISTS, lists))}
+        o.line(prof, dev_ms, parts, e2e_s, e2e_parts, bi, bo // max(1, args.steps), launches,
+               clk, workload_config(args.workload, s, seq=seq, st=st), cpu, extra)
+
+
+def run_ours(args):
+    o = Ours(args)
+    if WORKLOADS[args.workload]["kind"] == "ipr":
+        run_ours_ipr(args, o)
+    else:
+        run_ours_stb(args, o)
+    if o.world > 1:
+        o.dist.destroy_process_group()
     return 0
 
 

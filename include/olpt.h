@@ -63,9 +63,10 @@ olpt_status_t olpt_sync(olpt_ctx* ctx);
 olpt_status_t olpt_stream(olpt_ctx* ctx, void** stream);
 /* Per-kernel event timing (no reference counterpart; the reference prints clock()
  * CPU time per stage).  kernel: 0 = detection, 1 = stereo level expansion,
- * 2 = residual image, 3 = shake (device time from CUDA events); 4..8 = host
- * wall-clock phases of olpt_ipr_run (detection, stereo matching, candidate sort +
- * prune, shake, output compaction + residual).  read returns the summed duration,
+ * 2 = residual image, 3 = shake, 4 = predictive field (device time from CUDA
+ * events); 5..10 = host wall-clock phases (detection, stereo matching, candidate
+ * sort + prune, shake, output compaction + residual, STB track work outside the
+ * IPR and the shake of predictions).  read returns the summed duration,
  * the number of timed launches/phases and their algorithmic bytes since the last
  * read. */
 olpt_status_t olpt_profile(olpt_ctx* ctx, int enable);
@@ -280,6 +281,14 @@ olpt_status_t olpt_stb_process_frame(olpt_ctx* ctx, int frame);
  * last frame: predictions extended and new IPR objects (either pointer may be NULL). */
 olpt_status_t olpt_stb_counts(olpt_ctx* ctx, int64_t counts[4], int64_t* n_extended,
                               int64_t* n_new);
+/* The particles of the last frame, in list order: the extended long tracks' new
+ * points, then the new objects of the frame (STB::runConvPhase), or the IPR objects
+ * of an initial-phase frame.  Call with xyz = NULL to get n only; else n is the
+ * capacity on input and the count on output. */
+olpt_status_t olpt_stb_frame_objects(olpt_ctx* ctx, int64_t* n, double* xyz);
+/* Number of track points (rows of the track files) with frame id `frame` over the
+ * four lists: after olpt_stb_process_frame(frame), the particles that frame added. */
+olpt_status_t olpt_stb_frame_points(olpt_ctx* ctx, int frame, int64_t* n);
 /* Number of tracks and of points (rows) in one list. */
 olpt_status_t olpt_stb_track_rows(olpt_ctx* ctx, int which, int64_t* n_tracks, int64_t* n_rows);
 /* The rows of one list in the order of STB::saveTracks: track id (= position in the

@@ -310,6 +310,20 @@ class Context:
         self._check(self.L.olpt_stb_counts(self.h, c, C.byref(ne), C.byref(nn)))
         return tuple(c), ne.value, nn.value
 
+    def stb_frame_points(self, frame: int) -> int:
+        """Track points with this frame id over the four lists."""
+        n = C.c_int64(0)
+        self._check(self.L.olpt_stb_frame_points(self.h, int(frame), C.byref(n)))
+        return n.value
+
+    def stb_frame_objects(self) -> np.ndarray:
+        """Particles of the last frame (extended predictions, then new objects)."""
+        n = C.c_int64(0)
+        self._check(self.L.olpt_stb_frame_objects(self.h, C.byref(n), None))
+        xyz = np.empty((n.value, 3))
+        self._check(self.L.olpt_stb_frame_objects(self.h, C.byref(n), _p(xyz)))
+        return xyz
+
     def stb_tracks(self, which: int):
         """Rows of one track list: (track_id int32, frame int32, xyz (n, 3))."""
         nt = C.c_int64()

@@ -2,6 +2,8 @@
 // Declarations and reference citations: include/olpt.h.
 #include <cuda_runtime.h>
 
+#include <algorithm>
+
 #include <cmath>
 #include <new>
 #include <string>
@@ -190,6 +192,7 @@ void olpt_ctx_destroy(olpt_ctx* ctx) {
   ctx->shk.release(ctx->stream);
   ctx->ipr.release(ctx->stream);
   for (int c = 0; c < OLPT_MAX_CAM; ++c) ctx->resid[c].buf.release(ctx->stream);
+  ctx->stb.w.release(ctx->stream);
   ctx->prof.release();
   cudaStreamSynchronize(ctx->stream);
   if (ctx->own_stream) cudaStreamDestroy(ctx->stream);
@@ -825,6 +828,30 @@ olpt_status_t olpt_stb_counts(olpt_ctx* ctx, int64_t counts[4], int64_t* n_exten
       for (int w = 0; w < 4; ++w) counts[w] = (int64_t)stb_list(ctx, w).size();
     if (n_extended) *n_extended = ctx->stb.last_extended;
     if (n_new) *n_new = ctx->stb.last_new;
+  });
+}
+
+olpt_status_t olpt_stb_frame_objects(olpt_ctx* ctx, int64_t* n, double* xyz) {
+  return guard(ctx, [&] {
+    OLPT_REQUIRE(n, OLPT_ERR_INVALID_ARG, "null count");
+    const std::vector<double>& v = ctx->stb.last_xyz;
+    const int64_t m = (int64_t)(v.size() / 3);
+    if (xyz) {
+      OLPT_REQUIRE(*n >= m, OLPT_ERR_INVALID_ARG, "output capacity too small");
+      std::copy(v.begin(), v.end(), xyz);
+    }
+    *n = m;
+  });
+}
+
+olpt_status_t olpt_stb_frame_points(olpt_ctx* ctx, int frame, int64_t* n) {
+  return guard(ctx, [&] {
+    OLPT_REQUIRE(n, OLPT_ERR_INVALID_ARG, "null count");
+    int64_t m = 0;
+    for (int w = 0; w < 4; ++w)
+      for (const auto& tr : stb_list(ctx, w))
+        m += (int64_t)std::count(tr.t.begin(), tr.t.end(), frame);
+    *n = m;
   });
 }
 

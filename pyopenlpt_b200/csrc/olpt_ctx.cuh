@@ -248,6 +248,7 @@ struct StbState {
   std::vector<std::vector<char>> ipr_tracked;
   std::vector<double> linfit_kernel;          // 2 x n_pts
   int64_t last_new = 0, last_extended = 0;
+  std::vector<double> last_xyz;               // particles of the last frame
   StbWork w;
 };
 

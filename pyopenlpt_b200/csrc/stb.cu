@@ -904,6 +904,7 @@ void init_phase(olpt_ctx* ctx, int frame) {
   PhaseTimer pt(ctx->prof, PH_TRACK);
   S.ipr_tracked.emplace_back(xyz.size() / 3, 0);
   S.ipr_xyz.push_back(std::move(xyz));
+  S.last_xyz = S.ipr_xyz.back();
   S.last_new = (int64_t)(S.ipr_xyz.back().size() / 3);
   S.last_extended = 0;
   if (frame - S.p.frame_start != S.p.n_initial_frames - 1) return;
@@ -983,6 +984,7 @@ void conv_phase(olpt_ctx* ctx, int frame) {
 
   // 2. shake the predictions; residual without the ghost / repeated ones; extend
   int64_t extended = 0;
+  S.last_xyz.clear();
   if (n_la > 0) {
     ctx->obj.ensure(n_la, C, s);
     ctx->obj.n = n_la;
@@ -1000,6 +1002,7 @@ void conv_phase(olpt_ctx* ctx, int frame) {
     for (int i = 0; i < n_la; ++i) {
       TrackH& tr = S.long_active[i];
       if (fl[i] == 0) {
+        S.last_xyz.insert(S.last_xyz.end(), &sx[3 * i], &sx[3 * i] + 3);
         tr.xyz.insert(tr.xyz.end(), &sx[3 * i], &sx[3 * i] + 3);
         tr.t.push_back(frame);
         kept.push_back(std::move(tr));
@@ -1142,6 +1145,7 @@ void conv_phase(olpt_ctx* ctx, int frame) {
   }
   S.last_extended = extended;
   S.last_new = n_obj;
+  S.last_xyz.insert(S.last_xyz.end(), oxyz.begin(), oxyz.end());
 
   // every 500 frames the reference writes all tracks and forgets the inactive and
   // exited ones
