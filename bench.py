@@ -250,6 +250,8 @@ def workload_config(name, s, sc=None, seq=None, st=None):
 # ----------------------------------------------------------------------------- our arm
 PROF_NAMES = {0: "peak detection", 1: "stereo level expansion", 2: "residual image",
               3: "shake (warp per particle)", 4: "predictive field"}
+PHASE_NAMES = {5: "detection", 6: "stereo matching (all)", 7: "candidate sort + prune",
+               8: "shake (all)", 9: "output + residual", 10: "STB track work"}
 
 
 class Ours:
@@ -304,6 +306,7 @@ class Ours:
         ms, nl, by = prof[dom]
         achieved = (by / nl) / ((ms / nl) * 1e-3) / 1e9 if nl and ms > 0 else 0.0
         kernel_ms = {PROF_NAMES[k]: round(prof[k][0] / args.steps, 4) for k in PROF_NAMES}
+        phase_ms = {PHASE_NAMES[k]: round(prof[k][0] / args.steps, 3) for k in PHASE_NAMES}
         line = {
             "metric": METRIC, "value": parts / (dev_ms * 1e-3), "unit": "particles/s",
             "n_gpus": self.world, "steps": args.steps, "warmup": args.warmup,
@@ -317,6 +320,7 @@ class Ours:
                     "h2d_bytes_per_step": bi, "d2h_bytes_per_step": bo},
             "gpu_launches": int(launches),
             "kernel_ms_per_step": kernel_ms,
+            "host_phase_ms_per_step": phase_ms,
             "roofline": {"bound": "hbm", "kernel": PROF_NAMES[dom], "achieved": achieved,
                          "peak": peak, "unit": "GB/s", "frac": achieved / peak,
                          "peak_source": peak_kind,
@@ -371,7 +375,7 @@ def run_ours_ipr(args, o: Ours):
     torch.cuda.synchronize()
     o.barrier()
     launches = _ffi.launch_count() - launches0
-    prof = {k: ctx.profile_read(k) for k in PROF_NAMES}
+    prof = {k: ctx.profile_read(k) for k in list(PROF_NAMES) + list(PHASE_NAMES)}
     ctx.profile(False)
     clk = clocks.stop()
 
@@ -465,7 +469,7 @@ def run_ours_stb(args, o: Ours):
     torch.cuda.synchronize()
     o.barrier()
     launches = _ffi.launch_count() - launches0
-    prof = {k: ctx.profile_read(k) for k in PROF_NAMES}
+    prof = {k: ctx.profile_read(k) for k in list(PROF_NAMES) + list(PHASE_NAMES)}
     ctx.profile(False)
     clk = clocks.stop()
     lists, _, _ = ctx.stb_counts()

@@ -193,6 +193,7 @@ void olpt_ctx_destroy(olpt_ctx* ctx) {
   ctx->ipr.release(ctx->stream);
   for (int c = 0; c < OLPT_MAX_CAM; ++c) ctx->resid[c].buf.release(ctx->stream);
   ctx->stb.w.release(ctx->stream);
+  ctx->prune.release(ctx->stream);
   ctx->prof.release();
   cudaStreamSynchronize(ctx->stream);
   if (ctx->own_stream) cudaStreamDestroy(ctx->stream);

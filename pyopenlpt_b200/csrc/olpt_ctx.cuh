@@ -170,6 +170,33 @@ struct StereoWork {
   }
 };
 
+// Per camera: active flag, detection count and offset of its first detection in the
+// global point numbering of the prune.
+struct PruneView {
+  int active[OLPT_MAX_CAM];
+  int count[OLPT_MAX_CAM];
+  int offset[OLPT_MAX_CAM];
+};
+
+// Device workspace of the candidate sort and prune (prune.cu).
+struct PruneWork {
+  DevBuf key, val, key2, val2, hist, scan_tmp;
+  DevBuf ids_s, e_s, X_s;
+  DevBuf fl, slot_key, fcnt, slot_pct, slot_used, pct, flag;
+  DevBuf f_pct, f_both, pos_pct, pos_both, pcls, ecls, newc, excl, cstart;
+  DevBuf g_pts, g_cnt, g_pct, g_e, pool_e, pool_i;
+  Csr points;
+  HostBuf pin;  // pinned staging of the greedy's input
+  void release(cudaStream_t s) {
+    for (DevBuf* b : {&key, &val, &key2, &val2, &hist, &scan_tmp, &ids_s, &e_s, &X_s, &fl,
+                      &slot_key, &fcnt, &slot_pct, &slot_used, &pct, &flag, &f_pct, &f_both,
+                      &pos_pct, &pos_both, &pcls, &ecls, &newc, &excl, &cstart, &g_pts, &g_cnt,
+                      &g_pct, &g_e, &pool_e, &pool_i})
+      b->release(s);
+    points.release(s);
+  }
+};
+
 // 3D objects resident on the device (SoA).
 struct Objects {
   DevBuf xyz;    // n x 3 double
@@ -285,6 +312,7 @@ struct olpt_ctx {
   // stereo matching
   olpt::StereoWork sm;
   olpt::StereoResult sm_result;
+  olpt::PruneWork prune;
 
   // 3D objects (stereo output / shake input and output)
   olpt::Objects obj;

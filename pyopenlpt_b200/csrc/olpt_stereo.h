@@ -28,5 +28,9 @@ struct StereoResult {
 void sort_candidates(StereoResult& r);
 void prune_candidates(StereoResult& r, const std::vector<int>& det_counts,
                       const std::vector<int>& active);
+// The greedy of pruneMatch over candidates in greedy order: g_pts G x n global point
+// indices (g_cnt used), their percentile and e_check; sel[i] = 1 for kept ones.
+void greedy_select(int64_t G, int n, const int* g_pts, const uint8_t* g_cnt, const double* g_pct,
+                   const double* g_e, int64_t total_points, char* sel);
 
 }  // namespace olpt

@@ -343,7 +343,7 @@ __device__ __forceinline__ bool in_roi(const Rect& R, double u, double w) {
 }
 
 template <typename Real>
-__global__ void __launch_bounds__(128) shake_kernel(ShakeView v, int64_t n, double* xyz,
+__global__ void __launch_bounds__(128, 4) shake_kernel(ShakeView v, int64_t n, double* xyz,
                                                     double* uv, const Real* otfp, double* score,
                                                     double delta) {
   extern __shared__ __align__(16) unsigned char smem_raw[];

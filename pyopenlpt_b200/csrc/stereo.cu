@@ -29,6 +29,7 @@
 #include <vector>
 
 #include "olpt_ctx.cuh"
+#include "olpt_prune.h"
 #include "olpt_scan.cuh"
 #include "olpt_stereo.h"
 
@@ -282,7 +283,7 @@ constexpr double kCos6 = 0.99452189536827329;
 // (the single long strip of K = 1); otherwise one thread per path (K >= 2, where the
 // strips intersect in a few rows).
 template <int K, bool WARP>
-__global__ void __launch_bounds__(256) level_kernel(const SmView v, const Path* in, int n_in,
+__global__ void __launch_bounds__(256, 2) level_kernel(const SmView v, const Path* in, int n_in,
                                                     Path* out, int* out_count, int out_cap,
                                                     Path* term, int* term_count, int term_cap) {
   const int gtid = blockIdx.x * blockDim.x + threadIdx.x;
@@ -762,26 +763,72 @@ void stereo_match_device(olpt_ctx* ctx, const SmParams& prm, StereoResult& res) 
                                               cap_c);
   OLPT_CUDA(cudaGetLastError());
   const int M = read_count(3);
-  res.ids.resize((size_t)M * n_cam);
-  res.e.resize(M);
-  res.X.resize((size_t)M * 3);
-  if (M > 0) {
-    OLPT_CUDA(cudaMemcpyAsync(res.ids.data(), W.cand_ids.p, (size_t)M * n_cam * sizeof(int),
-                              cudaMemcpyDeviceToHost, s));
-    OLPT_CUDA(cudaMemcpyAsync(res.e.data(), W.cand_e.p, (size_t)M * sizeof(double),
-                              cudaMemcpyDeviceToHost, s));
-    OLPT_CUDA(cudaMemcpyAsync(res.X.data(), W.cand_x.p, (size_t)M * 3 * sizeof(double),
-                              cudaMemcpyDeviceToHost, s));
-    OLPT_CUDA(cudaStreamSynchronize(s));
-  }
   res.n_cam = n_cam;
   PhaseTimer pt(ctx->prof, PH_PRUNE);
-  sort_candidates(res);
   std::vector<int> counts(n_cam);
   std::vector<int> active(n_cam);
+  PruneView pv{};
+  int64_t total_points = 0;
+  int max_count = 0;
   for (int c = 0; c < n_cam; ++c) {
     counts[c] = (int)ctx->det_counts_h[c];
     active[c] = v.active[c];
+    pv.active[c] = v.active[c];
+    pv.count[c] = counts[c];
+    pv.offset[c] = (int)total_points;
+    total_points += counts[c];
+    max_count = std::max(max_count, counts[c]);
+  }
+  res.ids.resize((size_t)M * n_cam);
+  res.e.resize(M);
+  res.X.resize((size_t)M * 3);
+  PruneWork& P = ctx->prune;
+  auto download = [&](const void* ids, const void* e, const void* X) {
+    if (M == 0) return;
+    OLPT_CUDA(cudaMemcpyAsync(res.ids.data(), ids, (size_t)M * n_cam * sizeof(int),
+                              cudaMemcpyDeviceToHost, s));
+    OLPT_CUDA(cudaMemcpyAsync(res.e.data(), e, (size_t)M * sizeof(double),
+                              cudaMemcpyDeviceToHost, s));
+    OLPT_CUDA(cudaMemcpyAsync(res.X.data(), X, (size_t)M * 3 * sizeof(double),
+                              cudaMemcpyDeviceToHost, s));
+  };
+  // candidate order and prune on the device; the greedy on the host
+  if (sort_candidates_device(P, W.cand_ids.as<int>(), W.cand_e.as<double>(),
+                             W.cand_x.as<double>(), M, n_cam, max_count - 1, s)) {
+    int G = 0;
+    const bool ok = prune_order_device(P, pv, M, n_cam, total_points, &G, s);
+    download(P.ids_s.p, P.e_s.p, P.X_s.p);
+    if (ok) {
+      // the greedy reads its input straight from pinned staging
+      const size_t b_ord = (size_t)G * sizeof(int), b_pts = (size_t)G * n_cam * sizeof(int);
+      const size_t b_dbl = (size_t)G * sizeof(double);
+      P.pin.ensure(b_ord + b_pts + 2 * b_dbl + G + 64);
+      char* hp = P.pin.as<char>();
+      double* g_pct = reinterpret_cast<double*>(hp);
+      double* g_e = reinterpret_cast<double*>(hp + b_dbl);
+      int* order = reinterpret_cast<int*>(hp + 2 * b_dbl);
+      int* g_pts = reinterpret_cast<int*>(hp + 2 * b_dbl + b_ord);
+      uint8_t* g_cnt = reinterpret_cast<uint8_t*>(hp + 2 * b_dbl + b_ord + b_pts);
+      if (G > 0) {
+        OLPT_CUDA(cudaMemcpyAsync(order, P.val.p, b_ord, cudaMemcpyDeviceToHost, s));
+        OLPT_CUDA(cudaMemcpyAsync(g_pts, P.g_pts.p, b_pts, cudaMemcpyDeviceToHost, s));
+        OLPT_CUDA(cudaMemcpyAsync(g_cnt, P.g_cnt.p, (size_t)G, cudaMemcpyDeviceToHost, s));
+        OLPT_CUDA(cudaMemcpyAsync(g_pct, P.g_pct.p, b_dbl, cudaMemcpyDeviceToHost, s));
+        OLPT_CUDA(cudaMemcpyAsync(g_e, P.g_e.p, b_dbl, cudaMemcpyDeviceToHost, s));
+      }
+      OLPT_CUDA(cudaStreamSynchronize(s));
+      std::vector<char> sel(G, 0);
+      greedy_select(G, n_cam, g_pts, g_cnt, g_pct, g_e, total_points, sel.data());
+      res.selected.assign(M, 0);
+      for (int i = 0; i < G; ++i)
+        if (sel[i]) res.selected[order[i]] = 1;
+      return;
+    }
+    OLPT_CUDA(cudaStreamSynchronize(s));
+  } else {
+    download(W.cand_ids.p, W.cand_e.p, W.cand_x.p);
+    OLPT_CUDA(cudaStreamSynchronize(s));
+    sort_candidates(res);
   }
   prune_candidates(res, counts, active);
 }

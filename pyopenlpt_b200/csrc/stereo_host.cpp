@@ -94,6 +94,75 @@ void sort_candidates(StereoResult& r) {
   r.X.swap(X2);
 }
 
+// StereoMatch::pruneMatch step 5 (StereoMatch.cpp:880-975): greedy exclusive
+// ownership of 2D points with local replacement, over G candidates already in greedy
+// order (all with finite percentile and e_check).  Per point the owner's position and
+// its (percentile, e_check) are cached, so the loop reads the candidates in order and
+// touches other candidates only to release them.
+void greedy_select(int64_t G, int n, const int* g_pts, const uint8_t* g_cnt, const double* g_pct,
+                   const double* g_e, int64_t total_points, char* sel) {
+  const double rtol = 1e-9, atol = 1e-12;
+  auto eq_eps = [&](double a, double b) {
+    const double s = std::max(std::fabs(a), std::fabs(b));
+    return std::fabs(a - b) <= (s * rtol + atol);
+  };
+  const double swap_pct_margin = 1e-12, swap_err_margin = 1e-12;
+  struct Own {
+    int o;
+    double pct, e;
+  };
+  std::vector<Own> owner(total_points, Own{-1, 0.0, 0.0});
+  auto place = [&](int64_t i) {
+    for (int k = 0; k < g_cnt[i]; ++k) owner[g_pts[i * n + k]] = Own{(int)i, g_pct[i], g_e[i]};
+    sel[i] = 1;
+  };
+  auto clear_owner_of = [&](int o) {
+    for (int k = 0; k < g_cnt[o]; ++k) {
+      Own& w = owner[g_pts[(int64_t)o * n + k]];
+      if (w.o == o) w.o = -1;
+    }
+    sel[o] = 0;
+  };
+  std::vector<int> S_buf(std::max(n, 1));
+  int* S = S_buf.data();
+  constexpr int64_t kAhead = 16;  // owner entries of later candidates are prefetched
+  for (int64_t i = 0; i < G; ++i) {
+    if (i + kAhead < G)
+      for (int k = 0; k < g_cnt[i + kAhead]; ++k)
+        __builtin_prefetch(&owner[g_pts[(i + kAhead) * n + k]]);
+    const int cnt_i = g_cnt[i];
+    if (cnt_i == 0) continue;
+    const int* P = &g_pts[i * n];
+    int ns = 0;
+    double avg_pct = 0.0, avg_err = 0.0;
+    for (int k = 0; k < cnt_i; ++k) {
+      const Own& w = owner[P[k]];
+      if (w.o == -1) continue;
+      bool seen = false;
+      for (int t = 0; t < ns; ++t) seen |= (S[t] == w.o);
+      if (!seen) {
+        S[ns++] = w.o;
+        avg_pct += w.pct;  // owners are always finite in both
+        avg_err += w.e;
+      }
+    }
+    if (ns == 0) {
+      place(i);
+      continue;
+    }
+    avg_pct /= (double)ns;
+    avg_err /= (double)ns;
+    const double pj = g_pct[i], ej = g_e[i];
+    const bool better_pct = (!eq_eps(pj, avg_pct)) && ((pj + swap_pct_margin) < avg_pct);
+    const bool tie_better = eq_eps(pj, avg_pct) && (!eq_eps(ej, avg_err)) &&
+                            ((ej + swap_err_margin) < avg_err);
+    if (better_pct || tie_better) {
+      for (int t = 0; t < ns; ++t) clear_owner_of(S[t]);
+      place(i);
+    }
+  }
+}
+
 void prune_candidates(StereoResult& r, const std::vector<int>& det_counts,
                       const std::vector<int>& active) {
   const size_t M = r.e.size();
@@ -105,7 +174,6 @@ void prune_candidates(StereoResult& r, const std::vector<int>& det_counts,
     const double s = std::max(std::fabs(a), std::fabs(b));
     return std::fabs(a - b) <= (s * rtol + atol);
   };
-  const double swap_pct_margin = 1e-12, swap_err_margin = 1e-12;
   const std::vector<double>& e_checks = r.e;
 
   std::vector<int64_t> cam_offsets(n + 1, 0);
@@ -297,51 +365,9 @@ void prune_candidates(StereoResult& r, const std::vector<int>& det_counts,
     g_pct[i] = pct_score[j];
     g_e[i] = e_checks[j];
   }
-  std::vector<int> owner(total_points, -1);
   std::vector<char> sel(G, 0);
-  auto place = [&](int64_t i) {
-    for (int k = 0; k < g_cnt[i]; ++k) owner[g_pts[i * n + k]] = (int)i;
-    sel[i] = 1;
-  };
-  auto clear_owner_of = [&](int o) {
-    for (int k = 0; k < g_cnt[o]; ++k)
-      if (owner[g_pts[(int64_t)o * n + k]] == o) owner[g_pts[(int64_t)o * n + k]] = -1;
-    sel[o] = 0;
-  };
-  std::vector<int> S_buf(std::max(n, 1));
-  int* S = S_buf.data();
-  for (int64_t i = 0; i < G; ++i) {
-    const int cnt_i = g_cnt[i];
-    if (cnt_i == 0) continue;
-    const int* P = &g_pts[i * n];
-    int ns = 0;
-    for (int k = 0; k < cnt_i; ++k) {
-      const int o = owner[P[k]];
-      if (o == -1) continue;
-      bool seen = false;
-      for (int t = 0; t < ns; ++t) seen |= (S[t] == o);
-      if (!seen) S[ns++] = o;
-    }
-    if (ns == 0) {
-      place(i);
-      continue;
-    }
-    double avg_pct = 0.0, avg_err = 0.0;
-    for (int t = 0; t < ns; ++t) {  // owners are always finite in both
-      avg_pct += g_pct[S[t]];
-      avg_err += g_e[S[t]];
-    }
-    avg_pct /= (double)ns;
-    avg_err /= (double)ns;
-    const double pj = g_pct[i], ej = g_e[i];
-    const bool better_pct = (!eq_eps(pj, avg_pct)) && ((pj + swap_pct_margin) < avg_pct);
-    const bool tie_better = eq_eps(pj, avg_pct) && (!eq_eps(ej, avg_err)) &&
-                            ((ej + swap_err_margin) < avg_err);
-    if (better_pct || tie_better) {
-      for (int t = 0; t < ns; ++t) clear_owner_of(S[t]);
-      place(i);
-    }
-  }
+  greedy_select(G, n, g_pts.data(), g_cnt.data(), g_pct.data(), g_e.data(), total_points,
+                sel.data());
   for (int64_t i = 0; i < G; ++i)
     if (sel[i]) r.selected[order[i]] = 1;
 }
