@@ -286,6 +286,10 @@ olpt_status_t olpt_stb_counts(olpt_ctx* ctx, int64_t counts[4], int64_t* n_exten
  * of an initial-phase frame.  Call with xyz = NULL to get n only; else n is the
  * capacity on input and the count on output. */
 olpt_status_t olpt_stb_frame_objects(olpt_ctx* ctx, int64_t* n, double* xyz);
+/* The image of camera `cam` as STB::processFrame leaves it in img_list after the last
+ * frame (the input in the initial phase; in the convergence phase the residual of
+ * the shaken predictions, Shake::calResidualImage, STB.cpp:418), as F32 or F64. */
+olpt_status_t olpt_stb_frame_image(olpt_ctx* ctx, int cam, olpt_dtype_t dtype, void* out);
 /* Number of track points (rows of the track files) with frame id `frame` over the
  * four lists: after olpt_stb_process_frame(frame), the particles that frame added. */
 olpt_status_t olpt_stb_frame_points(olpt_ctx* ctx, int frame, int64_t* n);

@@ -227,7 +227,7 @@ class RefSTB:
     reference-format config files written by synth.write_stb_config."""
 
     def __init__(self, seq, ipr_settings, stb_settings, workdir: Optional[str] = None,
-                 threads: int = 0, n_frames: Optional[int] = None):
+                 threads: int = 0, n_frames: Optional[int] = None, otf_override: bool = True):
         from pyopenlpt_b200.synth import write_stb_config
         self.lib = lib = C.CDLL(REF_SO)
         lib.oref_stb_new.restype = C.c_void_p
@@ -241,7 +241,9 @@ class RefSTB:
         self.seq = seq
         self._tmp = workdir or tempfile.mkdtemp(prefix="oref_stb_")
         main = write_stb_config(seq, self._tmp, ipr_settings, stb_settings, n_frames=n_frames)
-        self.h = lib.oref_stb_new(main.encode(), os.path.join(self._tmp, "otf.txt").encode())
+        self.main_config = main
+        otf = os.path.join(self._tmp, "otf.txt") if otf_override else ""
+        self.h = lib.oref_stb_new(main.encode(), otf.encode())
         if not self.h:
             raise RuntimeError(lib.oref_last_error().decode())
 
@@ -264,6 +266,14 @@ class RefSTB:
                 self.lib.oref_res_copy(h, name.encode(), _as_dp(a))
             out[name] = a.reshape(-1, 5)
         self.lib.oref_res_free(h)
+        return out
+
+    def otf(self) -> np.ndarray:
+        """The OTF table the reference tracks with, [4][n_cam][n_grid]."""
+        self.lib.oref_stb_otf.restype = C.c_int
+        ng = self.lib.oref_stb_otf(C.c_void_p(self.h), None)
+        out = np.empty((4, self.seq.n_cam, ng))
+        self.lib.oref_stb_otf(C.c_void_p(self.h), _as_dp(out))
         return out
 
     def close(self):

@@ -464,7 +464,8 @@ int oref_otf_param(void* cfg_h, int cam, long long n, const double* xyz, double*
 // STB::processFrame (src/srcSTB/STB.cpp:40-89) on in-memory frames.  The STB is
 // built from reference-format config files (BasicSetting::readConfig and the
 // STB constructor, which estimates an OTF from the first frames); the OTF is then
-// replaced by the scene's exact table so that the device run sees the same one.
+// replaced by the scene's exact table (when one is given) so that the device run
+// sees the same one.
 struct DebugAccess_STB {
   static ObjectConfig& cfg(STB& s) { return *s._obj_config; }
 };
@@ -500,7 +501,7 @@ void* oref_stb_new(const char* main_cfg, const char* otf_file) {
     }
     r->stb = std::make_unique<STB>(r->bs, "Tracer", r->bs._object_config_paths.at(0));
     auto& tc = static_cast<TracerConfig&>(DebugAccess_STB::cfg(*r->stb));
-    tc._otf.loadParam(std::string(otf_file));
+    if (otf_file && *otf_file) tc._otf.loadParam(std::string(otf_file));
     return r;
   } catch (std::exception const& e) {
     g_last_error = e.what();
@@ -511,6 +512,21 @@ void* oref_stb_new(const char* main_cfg, const char* otf_file) {
 }
 
 void oref_stb_free(void* h) { delete static_cast<RefStb*>(h); }
+
+// The tracer config's OTF table [4][n_cam][n_grid] (a, b, c, alpha); returns n_grid.
+int oref_stb_otf(void* h, double* out) {
+  auto* r = static_cast<RefStb*>(h);
+  auto& tc = static_cast<TracerConfig&>(DebugAccess_STB::cfg(*r->stb));
+  const OTFParam& p = tc._otf._param;
+  const int n_cam = p.n_cam, n_grid = p.n_grid;
+  if (out) {
+    const Matrix<double>* m[4] = {&p.a, &p.b, &p.c, &p.alpha};
+    for (int q = 0; q < 4; ++q)
+      for (int c = 0; c < n_cam; ++c)
+        for (int g = 0; g < n_grid; ++g) out[((size_t)q * n_cam + c) * n_grid + g] = (*m[q])(c, g);
+  }
+  return n_grid;
+}
 
 int oref_stb_frame(void* h, int frame, int n_cam, const double* const* imgs, const int* H,
                    const int* W) {

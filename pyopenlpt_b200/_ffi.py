@@ -310,6 +310,12 @@ class Context:
         self._check(self.L.olpt_stb_counts(self.h, c, C.byref(ne), C.byref(nn)))
         return tuple(c), ne.value, nn.value
 
+    def stb_frame_image(self, cam: int, H: int, W: int) -> np.ndarray:
+        """The image of one camera as processFrame leaves it (FP64)."""
+        out = np.empty((H, W))
+        self._check(self.L.olpt_stb_frame_image(self.h, cam, 3, _p(out)))
+        return out
+
     def stb_frame_points(self, frame: int) -> int:
         """Track points with this frame id over the four lists."""
         n = C.c_int64(0)

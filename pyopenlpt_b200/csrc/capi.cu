@@ -193,6 +193,7 @@ void olpt_ctx_destroy(olpt_ctx* ctx) {
   ctx->ipr.release(ctx->stream);
   for (int c = 0; c < OLPT_MAX_CAM; ++c) ctx->resid[c].buf.release(ctx->stream);
   ctx->stb.w.release(ctx->stream);
+  for (int c = 0; c < OLPT_MAX_CAM; ++c) ctx->stb.frame_img[c].buf.release(ctx->stream);
   ctx->prune.release(ctx->stream);
   ctx->prof.release();
   cudaStreamSynchronize(ctx->stream);
@@ -842,6 +843,28 @@ olpt_status_t olpt_stb_frame_objects(olpt_ctx* ctx, int64_t* n, double* xyz) {
       std::copy(v.begin(), v.end(), xyz);
     }
     *n = m;
+  });
+}
+
+olpt_status_t olpt_stb_frame_image(olpt_ctx* ctx, int cam, olpt_dtype_t dtype, void* out) {
+  return guard(ctx, [&] {
+    OLPT_REQUIRE(cam >= 0 && cam < ctx->n_cam && out, OLPT_ERR_INVALID_ARG, "bad camera/buffer");
+    OLPT_REQUIRE(dtype == OLPT_F32 || dtype == OLPT_F64, OLPT_ERR_INVALID_ARG,
+                 "download dtype must be F32 or F64");
+    const ImagePlane& im = ctx->stb.frame_img[cam];
+    OLPT_REQUIRE(im.buf.p, OLPT_ERR_INVALID_ARG, "no frame processed");
+    const int64_t n = (int64_t)im.H * im.W;
+    ctx->scratch.ensure(n * 8, ctx->stream);
+    if (dtype == OLPT_F32)
+      convert_plane_kernel<float><<<OLPT_G(nblk(n)), 256, 0, ctx->stream>>>(
+          im.buf.as<unsigned char>(), im.pitch, im.H, im.W, im.dtype, ctx->scratch.as<float>());
+    else
+      convert_plane_kernel<double><<<OLPT_G(nblk(n)), 256, 0, ctx->stream>>>(
+          im.buf.as<unsigned char>(), im.pitch, im.H, im.W, im.dtype, ctx->scratch.as<double>());
+    OLPT_CUDA(cudaGetLastError());
+    OLPT_CUDA(cudaMemcpyAsync(out, ctx->scratch.p, n * esize(dtype), cudaMemcpyDeviceToHost,
+                              ctx->stream));
+    OLPT_CUDA(cudaStreamSynchronize(ctx->stream));
   });
 }
 

@@ -276,6 +276,7 @@ struct StbState {
   std::vector<double> linfit_kernel;          // 2 x n_pts
   int64_t last_new = 0, last_extended = 0;
   std::vector<double> last_xyz;               // particles of the last frame
+  ImagePlane frame_img[OLPT_MAX_CAM];         // the frame's images as processFrame leaves them
   StbWork w;
 };
 

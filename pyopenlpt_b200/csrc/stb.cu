@@ -679,6 +679,25 @@ void last_points(const TrackH& tr, int k, double* dst) {
   std::copy(tr.xyz.end() - 3 * k, tr.xyz.end(), dst);
 }
 
+// Copy of the current images: what STB::processFrame leaves in img_list (the input
+// in the initial phase, the residual of the shaken predictions in the convergence
+// phase; the IPR works on its own copy).
+void snapshot_images(olpt_ctx* ctx) {
+  for (int c = 0; c < ctx->n_cam; ++c) {
+    const ImagePlane& src = ctx->img[c];
+    ImagePlane& dst = ctx->stb.frame_img[c];
+    const size_t bytes = (size_t)src.pitch * src.H;
+    dst.buf.ensure(bytes + 16, ctx->stream);
+    dst.dtype = src.dtype;
+    dst.H = src.H;
+    dst.W = src.W;
+    dst.pitch = src.pitch;
+    if (bytes)
+      OLPT_CUDA(cudaMemcpyAsync(dst.buf.p, src.buf.p, bytes, cudaMemcpyDeviceToDevice,
+                                ctx->stream));
+  }
+}
+
 // IPR::runIPR on the current images; the objects come back to the host.
 std::vector<double> run_ipr_host(olpt_ctx* ctx) {
   ipr_device(ctx, ctx->stb.ipr);
@@ -900,6 +919,7 @@ void build_from_pf(olpt_ctx* ctx, int idx, const double* d_field, int frame) {
 // STB::runInitPhase (STB.cpp:91-158)
 void init_phase(olpt_ctx* ctx, int frame) {
   StbState& S = ctx->stb;
+  snapshot_images(ctx);
   std::vector<double> xyz = run_ipr_host(ctx);
   PhaseTimer pt(ctx->prof, PH_TRACK);
   S.ipr_tracked.emplace_back(xyz.size() / 3, 0);
@@ -1016,6 +1036,7 @@ void conv_phase(olpt_ctx* ctx, int frame) {
   }
 
   // 3. IPR on the residual images
+  snapshot_images(ctx);
   pause();
   std::vector<double> oxyz = run_ipr_host(ctx);
   resume();

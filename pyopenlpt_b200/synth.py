@@ -301,11 +301,33 @@ def write_raw_frame(path: str, img: np.ndarray):
         f.write(np.ascontiguousarray(img).tobytes())
 
 
+def write_tiff_frame(path: str, img: np.ndarray):
+    """Uncompressed baseline TIFF (one strip, 8 or 16 bits, little-endian)."""
+    img = np.ascontiguousarray(img)
+    bits = {np.dtype(np.uint8): 8, np.dtype(np.uint16): 16}[img.dtype]
+    rows, cols = img.shape
+    data = img.astype("<u2" if bits == 16 else "u1").tobytes()
+    entries = [(256, 3, 1, cols), (257, 3, 1, rows), (258, 3, 1, bits), (259, 3, 1, 1),
+               (262, 3, 1, 1), (273, 4, 1, 8), (277, 3, 1, 1), (278, 3, 1, rows),
+               (279, 4, 1, len(data)), (284, 3, 1, 1)]
+    ifd = bytearray(np.array([len(entries)], "<u2").tobytes())
+    for tag, typ, cnt, val in entries:
+        ifd += np.array([tag, typ], "<u2").tobytes() + np.array([cnt], "<u4").tobytes()
+        ifd += (np.array([val, 0], "<u2").tobytes() if typ == 3
+                else np.array([val], "<u4").tobytes())
+    ifd += bytes(4)
+    with open(path, "wb") as f:
+        f.write(b"II" + np.array([42], "<u2").tobytes() + np.array([8 + len(data)], "<u4").tobytes())
+        f.write(data)
+        f.write(bytes(ifd))
+
+
 def write_stb_config(seq, folder: str, ipr: "IPRSettings", stb: STBSettings,
-                     n_frames: Optional[int] = None) -> str:
+                     n_frames: Optional[int] = None, image_format: str = "raw") -> str:
     """Reference-format main config (BasicSetting::readConfig, Config.cpp:49-135), tracer
     config (readCommonConfig + TracerConfig::readConfig, Config.cpp:163-286), camera
-    files, image lists with raw frames, and the OTF file.  Returns the main config path."""
+    files, image lists with the frames ("raw": the oracle's raw format; "tif": TIFF),
+    and the OTF file.  Returns the main config path."""
     os.makedirs(folder, exist_ok=True)
     n_frames = n_frames or len(seq.frames)
     cam_paths = []
@@ -318,8 +340,12 @@ def write_stb_config(seq, folder: str, ipr: "IPRSettings", stb: STBSettings,
     for i in range(seq.n_cam):
         names = []
         for t in range(n_frames):
-            nm = f"cam{i + 1}_{t:05d}.raw"
-            write_raw_frame(os.path.join(folder, nm), seq.frames[t][i])
+            ext = "tif" if image_format == "tif" else "raw"
+            nm = f"cam{i + 1}_{t:05d}.{ext}"
+            if ext == "tif":
+                write_tiff_frame(os.path.join(folder, nm), seq.frames[t][i])
+            else:
+                write_raw_frame(os.path.join(folder, nm), seq.frames[t][i])
             names.append(os.path.join(folder, nm))
         lp = f"cam{i + 1}ImageNames.txt"
         with open(os.path.join(folder, lp), "w") as f:
