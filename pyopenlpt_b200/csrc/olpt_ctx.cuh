@@ -147,7 +147,7 @@ struct StereoWork {
   DevBuf cell_of[OLPT_MAX_CAM], los[OLPT_MAX_CAM];
   DevBuf l2d[OLPT_MAX_CAM * OLPT_MAX_CAM];
   DevBuf l2d_ptrs, active_d, counters, scan_tmp;
-  DevBuf path_a, path_b, term;
+  DevBuf path_a, path_b, term, pairs;
   DevBuf cand_ids, cand_e, cand_x;
   void release(cudaStream_t s) {
     for (int c = 0; c < OLPT_MAX_CAM; ++c) {
@@ -164,6 +164,7 @@ struct StereoWork {
     path_a.release(s);
     path_b.release(s);
     term.release(s);
+    pairs.release(s);
     cand_ids.release(s);
     cand_e.release(s);
     cand_x.release(s);

@@ -278,14 +278,31 @@ __device__ __forceinline__ double clamped_dot(const double a[3], const double b[
 // the smallest pairwise parallax lies inside (6, 174) degrees.
 constexpr double kCos6 = 0.99452189536827329;
 
-// Expand one level: each path has K chosen cameras; its candidates on the target
-// camera are enumerated over rows of cells.  WARP: one warp per path, lanes take rows
-// (the single long strip of K = 1); otherwise one thread per path (K >= 2, where the
-// strips intersect in a few rows).
+// A path and one of its candidates on the target camera that passed the 2D tests.
+struct Pair {
+  int path;
+  int pid;
+};
+
+// Slot in an append buffer for every active lane, one atomic per warp.
+__device__ __forceinline__ int append_slot(int* counter) {
+  const unsigned m = __activemask();
+  const int lane = threadIdx.x & 31;
+  const int leader = __ffs(m) - 1;
+  int base = 0;
+  if (lane == leader) base = atomicAdd(counter, __popc(m));
+  base = __shfl_sync(m, base, leader);
+  return base + __popc(m & ((1u << lane) - 1u));
+}
+
+// Expand one level, first half: each path has K chosen cameras; its candidates on
+// the target camera are enumerated over rows of cells and kept when they pass the
+// strip test (IDMap::visitPointsInRowSpans) and the back-projection test.  WARP: one
+// warp per path, lanes take rows (the single long strip of K = 1); otherwise one
+// thread per path (K >= 2, where the strips intersect in a few rows).
 template <int K, bool WARP>
-__global__ void __launch_bounds__(256, 2) level_kernel(const SmView v, const Path* in, int n_in,
-                                                    Path* out, int* out_count, int out_cap,
-                                                    Path* term, int* term_count, int term_cap) {
+__global__ void __launch_bounds__(256) enum_kernel(const SmView v, const Path* in, int n_in,
+                                                   Pair* pairs, int* pair_count, int pair_cap) {
   const int gtid = blockIdx.x * blockDim.x + threadIdx.x;
   const int pidx = WARP ? (gtid >> 5) : gtid;
   const int r0 = WARP ? (threadIdx.x & 31) : 0;
@@ -296,7 +313,6 @@ __global__ void __launch_bounds__(256, 2) level_kernel(const SmView v, const Pat
   // image lines of the chosen points on the target camera
   double lp[K][2], lU[K][2];
   double cpt[K][2];
-  double cp[K][3], cu[K][3];  // chosen lines of sight (build order)
 #pragma unroll
   for (int i = 0; i < K; ++i) {
     const int c = P.cams[i];
@@ -307,37 +323,7 @@ __global__ void __launch_bounds__(256, 2) level_kernel(const SmView v, const Pat
     lU[i][1] = L[5];
     cpt[i][0] = v.x[c][P.ids[i]];
     cpt[i][1] = v.y[c][P.ids[i]];
-    const double* S = v.los[c] + 6 * (int64_t)P.ids[i];
-#pragma unroll
-    for (int q = 0; q < 3; ++q) {
-      cp[i][q] = S[q];
-      cu[i][q] = S[3 + q];
-    }
   }
-  // Normal equations of the chosen lines, summed in build order: the candidate's
-  // term is added last, which is the reference's summation order
-  // (myMATH::triangulation sums lines in list order, myMATH.cpp:376-391).
-  double Mc[9], bc[3];
-#pragma unroll
-  for (int q = 0; q < 9; ++q) Mc[q] = 0.0;
-  bc[0] = bc[1] = bc[2] = 0.0;
-#pragma unroll
-  for (int i = 0; i < K; ++i) {
-    double tt[9];
-    normal_terms(cu[i], tt);
-#pragma unroll
-    for (int r = 0; r < 3; ++r)
-      bc[r] = bc[r] + (tt[3 * r] * cp[i][0] + tt[3 * r + 1] * cp[i][1] + tt[3 * r + 2] * cp[i][2]);
-#pragma unroll
-    for (int q = 0; q < 9; ++q) Mc[q] = Mc[q] + tt[q];
-  }
-  // largest pairwise dot (smallest parallax) among the chosen lines
-  double maxdot_c = -2.0;
-#pragma unroll
-  for (int i = 0; i < K; ++i)
-#pragma unroll
-    for (int j = i + 1; j < K; ++j) maxdot_c = fmax(maxdot_c, clamped_dot(cu[i], cu[j]));
-
   const int rows = v.rows[t], cols = v.cols[t];
   const double cellp = (double)v.cell;
   const double hw = 0.5 * v.cell, hh = 0.5 * v.cell;
@@ -444,6 +430,65 @@ __global__ void __launch_bounds__(256, 2) level_kernel(const SmView v, const Pat
           ok = !(z * z > tol2);
         }
         if (!ok) continue;
+        const int slot = append_slot(pair_count);
+        if (slot < pair_cap) pairs[slot] = Pair{pidx, pid};
+      }
+    }
+  }
+}
+
+// Expand one level, second half: one thread per (path, candidate) pair.  The quick
+// triangulation gate (computeMinParallaxDeg, calTriangulateTol,
+// TriangulationCheckWithTol: StereoMatch.cpp:1072-1141) on the path's lines plus the
+// candidate's, then the child path (terminal, or with its next target camera).
+template <int K>
+__global__ void __launch_bounds__(256, 2) tri_kernel(const SmView v, const Path* in,
+                                                     const Pair* pairs, int n_pairs, Path* out,
+                                                     int* out_count, int out_cap, Path* term,
+                                                     int* term_count, int term_cap) {
+  const int gi = blockIdx.x * blockDim.x + threadIdx.x;
+  if (gi >= n_pairs) return;
+  const Pair pr = pairs[gi];
+  const Path P = in[pr.path];
+  const int t = P.target;
+  const int pid = pr.pid;
+  double cp[K][3], cu[K][3];  // chosen lines of sight (build order)
+#pragma unroll
+  for (int i = 0; i < K; ++i) {
+    const double* S = v.los[P.cams[i]] + 6 * (int64_t)P.ids[i];
+#pragma unroll
+    for (int q = 0; q < 3; ++q) {
+      cp[i][q] = S[q];
+      cu[i][q] = S[3 + q];
+    }
+  }
+  // Normal equations of the chosen lines, summed in build order: the candidate's
+  // term is added last, which is the reference's summation order
+  // (myMATH::triangulation sums lines in list order, myMATH.cpp:376-391).
+  double Mc[9], bc[3];
+#pragma unroll
+  for (int q = 0; q < 9; ++q) Mc[q] = 0.0;
+  bc[0] = bc[1] = bc[2] = 0.0;
+#pragma unroll
+  for (int i = 0; i < K; ++i) {
+    double tt[9];
+    normal_terms(cu[i], tt);
+#pragma unroll
+    for (int r = 0; r < 3; ++r)
+      bc[r] = bc[r] + (tt[3 * r] * cp[i][0] + tt[3 * r + 1] * cp[i][1] + tt[3 * r + 2] * cp[i][2]);
+#pragma unroll
+    for (int q = 0; q < 9; ++q) Mc[q] = Mc[q] + tt[q];
+  }
+  // largest pairwise dot (smallest parallax) among the chosen lines
+  double maxdot_c = -2.0;
+#pragma unroll
+  for (int i = 0; i < K; ++i)
+#pragma unroll
+    for (int j = i + 1; j < K; ++j) maxdot_c = fmax(maxdot_c, clamped_dot(cu[i], cu[j]));
+
+  {
+    {
+      {
         // extend the path; quick triangulation gate (computeMinParallaxDeg,
         // calTriangulateTol, TriangulationCheckWithTol: StereoMatch.cpp:1072-1141)
         double qp[3], qu[3];
@@ -496,20 +541,20 @@ __global__ void __launch_bounds__(256, 2) level_kernel(const SmView v, const Pat
           const double* uu = (i < K) ? cu[i] : qu;
           thrown |= !line_error_term(X, pp, uu, e);
         }
-        if (thrown) continue;  // the reference's triangulation throws; the check fails
+        if (thrown) return;  // the reference's triangulation throws; the check fails
         const double err = sqrt(e / k1);
-        if (!(err <= tq)) continue;
+        if (!(err <= tq)) return;
         Path ch = P;
         ch.ids[K] = pid;
         ch.cams[K] = (signed char)t;
         ch.k = k1;
         if (k1 == v.m) {
           ch.target = -1;
-          int slot = atomicAdd(term_count, 1);
+          const int slot = append_slot(term_count);
           if (slot < term_cap) term[slot] = ch;
-          continue;
+          return;
         }
-        if (k1 >= OLPT_MAX_CAM) continue;
+        if (k1 >= OLPT_MAX_CAM) return;
         // StereoMatch::selectNextCameraByMaxPairAngle (StereoMatch.cpp:1375-1411)
         int best = -1;
         double best_score = -1.0;
@@ -540,14 +585,15 @@ __global__ void __launch_bounds__(256, 2) level_kernel(const SmView v, const Pat
             best = cam;
           }
         }
-        if (best < 0) continue;
+        if (best < 0) return;
         ch.target = best;
-        int slot = atomicAdd(out_count, 1);
+        const int slot = append_slot(out_count);
         if (slot < out_cap) out[slot] = ch;
       }
     }
   }
 }
+
 
 // StereoMatch::checkMatch, case "every active camera was used to build"
 // (StereoMatch.cpp:520-540): triangulate in camera order, gate on tol_3d and limit.
@@ -689,7 +735,7 @@ void stereo_match_device(olpt_ctx* ctx, const SmParams& prm, StereoResult& res) 
   }
 
   // breadth-first expansion of the build DFS
-  W.counters.ensure(4 * sizeof(int), s);
+  W.counters.ensure(8 * sizeof(int), s);
   int* cnt = W.counters.as<int>();
   auto read_count = [&](int idx) {
     int h = 0;
@@ -700,7 +746,7 @@ void stereo_match_device(olpt_ctx* ctx, const SmParams& prm, StereoResult& res) 
   int64_t n_ref = v.n[ref];
   int cap_a = (int)std::max<int64_t>(n_ref, 1024);
   W.path_a.ensure(cap_a * sizeof(Path), s);
-  OLPT_CUDA(cudaMemsetAsync(cnt, 0, 4 * sizeof(int), s));
+  OLPT_CUDA(cudaMemsetAsync(cnt, 0, 8 * sizeof(int), s));
   if (n_ref > 0) seed_kernel<<<OLPT_G(nblk(n_ref)), 256, 0, s>>>(v, ref, W.path_a.as<Path>(), cnt, cap_a);
   OLPT_CUDA(cudaGetLastError());
   int n_in = read_count(0);
@@ -710,29 +756,58 @@ void stereo_match_device(olpt_ctx* ctx, const SmParams& prm, StereoResult& res) 
   DevBuf* in_buf = &W.path_a;
   DevBuf* out_buf = &W.path_b;
   int out_cap = (int)std::max<int64_t>(16 * (int64_t)n_in, 4096);
+  int pair_cap = (int)std::max<int64_t>(8 * (int64_t)n_in, 4096);
   for (int level = 1; level < v.m && n_in > 0; ++level) {
+    // candidates of every path that pass the 2D tests
+    int n_pairs = 0;
+    for (;;) {
+      W.pairs.ensure((size_t)pair_cap * sizeof(Pair), s);
+      OLPT_CUDA(cudaMemsetAsync(cnt + 4, 0, sizeof(int), s));
+      const int pid = ctx->prof.begin(PROF_STEREO, s);
+      auto kern = enum_kernel<1, true>;
+      switch (level) {
+        case 1: kern = enum_kernel<1, true>; break;
+        case 2: kern = enum_kernel<2, false>; break;
+        case 3: kern = enum_kernel<3, false>; break;
+        case 4: kern = enum_kernel<4, false>; break;
+        case 5: kern = enum_kernel<5, false>; break;
+        case 6: kern = enum_kernel<6, false>; break;
+        default: kern = enum_kernel<7, false>; break;
+      }
+      const int64_t work = level == 1 ? (int64_t)n_in * 32 : (int64_t)n_in;
+      kern<<<OLPT_G(nblk(work)), 256, 0, s>>>(v, in_buf->as<Path>(), n_in, W.pairs.as<Pair>(),
+                                                cnt + 4, pair_cap);
+      ctx->prof.end(PROF_STEREO, pid, s, 0.0);
+      OLPT_CUDA(cudaGetLastError());
+      n_pairs = read_count(4);
+      if (n_pairs > pair_cap) {  // grow and redo
+        pair_cap = n_pairs + n_pairs / 4 + 1024;
+        continue;
+      }
+      break;
+    }
+    // quick triangulation gate and the children
     for (;;) {
       out_buf->ensure((size_t)out_cap * sizeof(Path), s);
       W.term.ensure((size_t)term_cap * sizeof(Path), s);
       // counters: [1] = children, [2] = terminals (terminals accumulate across levels)
       OLPT_CUDA(cudaMemsetAsync(cnt + 1, 0, sizeof(int), s));
       OLPT_CUDA(cudaMemcpyAsync(cnt + 2, &n_term, sizeof(int), cudaMemcpyHostToDevice, s));
-      const int64_t threads = (int64_t)n_in * 32;
       const int pid = ctx->prof.begin(PROF_STEREO, s);
-      auto kern = level_kernel<1, true>;
+      auto kern = tri_kernel<1>;
       switch (level) {
-        case 1: kern = level_kernel<1, true>; break;
-        case 2: kern = level_kernel<2, false>; break;
-        case 3: kern = level_kernel<3, false>; break;
-        case 4: kern = level_kernel<4, false>; break;
-        case 5: kern = level_kernel<5, false>; break;
-        case 6: kern = level_kernel<6, false>; break;
-        default: kern = level_kernel<7, false>; break;
+        case 1: kern = tri_kernel<1>; break;
+        case 2: kern = tri_kernel<2>; break;
+        case 3: kern = tri_kernel<3>; break;
+        case 4: kern = tri_kernel<4>; break;
+        case 5: kern = tri_kernel<5>; break;
+        case 6: kern = tri_kernel<6>; break;
+        default: kern = tri_kernel<7>; break;
       }
-      const int64_t work = level == 1 ? threads : (int64_t)n_in;
-      kern<<<OLPT_G(nblk(work)), 256, 0, s>>>(v, in_buf->as<Path>(), n_in, out_buf->as<Path>(),
-                                                 cnt + 1, out_cap, W.term.as<Path>(), cnt + 2,
-                                                 term_cap);
+      if (n_pairs > 0)
+        kern<<<OLPT_G(nblk(n_pairs)), 256, 0, s>>>(v, in_buf->as<Path>(), W.pairs.as<Pair>(),
+                                                   n_pairs, out_buf->as<Path>(), cnt + 1, out_cap,
+                                                   W.term.as<Path>(), cnt + 2, term_cap);
       ctx->prof.end(PROF_STEREO, pid, s, 0.0);
       OLPT_CUDA(cudaGetLastError());
       int h[2];
