@@ -250,8 +250,9 @@ def workload_config(name, s, sc=None, seq=None, st=None):
 # ----------------------------------------------------------------------------- our arm
 PROF_NAMES = {0: "peak detection", 1: "stereo level expansion", 2: "residual image",
               3: "shake (warp per particle)", 4: "predictive field"}
-PHASE_NAMES = {5: "detection", 6: "stereo matching (all)", 7: "candidate sort + prune",
-               8: "shake (all)", 9: "output + residual", 10: "STB track work"}
+PHASE_NAMES = {5: "detection", 6: "stereo matching (all)", 7: "candidate sort + prune + greedy",
+               8: "shake (all)", 9: "output + residual", 10: "STB track work",
+               11: "sequential greedy (replacement fallback)"}
 
 
 class Ours:

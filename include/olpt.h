@@ -64,9 +64,10 @@ olpt_status_t olpt_stream(olpt_ctx* ctx, void** stream);
 /* Per-kernel event timing (no reference counterpart; the reference prints clock()
  * CPU time per stage).  kernel: 0 = detection, 1 = stereo level expansion,
  * 2 = residual image, 3 = shake, 4 = predictive field (device time from CUDA
- * events); 5..10 = host wall-clock phases (detection, stereo matching, candidate
- * sort + prune, shake, output compaction + residual, STB track work outside the
- * IPR and the shake of predictions).  read returns the summed duration,
+ * events); 5..11 = host wall-clock phases (detection, stereo matching, candidate
+ * sort + prune + greedy, shake, output compaction + residual, STB track work outside
+ * the IPR and the shake of predictions, the sequential greedy run when the device
+ * greedy meets a replacement).  read returns the summed duration,
  * the number of timed launches/phases and their algorithmic bytes since the last
  * read. */
 olpt_status_t olpt_profile(olpt_ctx* ctx, int enable);
@@ -179,6 +180,13 @@ olpt_status_t olpt_get_matches(olpt_ctx* ctx, int32_t* ids, double* xyz);
  * det_counts/active per camera; selected[j] = 1 for kept candidates.  Host only. */
 olpt_status_t olpt_prune_matches(int n_cam, int64_t M, const int32_t* ids, const double* e_check,
                                  const int64_t* det_counts, const int* active, uint8_t* selected);
+/* The same prune run on the context's device (the path olpt_stereo_match takes):
+ * percentile scores and tolerance classes, the greedy order and the greedy itself on
+ * the device, the sequential greedy on the host only when a replacement fires.
+ * Identical output to olpt_prune_matches. */
+olpt_status_t olpt_prune_matches_device(olpt_ctx* ctx, int n_cam, int64_t M, const int32_t* ids,
+                                        const double* e_check, const int64_t* det_counts,
+                                        const int* active, uint8_t* selected);
 
 /* ------------------------------------------------------------------ 3D objects */
 /* Replace the context's 3D objects with n tracers at xyz (n x 3); their 2D

@@ -250,6 +250,20 @@ class Context:
         self._check(self.L.olpt_get_matches(self.h, _p(ids, _i32p), _p(x)))
         return ids, x
 
+    def prune_matches(self, ids: np.ndarray, e_check: np.ndarray, det_counts, active=None):
+        """StereoMatch::pruneMatch on a candidate list (reference order) on the device;
+        returns the kept flags."""
+        ids = np.ascontiguousarray(ids, dtype=np.int32)
+        M, n = ids.shape
+        e = np.ascontiguousarray(e_check, dtype=np.float64)
+        cnt = np.ascontiguousarray(det_counts, dtype=np.int64)
+        act = (C.c_int * n)(*([1] * n if active is None else [int(a) for a in active]))
+        sel = np.zeros(M, dtype=np.uint8)
+        self._check(self.L.olpt_prune_matches_device(
+            self.h, n, C.c_int64(M), _p(ids, _i32p), _p(e), _p(cnt, _i64p), act,
+            sel.ctypes.data_as(C.POINTER(C.c_uint8))))
+        return sel.astype(bool)
+
     # ---------------------------------------------------------------- objects / shake
     def upload_objects(self, xyz: np.ndarray):
         xyz = np.ascontiguousarray(xyz, dtype=np.float64).reshape(-1, 3)
@@ -377,7 +391,8 @@ class Context:
 PROF_PEAKS, PROF_STEREO, PROF_RESIDUAL, PROF_SHAKE, PROF_PF = 0, 1, 2, 3, 4
 # host phases (wall clock): id = PROF_N + phase
 PROF_N = 5
-PH_DETECT, PH_STEREO, PH_PRUNE, PH_SHAKE, PH_OUTPUT, PH_TRACK = range(PROF_N, PROF_N + 6)
+PH_DETECT, PH_STEREO, PH_PRUNE, PH_SHAKE, PH_OUTPUT, PH_TRACK, PH_GREEDY_HOST = range(
+    PROF_N, PROF_N + 7)
 
 
 class IprParams(C.Structure):

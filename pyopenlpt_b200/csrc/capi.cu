@@ -621,6 +621,60 @@ olpt_status_t olpt_prune_matches(int n_cam, int64_t M, const int32_t* ids, const
   }
 }
 
+olpt_status_t olpt_prune_matches_device(olpt_ctx* ctx, int n_cam, int64_t M, const int32_t* ids,
+                                        const double* e_check, const int64_t* det_counts,
+                                        const int* active, uint8_t* selected) {
+  if (!ctx) return OLPT_ERR_INVALID_ARG;
+  return guard(ctx, [&] {
+    OLPT_REQUIRE(n_cam >= 1 && n_cam <= OLPT_MAX_CAM && M >= 0 && M < (int64_t)INT32_MAX / n_cam &&
+                     (M == 0 || (ids && e_check && selected)) && det_counts && active,
+                 OLPT_ERR_INVALID_ARG, "prune_matches_device: bad arguments");
+    cudaStream_t s = ctx->stream;
+    PruneView pv{};
+    int64_t total = 0;
+    for (int c = 0; c < n_cam; ++c) {
+      OLPT_REQUIRE(det_counts[c] >= 0 && det_counts[c] < INT32_MAX, OLPT_ERR_INVALID_ARG,
+                   "prune_matches_device: bad det_counts");
+      pv.active[c] = active[c];
+      pv.count[c] = (int)det_counts[c];
+      pv.offset[c] = (int)total;
+      total += det_counts[c];
+    }
+    OLPT_REQUIRE(total < INT32_MAX, OLPT_ERR_UNSUPPORTED, "prune_matches_device: too many points");
+    for (int64_t j = 0; j < M * n_cam; ++j) {
+      const int c = (int)(j % n_cam);
+      OLPT_REQUIRE(ids[j] >= -1 && (!active[c] || ids[j] < det_counts[c]), OLPT_ERR_INVALID_ARG,
+                   "prune_matches_device: id out of range");
+    }
+    PruneWork& P = ctx->prune;
+    P.ids_s.ensure((size_t)(M + 1) * n_cam * sizeof(int), s);
+    P.e_s.ensure((size_t)(M + 1) * sizeof(double), s);
+    if (M > 0) {
+      OLPT_CUDA(cudaMemcpyAsync(P.ids_s.p, ids, (size_t)M * n_cam * sizeof(int),
+                                cudaMemcpyHostToDevice, s));
+      OLPT_CUDA(cudaMemcpyAsync(P.e_s.p, e_check, (size_t)M * sizeof(double),
+                                cudaMemcpyHostToDevice, s));
+    }
+    std::vector<char> sel(M, 0);
+    if (!prune_select_device(ctx, pv, (int)M, n_cam, total, sel.data())) {
+      OLPT_CUDA(cudaStreamSynchronize(s));
+      StereoResult r;
+      r.n_cam = n_cam;
+      r.ids.assign(ids, ids + M * n_cam);
+      r.e.assign(e_check, e_check + M);
+      r.X.assign(3 * M, 0.0);
+      std::vector<int> counts(n_cam), act(n_cam);
+      for (int c = 0; c < n_cam; ++c) {
+        counts[c] = pv.count[c];
+        act[c] = active[c];
+      }
+      prune_candidates(r, counts, act);
+      sel.assign(r.selected.begin(), r.selected.end());
+    }
+    for (int64_t j = 0; j < M; ++j) selected[j] = (uint8_t)sel[j];
+  });
+}
+
 olpt_status_t olpt_get_matches(olpt_ctx* ctx, int32_t* ids, double* xyz) {
   return guard(ctx, [&] {
     const StereoResult& r = ctx->sm_result;

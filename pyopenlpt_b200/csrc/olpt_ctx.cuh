@@ -186,15 +186,17 @@ struct PruneWork {
   DevBuf fl, slot_key, fcnt, slot_pct, slot_used, pct, flag;
   DevBuf f_pct, f_both, pos_pct, pos_both, pcls, ecls, newc, excl, cstart;
   DevBuf g_pts, g_cnt, g_pct, g_e, pool_e, pool_i;
-  Csr points;
+  DevBuf gkey, gstate, gfirst, gowner, sel;
+  Csr points, gpoints;
   HostBuf pin;  // pinned staging of the greedy's input
   void release(cudaStream_t s) {
     for (DevBuf* b : {&key, &val, &key2, &val2, &hist, &scan_tmp, &ids_s, &e_s, &X_s, &fl,
                       &slot_key, &fcnt, &slot_pct, &slot_used, &pct, &flag, &f_pct, &f_both,
                       &pos_pct, &pos_both, &pcls, &ecls, &newc, &excl, &cstart, &g_pts, &g_cnt,
-                      &g_pct, &g_e, &pool_e, &pool_i})
+                      &g_pct, &g_e, &pool_e, &pool_i, &gkey, &gstate, &gfirst, &gowner, &sel})
       b->release(s);
     points.release(s);
+    gpoints.release(s);
   }
 };
 
@@ -248,6 +250,8 @@ struct IprWork {
 };
 
 void stereo_match_device(olpt_ctx* ctx, const SmParams& prm, StereoResult& res);
+bool prune_select_device(olpt_ctx* ctx, const PruneView& pv, int M, int n_cam,
+                         int64_t total_points, char* selected);
 void ipr_device(olpt_ctx* ctx, const IprParams& p);
 OtfView otf_view(olpt_ctx* ctx);
 void shake_device(olpt_ctx* ctx, const ShakeParams& sp);

@@ -23,11 +23,12 @@ enum ProfKernel : int {
 enum ProfPhase : int {
   PH_DETECT = 0,   // detection incl. count read-back
   PH_STEREO = 1,   // whole stereo match (device + host)
-  PH_PRUNE = 2,    // host candidate sort + prune
+  PH_PRUNE = 2,    // candidate sort + prune + greedy (device and host)
   PH_SHAKE = 3,    // whole shake (all iterations + flags)
   PH_OUTPUT = 4,   // compaction of kept objects + final residual
   PH_TRACK = 5,    // STB track bookkeeping, prediction, linking and pruning
-  PH_N = 6
+  PH_GREEDY_HOST = 6,  // sequential greedy, run when the device greedy meets a replacement
+  PH_N = 7
 };
 
 struct Prof {

@@ -1,5 +1,5 @@
-// Device candidate ordering and prune (prune.cu); the greedy stays on the host
-// (greedy_select, stereo_host.cpp).
+// Device candidate ordering and prune (prune.cu); the sequential greedy
+// (greedy_select, stereo_host.cpp) remains the fallback.
 #pragma once
 #include <cuda_runtime.h>
 
@@ -13,5 +13,7 @@ bool sort_candidates_device(PruneWork& W, const int* ids, const double* e, const
                             int n, int max_id, cudaStream_t s);
 bool prune_order_device(PruneWork& W, const PruneView& pv, int M, int n, int64_t total_points,
                         int* G_out, cudaStream_t s);
+bool greedy_device(PruneWork& W, int M, int G, int n, int64_t total_points, uint8_t* sel,
+                   cudaStream_t s);
 
 }  // namespace olpt

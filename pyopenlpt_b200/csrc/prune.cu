@@ -17,7 +17,9 @@
 //     can take: tolerance classes of the percentiles, then of e_check inside every
 //     percentile class (computed and checked the same way over the sorted values),
 //     and a radix sort by class;
-//  6. the greedy itself runs on the host over the gathered candidates.
+//  6. the greedy: parallel rounds of the in-order greedy independent set, checked
+//     against the replacement rule (greedy_device); the sequential loop on the host
+//     when a replacement would fire.
 // Whenever a check fails (a tolerance class wider than the tolerance, a key wider
 // than 64 bits) the caller falls back to the host implementation, which keeps the
 // reference's std::stable_sort.
@@ -346,6 +348,109 @@ __global__ void gather_greedy_kernel(const int* order, int G, int n, const int* 
   g_e[i] = e[j];
 }
 
+// ---------------------------------------------------------------- greedy
+// The greedy of pruneMatch over candidates in greedy order.  Without replacements it
+// is the in-order greedy independent set (a candidate is taken iff no earlier taken
+// candidate shares one of its points), which these rounds compute in parallel: a
+// candidate is taken once it is the earliest candidate not yet rejected on every one
+// of its points, and rejected once an earlier taken candidate shares a point.  Then
+// every rejected candidate evaluates the replacement rule against its owners (the
+// taken candidates before it on its points) exactly as the sequential loop would; if
+// any would replace, the caller runs the sequential loop instead.
+constexpr uint8_t kUndecided = 0, kTaken = 1, kRejected = 2, kSkipped = 3;
+
+// candidates without a point are passed over by the loop (neither kept nor owners)
+__global__ void greedy_init_kernel(const uint8_t* g_cnt, int G, uint8_t* state) {
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i < G) state[i] = g_cnt[i] == 0 ? kSkipped : kUndecided;
+}
+
+__global__ void greedy_keys_kernel(const int* g_pts, const uint8_t* g_cnt, int G, int n,
+                                   int* key) {
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= G) return;
+  for (int k = 0; k < n; ++k) key[(int64_t)i * n + k] = k < g_cnt[i] ? g_pts[(int64_t)i * n + k] : -1;
+}
+
+// first[f]: position in the point's list of its earliest candidate not rejected
+__global__ void greedy_advance_kernel(const int* pstart, const int* items, int n_points, int n,
+                                      const uint8_t* state, int* first) {
+  const int f = blockIdx.x * blockDim.x + threadIdx.x;
+  if (f >= n_points) return;
+  int q = first[f];
+  const int end = pstart[f + 1];
+  while (q < end && state[items[q] / n] == kRejected) ++q;
+  first[f] = q;
+}
+
+__global__ void greedy_decide_kernel(const int* g_pts, const uint8_t* g_cnt, int G, int n,
+                                     const int* pstart, const int* items, const int* first,
+                                     uint8_t* state, int* undecided) {
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= G || state[i] != kUndecided) return;
+  bool all_first = true, blocked = false;
+  for (int k = 0; k < g_cnt[i]; ++k) {
+    const int f = g_pts[(int64_t)i * n + k];
+    const int q = first[f];
+    const int p = q < pstart[f + 1] ? items[q] / n : i;
+    if (p != i) {
+      all_first = false;
+      if (state[p] == kTaken) blocked = true;
+    }
+  }
+  if (blocked)
+    state[i] = kRejected;
+  else if (all_first)
+    state[i] = kTaken;
+  else
+    atomicAdd(undecided, 1);
+}
+
+__global__ void greedy_owner_kernel(const int* g_pts, const uint8_t* g_cnt, int G, int n,
+                                    const uint8_t* state, int* owner) {
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= G || state[i] != kTaken) return;
+  for (int k = 0; k < g_cnt[i]; ++k) owner[g_pts[(int64_t)i * n + k]] = i;
+}
+
+// StereoMatch::pruneMatch replacement rule (StereoMatch.cpp:930-975) for a rejected
+// candidate against the owners of its points, averaged in point order.
+__global__ void greedy_check_kernel(const int* g_pts, const uint8_t* g_cnt, int G, int n,
+                                    const uint8_t* state, const int* owner, const double* g_pct,
+                                    const double* g_e, int* flag) {
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= G || state[i] != kRejected) return;
+  int S[OLPT_MAX_CAM];
+  int ns = 0;
+  double avg_pct = 0.0, avg_err = 0.0;
+  for (int k = 0; k < g_cnt[i]; ++k) {
+    const int o = owner[g_pts[(int64_t)i * n + k]];
+    if (o < 0 || o >= i) continue;
+    bool seen = false;
+    for (int t = 0; t < ns; ++t) seen |= (S[t] == o);
+    if (seen) continue;
+    S[ns++] = o;
+    avg_pct += g_pct[o];
+    avg_err += g_e[o];
+  }
+  if (ns == 0) {  // cannot happen for a rejected candidate
+    atomicOr(flag, 1);
+    return;
+  }
+  avg_pct /= (double)ns;
+  avg_err /= (double)ns;
+  const double pj = g_pct[i], ej = g_e[i];
+  const bool better_pct = (!eq_eps(pj, avg_pct)) && ((pj + 1e-12) < avg_pct);
+  const bool tie_better = eq_eps(pj, avg_pct) && (!eq_eps(ej, avg_err)) && ((ej + 1e-12) < avg_err);
+  if (better_pct || tie_better) atomicOr(flag, 1);
+}
+
+__global__ void greedy_select_kernel(const int* order, const uint8_t* state, int G, uint8_t* sel) {
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= G) return;
+  sel[order[i]] = state[i] == kTaken ? 1 : 0;
+}
+
 int bit_width(uint64_t x) {
   int b = 0;
   while (x) {
@@ -531,6 +636,64 @@ bool prune_order_device(PruneWork& W, const PruneView& pv, int M, int n, int64_t
       W.g_e.as<double>());
   OLPT_CUDA(cudaGetLastError());
   return true;
+}
+
+// The greedy on the device (see greedy_*_kernel); sel[j] = 1 for kept candidates
+// (M entries, candidate order).  False when a replacement would have happened, in
+// which case the caller runs the sequential greedy.
+bool greedy_device(PruneWork& W, int M, int G, int n, int64_t total_points, uint8_t* sel,
+                   cudaStream_t s) {
+  if (M > 0) OLPT_CUDA(cudaMemsetAsync(sel, 0, (size_t)M, s));
+  if (G == 0) return true;
+  const size_t slots = (size_t)G * n;
+  W.gkey.ensure((slots + 1) * sizeof(int), s);
+  W.gstate.ensure(G + 16, s);
+  W.gfirst.ensure((size_t)(total_points + 1) * sizeof(int), s);
+  W.gowner.ensure((size_t)(total_points + 1) * sizeof(int), s);
+  W.flag.ensure(2 * sizeof(int), s);
+  const int* pts = W.g_pts.as<int>();
+  const uint8_t* cnt = W.g_cnt.as<uint8_t>();
+  uint8_t* state = W.gstate.as<uint8_t>();
+  greedy_keys_kernel<<<OLPT_G(nblk(G)), 256, 0, s>>>(pts, cnt, G, n, W.gkey.as<int>());
+  W.gpoints.build(W.gkey.as<int>(), (int)slots, (int)total_points, s, true);
+  greedy_init_kernel<<<OLPT_G(nblk(G)), 256, 0, s>>>(cnt, G, state);
+  OLPT_CUDA(cudaMemcpyAsync(W.gfirst.p, W.gpoints.start.p, (size_t)total_points * sizeof(int),
+                            cudaMemcpyDeviceToDevice, s));
+  int* und = W.flag.as<int>() + 1;
+  // every round decides at least the earliest undecided candidate; a few rounds are
+  // queued per look at the count
+  constexpr int kRoundsPerSync = 4;
+  for (int64_t round = 0;; round += kRoundsPerSync) {
+    for (int r = 0; r < kRoundsPerSync; ++r) {
+      OLPT_CUDA(cudaMemsetAsync(und, 0, sizeof(int), s));
+      if (total_points > 0)
+        greedy_advance_kernel<<<OLPT_G(nblk(total_points)), 256, 0, s>>>(
+            W.gpoints.start.as<int>(), W.gpoints.items.as<int>(), (int)total_points, n, state,
+            W.gfirst.as<int>());
+      greedy_decide_kernel<<<OLPT_G(nblk(G)), 256, 0, s>>>(pts, cnt, G, n,
+                                                          W.gpoints.start.as<int>(),
+                                                          W.gpoints.items.as<int>(),
+                                                          W.gfirst.as<int>(), state, und);
+    }
+    OLPT_CUDA(cudaGetLastError());
+    int left = 0;
+    OLPT_CUDA(cudaMemcpyAsync(&left, und, sizeof(int), cudaMemcpyDeviceToHost, s));
+    OLPT_CUDA(cudaStreamSynchronize(s));
+    if (left == 0) break;
+    OLPT_REQUIRE(round <= (int64_t)G, OLPT_ERR_INTERNAL, "device greedy did not converge");
+  }
+  OLPT_CUDA(cudaMemsetAsync(W.gowner.p, 0xff, (size_t)total_points * sizeof(int), s));
+  OLPT_CUDA(cudaMemsetAsync(W.flag.p, 0, sizeof(int), s));
+  greedy_owner_kernel<<<OLPT_G(nblk(G)), 256, 0, s>>>(pts, cnt, G, n, state, W.gowner.as<int>());
+  greedy_check_kernel<<<OLPT_G(nblk(G)), 256, 0, s>>>(pts, cnt, G, n, state, W.gowner.as<int>(),
+                                                     W.g_pct.as<double>(), W.g_e.as<double>(),
+                                                     W.flag.as<int>());
+  greedy_select_kernel<<<OLPT_G(nblk(G)), 256, 0, s>>>(W.val.as<int>(), state, G, sel);
+  OLPT_CUDA(cudaGetLastError());
+  int flag = 0;
+  OLPT_CUDA(cudaMemcpyAsync(&flag, W.flag.p, sizeof(int), cudaMemcpyDeviceToHost, s));
+  OLPT_CUDA(cudaStreamSynchronize(s));
+  return flag == 0;
 }
 
 }  // namespace olpt

@@ -632,6 +632,50 @@ __global__ void check_kernel(const SmView v, const Path* term, int n_term, int* 
 }  // namespace
 
 // ---------------------------------------------------------------- host driver
+// Steps 2-6 of pruneMatch on the candidates in ctx->prune.ids_s / e_s (M x n_cam, in
+// the reference's order); selected (host, M bytes, zeroed by the caller) receives
+// the kept flags and the stream is synchronised.  False when the comparator sorts
+// must run on the host (prune_candidates) instead.
+bool prune_select_device(olpt_ctx* ctx, const PruneView& pv, int M, int n_cam,
+                         int64_t total_points, char* selected) {
+  cudaStream_t s = ctx->stream;
+  PruneWork& P = ctx->prune;
+  int G = 0;
+  if (!prune_order_device(P, pv, M, n_cam, total_points, &G, s)) return false;
+  P.sel.ensure((size_t)M + 16, s);
+  if (greedy_device(P, M, G, n_cam, total_points, P.sel.as<uint8_t>(), s)) {
+    if (M > 0)
+      OLPT_CUDA(cudaMemcpyAsync(selected, P.sel.p, (size_t)M, cudaMemcpyDeviceToHost, s));
+    OLPT_CUDA(cudaStreamSynchronize(s));
+    return true;
+  }
+  // a replacement fires: the sequential greedy over pinned staging
+  PhaseTimer pg(ctx->prof, PH_GREEDY_HOST);
+  const size_t b_ord = (size_t)G * sizeof(int), b_pts = (size_t)G * n_cam * sizeof(int);
+  const size_t b_dbl = (size_t)G * sizeof(double);
+  P.pin.ensure(b_ord + b_pts + 2 * b_dbl + G + 64);
+  char* hp = P.pin.as<char>();
+  double* g_pct = reinterpret_cast<double*>(hp);
+  double* g_e = reinterpret_cast<double*>(hp + b_dbl);
+  int* order = reinterpret_cast<int*>(hp + 2 * b_dbl);
+  int* g_pts = reinterpret_cast<int*>(hp + 2 * b_dbl + b_ord);
+  uint8_t* g_cnt = reinterpret_cast<uint8_t*>(hp + 2 * b_dbl + b_ord + b_pts);
+  if (G > 0) {
+    OLPT_CUDA(cudaMemcpyAsync(order, P.val.p, b_ord, cudaMemcpyDeviceToHost, s));
+    OLPT_CUDA(cudaMemcpyAsync(g_pts, P.g_pts.p, b_pts, cudaMemcpyDeviceToHost, s));
+    OLPT_CUDA(cudaMemcpyAsync(g_cnt, P.g_cnt.p, (size_t)G, cudaMemcpyDeviceToHost, s));
+    OLPT_CUDA(cudaMemcpyAsync(g_pct, P.g_pct.p, b_dbl, cudaMemcpyDeviceToHost, s));
+    OLPT_CUDA(cudaMemcpyAsync(g_e, P.g_e.p, b_dbl, cudaMemcpyDeviceToHost, s));
+  }
+  OLPT_CUDA(cudaStreamSynchronize(s));
+  std::vector<char> sel(G, 0);
+  greedy_select(G, n_cam, g_pts, g_cnt, g_pct, g_e, total_points, sel.data());
+  std::fill(selected, selected + M, 0);
+  for (int i = 0; i < G; ++i)
+    if (sel[i]) selected[order[i]] = 1;
+  return true;
+}
+
 void stereo_match_device(olpt_ctx* ctx, const SmParams& prm, StereoResult& res) {
   cudaStream_t s = ctx->stream;
   const int n_cam = ctx->n_cam;
@@ -867,38 +911,12 @@ void stereo_match_device(olpt_ctx* ctx, const SmParams& prm, StereoResult& res) 
     OLPT_CUDA(cudaMemcpyAsync(res.X.data(), X, (size_t)M * 3 * sizeof(double),
                               cudaMemcpyDeviceToHost, s));
   };
-  // candidate order and prune on the device; the greedy on the host
+  // candidate order, prune and greedy on the device
   if (sort_candidates_device(P, W.cand_ids.as<int>(), W.cand_e.as<double>(),
                              W.cand_x.as<double>(), M, n_cam, max_count - 1, s)) {
-    int G = 0;
-    const bool ok = prune_order_device(P, pv, M, n_cam, total_points, &G, s);
     download(P.ids_s.p, P.e_s.p, P.X_s.p);
-    if (ok) {
-      // the greedy reads its input straight from pinned staging
-      const size_t b_ord = (size_t)G * sizeof(int), b_pts = (size_t)G * n_cam * sizeof(int);
-      const size_t b_dbl = (size_t)G * sizeof(double);
-      P.pin.ensure(b_ord + b_pts + 2 * b_dbl + G + 64);
-      char* hp = P.pin.as<char>();
-      double* g_pct = reinterpret_cast<double*>(hp);
-      double* g_e = reinterpret_cast<double*>(hp + b_dbl);
-      int* order = reinterpret_cast<int*>(hp + 2 * b_dbl);
-      int* g_pts = reinterpret_cast<int*>(hp + 2 * b_dbl + b_ord);
-      uint8_t* g_cnt = reinterpret_cast<uint8_t*>(hp + 2 * b_dbl + b_ord + b_pts);
-      if (G > 0) {
-        OLPT_CUDA(cudaMemcpyAsync(order, P.val.p, b_ord, cudaMemcpyDeviceToHost, s));
-        OLPT_CUDA(cudaMemcpyAsync(g_pts, P.g_pts.p, b_pts, cudaMemcpyDeviceToHost, s));
-        OLPT_CUDA(cudaMemcpyAsync(g_cnt, P.g_cnt.p, (size_t)G, cudaMemcpyDeviceToHost, s));
-        OLPT_CUDA(cudaMemcpyAsync(g_pct, P.g_pct.p, b_dbl, cudaMemcpyDeviceToHost, s));
-        OLPT_CUDA(cudaMemcpyAsync(g_e, P.g_e.p, b_dbl, cudaMemcpyDeviceToHost, s));
-      }
-      OLPT_CUDA(cudaStreamSynchronize(s));
-      std::vector<char> sel(G, 0);
-      greedy_select(G, n_cam, g_pts, g_cnt, g_pct, g_e, total_points, sel.data());
-      res.selected.assign(M, 0);
-      for (int i = 0; i < G; ++i)
-        if (sel[i]) res.selected[order[i]] = 1;
-      return;
-    }
+    res.selected.assign(M, 0);
+    if (prune_select_device(ctx, pv, M, n_cam, total_points, res.selected.data())) return;
     OLPT_CUDA(cudaStreamSynchronize(s));
   } else {
     download(W.cand_ids.p, W.cand_e.p, W.cand_x.p);
