@@ -570,25 +570,17 @@ olpt_status_t olpt_stereo_match(olpt_ctx* ctx, const olpt_sm_params* p, int64_t*
     StereoResult& r = ctx->sm_result;
     stereo_match_device(ctx, prm, r);
     // selected matches become the current 3D objects (triangulateMatch order)
-    const size_t M = r.e.size();
-    std::vector<double> xyz;
-    for (size_t j = 0; j < M; ++j)
-      if (r.selected[j]) xyz.insert(xyz.end(), &r.X[3 * j], &r.X[3 * j] + 3);
-    const int64_t n = (int64_t)(xyz.size() / 3);
-    ctx->obj.ensure(std::max<int64_t>(n, 1), ctx->n_cam, ctx->stream);
-    ctx->obj.n = n;
-    if (n)
-      OLPT_CUDA(cudaMemcpyAsync(ctx->obj.xyz.p, xyz.data(), xyz.size() * sizeof(double),
-                                cudaMemcpyHostToDevice, ctx->stream));
+    const int64_t n = stereo_objects(ctx, r);
     OLPT_CUDA(cudaStreamSynchronize(ctx->stream));
-    if (n_candidates) *n_candidates = (int64_t)M;
+    if (n_candidates) *n_candidates = r.M;
     if (n_matches) *n_matches = n;
   });
 }
 
 olpt_status_t olpt_get_candidates(olpt_ctx* ctx, int32_t* ids, double* e_check, double* xyz) {
   return guard(ctx, [&] {
-    const StereoResult& r = ctx->sm_result;
+    StereoResult& r = ctx->sm_result;
+    stereo_result_to_host(ctx, r);
     const size_t M = r.e.size();
     if (ids) std::copy(r.ids.begin(), r.ids.end(), ids);
     if (e_check) std::copy(r.e.begin(), r.e.end(), e_check);
@@ -646,6 +638,7 @@ olpt_status_t olpt_prune_matches_device(olpt_ctx* ctx, int n_cam, int64_t M, con
       OLPT_REQUIRE(ids[j] >= -1 && (!active[c] || ids[j] < det_counts[c]), OLPT_ERR_INVALID_ARG,
                    "prune_matches_device: id out of range");
     }
+    stereo_result_to_host(ctx, ctx->sm_result);  // its arrays live in the same workspace
     PruneWork& P = ctx->prune;
     P.ids_s.ensure((size_t)(M + 1) * n_cam * sizeof(int), s);
     P.e_s.ensure((size_t)(M + 1) * sizeof(double), s);
@@ -677,7 +670,8 @@ olpt_status_t olpt_prune_matches_device(olpt_ctx* ctx, int n_cam, int64_t M, con
 
 olpt_status_t olpt_get_matches(olpt_ctx* ctx, int32_t* ids, double* xyz) {
   return guard(ctx, [&] {
-    const StereoResult& r = ctx->sm_result;
+    StereoResult& r = ctx->sm_result;
+    stereo_result_to_host(ctx, r);
     const int n = r.n_cam;
     int64_t k = 0;
     for (size_t j = 0; j < r.e.size(); ++j) {

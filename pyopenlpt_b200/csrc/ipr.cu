@@ -169,15 +169,7 @@ void single_iteration(olpt_ctx* ctx, const IprParams& p, const SmParams& sm) {
     PhaseTimer pt(ctx->prof, PH_STEREO);
     stereo_match_device(ctx, sm, r);
   }
-  std::vector<double> xyz;
-  for (size_t j = 0; j < r.e.size(); ++j)
-    if (r.selected[j]) xyz.insert(xyz.end(), &r.X[3 * j], &r.X[3 * j] + 3);
-  const int64_t n = (int64_t)(xyz.size() / 3);
-  ctx->obj.ensure(std::max<int64_t>(n, 1), ctx->n_cam, ctx->stream);
-  ctx->obj.n = n;
-  if (n == 0) return;
-  OLPT_CUDA(cudaMemcpyAsync(ctx->obj.xyz.p, xyz.data(), xyz.size() * sizeof(double),
-                            cudaMemcpyHostToDevice, ctx->stream));
+  if (stereo_objects(ctx, r) == 0) return;
   {
     PhaseTimer pt(ctx->prof, PH_SHAKE);
     shake_device(ctx, p.shake);

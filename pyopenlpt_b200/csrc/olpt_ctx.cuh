@@ -186,14 +186,14 @@ struct PruneWork {
   DevBuf fl, slot_key, fcnt, slot_pct, slot_used, pct, flag;
   DevBuf f_pct, f_both, pos_pct, pos_both, pcls, ecls, newc, excl, cstart;
   DevBuf g_pts, g_cnt, g_pct, g_e, pool_e, pool_i;
-  DevBuf gkey, gstate, gfirst, gowner, sel;
+  DevBuf gkey, gstate, gfirst, gowner, sel, spos, scnt;
   Csr points, gpoints;
   HostBuf pin;  // pinned staging of the greedy's input
   void release(cudaStream_t s) {
     for (DevBuf* b : {&key, &val, &key2, &val2, &hist, &scan_tmp, &ids_s, &e_s, &X_s, &fl,
                       &slot_key, &fcnt, &slot_pct, &slot_used, &pct, &flag, &f_pct, &f_both,
                       &pos_pct, &pos_both, &pcls, &ecls, &newc, &excl, &cstart, &g_pts, &g_cnt,
-                      &g_pct, &g_e, &pool_e, &pool_i, &gkey, &gstate, &gfirst, &gowner, &sel})
+                      &g_pct, &g_e, &pool_e, &pool_i, &gkey, &gstate, &gfirst, &gowner, &sel, &spos, &scnt})
       b->release(s);
     points.release(s);
     gpoints.release(s);
@@ -252,6 +252,11 @@ struct IprWork {
 void stereo_match_device(olpt_ctx* ctx, const SmParams& prm, StereoResult& res);
 bool prune_select_device(olpt_ctx* ctx, const PruneView& pv, int M, int n_cam,
                          int64_t total_points, char* selected);
+// Download a device-resident stereo result (no-op for a host one).
+void stereo_result_to_host(olpt_ctx* ctx, StereoResult& r);
+// The kept matches become the context's 3D objects (triangulateMatch order); returns
+// their number.
+int64_t stereo_objects(olpt_ctx* ctx, const StereoResult& r);
 void ipr_device(olpt_ctx* ctx, const IprParams& p);
 OtfView otf_view(olpt_ctx* ctx);
 void shake_device(olpt_ctx* ctx, const ShakeParams& sp);

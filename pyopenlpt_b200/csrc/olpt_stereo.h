@@ -16,9 +16,13 @@ struct SmParams {
 
 // Candidate set after checkMatch, sorted by ids (StereoMatch.cpp:153-156), and the
 // prune selection (StereoMatch.cpp:631-980).
+// After the device prune the arrays stay on the device (the context's prune
+// workspace) until a caller asks for them (on_device; stereo_result_to_host).
 struct StereoResult {
   int n_cam = 0;
   int ref_cam = -1;
+  int64_t M = 0;               // candidates
+  bool on_device = false;      // ids / e / X / selected not yet downloaded
   std::vector<int> ids;        // M x n_cam, -1 = camera unused
   std::vector<double> e;       // e_check
   std::vector<double> X;       // M x 3, triangulated position (camera order)

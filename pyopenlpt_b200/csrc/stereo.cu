@@ -633,9 +633,9 @@ __global__ void check_kernel(const SmView v, const Path* term, int n_term, int* 
 
 // ---------------------------------------------------------------- host driver
 // Steps 2-6 of pruneMatch on the candidates in ctx->prune.ids_s / e_s (M x n_cam, in
-// the reference's order); selected (host, M bytes, zeroed by the caller) receives
-// the kept flags and the stream is synchronised.  False when the comparator sorts
-// must run on the host (prune_candidates) instead.
+// the reference's order): the kept flags end in ctx->prune.sel (device, M bytes) and,
+// when selected is given, on the host.  False when the comparator sorts must run on
+// the host (prune_candidates) instead.
 bool prune_select_device(olpt_ctx* ctx, const PruneView& pv, int M, int n_cam,
                          int64_t total_points, char* selected) {
   cudaStream_t s = ctx->stream;
@@ -644,9 +644,10 @@ bool prune_select_device(olpt_ctx* ctx, const PruneView& pv, int M, int n_cam,
   if (!prune_order_device(P, pv, M, n_cam, total_points, &G, s)) return false;
   P.sel.ensure((size_t)M + 16, s);
   if (greedy_device(P, M, G, n_cam, total_points, P.sel.as<uint8_t>(), s)) {
-    if (M > 0)
+    if (selected && M > 0) {
       OLPT_CUDA(cudaMemcpyAsync(selected, P.sel.p, (size_t)M, cudaMemcpyDeviceToHost, s));
-    OLPT_CUDA(cudaStreamSynchronize(s));
+      OLPT_CUDA(cudaStreamSynchronize(s));
+    }
     return true;
   }
   // a replacement fires: the sequential greedy over pinned staging
@@ -670,9 +671,14 @@ bool prune_select_device(olpt_ctx* ctx, const PruneView& pv, int M, int n_cam,
   OLPT_CUDA(cudaStreamSynchronize(s));
   std::vector<char> sel(G, 0);
   greedy_select(G, n_cam, g_pts, g_cnt, g_pct, g_e, total_points, sel.data());
-  std::fill(selected, selected + M, 0);
+  std::vector<char> flags(M, 0);
   for (int i = 0; i < G; ++i)
-    if (sel[i]) selected[order[i]] = 1;
+    if (sel[i]) flags[order[i]] = 1;
+  if (M > 0) {
+    OLPT_CUDA(cudaMemcpyAsync(P.sel.p, flags.data(), (size_t)M, cudaMemcpyHostToDevice, s));
+    OLPT_CUDA(cudaStreamSynchronize(s));
+  }
+  if (selected) std::copy(flags.begin(), flags.end(), selected);
   return true;
 }
 
@@ -681,6 +687,8 @@ void stereo_match_device(olpt_ctx* ctx, const SmParams& prm, StereoResult& res) 
   const int n_cam = ctx->n_cam;
   SmView v{};
   v.n_cam = n_cam;
+  res.on_device = false;
+  res.M = 0;
   int n_active = 0;
   for (int c = 0; c < n_cam; ++c) {
     v.active[c] = ctx->cams_h[c].is_active;
@@ -898,11 +906,12 @@ void stereo_match_device(olpt_ctx* ctx, const SmParams& prm, StereoResult& res) 
     total_points += counts[c];
     max_count = std::max(max_count, counts[c]);
   }
-  res.ids.resize((size_t)M * n_cam);
-  res.e.resize(M);
-  res.X.resize((size_t)M * 3);
+  res.M = M;
   PruneWork& P = ctx->prune;
   auto download = [&](const void* ids, const void* e, const void* X) {
+    res.ids.resize((size_t)M * n_cam);
+    res.e.resize(M);
+    res.X.resize((size_t)M * 3);
     if (M == 0) return;
     OLPT_CUDA(cudaMemcpyAsync(res.ids.data(), ids, (size_t)M * n_cam * sizeof(int),
                               cudaMemcpyDeviceToHost, s));
@@ -914,9 +923,15 @@ void stereo_match_device(olpt_ctx* ctx, const SmParams& prm, StereoResult& res) 
   // candidate order, prune and greedy on the device
   if (sort_candidates_device(P, W.cand_ids.as<int>(), W.cand_e.as<double>(),
                              W.cand_x.as<double>(), M, n_cam, max_count - 1, s)) {
+    if (prune_select_device(ctx, pv, M, n_cam, total_points, nullptr)) {
+      res.ids.clear();
+      res.e.clear();
+      res.X.clear();
+      res.selected.clear();
+      res.on_device = true;  // downloaded on demand (stereo_result_to_host)
+      return;
+    }
     download(P.ids_s.p, P.e_s.p, P.X_s.p);
-    res.selected.assign(M, 0);
-    if (prune_select_device(ctx, pv, M, n_cam, total_points, res.selected.data())) return;
     OLPT_CUDA(cudaStreamSynchronize(s));
   } else {
     download(W.cand_ids.p, W.cand_e.p, W.cand_x.p);
@@ -924,6 +939,81 @@ void stereo_match_device(olpt_ctx* ctx, const SmParams& prm, StereoResult& res) 
     sort_candidates(res);
   }
   prune_candidates(res, counts, active);
+}
+
+__global__ void sel_count_kernel(const uint8_t* sel, int M, int* f) {
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i < M) f[i] = sel[i] ? 1 : 0;
+}
+
+__global__ void sel_gather_kernel(const uint8_t* sel, const int* pos, int M, const double* X,
+                                  double* out) {
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= M || !sel[i]) return;
+  const int k = pos[i];
+  out[3 * k] = X[3 * i];
+  out[3 * k + 1] = X[3 * i + 1];
+  out[3 * k + 2] = X[3 * i + 2];
+}
+
+void stereo_result_to_host(olpt_ctx* ctx, StereoResult& r) {
+  if (!r.on_device) return;
+  cudaStream_t s = ctx->stream;
+  PruneWork& P = ctx->prune;
+  const int64_t M = r.M;
+  const int n = r.n_cam;
+  r.ids.resize((size_t)M * n);
+  r.e.resize(M);
+  r.X.resize((size_t)M * 3);
+  r.selected.resize(M);
+  if (M > 0) {
+    OLPT_CUDA(cudaMemcpyAsync(r.ids.data(), P.ids_s.p, (size_t)M * n * sizeof(int),
+                              cudaMemcpyDeviceToHost, s));
+    OLPT_CUDA(cudaMemcpyAsync(r.e.data(), P.e_s.p, (size_t)M * sizeof(double),
+                              cudaMemcpyDeviceToHost, s));
+    OLPT_CUDA(cudaMemcpyAsync(r.X.data(), P.X_s.p, (size_t)M * 3 * sizeof(double),
+                              cudaMemcpyDeviceToHost, s));
+    OLPT_CUDA(cudaMemcpyAsync(r.selected.data(), P.sel.p, (size_t)M, cudaMemcpyDeviceToHost, s));
+  }
+  OLPT_CUDA(cudaStreamSynchronize(s));
+  r.on_device = false;
+}
+
+int64_t stereo_objects(olpt_ctx* ctx, const StereoResult& r) {
+  cudaStream_t s = ctx->stream;
+  int64_t n = 0;
+  if (r.on_device) {
+    PruneWork& P = ctx->prune;
+    const int M = (int)r.M;
+    P.spos.ensure((size_t)(M + 1) * sizeof(int), s);
+    P.scnt.ensure((size_t)(M + 1) * sizeof(int), s);
+    if (M > 0)
+      sel_count_kernel<<<OLPT_G(nblk(M)), 256, 0, s>>>(P.sel.as<uint8_t>(), M, P.scnt.as<int>());
+    exclusive_scan(P.scnt.as<int>(), M, P.spos.as<int>(), P.scan_tmp, s);
+    int total = 0;
+    OLPT_CUDA(cudaMemcpyAsync(&total, P.spos.as<int>() + M, sizeof(int), cudaMemcpyDeviceToHost, s));
+    OLPT_CUDA(cudaStreamSynchronize(s));
+    n = total;
+    ctx->obj.ensure(std::max<int64_t>(n, 1), ctx->n_cam, s);
+    ctx->obj.n = n;
+    if (n > 0)
+      sel_gather_kernel<<<OLPT_G(nblk(M)), 256, 0, s>>>(P.sel.as<uint8_t>(), P.spos.as<int>(), M,
+                                                       P.X_s.as<double>(), ctx->obj.xyz.as<double>());
+    OLPT_CUDA(cudaGetLastError());
+    return n;
+  }
+  std::vector<double> xyz;
+  for (size_t j = 0; j < r.selected.size(); ++j)
+    if (r.selected[j]) xyz.insert(xyz.end(), &r.X[3 * j], &r.X[3 * j] + 3);
+  n = (int64_t)(xyz.size() / 3);
+  ctx->obj.ensure(std::max<int64_t>(n, 1), ctx->n_cam, s);
+  ctx->obj.n = n;
+  if (n > 0) {
+    OLPT_CUDA(cudaMemcpyAsync(ctx->obj.xyz.p, xyz.data(), xyz.size() * sizeof(double),
+                              cudaMemcpyHostToDevice, s));
+    OLPT_CUDA(cudaStreamSynchronize(s));  // xyz is a local host buffer
+  }
+  return n;
 }
 
 }  // namespace olpt
