@@ -315,6 +315,63 @@ olpt_status_t olpt_stb_set_tracks(olpt_ctx* ctx, int which, const int32_t* track
 olpt_status_t olpt_stb_save_tracks(olpt_ctx* ctx, int which, const char* path);
 olpt_status_t olpt_stb_load_tracks(olpt_ctx* ctx, int which, const char* path);
 
+/* ------------------------------------------------------------------ learned proposal */
+/* No reference counterpart: a small MLP that reads, for each candidate after stereo
+ * matching, 4 cameras x 11 x 11 patches of max(0, residual + own projection) divided
+ * by the candidate's OTF amplitude, the 8 sub-pixel offsets of its projections and a
+ * constant 1 (OLPT_MLP_IN values, camera-major, patches row-major), and predicts a 3D
+ * correction (units of out_scale_mm) and a ghost logit.  Layers 493 -> 256 -> 256 ->
+ * 256 (GELU, erf form) -> 4; bf16 weights and activations on tcgen05 GEMMs with f32
+ * accumulation.  Parameters are one flat f32 array: W1[256][493], b1[256],
+ * W2[256][256], b2[256], W3[256][256], b3[256], W4[4][256], b4[4]. */
+#define OLPT_MLP_IN 493
+#define OLPT_MLP_OUT 4
+#define OLPT_MLP_PARAMS 259076
+
+/* The learned shake used by olpt_ipr_run (and the IPR inside the STB frame loop) when
+ * enable != 0, in place of the plain runShake: the network corrects every candidate
+ * and drops those with a ghost logit above ghost_logit; refine_loops plain shake
+ * iterations from refine_width_mm follow; objects whose residue (divided by the mean
+ * squared OTF amplitude) stays above fallback_residual restart the full plain shake
+ * from their stereo position.  Repeated / ghost flags as in runShake. */
+typedef struct olpt_learned_params {
+  int enable;
+  double out_scale_mm;
+  double ghost_logit;
+  int refine_loops;
+  double refine_width_mm;
+  double fallback_residual;
+} olpt_learned_params;
+
+/* Initialise the parameters (He-uniform, seeded; zero biases; Adam state reset). */
+olpt_status_t olpt_mlp_init(olpt_ctx* ctx, uint64_t seed);
+olpt_status_t olpt_mlp_set_params(olpt_ctx* ctx, const float* params);
+olpt_status_t olpt_mlp_get_params(olpt_ctx* ctx, float* params);
+/* out (n x 4) = network(x (n x OLPT_MLP_IN)); host or device pointers (on_device). */
+olpt_status_t olpt_mlp_forward(olpt_ctx* ctx, int64_t n, const float* x, float* out,
+                               int on_device);
+/* One training step on a batch: targets n x 4 (dx, dy, dz in units of out_scale_mm,
+ * ghost label 0/1); loss = mean[(1 - ghost) * mean_d (o_d - t_d)^2 + ghost_weight *
+ * BCE(o_3, ghost)].  Gradients of the mean loss go to grad (host, OLPT_MLP_PARAMS,
+ * optional); update != 0 applies Adam (lr, 0.9, 0.999, 1e-8). */
+olpt_status_t olpt_mlp_train_step(olpt_ctx* ctx, int64_t n, const float* x, const float* targets,
+                                  int on_device, double lr, double ghost_weight, int update,
+                                  double* loss, float* grad);
+/* Features (n_objects x OLPT_MLP_IN) of the context's objects, against a residual of
+ * the current images with every object projected (4 cameras). */
+olpt_status_t olpt_mlp_features(olpt_ctx* ctx, const olpt_shake_params* p, float* x,
+                                int on_device);
+olpt_status_t olpt_learned_configure(olpt_ctx* ctx, const olpt_learned_params* p);
+/* The learned shake on the context's objects (as olpt_shake). */
+olpt_status_t olpt_shake_learned(olpt_ctx* ctx, const olpt_shake_params* p);
+/* Objects that went through the learned shake and how many fell back, since the
+ * context was created. */
+olpt_status_t olpt_learned_stats(olpt_ctx* ctx, int64_t* n_learned, int64_t* n_fallback);
+/* out (M x N, f32) = A (M x K) * B (N x K)^T (+ bias, GELU when gelu != 0) on the
+ * tensor-core GEMM; A and B bf16 bit patterns, all host buffers. */
+olpt_status_t olpt_bf16_gemm(olpt_ctx* ctx, int M, int N, int K, const uint16_t* A,
+                             const uint16_t* B, const float* bias, int gelu, float* out);
+
 #ifdef __cplusplus
 }
 #endif

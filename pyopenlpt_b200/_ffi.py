@@ -19,8 +19,19 @@ _DTYPES = {np.dtype(np.uint8): OLPT_U8, np.dtype(np.uint16): OLPT_U16,
            np.dtype(np.float32): OLPT_F32, np.dtype(np.float64): OLPT_F64}
 
 _dp = C.POINTER(C.c_double)
+_fp = C.POINTER(C.c_float)
+_u16p = C.POINTER(C.c_uint16)
 _i64p = C.POINTER(C.c_int64)
 _i32p = C.POINTER(C.c_int32)
+
+MLP_IN, MLP_OUT, MLP_PARAMS = 493, 4, 259076
+
+
+class LearnedParams(C.Structure):
+    """olpt_learned_params: the learned shake used inside IPR when enable != 0."""
+    _fields_ = [("enable", C.c_int), ("out_scale_mm", C.c_double), ("ghost_logit", C.c_double),
+                ("refine_loops", C.c_int), ("refine_width_mm", C.c_double),
+                ("fallback_residual", C.c_double)]
 
 
 class CameraDesc(C.Structure):
@@ -376,6 +387,79 @@ class Context:
         s = C.c_void_p()
         self._check(self.L.olpt_stream(self.h, C.byref(s)))
         return s.value or 0
+
+    # ---------------------------------------------------------------- learned proposal
+    def mlp_init(self, seed: int = 0):
+        self._check(self.L.olpt_mlp_init(self.h, C.c_uint64(seed)))
+
+    def mlp_set_params(self, flat: np.ndarray):
+        flat = np.ascontiguousarray(flat, dtype=np.float32)
+        assert flat.size == MLP_PARAMS
+        self._check(self.L.olpt_mlp_set_params(self.h, _p(flat, _fp)))
+
+    def mlp_get_params(self) -> np.ndarray:
+        out = np.empty(MLP_PARAMS, np.float32)
+        self._check(self.L.olpt_mlp_get_params(self.h, _p(out, _fp)))
+        return out
+
+    def mlp_forward(self, x: np.ndarray) -> np.ndarray:
+        x = np.ascontiguousarray(x, dtype=np.float32).reshape(-1, MLP_IN)
+        out = np.empty((len(x), MLP_OUT), np.float32)
+        self._check(self.L.olpt_mlp_forward(self.h, C.c_int64(len(x)), _p(x, _fp), _p(out, _fp), 0))
+        return out
+
+    def mlp_forward_device(self, x_ptr: int, n: int, out_ptr: int):
+        """Device pointers (e.g. torch tensors' data_ptr())."""
+        self._check(self.L.olpt_mlp_forward(self.h, C.c_int64(n), C.c_void_p(x_ptr),
+                                            C.c_void_p(out_ptr), 1))
+
+    def mlp_train_step(self, x: np.ndarray, t: np.ndarray, lr: float = 1e-3,
+                       ghost_weight: float = 1.0, update: bool = True, want_grad: bool = False):
+        x = np.ascontiguousarray(x, dtype=np.float32).reshape(-1, MLP_IN)
+        t = np.ascontiguousarray(t, dtype=np.float32).reshape(-1, MLP_OUT)
+        loss = C.c_double()
+        g = np.empty(MLP_PARAMS, np.float32) if want_grad else None
+        self._check(self.L.olpt_mlp_train_step(self.h, C.c_int64(len(x)), _p(x, _fp), _p(t, _fp), 0,
+                                               C.c_double(lr), C.c_double(ghost_weight),
+                                               int(update), C.byref(loss), _p(g, _fp)))
+        return (loss.value, g) if want_grad else loss.value
+
+    def mlp_train_step_device(self, x_ptr: int, t_ptr: int, n: int, lr: float,
+                              ghost_weight: float = 1.0) -> float:
+        loss = C.c_double()
+        self._check(self.L.olpt_mlp_train_step(self.h, C.c_int64(n), C.c_void_p(x_ptr),
+                                               C.c_void_p(t_ptr), 1, C.c_double(lr),
+                                               C.c_double(ghost_weight), 1, C.byref(loss), None))
+        return loss.value
+
+    def mlp_features(self, params: ShakeParams) -> np.ndarray:
+        n = self.n_objects()
+        x = np.zeros((n, MLP_IN), np.float32)
+        if n:
+            self._check(self.L.olpt_mlp_features(self.h, C.byref(params), _p(x, _fp), 0))
+        return x
+
+    def learned_configure(self, p: LearnedParams):
+        self._check(self.L.olpt_learned_configure(self.h, C.byref(p)))
+
+    def shake_learned(self, params: ShakeParams):
+        self._check(self.L.olpt_shake_learned(self.h, C.byref(params)))
+
+    def learned_stats(self):
+        a, b = C.c_int64(), C.c_int64()
+        self._check(self.L.olpt_learned_stats(self.h, C.byref(a), C.byref(b)))
+        return a.value, b.value
+
+    def bf16_gemm(self, a_bits: np.ndarray, b_bits: np.ndarray, bias=None, gelu=False):
+        a = np.ascontiguousarray(a_bits, dtype=np.uint16)
+        b = np.ascontiguousarray(b_bits, dtype=np.uint16)
+        M, K = a.shape
+        N = b.shape[0]
+        bias = None if bias is None else np.ascontiguousarray(bias, dtype=np.float32)
+        out = np.empty((M, N), np.float32)
+        self._check(self.L.olpt_bf16_gemm(self.h, M, N, K, _p(a, _u16p), _p(b, _u16p),
+                                          _p(bias, _fp), int(gelu), _p(out, _fp)))
+        return out
 
     def profile(self, enable: bool):
         self._check(self.L.olpt_profile(self.h, int(enable)))

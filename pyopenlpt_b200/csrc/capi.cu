@@ -10,6 +10,7 @@
 #include <vector>
 
 #include "olpt_ctx.cuh"
+#include "olpt_gemm.h"
 #include "olpt_otf.cuh"
 
 namespace olpt {
@@ -195,6 +196,7 @@ void olpt_ctx_destroy(olpt_ctx* ctx) {
   ctx->stb.w.release(ctx->stream);
   for (int c = 0; c < OLPT_MAX_CAM; ++c) ctx->stb.frame_img[c].buf.release(ctx->stream);
   ctx->prune.release(ctx->stream);
+  ctx->mlp.release(ctx->stream);
   ctx->prof.release();
   cudaStreamSynchronize(ctx->stream);
   if (ctx->own_stream) cudaStreamDestroy(ctx->stream);
@@ -981,6 +983,172 @@ olpt_status_t olpt_stb_load_tracks(olpt_ctx* ctx, int which, const char* path) {
   return guard(ctx, [&] {
     OLPT_REQUIRE(path, OLPT_ERR_INVALID_ARG, "null path");
     stb_load_tracks(ctx, which, path);
+  });
+}
+
+
+// ---------------------------------------------------------------- learned proposal
+olpt_status_t olpt_mlp_init(olpt_ctx* ctx, uint64_t seed) {
+  return guard(ctx, [&] { mlp_init(ctx, seed); });
+}
+
+olpt_status_t olpt_mlp_set_params(olpt_ctx* ctx, const float* params) {
+  return guard(ctx, [&] {
+    OLPT_REQUIRE(params, OLPT_ERR_INVALID_ARG, "null params");
+    mlp_set_params(ctx, params);
+  });
+}
+
+olpt_status_t olpt_mlp_get_params(olpt_ctx* ctx, float* params) {
+  return guard(ctx, [&] {
+    OLPT_REQUIRE(params, OLPT_ERR_INVALID_ARG, "null params");
+    mlp_get_params(ctx, params);
+  });
+}
+
+olpt_status_t olpt_mlp_forward(olpt_ctx* ctx, int64_t n, const float* x, float* out,
+                               int on_device) {
+  return guard(ctx, [&] {
+    OLPT_REQUIRE(n >= 0 && n < (int64_t)INT32_MAX && (n == 0 || (x && out)),
+                 OLPT_ERR_INVALID_ARG, "mlp_forward: bad arguments");
+    if (n == 0) return;
+    MlpWork& W = ctx->mlp;
+    cudaStream_t s = ctx->stream;
+    const float* dx = x;
+    if (!on_device) {
+      W.xin.ensure((size_t)n * OLPT_MLP_IN * 4, s);
+      OLPT_CUDA(cudaMemcpyAsync(W.xin.p, x, (size_t)n * OLPT_MLP_IN * 4, cudaMemcpyHostToDevice, s));
+      dx = W.xin.as<float>();
+    }
+    W.x.ensure((size_t)n * kMlpInPad * 2, s);
+    W.o.ensure((size_t)n * kMlpOut * 4, s);
+    mlp_input_device(ctx, dx, n, W.x.as<__nv_bfloat16>());
+    mlp_infer_device(ctx, W.x.as<__nv_bfloat16>(), n, W.o.as<float>());
+    OLPT_CUDA(cudaMemcpyAsync(out, W.o.p, (size_t)n * kMlpOut * 4,
+                              on_device ? cudaMemcpyDeviceToDevice : cudaMemcpyDeviceToHost, s));
+    OLPT_CUDA(cudaStreamSynchronize(s));
+  });
+}
+
+olpt_status_t olpt_mlp_train_step(olpt_ctx* ctx, int64_t n, const float* x, const float* targets,
+                                  int on_device, double lr, double ghost_weight, int update,
+                                  double* loss, float* grad) {
+  return guard(ctx, [&] {
+    OLPT_REQUIRE(n > 0 && n < (int64_t)INT32_MAX && x && targets, OLPT_ERR_INVALID_ARG,
+                 "mlp_train_step: bad arguments");
+    MlpWork& W = ctx->mlp;
+    cudaStream_t s = ctx->stream;
+    const float* dx = x;
+    const float* dt = targets;
+    if (!on_device) {
+      W.xin.ensure((size_t)n * OLPT_MLP_IN * 4, s);
+      W.tgt.ensure((size_t)n * kMlpOut * 4, s);
+      OLPT_CUDA(cudaMemcpyAsync(W.xin.p, x, (size_t)n * OLPT_MLP_IN * 4, cudaMemcpyHostToDevice, s));
+      OLPT_CUDA(cudaMemcpyAsync(W.tgt.p, targets, (size_t)n * kMlpOut * 4, cudaMemcpyHostToDevice,
+                                s));
+      dx = W.xin.as<float>();
+      dt = W.tgt.as<float>();
+    }
+    const double l = mlp_train_device(ctx, dx, dt, n, lr, ghost_weight, update != 0);
+    if (loss) *loss = l;
+    if (grad) {
+      OLPT_CUDA(cudaMemcpyAsync(grad, W.grad.p, (size_t)kMlpParams * 4, cudaMemcpyDeviceToHost, s));
+      OLPT_CUDA(cudaStreamSynchronize(s));
+    }
+  });
+}
+
+olpt_status_t olpt_mlp_features(olpt_ctx* ctx, const olpt_shake_params* p, float* x,
+                                int on_device) {
+  return guard(ctx, [&] {
+    OLPT_REQUIRE(p, OLPT_ERR_INVALID_ARG, "null params");
+    const ShakeParams sp = to_shake_params(p);
+    const int64_t n = ctx->obj.n;
+    if (n == 0) return;
+    OLPT_REQUIRE(x, OLPT_ERR_INVALID_ARG, "null output");
+    residual_all_device(ctx, sp);
+    MlpWork& W = ctx->mlp;
+    cudaStream_t s = ctx->stream;
+    W.x.ensure((size_t)n * kMlpInPad * 2, s);
+    float* f = x;
+    if (!on_device) {
+      W.xin.ensure((size_t)n * OLPT_MLP_IN * 4, s);
+      f = W.xin.as<float>();
+    }
+    mlp_features_device(ctx, sp, W.x.as<__nv_bfloat16>(), f);
+    if (!on_device)
+      OLPT_CUDA(cudaMemcpyAsync(x, f, (size_t)n * OLPT_MLP_IN * 4, cudaMemcpyDeviceToHost, s));
+    OLPT_CUDA(cudaStreamSynchronize(s));
+  });
+}
+
+olpt_status_t olpt_learned_configure(olpt_ctx* ctx, const olpt_learned_params* p) {
+  return guard(ctx, [&] {
+    OLPT_REQUIRE(p, OLPT_ERR_INVALID_ARG, "null params");
+    OLPT_REQUIRE(p->out_scale_mm > 0 && p->refine_loops >= 0 && p->refine_width_mm >= 0,
+                 OLPT_ERR_INVALID_ARG, "learned params out of range");
+    OLPT_REQUIRE(!p->enable || ctx->mlp.ready, OLPT_ERR_INVALID_ARG,
+                 "learned shake enabled before the network was initialised");
+    LearnedParams& lp = ctx->mlp.lp;
+    lp.enable = p->enable;
+    lp.out_scale_mm = p->out_scale_mm;
+    lp.ghost_logit = p->ghost_logit;
+    lp.refine_loops = p->refine_loops;
+    lp.refine_width_mm = p->refine_width_mm;
+    lp.fallback_residual = p->fallback_residual;
+  });
+}
+
+olpt_status_t olpt_shake_learned(olpt_ctx* ctx, const olpt_shake_params* p) {
+  return guard(ctx, [&] {
+    OLPT_REQUIRE(p, OLPT_ERR_INVALID_ARG, "null params");
+    learned_shake_device(ctx, to_shake_params(p));
+    OLPT_CUDA(cudaStreamSynchronize(ctx->stream));
+  });
+}
+
+olpt_status_t olpt_learned_stats(olpt_ctx* ctx, int64_t* n_learned, int64_t* n_fallback) {
+  return guard(ctx, [&] {
+    if (n_learned) *n_learned = ctx->mlp.n_learned;
+    if (n_fallback) *n_fallback = ctx->mlp.n_fallback;
+  });
+}
+
+olpt_status_t olpt_bf16_gemm(olpt_ctx* ctx, int M, int N, int K, const uint16_t* A,
+                             const uint16_t* B, const float* bias, int gelu, float* out) {
+  return guard(ctx, [&] {
+    OLPT_REQUIRE(M > 0 && N > 0 && K > 0 && A && B && out, OLPT_ERR_INVALID_ARG,
+                 "bf16_gemm: bad arguments");
+    cudaStream_t s = ctx->stream;
+    const int ld = (K + 7) / 8 * 8;
+    DevBuf dA, dB, dBias, dO, dErr;
+    dA.ensure((size_t)M * ld * 2, s);
+    dB.ensure((size_t)N * ld * 2, s);
+    dO.ensure((size_t)M * N * 4, s);
+    dErr.ensure(16, s);
+    OLPT_CUDA(cudaMemsetAsync(dErr.p, 0, 16, s));
+    OLPT_CUDA(cudaMemcpy2DAsync(dA.p, (size_t)ld * 2, A, (size_t)K * 2, (size_t)K * 2, M,
+                                cudaMemcpyHostToDevice, s));
+    OLPT_CUDA(cudaMemcpy2DAsync(dB.p, (size_t)ld * 2, B, (size_t)K * 2, (size_t)K * 2, N,
+                                cudaMemcpyHostToDevice, s));
+    GemmEpilogue e;
+    if (bias) {
+      dBias.ensure((size_t)N * 4, s);
+      OLPT_CUDA(cudaMemcpyAsync(dBias.p, bias, (size_t)N * 4, cudaMemcpyHostToDevice, s));
+      e.bias = dBias.as<float>();
+    }
+    e.out_f32 = dO.as<float>();
+    e.ld_f32 = N;
+    e.gelu = false;
+    gemm_bf16(dA.as<__nv_bfloat16>(), ld, dB.as<__nv_bfloat16>(), ld, M, N, K, e, 1,
+              dErr.as<int>(), s);
+    if (gelu) gelu_inplace_device(dO.as<float>(), (int64_t)M * N, s);
+    int err = 0;
+    OLPT_CUDA(cudaMemcpyAsync(&err, dErr.p, sizeof(int), cudaMemcpyDeviceToHost, s));
+    OLPT_CUDA(cudaMemcpyAsync(out, dO.p, (size_t)M * N * 4, cudaMemcpyDeviceToHost, s));
+    OLPT_CUDA(cudaStreamSynchronize(s));
+    for (DevBuf* b : {&dA, &dB, &dBias, &dO, &dErr}) b->release(s);
+    OLPT_REQUIRE(err == 0, OLPT_ERR_TIMEOUT, "tensor-core GEMM: a pipeline wait timed out");
   });
 }
 

@@ -172,7 +172,10 @@ void single_iteration(olpt_ctx* ctx, const IprParams& p, const SmParams& sm) {
   if (stereo_objects(ctx, r) == 0) return;
   {
     PhaseTimer pt(ctx->prof, PH_SHAKE);
-    shake_device(ctx, p.shake);
+    if (ctx->mlp.lp.enable)
+      learned_shake_device(ctx, p.shake);
+    else
+      shake_device(ctx, p.shake);
     if (ctx->prof.on) OLPT_CUDA(cudaStreamSynchronize(ctx->stream));
   }
   PhaseTimer pt(ctx->prof, PH_OUTPUT);

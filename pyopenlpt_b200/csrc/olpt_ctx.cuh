@@ -10,6 +10,7 @@
 
 #include "../../include/olpt.h"
 #include "olpt_device.cuh"
+#include "olpt_mlp.h"
 #include "olpt_prof.h"
 #include "olpt_shake.h"
 #include "olpt_stb.h"
@@ -290,6 +291,53 @@ struct StbState {
   StbWork w;
 };
 
+// Device state of the learned proposal (mlp.cu): f32 master parameters, Adam moments
+// and gradients (flat, kMlpParams), bf16 weight copies for the GEMMs (row-major and
+// transposed), and the activations of one batch.
+struct MlpWork {
+  bool ready = false;
+  int adam_t = 0;
+  LearnedParams lp;
+  int64_t n_learned = 0, n_fallback = 0;  // objects through the learned shake / its fallback
+  int64_t cap = 0;  // batch capacity of the activation buffers
+  DevBuf master, grad, am, av, wb1, wb2, wb3, wt2, wt3;
+  DevBuf x, xt, xin, tgt, z1, z2, z3, h1, h2, h3, h1t, h2t, o, dout;
+  DevBuf dz1f, dz2f, dz3f, dz2b, dz3b, dz1t, dz2t, dz3t, part, hpart, loss, err;
+  DevBuf keep, pos, start_xyz, act, nres;
+  void release(cudaStream_t s) {
+    for (DevBuf* b : {&master, &grad, &am, &av, &wb1, &wb2, &wb3, &wt2, &wt3, &x, &xt, &xin, &tgt,
+                      &z1, &z2, &z3, &h1, &h2, &h3, &h1t, &h2t, &o, &dout, &dz1f, &dz2f, &dz3f,
+                      &dz2b, &dz3b, &dz1t, &dz2t, &dz3t, &part, &hpart, &loss, &err, &keep, &pos,
+                      &start_xyz, &act, &nres})
+      b->release(s);
+    ready = false;
+    cap = 0;
+  }
+};
+
+// mlp.cu
+void mlp_init(olpt_ctx* ctx, uint64_t seed);
+void mlp_set_params(olpt_ctx* ctx, const float* host);
+void mlp_get_params(olpt_ctx* ctx, float* host);
+// features of the context's objects against residual planes computed with all of
+// them (FP32 or FP64 planes per sp.precision); x: n x kMlpInPad bf16 (device),
+// f32 (optional, device): n x kMlpIn
+void mlp_features_device(olpt_ctx* ctx, const ShakeParams& sp, __nv_bfloat16* x, float* f32);
+// f32 rows of kMlpIn (device) -> bf16 rows of kMlpInPad
+void mlp_input_device(olpt_ctx* ctx, const float* x_f32, int64_t n, __nv_bfloat16* x);
+void gelu_inplace_device(float* p, int64_t n, cudaStream_t s);
+// residual planes of the current images with every object projected (the first step
+// of a shake iteration)
+void residual_all_device(olpt_ctx* ctx, const ShakeParams& sp);
+// o (device, n x 4) = network(x)
+void mlp_infer_device(olpt_ctx* ctx, const __nv_bfloat16* x, int64_t n, float* o);
+// one training batch: loss (mean), gradients into MlpWork::grad, Adam update when lr > 0
+double mlp_train_device(olpt_ctx* ctx, const float* x_f32, const float* tgt, int64_t n, double lr,
+                        double ghost_weight, bool update);
+// the learned shake: features -> network -> correction and ghost pruning -> short
+// plain refinement -> full plain shake for objects whose residue stays high
+void learned_shake_device(olpt_ctx* ctx, const ShakeParams& sp);
+
 void stb_configure(olpt_ctx* ctx, const StbParams& p, const IprParams& ipr);
 void stb_process_frame(olpt_ctx* ctx, int frame);
 std::deque<TrackH>& stb_list(olpt_ctx* ctx, int which);
@@ -337,6 +385,9 @@ struct olpt_ctx {
 
   // Shake-the-Box frame loop
   olpt::StbState stb;
+
+  // learned proposal
+  olpt::MlpWork mlp;
 
   // optional per-kernel event timing
   olpt::Prof prof;

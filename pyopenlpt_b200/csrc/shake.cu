@@ -30,6 +30,7 @@
 #include <vector>
 
 #include "olpt_ctx.cuh"
+#include "olpt_shake_dev.cuh"
 #include "olpt_otf.cuh"
 #include "olpt_scan.cuh"
 #include "olpt_shake.h"
@@ -37,59 +38,6 @@
 namespace olpt {
 
 constexpr int kTile = 32;
-
-struct Rect {
-  int rmin, rmax, cmin, cmax;  // [min, max)
-};
-
-// Shake::calROIBound (Shake.cpp:246-277)
-__host__ __device__ __forceinline__ Rect roi_bound(int H, int W, double cx, double cy, double dx,
-                                                   double dy) {
-  Rect e{1, 0, 1, 0};
-  if (H <= 0 || W <= 0 || dx <= 0.0 || dy <= 0.0 || cx <= 0 || cy <= 0 || cx >= W || cy >= H)
-    return e;
-  const int width = (int)round(2.0 * dx);
-  const int height = (int)round(2.0 * dy);
-  int cmin = (int)round(cx - (width - 1) / 2.0);
-  int rmin = (int)round(cy - (height - 1) / 2.0);
-  int cmax = cmin + width;
-  int rmax = rmin + height;
-  rmin = rmin > 0 ? rmin : 0;
-  cmin = cmin > 0 ? cmin : 0;
-  rmax = rmax < H ? rmax : H;
-  cmax = cmax < W ? cmax : W;
-  if (rmax < rmin || cmax < cmin) return e;
-  return Rect{rmin, rmax, cmin, cmax};
-}
-
-__device__ __forceinline__ bool rect_empty(const Rect& r) {
-  return r.rmax < r.rmin || r.cmax < r.cmin;
-}
-
-// TracerShakeStrategy::gaussIntensity (Shake.cpp:901-916)
-template <typename Real>
-__device__ __forceinline__ Real gauss(int col, int row, double u, double v, const Real* o) {
-  const Real dx = (Real)((double)col - u);
-  const Real dy = (Real)((double)row - v);
-  const Real xx = dx * o[3] + dy * o[4];
-  const Real yy = -dx * o[4] + dy * o[3];
-  const Real val = o[0] * exp(-(o[1] * xx * xx + o[2] * yy * yy));
-  return val > (Real)0 ? val : (Real)0;
-}
-
-template <typename T>
-__device__ __forceinline__ double load_px(const unsigned char* base, int64_t pitch, int r, int c) {
-  return (double)reinterpret_cast<const T*>(base + (int64_t)r * pitch)[c];
-}
-
-__device__ __forceinline__ double load_any(const PlaneView& p, int r, int c) {
-  switch (p.dtype) {
-    case OLPT_U8: return load_px<uint8_t>(p.p, p.pitch, r, c);
-    case OLPT_U16: return load_px<uint16_t>(p.p, p.pitch, r, c);
-    case OLPT_F32: return load_px<float>(p.p, p.pitch, r, c);
-    default: return load_px<double>(p.p, p.pitch, r, c);
-  }
-}
 
 namespace {
 
@@ -345,7 +293,8 @@ __device__ __forceinline__ bool in_roi(const Rect& R, double u, double w) {
 template <typename Real>
 __global__ void __launch_bounds__(128, 4) shake_kernel(ShakeView v, int64_t n, double* xyz,
                                                     double* uv, const Real* otfp, double* score,
-                                                    double delta) {
+                                                    double delta, const uint8_t* active,
+                                                    double* resid_out) {
   extern __shared__ __align__(16) unsigned char smem_raw[];
   const int warp_in_blk = threadIdx.x >> 5;
   const int lane = threadIdx.x & 31;
@@ -359,8 +308,10 @@ __global__ void __launch_bounds__(128, 4) shake_kernel(ShakeView v, int64_t n, d
   S.otf = reinterpret_cast<Real*>(base + v.off_otf);
   S.uvc = reinterpret_cast<double*>(base + v.off_uv);
   if (o >= n) return;
+  if (active && !active[o]) return;  // held fixed (learned shake: not in this pass)
 
   double P[3] = {xyz[3 * o], xyz[3 * o + 1], xyz[3 * o + 2]};
+  double f_final = 0.0;
   // ---- buildROIInfo (Shake.cpp:279-328)
   Rect roi[OLPT_MAX_CAM];
   const double* uvo = uv + o * C * 2;
@@ -515,6 +466,7 @@ __global__ void __launch_bounds__(128, 4) shake_kernel(ShakeView v, int64_t n, d
         best = t;
       }
     P[ax] = ca[best];
+    f_final = bf;  // after the last axis: the residue at the final position
   }
 
   // ---- final projection + calObjectScore (Shake.cpp:668-782)
@@ -596,6 +548,7 @@ __global__ void __launch_bounds__(128, 4) shake_kernel(ShakeView v, int64_t n, d
     xyz[3 * o + 1] = P[1];
     xyz[3 * o + 2] = P[2];
     score[o] *= sc;
+    if (resid_out) resid_out[o] = f_final;
   }
   if (lane < C) {
     uv[(o * C + lane) * 2] = S.uvc[2 * lane];
@@ -722,6 +675,66 @@ __global__ void fill_kernel(double* p, int64_t n, double v) {
 }  // namespace
 
 // ---------------------------------------------------------------- host drivers
+// ---------------------------------------------------------------- learned shake
+// correction in units of scale (mm); keep = not a ghost by the network's logit
+__global__ void learned_apply_kernel(double* xyz, const float* o, int64_t n, double scale,
+                                     float ghost_logit, int* keep) {
+  const int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+  if (i >= n) return;
+  const float* oi = o + 4 * i;
+  const bool fin = isfinite(oi[0]) && isfinite(oi[1]) && isfinite(oi[2]) && isfinite(oi[3]);
+  if (fin)
+    for (int d = 0; d < 3; ++d) xyz[3 * i + d] += (double)oi[d] * scale;
+  keep[i] = (fin && oi[3] <= ghost_logit) ? 1 : 0;
+}
+
+__global__ void compact_xyz_kernel(const int* keep, const int* pos, int64_t n, const double* a,
+                                   double* a_out, const double* b, double* b_out) {
+  const int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+  if (i >= n || !keep[i]) return;
+  const int64_t k = pos[i];
+  for (int d = 0; d < 3; ++d) {
+    a_out[3 * k + d] = a[3 * i + d];
+    b_out[3 * k + d] = b[3 * i + d];
+  }
+}
+
+// objects whose residue after the refinement, divided by the mean squared OTF
+// amplitude over the active cameras, exceeds thr (or is not finite) restart the
+// full shake from their stereo position
+template <typename Real>
+__global__ void fallback_kernel(const double* res, const Real* otfp, const CamDev* cams, int C,
+                                int64_t n, double thr, uint8_t* act, double* xyz,
+                                const double* start, double* score, int* count) {
+  const int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+  if (i >= n) return;
+  double a2 = 0.0;
+  int k = 0;
+  for (int c = 0; c < C; ++c) {
+    if (!cams[c].is_active) continue;
+    const double a = (double)otfp[(i * C + c) * 5];
+    a2 += a * a;
+    ++k;
+  }
+  a2 = k > 0 ? a2 / k : 1.0;
+  const double r = res[i] / (a2 > 1e-12 ? a2 : 1e-12);
+  const bool fb = !(r <= thr);
+  act[i] = fb ? 1 : 0;
+  if (fb) {
+    for (int d = 0; d < 3; ++d) xyz[3 * i + d] = start[3 * i + d];
+    score[i] = 1.0;
+    atomicAdd(count, 1);
+  }
+}
+
+// refined objects carry a score over refine_loops iterations: bring it to the
+// n_shake_loop scale of the plain schedule
+__global__ void score_scale_kernel(double* score, const uint8_t* act, int64_t n, double expo) {
+  const int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+  if (i >= n || act[i]) return;
+  score[i] = pow(score[i], expo);
+}
+
 static ShakeView make_view(olpt_ctx* ctx, const ShakeParams& sp, bool fp64) {
   ShakeView v{};
   v.n_cam = ctx->n_cam;
@@ -812,25 +825,22 @@ static void residual_pass(olpt_ctx* ctx, ShakeView& v, const uint8_t* flags, int
   OLPT_CUDA(cudaGetLastError());
 }
 
+// n_loop shake iterations from the width delta (halved per iteration, clamped at the
+// minimum); objects with active[o] == 0 stay fixed but still enter the residual
 template <typename Real>
-static void shake_impl(olpt_ctx* ctx, const ShakeParams& sp) {
-  const bool fp64 = sizeof(Real) == 8;
+static void shake_iterations(olpt_ctx* ctx, const ShakeParams& sp, ShakeView& v, int n_loop,
+                             double delta, const uint8_t* active, double* resid_out) {
   cudaStream_t s = ctx->stream;
-  ShakeView v = make_view(ctx, sp, fp64);
-  ensure_residual_planes(ctx, v, fp64);
   const int64_t n = ctx->obj.n;
   const int C = ctx->n_cam;
   ShakeWork& W = ctx->shk;
-  ctx->obj.ensure(std::max<int64_t>(n, 1), C, s);
-  if (n > 0) fill_kernel<<<OLPT_G(nblk(n)), 256, 0, s>>>(ctx->obj.score.as<double>(), n, 1.0);
-  double delta = sp.shake_width;
   double dmin = sp.shakewidth_min;
-  dmin = (dmin > 0) ? dmin : delta / 20;
+  dmin = (dmin > 0) ? dmin : sp.shake_width / 20;
   const int warps_per_blk = 4;
   const size_t smem = v.smem_per_warp * warps_per_blk;
   OLPT_CUDA(cudaFuncSetAttribute(shake_kernel<Real>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                  (int)smem));
-  for (int it = 0; it < sp.n_shake_loop; ++it) {
+  for (int it = 0; it < n_loop; ++it) {
     residual_pass<Real>(ctx, v, nullptr, 0, 0);
     // algorithmic bytes: the augmented ROI of every active camera plus the object
     // state (xyz, projections, OTF parameters, score) read and written once
@@ -842,13 +852,20 @@ static void shake_impl(olpt_ctx* ctx, const ShakeParams& sp) {
     if (n > 0)
       shake_kernel<Real><<<OLPT_G(nblk(n, warps_per_blk)), 32 * warps_per_blk, smem, s>>>(
           v, n, ctx->obj.xyz.as<double>(), ctx->obj.uv.as<double>(), W.otfp.as<Real>(),
-          ctx->obj.score.as<double>(), delta);
+          ctx->obj.score.as<double>(), delta, active, resid_out);
     ctx->prof.end(PROF_SHAKE, pid, s, bytes);
     OLPT_CUDA(cudaGetLastError());
     delta *= 0.5;
     if (delta < dmin) delta = dmin;
   }
-  // repeated + ghost flags
+}
+
+// Shake::runShake (Shake.cpp:103-136): repeated objects (greedy over the tol_3d
+// neighbourhood) and ghosts (score below thred_ghost x mean score)
+static void shake_flags(olpt_ctx* ctx, const ShakeParams& sp) {
+  cudaStream_t s = ctx->stream;
+  const int64_t n = ctx->obj.n;
+  ShakeWork& W = ctx->shk;
   W.rep.ensure(n + 16, s);
   OLPT_CUDA(cudaMemsetAsync(W.rep.p, 0, n + 16, s));
   if (n > 0) {
@@ -877,6 +894,119 @@ static void shake_impl(olpt_ctx* ctx, const ShakeParams& sp) {
                                     sp.thred_ghost, ctx->obj.flags.as<uint8_t>());
     OLPT_CUDA(cudaGetLastError());
   }
+}
+
+template <typename Real>
+static void shake_impl(olpt_ctx* ctx, const ShakeParams& sp) {
+  const bool fp64 = sizeof(Real) == 8;
+  cudaStream_t s = ctx->stream;
+  ShakeView v = make_view(ctx, sp, fp64);
+  ensure_residual_planes(ctx, v, fp64);
+  const int64_t n = ctx->obj.n;
+  ctx->obj.ensure(std::max<int64_t>(n, 1), ctx->n_cam, s);
+  if (n > 0) fill_kernel<<<OLPT_G(nblk(n)), 256, 0, s>>>(ctx->obj.score.as<double>(), n, 1.0);
+  shake_iterations<Real>(ctx, sp, v, sp.n_shake_loop, sp.shake_width, nullptr, nullptr);
+  shake_flags(ctx, sp);
+}
+
+template <typename Real>
+static void learned_impl(olpt_ctx* ctx, const ShakeParams& sp) {
+  const bool fp64 = sizeof(Real) == 8;
+  cudaStream_t s = ctx->stream;
+  MlpWork& M = ctx->mlp;
+  const LearnedParams& lp = M.lp;
+  ShakeView v = make_view(ctx, sp, fp64);
+  ensure_residual_planes(ctx, v, fp64);
+  int64_t n = ctx->obj.n;
+  const int C = ctx->n_cam;
+  if (n > 0) {
+    // 1. residual with every candidate at its stereo position, features, network
+    residual_pass<Real>(ctx, v, nullptr, 0, 0);
+    M.x.ensure((size_t)n * kMlpInPad * 2, s);
+    mlp_features_device(ctx, sp, M.x.as<__nv_bfloat16>(), nullptr);
+    M.o.ensure((size_t)n * kMlpOut * 4, s);
+    mlp_infer_device(ctx, M.x.as<__nv_bfloat16>(), n, M.o.as<float>());
+    // 2. correction, and the network's ghosts leave before any shaking
+    M.keep.ensure((size_t)(n + 1) * sizeof(int), s);
+    M.pos.ensure((size_t)(n + 1) * sizeof(int), s);
+    M.start_xyz.ensure((size_t)n * 3 * sizeof(double), s);
+    OLPT_CUDA(cudaMemcpyAsync(M.start_xyz.p, ctx->obj.xyz.p, (size_t)n * 3 * sizeof(double),
+                              cudaMemcpyDeviceToDevice, s));
+    learned_apply_kernel<<<OLPT_G(nblk(n)), 256, 0, s>>>(ctx->obj.xyz.as<double>(), M.o.as<float>(),
+                                                        n, lp.out_scale_mm, (float)lp.ghost_logit,
+                                                        M.keep.as<int>());
+    exclusive_scan(M.keep.as<int>(), (int)n, M.pos.as<int>(), ctx->shk.scan_tmp, s);
+    int kept = 0;
+    OLPT_CUDA(cudaMemcpyAsync(&kept, M.pos.as<int>() + n, sizeof(int), cudaMemcpyDeviceToHost, s));
+    OLPT_CUDA(cudaStreamSynchronize(s));
+    // compacted copies (through the scratch pair act / nres, then back)
+    M.act.ensure((size_t)(n + 1) * 3 * sizeof(double), s);
+    M.nres.ensure((size_t)(n + 1) * 3 * sizeof(double), s);
+    compact_xyz_kernel<<<OLPT_G(nblk(n)), 256, 0, s>>>(
+        M.keep.as<int>(), M.pos.as<int>(), n, ctx->obj.xyz.as<double>(), M.act.as<double>(),
+        M.start_xyz.as<double>(), M.nres.as<double>());
+    OLPT_CUDA(cudaGetLastError());
+    n = kept;
+    ctx->obj.n = n;
+    if (n > 0) {
+      OLPT_CUDA(cudaMemcpyAsync(ctx->obj.xyz.p, M.act.p, (size_t)n * 3 * sizeof(double),
+                                cudaMemcpyDeviceToDevice, s));
+      OLPT_CUDA(cudaMemcpyAsync(M.start_xyz.p, M.nres.p, (size_t)n * 3 * sizeof(double),
+                                cudaMemcpyDeviceToDevice, s));
+    }
+  }
+  ctx->obj.ensure(std::max<int64_t>(n, 1), C, s);
+  if (n > 0) {
+    // 3. short plain refinement from the corrected positions
+    fill_kernel<<<OLPT_G(nblk(n)), 256, 0, s>>>(ctx->obj.score.as<double>(), n, 1.0);
+    M.nres.ensure((size_t)(n + 1) * sizeof(double), s);
+    shake_iterations<Real>(ctx, sp, v, lp.refine_loops, lp.refine_width_mm, nullptr,
+                           M.nres.as<double>());
+    // 4. fallback: the full plain shake for objects whose residue stays high
+    M.act.ensure((size_t)n + 16, s);
+    M.keep.ensure(16, s);
+    int* cnt = M.keep.as<int>();
+    OLPT_CUDA(cudaMemsetAsync(cnt, 0, sizeof(int), s));
+    fallback_kernel<Real><<<OLPT_G(nblk(n)), 256, 0, s>>>(
+        M.nres.as<double>(), ctx->shk.otfp.as<Real>(), ctx->cams_d.as<CamDev>(), C, n,
+        lp.fallback_residual, M.act.as<uint8_t>(), ctx->obj.xyz.as<double>(),
+        M.start_xyz.as<double>(), ctx->obj.score.as<double>(), cnt);
+    OLPT_CUDA(cudaGetLastError());
+    int n_fb = 0;
+    OLPT_CUDA(cudaMemcpyAsync(&n_fb, cnt, sizeof(int), cudaMemcpyDeviceToHost, s));
+    OLPT_CUDA(cudaStreamSynchronize(s));
+    M.n_fallback += n_fb;
+    M.n_learned += n;
+    if (n_fb > 0)
+      shake_iterations<Real>(ctx, sp, v, sp.n_shake_loop, sp.shake_width, M.act.as<uint8_t>(),
+                             nullptr);
+    if (lp.refine_loops > 0 && lp.refine_loops != sp.n_shake_loop)
+      score_scale_kernel<<<OLPT_G(nblk(n)), 256, 0, s>>>(
+          ctx->obj.score.as<double>(), M.act.as<uint8_t>(), n,
+          (double)sp.n_shake_loop / (double)lp.refine_loops);
+    OLPT_CUDA(cudaGetLastError());
+  }
+  shake_flags(ctx, sp);
+}
+
+void residual_all_device(olpt_ctx* ctx, const ShakeParams& sp) {
+  const bool fp64 = sp.precision == 1;
+  ShakeView v = make_view(ctx, sp, fp64);
+  ensure_residual_planes(ctx, v, fp64);
+  if (fp64)
+    residual_pass<double>(ctx, v, nullptr, 0, 0);
+  else
+    residual_pass<float>(ctx, v, nullptr, 0, 0);
+}
+
+void learned_shake_device(olpt_ctx* ctx, const ShakeParams& sp) {
+  OLPT_REQUIRE(ctx->n_cam == kMlpCams, OLPT_ERR_UNSUPPORTED,
+               "the learned shake is defined for 4 cameras");
+  OLPT_REQUIRE(ctx->mlp.ready, OLPT_ERR_INVALID_ARG, "learned shake: network not initialised");
+  if (sp.precision == 1)
+    learned_impl<double>(ctx, sp);
+  else
+    learned_impl<float>(ctx, sp);
 }
 
 void shake_device(olpt_ctx* ctx, const ShakeParams& sp) {
