@@ -1,0 +1,158 @@
+"""The learned proposal end to end: training tuples generated by the plain GPU
+pipeline, training on the device kernels, calibration of the fallback threshold,
+and evaluation against the generator's ground truth.
+
+Tuples come from IPR loops run step by step through the C ABI exactly as
+``olpt_ipr_run`` runs them (detection, stereo matching, shake, residual): for every
+candidate of a loop, the features against the residual with all candidates
+(``olpt_mlp_features``, the input the learned shake sees), the converged plain-shake
+correction in units of ``out_scale_mm``, and a ghost label from the ground truth (no
+particle within ``ghost_tol_mm`` of the converged position).
+"""
+from __future__ import annotations
+
+import dataclasses
+import time
+from typing import Dict, List, Optional, Sequence, Tuple
+
+import numpy as np
+from scipy.spatial import cKDTree
+
+from . import _ffi, synth
+
+
+@dataclasses.dataclass
+class LearnedSettings:
+    out_scale_mm: float = 0.05
+    ghost_tol_mm: float = 0.1
+    ghost_logit: float = 2.0
+    refine_loops: int = 1
+    refine_width_mm: float = 0.02
+    fallback_residual: float = 0.01
+
+    def params(self, enable: bool = True) -> _ffi.LearnedParams:
+        return _ffi.LearnedParams(enable=int(enable), out_scale_mm=self.out_scale_mm,
+                                  ghost_logit=self.ghost_logit, refine_loops=self.refine_loops,
+                                  refine_width_mm=self.refine_width_mm,
+                                  fallback_residual=self.fallback_residual)
+
+
+def scene(seed: int, ppp: float, size: int = 1024, n_cam: int = 4,
+          bc: Optional[Tuple[float, float]] = None) -> synth.Scene:
+    """A learned-proposal frame: 4 cameras, size^2 uint8, ppp particles per pixel,
+    OTF b, c uniform in [0.3, 0.8] unless given."""
+    rng = np.random.default_rng(10_000 + seed)
+    b, c = bc if bc is not None else rng.uniform(0.3, 0.8, 2)
+    return synth.make_scene(n_particles=int(ppp * size * size), n_cam=n_cam, size=size,
+                            focal=5000.0 * size / 1024.0, b=float(b), c=float(c), seed=seed)
+
+
+def bind(ctx: _ffi.Context, sc: synth.Scene):
+    """Cameras, OTF table and images of a frame into the context."""
+    ctx.upload_cameras([_ffi.camera_desc_from_pinhole(c) for c in sc.cams])
+    ctx.upload_otf(2, 2, 2, sc.volume, synth.otf_table_array(sc.n_cam, sc.otf_abc))
+    ctx.upload_images(sc.images)
+
+
+def collect(ctx: _ffi.Context, sc: synth.Scene, s: synth.IPRSettings,
+            ls: LearnedSettings) -> Tuple[np.ndarray, np.ndarray]:
+    """Training tuples of one frame: features (n x 493) and targets (n x 4)."""
+    bind(ctx, sc)
+    ctx.learned_configure(ls.params(enable=False))
+    sm = _ffi.sm_params(s, sc.volume)
+    sp = _ffi.shake_params(s, 0)
+    tree = cKDTree(sc.xyz)
+    tol0 = sm.tol_2d_px
+    xs: List[np.ndarray] = []
+    ts: List[np.ndarray] = []
+    for loop in range(s.n_loop_ipr):
+        sm.tol_2d_px = tol0 * 1.5 ** loop
+        ctx.find_peaks(s.min_obj_int)
+        _, nm = ctx.stereo_match(sm)
+        if nm == 0:
+            break
+        x = ctx.mlp_features(sp)
+        x0 = ctx.objects()["xyz"]
+        ctx.shake(sp)
+        o = ctx.objects()
+        d, _ = tree.query(o["xyz"])
+        t = np.zeros((nm, 4), np.float32)
+        t[:, :3] = (o["xyz"] - x0) / ls.out_scale_mm
+        t[:, 3] = (d > ls.ghost_tol_mm).astype(np.float32)
+        xs.append(x)
+        ts.append(t)
+        ctx.residual(sp, use_flags=True, make_current=True)
+    return np.concatenate(xs), np.concatenate(ts)
+
+
+def train(ctx: _ffi.Context, x: np.ndarray, t: np.ndarray, steps: int, batch: int = 8192,
+          lr: float = 2e-3, ghost_weight: float = 1.0, seed: int = 0,
+          time_budget_s: Optional[float] = None) -> List[float]:
+    """Adam on random mini-batches, learning rate decayed by cosine to 5% of lr."""
+    rng = np.random.default_rng(seed)
+    losses = []
+    t0 = time.perf_counter()
+    n = len(x)
+    for it in range(steps):
+        idx = rng.integers(0, n, min(batch, n))
+        a = lr * (0.05 + 0.95 * 0.5 * (1 + np.cos(np.pi * it / max(steps, 1))))
+        losses.append(ctx.mlp_train_step(x[idx], t[idx], lr=a, ghost_weight=ghost_weight))
+        if time_budget_s is not None and time.perf_counter() - t0 > time_budget_s:
+            break
+    return losses
+
+
+def metrics(xyz: np.ndarray, truth: np.ndarray) -> Dict[str, float]:
+    """Recall and ghost rate at 0.05 and 0.1 mm, RMSE of the matched positions."""
+    out: Dict[str, float] = {"n": float(len(xyz))}
+    if len(xyz) == 0:
+        return {**out, "recall_05": 0.0, "recall_10": 0.0, "ghost_05": 0.0, "ghost_10": 0.0,
+                "rmse_mm": float("nan")}
+    rt = cKDTree(xyz)
+    gt = cKDTree(truth)
+    d_truth, _ = rt.query(truth)
+    d_rec, _ = gt.query(xyz)
+    for tol, key in ((0.05, "05"), (0.1, "10")):
+        out["recall_" + key] = float(np.mean(d_truth <= tol))
+        out["ghost_" + key] = float(np.mean(d_rec > tol))
+    ok = d_rec <= 0.1
+    out["rmse_mm"] = float(np.sqrt(np.mean(d_rec[ok] ** 2))) if ok.any() else float("nan")
+    return out
+
+
+def run_ipr(ctx: _ffi.Context, sc: synth.Scene, s: synth.IPRSettings,
+            ls: Optional[LearnedSettings]) -> Dict[str, float]:
+    """One olpt_ipr_run on the frame, plain (ls None) or learned; metrics + wall ms."""
+    bind(ctx, sc)
+    ctx.learned_configure((ls or LearnedSettings()).params(enable=ls is not None))
+    p = _ffi.ipr_params(s, sc.volume)
+    t0 = time.perf_counter()
+    n = ctx.ipr_run(p)
+    ms = 1e3 * (time.perf_counter() - t0)
+    xyz, _ = ctx.ipr_result(n)
+    m = metrics(xyz, sc.xyz)
+    m["ms"] = ms
+    return m
+
+
+def calibrate(ctx: _ffi.Context, sc: synth.Scene, s: synth.IPRSettings, ls: LearnedSettings,
+              recall_slack: float = 0.005,
+              grid: Sequence[float] = (1e9, 3.0, 1.0, 0.3, 0.1, 0.03, 0.01, 0.0)
+              ) -> Tuple[LearnedSettings, Dict[str, float], List[Tuple[float, Dict[str, float]]]]:
+    """The largest fallback threshold (fewest objects through the full shake) whose
+    recall at 0.05 mm stays within recall_slack of the plain method's and whose ghost
+    rate is not higher.  Returns the settings, the plain metrics and the sweep."""
+    plain = run_ipr(ctx, sc, s, None)
+    sweep = []
+    best = None
+    for thr in grid:
+        cand = dataclasses.replace(ls, fallback_residual=float(thr))
+        m = run_ipr(ctx, sc, s, cand)
+        sweep.append((float(thr), m))
+        if (m["recall_05"] >= plain["recall_05"] - recall_slack and
+                m["ghost_05"] <= plain["ghost_05"] + 1e-9):
+            best = cand
+            break
+    if best is None:
+        best = dataclasses.replace(ls, fallback_residual=0.0)
+    return best, plain, sweep
