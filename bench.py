@@ -334,7 +334,7 @@ class Ours:
         print(json.dumps(line), flush=True)
 
 
-def run_ours_ipr(args, o: Ours):
+def run_ours_ipr(args, o: Ours, learned=None):
     from pyopenlpt_b200 import _ffi
     torch = o.torch
     sc, s = build_scene(args.workload, 1234 + o.rank)
@@ -407,11 +407,12 @@ def run_ours_ipr(args, o: Ours):
                    "sample": "one whole frame of the same workload (IPR::runIPR compiled "
                              "from the reference sources, OpenMP)"}
         o.line(prof, dev_ms, parts, e2e_s, e2e_parts, bi, bo // max(1, args.steps), launches,
-               clk, workload_config(args.workload, s, sc=sc), cpu, {})
+               clk, workload_config(args.workload, s, sc=sc), cpu,
+               {} if learned is None else {"learned": learned})
     ctx.close()
 
 
-def run_ours_stb(args, o: Ours):
+def run_ours_stb(args, o: Ours, learned=None):
     from pyopenlpt_b200 import _ffi
     torch = o.torch
     nf = N_INIT + args.warmup + args.steps
@@ -514,16 +515,111 @@ def run_ours_stb(args, o: Ours):
         extra = {"initial_phase_ms_per_frame": [round(x, 1) for x in init_ms],
                  "extended_plus_new_per_step": ext_new / args.steps,
                  "track_lists_after": dict(zip(_ffi.TRACK_LISTS, lists))}
+        if learned is not None:
+            extra["learned"] = learned
         o.line(prof, dev_ms, parts, e2e_s, e2e_parts, bi, bo // max(1, args.steps), launches,
                clk, workload_config(args.workload, s, seq=seq, st=st), cpu, extra)
 
 
+# ----------------------------------------------------------------------------- learned
+LEARN_PPP = (0.01, 0.02, 0.03, 0.05, 0.08, 0.1)
+
+
+def learned_comparison(args, o: Ours):
+    """The learned proposal against the plain GPU form on its own workload (4 cameras,
+    1024^2 uint8, OTF b, c uniform in [0.3, 0.8]): tuples from the plain pipeline on
+    seeded frames at 0.01-0.1 ppp, training on the device, calibration on a validation
+    frame (fewest IPR loops whose recall is within 0.5% of the plain 4-loop IPR and
+    whose ghost rate is not higher, at 0.05 and 0.1 mm), then device-timed IPR of both
+    forms on held-out frames at 0.02 and 0.08 ppp."""
+    from pyopenlpt_b200 import _ffi, learned as L
+    import dataclasses
+    torch = o.torch
+    s = synth.IPRSettings()
+    ls = L.LearnedSettings()
+    ctx = _ffi.Context(o.local)
+    t0 = time.perf_counter()
+    xs, ts = [], []
+    for i in range(args.learn_frames):
+        x, t = L.collect(ctx, L.scene(i, LEARN_PPP[i % len(LEARN_PPP)]), s, ls)
+        xs.append(x)
+        ts.append(t)
+    x, t = np.concatenate(xs), np.concatenate(ts)
+    del xs, ts
+    t_collect = time.perf_counter() - t0
+    ctx.mlp_init(1)
+    t0 = time.perf_counter()
+    losses = L.train(ctx, x, t, steps=args.learn_steps, batch=8192, lr=2e-3)
+    t_train = time.perf_counter() - t0
+    n_tuples = len(x)
+    del x, t
+    k, cfg, plain_val, _ = L.calibrate(ctx, L.scene(900, 0.02), s, ls)
+    stream = torch.cuda.ExternalStream(ctx.stream())
+
+    def timed(sc, sk, lsx, reps):
+        L.bind(ctx, sc)
+        ctx.learned_configure((lsx or L.LearnedSettings()).params(enable=lsx is not None))
+        p = _ffi.ipr_params(sk, sc.volume)
+        ctx.ipr_run(p)  # warm-up
+        ms = []
+        for _ in range(reps):
+            ctx.upload_images(sc.images)
+            with torch.cuda.stream(stream):
+                o.flush.zero_()
+                e0 = torch.cuda.Event(enable_timing=True)
+                e1 = torch.cuda.Event(enable_timing=True)
+                e0.record(stream)
+            n = ctx.ipr_run(p)
+            e1.record(stream)
+            e1.synchronize()
+            ms.append(e0.elapsed_time(e1))
+        xyz, _ = ctx.ipr_result(n)
+        m = L.metrics(xyz, sc.xyz)
+        m["ms"] = float(np.median(ms))
+        m["particles_per_s"] = m["n"] / (m["ms"] * 1e-3)
+        m["true_particles_per_s"] = m["recall_10"] * len(sc.xyz) / (m["ms"] * 1e-3)
+        return {kk: round(v, 5) for kk, v in m.items()}
+
+    evals = {}
+    for i, ppp in enumerate((0.02, 0.08)):
+        sc = L.scene(901 + i, ppp)
+        plain = timed(sc, s, None, args.learn_reps)
+        a0, b0 = ctx.learned_stats()
+        learned = timed(sc, dataclasses.replace(s, n_loop_ipr=k), cfg, args.learn_reps)
+        a1, b1 = ctx.learned_stats()
+        learned["fallback_fraction"] = round((b1 - b0) / max(1, a1 - a0), 4)
+        evals[f"ppp_{ppp}"] = {
+            "n_true": len(sc.xyz), "plain": plain, "learned": learned,
+            "speedup_particles_per_s": round(learned["particles_per_s"] / plain["particles_per_s"], 3),
+            "speedup_time": round(plain["ms"] / learned["ms"], 3),
+            "meets_recall_and_ghost": L.meets(learned, plain)}
+    ctx.close()
+    return {
+        "workload": "4 pinhole cams, 1024^2 uint8, a=200, OTF b,c ~ U[0.3,0.8], noise 2; "
+                    "plain = olpt_ipr_run 4 loops x 4 shakes; learned = MLP proposal + 1 "
+                    "refine shake, calibrated loop count; device time per IPR, L2 flushed",
+        "batched": False,
+        "train": {"frames": args.learn_frames, "tuples": n_tuples, "steps": len(losses),
+                  "collect_s": round(t_collect, 1), "train_s": round(t_train, 1),
+                  "loss_first": round(losses[0], 4),
+                  "loss_last50": round(float(np.mean(losses[-50:])), 4)},
+        "calibrated": {"n_loop_ipr": k, "ghost_logit": cfg.ghost_logit,
+                       "fallback_residual": cfg.fallback_residual,
+                       "refine_loops": cfg.refine_loops, "refine_width_mm": cfg.refine_width_mm},
+        "eval": evals,
+    }
+
+
 def run_ours(args):
     o = Ours(args)
+    learned = None
+    if o.world == 1 and args.learn_frames > 0:
+        learned = learned_comparison(args, o)
+        o.torch.cuda.synchronize()
     if WORKLOADS[args.workload]["kind"] == "ipr":
-        run_ours_ipr(args, o)
+        run_ours_ipr(args, o, learned)
     else:
-        run_ours_stb(args, o)
+        run_ours_stb(args, o, learned)
     if o.world > 1:
         o.dist.destroy_process_group()
     return 0
@@ -538,6 +634,10 @@ def main():
     ap.add_argument("--workload", choices=sorted(WORKLOADS), default=DEFAULT_WORKLOAD)
     ap.add_argument("--precision", choices=["fp32", "fp64"], default="fp32")
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--learn-frames", type=int, default=24,
+                    help="frames of training tuples for the learned comparison (0 = skip)")
+    ap.add_argument("--learn-steps", type=int, default=3000)
+    ap.add_argument("--learn-reps", type=int, default=5)
     args = ap.parse_args()
     if args.warmup < 3:
         args.warmup = 3

@@ -25,10 +25,10 @@ from . import _ffi, synth
 class LearnedSettings:
     out_scale_mm: float = 0.05
     ghost_tol_mm: float = 0.1
-    ghost_logit: float = 2.0
+    ghost_logit: float = 5.0
     refine_loops: int = 1
     refine_width_mm: float = 0.02
-    fallback_residual: float = 0.01
+    fallback_residual: float = 1e9
 
     def params(self, enable: bool = True) -> _ffi.LearnedParams:
         return _ffi.LearnedParams(enable=int(enable), out_scale_mm=self.out_scale_mm,
@@ -135,24 +135,35 @@ def run_ipr(ctx: _ffi.Context, sc: synth.Scene, s: synth.IPRSettings,
     return m
 
 
+def meets(m: Dict[str, float], plain: Dict[str, float], slack: float = 0.005) -> bool:
+    """Recall within slack of the plain method's and no higher ghost rate, at both
+    0.05 and 0.1 mm."""
+    return all(m["recall_" + k] >= plain["recall_" + k] - slack and
+               m["ghost_" + k] <= plain["ghost_" + k] for k in ("05", "10"))
+
+
 def calibrate(ctx: _ffi.Context, sc: synth.Scene, s: synth.IPRSettings, ls: LearnedSettings,
-              recall_slack: float = 0.005,
-              grid: Sequence[float] = (1e9, 3.0, 1.0, 0.3, 0.1, 0.03, 0.01, 0.0)
-              ) -> Tuple[LearnedSettings, Dict[str, float], List[Tuple[float, Dict[str, float]]]]:
-    """The largest fallback threshold (fewest objects through the full shake) whose
-    recall at 0.05 mm stays within recall_slack of the plain method's and whose ghost
-    rate is not higher.  Returns the settings, the plain metrics and the sweep."""
+              loops: Sequence[int] = (1, 2, 3, 4), logits: Sequence[float] = (5.0, 3.0),
+              fallback_grid: Sequence[float] = (3.0, 1.0, 0.3, 0.1, 0.03, 0.0),
+              slack: float = 0.005):
+    """The fastest learned form that meets the plain method (s.n_loop_ipr loops) on a
+    validation frame: fewest IPR loops first, then the ghost logit; if none does, the
+    largest fallback threshold at the full loop count.  Returns (n_loop_ipr,
+    settings, plain metrics, sweep)."""
     plain = run_ipr(ctx, sc, s, None)
     sweep = []
-    best = None
-    for thr in grid:
-        cand = dataclasses.replace(ls, fallback_residual=float(thr))
+    for k in loops:
+        sk = dataclasses.replace(s, n_loop_ipr=k)
+        for g in logits:
+            cand = dataclasses.replace(ls, ghost_logit=float(g), fallback_residual=1e9)
+            m = run_ipr(ctx, sc, sk, cand)
+            sweep.append(((k, g, 1e9), m))
+            if meets(m, plain, slack):
+                return k, cand, plain, sweep
+    for thr in fallback_grid:
+        cand = dataclasses.replace(ls, ghost_logit=float(logits[0]), fallback_residual=float(thr))
         m = run_ipr(ctx, sc, s, cand)
-        sweep.append((float(thr), m))
-        if (m["recall_05"] >= plain["recall_05"] - recall_slack and
-                m["ghost_05"] <= plain["ghost_05"] + 1e-9):
-            best = cand
-            break
-    if best is None:
-        best = dataclasses.replace(ls, fallback_residual=0.0)
-    return best, plain, sweep
+        sweep.append(((s.n_loop_ipr, logits[0], thr), m))
+        if meets(m, plain, slack):
+            return s.n_loop_ipr, cand, plain, sweep
+    return s.n_loop_ipr, dataclasses.replace(ls, fallback_residual=0.0), plain, sweep
