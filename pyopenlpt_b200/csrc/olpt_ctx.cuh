@@ -147,7 +147,8 @@ struct StereoWork {
   DevBuf cell_start[OLPT_MAX_CAM], cell_cursor[OLPT_MAX_CAM], cell_items[OLPT_MAX_CAM];
   DevBuf cell_of[OLPT_MAX_CAM], los[OLPT_MAX_CAM];
   DevBuf l2d[OLPT_MAX_CAM * OLPT_MAX_CAM];
-  DevBuf l2d_ptrs, active_d, counters, scan_tmp;
+  DevBuf cxy[OLPT_MAX_CAM], cbp[OLPT_MAX_CAM * OLPT_MAX_CAM];
+  DevBuf l2d_ptrs, cbp_ptrs, active_d, counters, scan_tmp;
   DevBuf path_a, path_b, term, pairs;
   DevBuf cand_ids, cand_e, cand_x;
   void release(cudaStream_t s) {
@@ -159,7 +160,10 @@ struct StereoWork {
       los[c].release(s);
     }
     for (auto& b : l2d) b.release(s);
+    for (auto& b : cxy) b.release(s);
+    for (auto& b : cbp) b.release(s);
     l2d_ptrs.release(s);
+    cbp_ptrs.release(s);
     active_d.release(s);
     counters.release(s);
     path_a.release(s);

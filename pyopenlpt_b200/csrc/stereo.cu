@@ -48,6 +48,10 @@ struct SmView {
   int64_t n[OLPT_MAX_CAM];
   const double* los[OLPT_MAX_CAM];                  // n x 6
   const double* l2d[OLPT_MAX_CAM][OLPT_MAX_CAM];    // [c][t]: n[c] x 6 (pt, unit, U)
+  // cell-ordered copies of camera t's detections (position q of cell_items[t]):
+  // their coordinates, and the first four values of their image lines on camera c
+  const double2* cxy[OLPT_MAX_CAM];
+  const double* cbp[OLPT_MAX_CAM][OLPT_MAX_CAM];    // [t][c]: n[t] x 4
   double tol2d, tol3d;
   double limit[6];
 };
@@ -136,6 +140,27 @@ __global__ void lines_kernel(const CamDev* cams, int c, const double* x, const d
       d[4] = o[2] * inv;
       d[5] = o[3] * inv;
     }
+  }
+}
+
+// Cell-ordered copies of camera t's detections for the enumeration's inner loop:
+// coordinates, and for every other active camera c the point and direction of the
+// detection's image line on c.
+__global__ void cell_pack_kernel(const int* items, int64_t n, const double* x, const double* y,
+                                 double2* cxy, double* const* bp_out, const double* const* l2d,
+                                 int n_cam, int t) {
+  const int64_t q = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+  if (q >= n) return;
+  const int pid = items[q];
+  cxy[q] = make_double2(x[pid], y[pid]);
+  for (int c = 0; c < n_cam; ++c) {
+    double* o = bp_out[c];
+    if (c == t || !o) continue;
+    const double* L = l2d[c] + 6 * (int64_t)pid;
+    o[4 * q] = L[0];
+    o[4 * q + 1] = L[1];
+    o[4 * q + 2] = L[2];
+    o[4 * q + 3] = L[3];
   }
 }
 
@@ -332,8 +357,10 @@ __global__ void __launch_bounds__(256) enum_kernel(const SmView v, const Path* i
   const double tol2 = v.tol2d * v.tol2d;
   const int* cstart = v.cell_start[t];
   const int* citems = v.cell_items[t];
-  const double* tx = v.x[t];
-  const double* ty = v.y[t];
+  const double2* cxy = v.cxy[t];
+  const double* cbp[K];
+#pragma unroll
+  for (int i = 0; i < K; ++i) cbp[i] = v.cbp[t][P.cams[i]];
 
   // Rows that can hold a non-empty span: with two or more strips, the cell-centre rows
   // inside the y-extent of the first two strips' intersection parallelogram (plus one
@@ -406,33 +433,33 @@ __global__ void __launch_bounds__(256) enum_kernel(const SmView v, const Path* i
       xmax = xmax < b ? xmax : b;
     }
     if (xmin > xmax) continue;
-    for (int cx = xmin; cx <= xmax; ++cx) {
-      const int c = cy * cols + cx;
-      for (int q = cstart[c]; q < cstart[c + 1]; ++q) {
-        const int pid = citems[q];
-        const double qx = tx[pid], qy = ty[pid];
-        bool ok = true;
-        // IDMap::visitPointsInRowSpans precise test
+    // the cells xmin..xmax of this row are adjacent in cell order: one item range,
+    // visited in the same order as cell by cell
+    const int q1 = cstart[cy * cols + xmax + 1];
+    for (int q = cstart[cy * cols + xmin]; q < q1; ++q) {
+      const double2 xy = cxy[q];
+      bool ok = true;
+      // IDMap::visitPointsInRowSpans precise test
 #pragma unroll
-        for (int i = 0; i < K; ++i) {
-          const double dx = qx - lp[i][0], dy = qy - lp[i][1];
-          const double z = dy * lU[i][0] - dx * lU[i][1];
-          ok = ok && !(z * z > tol2);
-        }
-        if (!ok) continue;
-        // checkBackProjection (StereoMatch.cpp:1206-1227)
-#pragma unroll
-        for (int i = 0; i < K; ++i) {
-          if (!ok) break;
-          const double* L = v.l2d[t][P.cams[i]] + 6 * (int64_t)pid;
-          const double d0 = cpt[i][0] - L[0], d1 = cpt[i][1] - L[1];
-          const double z = d1 * L[2] - d0 * L[3];
-          ok = !(z * z > tol2);
-        }
-        if (!ok) continue;
-        const int slot = append_slot(pair_count);
-        if (slot < pair_cap) pairs[slot] = Pair{pidx, pid};
+      for (int i = 0; i < K; ++i) {
+        const double dx = xy.x - lp[i][0], dy = xy.y - lp[i][1];
+        const double z = dy * lU[i][0] - dx * lU[i][1];
+        ok = ok && !(z * z > tol2);
       }
+      if (!ok) continue;
+      // checkBackProjection (StereoMatch.cpp:1206-1227)
+#pragma unroll
+      for (int i = 0; i < K; ++i) {
+        if (!ok) break;
+        const double2 a = reinterpret_cast<const double2*>(cbp[i])[2 * q];
+        const double2 b = reinterpret_cast<const double2*>(cbp[i])[2 * q + 1];
+        const double d0 = cpt[i][0] - a.x, d1 = cpt[i][1] - a.y;
+        const double z = d1 * b.x - d0 * b.y;
+        ok = !(z * z > tol2);
+      }
+      if (!ok) continue;
+      const int slot = append_slot(pair_count);
+      if (slot < pair_cap) pairs[slot] = Pair{pidx, citems[q]};
     }
   }
 }
@@ -782,6 +809,35 @@ void stereo_match_device(olpt_ctx* ctx, const SmParams& prm, StereoResult& res) 
       lines_kernel<<<OLPT_G(nblk(v.n[c], 128)), 128, 0, s>>>(
           ctx->cams_d.as<CamDev>(), c, v.x[c], v.y[c], v.n[c], n_cam, W.active_d.as<int>(),
           W.los[c].as<double>(), W.l2d_ptrs.as<double*>() + c * OLPT_MAX_CAM);
+      OLPT_CUDA(cudaGetLastError());
+    }
+    // cell-ordered copies for the enumeration
+    W.cbp_ptrs.ensure(2 * OLPT_MAX_CAM * OLPT_MAX_CAM * sizeof(double*), s);
+    std::vector<double*> bp(2 * OLPT_MAX_CAM * OLPT_MAX_CAM, nullptr);
+    for (int t = 0; t < n_cam; ++t) {
+      if (!v.active[t]) continue;
+      W.cxy[t].ensure((v.n[t] + 1) * sizeof(double2), s);
+      v.cxy[t] = W.cxy[t].as<double2>();
+      for (int c = 0; c < n_cam; ++c) {
+        if (c == t || !v.active[c]) continue;
+        DevBuf& b = W.cbp[t * OLPT_MAX_CAM + c];
+        b.ensure((v.n[t] + 1) * 4 * sizeof(double), s);
+        bp[t * OLPT_MAX_CAM + c] = b.as<double>();
+        v.cbp[t][c] = b.as<double>();
+      }
+      for (int c = 0; c < n_cam; ++c)
+        bp[OLPT_MAX_CAM * OLPT_MAX_CAM + t * OLPT_MAX_CAM + c] = ptrs[t * OLPT_MAX_CAM + c];
+    }
+    OLPT_CUDA(cudaMemcpyAsync(W.cbp_ptrs.p, bp.data(), bp.size() * sizeof(double*),
+                              cudaMemcpyHostToDevice, s));
+    for (int t = 0; t < n_cam; ++t) {
+      if (!v.active[t] || v.n[t] == 0) continue;
+      double* const* outs = W.cbp_ptrs.as<double*>() + t * OLPT_MAX_CAM;
+      const double* const* lines =
+          W.cbp_ptrs.as<const double*>() + OLPT_MAX_CAM * OLPT_MAX_CAM + t * OLPT_MAX_CAM;
+      cell_pack_kernel<<<OLPT_G(nblk(v.n[t])), 256, 0, s>>>(
+          W.cell_items[t].as<int>(), v.n[t], v.x[t], v.y[t], W.cxy[t].as<double2>(), outs, lines,
+          n_cam, t);
       OLPT_CUDA(cudaGetLastError());
     }
   }
