@@ -291,7 +291,7 @@ __device__ __forceinline__ bool in_roi(const Rect& R, double u, double w) {
 }
 
 template <typename Real>
-__global__ void __launch_bounds__(128, 4) shake_kernel(ShakeView v, int64_t n, double* xyz,
+__global__ void __launch_bounds__(128, 8) shake_kernel(ShakeView v, int64_t n, double* xyz,
                                                     double* uv, const Real* otfp, double* score,
                                                     double delta, const uint8_t* active,
                                                     double* resid_out) {

@@ -326,7 +326,7 @@ __device__ __forceinline__ int append_slot(int* counter) {
 // warp per path, lanes take rows (the single long strip of K = 1); otherwise one
 // thread per path (K >= 2, where the strips intersect in a few rows).
 template <int K, bool WARP>
-__global__ void __launch_bounds__(256) enum_kernel(const SmView v, const Path* in, int n_in,
+__global__ void __launch_bounds__(256, 4) enum_kernel(const SmView v, const Path* in, int n_in,
                                                    Pair* pairs, int* pair_count, int pair_cap) {
   const int gtid = blockIdx.x * blockDim.x + threadIdx.x;
   const int pidx = WARP ? (gtid >> 5) : gtid;
