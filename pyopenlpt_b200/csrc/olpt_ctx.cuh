@@ -285,7 +285,7 @@ struct StbState {
   StbParams p;
   IprParams ipr;
   bool configured = false;
-  std::deque<TrackH> short_active, long_active, long_inactive, exited;
+  TrackList short_active, long_active, long_inactive, exited;
   std::vector<std::vector<double>> ipr_xyz;   // initial phase, per frame
   std::vector<std::vector<char>> ipr_tracked;
   std::vector<double> linfit_kernel;          // 2 x n_pts
@@ -344,7 +344,7 @@ void learned_shake_device(olpt_ctx* ctx, const ShakeParams& sp);
 
 void stb_configure(olpt_ctx* ctx, const StbParams& p, const IprParams& ipr);
 void stb_process_frame(olpt_ctx* ctx, int frame);
-std::deque<TrackH>& stb_list(olpt_ctx* ctx, int which);
+TrackList& stb_list(olpt_ctx* ctx, int which);
 void stb_save_tracks(olpt_ctx* ctx, int which, const std::string& path);
 void stb_load_tracks(olpt_ctx* ctx, int which, const std::string& path);
 

@@ -33,7 +33,6 @@
 #include <chrono>
 #include <cmath>
 #include <cstdio>
-#include <deque>
 #include <filesystem>
 #include <fstream>
 #include <sstream>
@@ -716,7 +715,7 @@ void put_f6(std::string& o, double v) {
 // (ObjectInfo.cpp:76-94).  The 2D columns are each point's projection on every
 // camera: the reference's objects always hold projectObject2D of their centre
 // (end of Shake::shakeOneObject, buildTrackFromPredField, loadTrack).
-void save_tracks_file(olpt_ctx* ctx, const std::deque<TrackH>& tracks, const std::string& file) {
+void save_tracks_file(olpt_ctx* ctx, const TrackList& tracks, const std::string& file) {
   int64_t n = 0;
   for (const TrackH& t : tracks) n += (int64_t)t.size();
   std::vector<double> xyz;
@@ -895,7 +894,7 @@ void build_from_pf(olpt_ctx* ctx, int idx, const double* d_field, int frame) {
       OLPT_CUDA(cudaGetLastError());
       link = download(W.link.as<int>(), n_sa, s);
     }
-    std::deque<TrackH> kept;
+    TrackList kept;
     for (int j = 0; j < n_sa; ++j) {
       if (link[j] < 0) continue;
       tracked[link[j]] = 1;
@@ -933,7 +932,7 @@ void init_phase(olpt_ctx* ctx, int frame) {
     build_from_pf(ctx, i, i == 0 ? nullptr : cal_pred_field(ctx, i), fid);
   }
   const size_t need = (size_t)S.p.n_initial_frames;
-  std::deque<TrackH> still_short;
+  TrackList still_short;
   for (TrackH& tr : S.short_active) {
     if (tr.size() >= need)
       S.long_active.push_back(std::move(tr));
@@ -985,7 +984,8 @@ void conv_phase(olpt_ctx* ctx, int frame) {
     OLPT_CUDA(cudaGetLastError());
     pred = download(W.b.as<double>(), 3 * (size_t)n_la, s);
     const std::vector<int> in_range = download(W.link.as<int>(), n_la, s);
-    std::deque<TrackH> kept;
+    TrackList kept;
+    kept.reserve(n_la);
     size_t w = 0;
     for (int i = 0; i < n_la; ++i) {
       if (!in_range[i]) {
@@ -1018,7 +1018,8 @@ void conv_phase(olpt_ctx* ctx, int frame) {
     resume();
     const std::vector<double> sx = download(ctx->obj.xyz.as<double>(), 3 * (size_t)n_la, s);
     const std::vector<uint8_t> fl = download(ctx->obj.flags.as<uint8_t>(), n_la, s);
-    std::deque<TrackH> kept;
+    TrackList kept;
+    kept.reserve(n_la);
     for (int i = 0; i < n_la; ++i) {
       TrackH& tr = S.long_active[i];
       if (fl[i] == 0) {
@@ -1112,7 +1113,8 @@ void conv_phase(olpt_ctx* ctx, int frame) {
         link[j] = -1;
     }
     std::vector<char> used(n_obj, 0);
-    std::deque<TrackH> keep;
+    TrackList keep;
+    keep.reserve(n_sa + n_obj);
     for (int i = 0; i < n_sa; ++i) {
       const int lid = link[i];
       if (lid < 0 || lid >= n_obj) continue;
@@ -1126,6 +1128,7 @@ void conv_phase(olpt_ctx* ctx, int frame) {
         keep.push_back(std::move(tr));
     }
     S.short_active.swap(keep);
+    S.short_active.reserve(S.short_active.size() + n_obj);
     for (int i = 0; i < n_obj; ++i) {
       if (used[i]) continue;
       TrackH tr;
@@ -1154,7 +1157,8 @@ void conv_phase(olpt_ctx* ctx, int frame) {
                                                     W.link.as<int>());
     OLPT_CUDA(cudaGetLastError());
     const std::vector<int> ok = download(W.link.as<int>(), n_la, s);
-    std::deque<TrackH> kept;
+    TrackList kept;
+    kept.reserve(n_la);
     for (int i = 0; i < n_la; ++i) {
       TrackH& tr = S.long_active[i];
       if (ok[i])
@@ -1226,7 +1230,7 @@ void stb_process_frame(olpt_ctx* ctx, int frame) {
     save_tracks_all(ctx, S.p.output_path + "ConvergeTrack/", frame);
 }
 
-std::deque<TrackH>& stb_list(olpt_ctx* ctx, int which) {
+TrackList& stb_list(olpt_ctx* ctx, int which) {
   StbState& S = ctx->stb;
   switch (which) {
     case OLPT_TRACK_LONG_ACTIVE: return S.long_active;
@@ -1246,7 +1250,7 @@ void stb_save_tracks(olpt_ctx* ctx, int which, const std::string& path) {
 void stb_load_tracks(olpt_ctx* ctx, int which, const std::string& path) {
   std::ifstream fin(path);
   OLPT_REQUIRE(fin.is_open(), OLPT_ERR_INVALID_ARG, "LoadTracks: cannot open file: " + path);
-  std::deque<TrackH>& tracks = stb_list(ctx, which);
+  TrackList& tracks = stb_list(ctx, which);
   tracks.clear();
   std::string line;
   std::getline(fin, line);  // header
