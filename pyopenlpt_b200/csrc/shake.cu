@@ -237,6 +237,89 @@ __device__ double residue(const ShakeView& v, const Rect* roi, Smem<Real>& S) {
   return used > 1 ? cost / (double)used : __longlong_as_double(0x7ff0000000000000LL);
 }
 
+// Three trial points at once (the -delta / 0 / +delta evaluations of one axis):
+// lanes 3 x n_cam project point j = lane / n_cam on camera lane % n_cam; slot j of
+// the geometry arrays receives it (slot 0 is the one eval_geom uses).
+template <typename Real>
+__device__ void eval_geom3(const ShakeView& v, const double P[3], int ax, double x0,
+                           const double rel[3], Smem<Real>& S) {
+  const int lane = threadIdx.x & 31;
+  const int C = v.n_cam;
+  if (lane < 3 * C) {
+    const int j = lane / C, c = lane % C;
+    double Q[3] = {P[0], P[1], P[2]};
+    Q[ax] = x0 + rel[j];
+    double u, w;
+    cam_project(v.cams[c], Q[0], Q[1], Q[2], u, w);
+    S.uvc[2 * lane] = u;
+    S.uvc[2 * lane + 1] = w;
+    double q[5];
+    otf_param(v.otf, c, Q[0], Q[1], Q[2], q);
+    for (int k = 0; k < 5; ++k) S.otf[5 * lane + k] = (Real)q[k];
+  }
+  __syncwarp();
+}
+
+// calShakeResidue for the three points of eval_geom3 (FP32 production path): each
+// lane visits the same pixels in the same order as three single evaluations would,
+// so the costs are the single evaluations' bit for bit; the three run interleaved.
+template <typename Real>
+__device__ void residue3(const ShakeView& v, const Rect* roi, Smem<Real>& S, double f[3]) {
+  const int lane = threadIdx.x & 31;
+  const int area = v.roi_area;
+  const int C = v.n_cam;
+  double cost[3] = {0.0, 0.0, 0.0};
+  int used = 0;
+#pragma unroll 1
+  for (int c = 0; c < C; ++c) {
+    const Rect R = roi[c];
+    if (rect_empty(R)) continue;
+    const int w = R.cmax - R.cmin, h = R.rmax - R.rmin;
+    if (w <= 0 || h <= 0) continue;
+    double u[3], vv[3];
+    int prmin[3], prmax[3], pcmin[3], pcmax[3];
+#pragma unroll
+    for (int j = 0; j < 3; ++j) {
+      u[j] = S.uvc[2 * (j * C + c)];
+      vv[j] = S.uvc[2 * (j * C + c) + 1];
+      prmin[j] = (int)floor(vv[j] - v.r_px);
+      prmax[j] = (int)ceil(vv[j] + v.r_px + 1);
+      pcmin[j] = (int)floor(u[j] - v.r_px);
+      pcmax[j] = (int)ceil(u[j] + v.r_px + 1);
+    }
+    // the pixels of camera c that this lane visits in the single evaluation's loop
+    // over q = lane, lane + 32, ... < C * area, in the same order
+    int first = lane - (c * area) % 32;
+    if (first < 0) first += 32;
+    Real part[3] = {(Real)0, (Real)0, (Real)0};
+    for (int pix = first; pix < area; pix += 32) {
+      if (pix >= w * h) continue;
+      const int row = R.rmin + pix / w, col = R.cmin + pix % w;
+      const Real a = S.aug[c * area + pix];
+#pragma unroll
+      for (int j = 0; j < 3; ++j) {
+        Real pred = (Real)0;
+        if (row >= prmin[j] && row < prmax[j] && col >= pcmin[j] && col < pcmax[j])
+          pred = gauss<Real>(col, row, u[j], vv[j], S.otf + 5 * (j * C + c));
+        const Real d = a - pred;
+        part[j] += d * d;
+      }
+    }
+#pragma unroll
+    for (int j = 0; j < 3; ++j)
+#pragma unroll
+      for (int o = 16; o > 0; o >>= 1) part[j] += __shfl_xor_sync(0xffffffffu, part[j], o);
+    if (!v.cams[c].is_active) continue;
+    const int n = w * h;
+#pragma unroll
+    for (int j = 0; j < 3; ++j) cost[j] += (double)part[j] / (double)n;
+    ++used;
+  }
+#pragma unroll
+  for (int j = 0; j < 3; ++j)
+    f[j] = used > 1 ? cost[j] / (double)used : __longlong_as_double(0x7ff0000000000000LL);
+}
+
 // myMATH::polyfit order 2 (myMATH.cpp:490-534): (X^T X)^-1 X^T y with the
 // reference's operation order.
 __device__ void polyfit2(const double* x, const double* y, int n, double coef[3]) {
@@ -346,16 +429,29 @@ __global__ void __launch_bounds__(128, 8) shake_kernel(ShakeView v, int64_t n, d
     double f[3];
     double su[3][OLPT_MAX_CAM], sv[3][OLPT_MAX_CAM];
     bool sok[3][OLPT_MAX_CAM];
-    for (int j = 0; j < 3; ++j) {
-      tmp[ax] = x0 + rel[j];
-      eval_geom<Real>(v, tmp, S);
-      f[j] = residue<Real>(v, roi, S);
-      for (int c = 0; c < C; ++c) {
-        su[j][c] = S.uvc[2 * c];
-        sv[j][c] = S.uvc[2 * c + 1];
-        sok[j][c] = in_roi(roi[c], su[j][c], sv[j][c]);
+    if (v.exact_sums) {
+      for (int j = 0; j < 3; ++j) {
+        tmp[ax] = x0 + rel[j];
+        eval_geom<Real>(v, tmp, S);
+        f[j] = residue<Real>(v, roi, S);
+        for (int c = 0; c < C; ++c) {
+          su[j][c] = S.uvc[2 * c];
+          sv[j][c] = S.uvc[2 * c + 1];
+          sok[j][c] = in_roi(roi[c], su[j][c], sv[j][c]);
+        }
+        __syncwarp();
       }
+    } else {
+      eval_geom3<Real>(v, tmp, ax, x0, rel, S);
+      residue3<Real>(v, roi, S, f);
+      for (int j = 0; j < 3; ++j)
+        for (int c = 0; c < C; ++c) {
+          su[j][c] = S.uvc[2 * (j * C + c)];
+          sv[j][c] = S.uvc[2 * (j * C + c) + 1];
+          sok[j][c] = in_roi(roi[c], su[j][c], sv[j][c]);
+        }
       __syncwarp();
+      tmp[ax] = x0 + rel[2];  // as left by the last single evaluation
     }
     const double fL = f[0], f0 = f[1], fR = f[2];
     const double tol = 1e-3 * fmax(1.0, f0);
@@ -770,10 +866,10 @@ static ShakeView make_view(olpt_ctx* ctx, const ShakeParams& sp, bool fp64) {
   if (fp64) off += (size_t)v.n_cam * v.roi_area * 8;
   off = (off + 15) / 16 * 16;
   v.off_otf = off;
-  off += (size_t)v.n_cam * 5 * rsz;
+  off += 3 * (size_t)v.n_cam * 5 * rsz;  // three trial points (slot 0: single evaluations)
   off = (off + 15) / 16 * 16;
   v.off_uv = off;
-  off += (size_t)v.n_cam * 2 * 8;
+  off += 3 * (size_t)v.n_cam * 2 * 8;
   v.smem_per_warp = (off + 15) / 16 * 16;
   return v;
 }
