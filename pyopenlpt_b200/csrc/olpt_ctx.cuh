@@ -126,7 +126,7 @@ struct ShakeWork {
   DevBuf otfp;      // n x n_cam x 5 OTF parameters at the object centres
   DevBuf pair_key;  // n x n_cam tile keys
   Csr bins;         // (object, camera) pairs per image tile
-  DevBuf rep, hkey, has_nb, nb_pos, nb_list, scan_tmp;
+  DevBuf rep, hkey, has_nb, nb_pos, nb_list, scan_tmp, gpart;
   Csr hash;         // 3D hash grid of object centres
   void release(cudaStream_t s) {
     nb_pos.release(s);
@@ -138,6 +138,7 @@ struct ShakeWork {
     rep.release(s);
     hkey.release(s);
     has_nb.release(s);
+    gpart.release(s);
     hash.release(s);
   }
 };

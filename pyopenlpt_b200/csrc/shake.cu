@@ -724,10 +724,72 @@ __global__ void repeat_greedy_kernel(const double* xyz, int n, double cell, int 
   }
 }
 
-// Shake.cpp:118-136: mean score over non-repeated objects (summed in index order,
-// as the reference does) and the ghost rule.
+// Shake.cpp:118-136: the ghost rule against the mean score of the non-repeated
+// objects, which the reference sums in index order.  The flags are first decided with
+// a tree-summed mean; a score within the bound by which the sequential and the tree
+// sum can differ (|S_seq - S_tree| <= 2 n 2^-53 sum|x|) of the threshold marks the
+// result ambiguous, and only then does ghost_kernel redo the sequential sum.
+constexpr int kScoreBlocks = 296;
+
+__global__ void score_partial_kernel(const double* score, const uint8_t* rep, int n,
+                                     double* part) {
+  __shared__ double s1[256], s2[256], s3[256];
+  double a = 0.0, b = 0.0, c = 0.0;
+  for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x)
+    if (!rep[i]) {
+      a += score[i];
+      b += fabs(score[i]);
+      c += 1.0;
+    }
+  s1[threadIdx.x] = a;
+  s2[threadIdx.x] = b;
+  s3[threadIdx.x] = c;
+  __syncthreads();
+  for (int k = blockDim.x / 2; k > 0; k >>= 1) {
+    if ((int)threadIdx.x < k) {
+      s1[threadIdx.x] += s1[threadIdx.x + k];
+      s2[threadIdx.x] += s2[threadIdx.x + k];
+      s3[threadIdx.x] += s3[threadIdx.x + k];
+    }
+    __syncthreads();
+  }
+  if (threadIdx.x == 0) {
+    part[3 * blockIdx.x] = s1[0];
+    part[3 * blockIdx.x + 1] = s2[0];
+    part[3 * blockIdx.x + 2] = s3[0];
+  }
+}
+
+__global__ void ghost_flag_kernel(const double* score, const uint8_t* rep, int n, double thred,
+                                  const double* part, int nb, uint8_t* flags, int* amb) {
+  __shared__ double st[3];
+  if (threadIdx.x < 3) {
+    double t = 0.0;
+    for (int b = 0; b < nb; ++b) t += part[3 * b + threadIdx.x];
+    st[threadIdx.x] = t;
+  }
+  __syncthreads();
+  const double cnt = st[2];
+  const double m = cnt > 0 ? st[0] / cnt : 0.0;
+  const double thr = m * thred;
+  const double e = cnt > 0 ? (2.0 * (double)n * 1.1102230246251565e-16 * st[1]) / cnt : 0.0;
+  const double band = 2.0 * (e * fabs(thred) + fabs(thr) * 4.5e-16);
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= n) return;
+  const double sc = score[i];
+  uint8_t f = rep[i] ? 2 : 0;
+  if (sc == 0.0 || sc < thr - band) {
+    f |= 1;
+  } else if (!(sc >= thr + band)) {
+    atomicOr(amb, 1);
+    if (sc < thr) f |= 1;
+  }
+  flags[i] = f;
+}
+
 __global__ void ghost_kernel(const double* score, const uint8_t* rep, int n, double thred,
-                             uint8_t* flags) {
+                             uint8_t* flags, const int* amb) {
+  if (!*amb) return;
   __shared__ double s_mean;
   if (threadIdx.x < 32) {
     // warp 0 streams the scores in; lane 0 adds them strictly in index order
@@ -986,8 +1048,19 @@ static void shake_flags(olpt_ctx* ctx, const ShakeParams& sp) {
                                           W.hash.start.as<int>(), W.hash.items.as<int>(), r2,
                                           W.nb_list.as<int>(), W.nb_pos.as<int>() + n,
                                           W.rep.as<uint8_t>());
+    const int sb = std::max(1, std::min(kScoreBlocks, nblk(n)));
+    W.gpart.ensure((size_t)sb * 3 * sizeof(double) + sizeof(int) + 64, s);
+    int* amb = reinterpret_cast<int*>(W.gpart.as<double>() + 3 * sb);
+    OLPT_CUDA(cudaMemsetAsync(amb, 0, sizeof(int), s));
+    score_partial_kernel<<<OLPT_G(sb), 256, 0, s>>>(ctx->obj.score.as<double>(),
+                                                    W.rep.as<uint8_t>(), (int)n,
+                                                    W.gpart.as<double>());
+    ghost_flag_kernel<<<OLPT_G(nblk(n)), 256, 0, s>>>(ctx->obj.score.as<double>(),
+                                                      W.rep.as<uint8_t>(), (int)n, sp.thred_ghost,
+                                                      W.gpart.as<double>(), sb,
+                                                      ctx->obj.flags.as<uint8_t>(), amb);
     ghost_kernel<<<OLPT_G(1), 1024, 0, s>>>(ctx->obj.score.as<double>(), W.rep.as<uint8_t>(), (int)n,
-                                    sp.thred_ghost, ctx->obj.flags.as<uint8_t>());
+                                    sp.thred_ghost, ctx->obj.flags.as<uint8_t>(), amb);
     OLPT_CUDA(cudaGetLastError());
   }
 }
