@@ -868,6 +868,8 @@ void stereo_match_device(olpt_ctx* ctx, const SmParams& prm, StereoResult& res) 
   for (int level = 1; level < v.m && n_in > 0; ++level) {
     // candidates of every path that pass the 2D tests
     int n_pairs = 0;
+    // buffers are grow-only: their capacity from earlier calls avoids a redo
+    pair_cap = (int)std::max<int64_t>(pair_cap, (int64_t)(W.pairs.bytes / sizeof(Pair)) - 1);
     for (;;) {
       W.pairs.ensure((size_t)pair_cap * sizeof(Pair), s);
       OLPT_CUDA(cudaMemsetAsync(cnt + 4, 0, sizeof(int), s));
@@ -895,6 +897,8 @@ void stereo_match_device(olpt_ctx* ctx, const SmParams& prm, StereoResult& res) 
       break;
     }
     // quick triangulation gate and the children
+    out_cap = (int)std::max<int64_t>(out_cap, (int64_t)(out_buf->bytes / sizeof(Path)) - 1);
+    term_cap = (int)std::max<int64_t>(term_cap, (int64_t)(W.term.bytes / sizeof(Path)) - 1);
     for (;;) {
       out_buf->ensure((size_t)out_cap * sizeof(Path), s);
       W.term.ensure((size_t)term_cap * sizeof(Path), s);
