@@ -159,10 +159,10 @@ struct Smem {
 };
 
 // All lanes: project point P on every camera and evaluate the OTF there.
-template <typename Real>
+template <typename Real, int NC>
 __device__ void eval_geom(const ShakeView& v, const double P[3], Smem<Real>& S) {
   const int lane = threadIdx.x & 31;
-  if (lane < v.n_cam) {
+  if (lane < NC) {
     double u, w;
     cam_project(v.cams[lane], P[0], P[1], P[2], u, w);
     S.uvc[2 * lane] = u;
@@ -176,14 +176,14 @@ __device__ void eval_geom(const ShakeView& v, const double P[3], Smem<Real>& S) 
 
 // TracerShakeStrategy::calShakeResidue (Shake.cpp:951-1045) for the point whose
 // geometry is in S (eval_geom), against the staged augmented ROIs.
-template <typename Real>
+template <typename Real, int NC>
 __device__ double residue(const ShakeView& v, const Rect* roi, Smem<Real>& S) {
   const int lane = threadIdx.x & 31;
   const int area = v.roi_area;
-  double mse[OLPT_MAX_CAM];
-  Real part[OLPT_MAX_CAM];
-  for (int c = 0; c < v.n_cam; ++c) part[c] = (Real)0;
-  for (int q = lane; q < v.n_cam * area; q += 32) {
+  double mse[NC];
+  Real part[NC];
+  for (int c = 0; c < NC; ++c) part[c] = (Real)0;
+  for (int q = lane; q < NC * area; q += 32) {
     const int c = q / area, pix = q % area;
     const Rect& R = roi[c];
     if (rect_empty(R)) continue;
@@ -204,7 +204,7 @@ __device__ double residue(const ShakeView& v, const Rect* roi, Smem<Real>& S) {
   }
   if (v.exact_sums) {
     __syncwarp();
-    if (lane < v.n_cam) {
+    if (lane < NC) {
       const Rect& R = roi[lane];
       const int n = rect_empty(R) ? 0 : (R.cmax - R.cmin) * (R.rmax - R.rmin);
       double sse = 0.0;
@@ -212,10 +212,10 @@ __device__ double residue(const ShakeView& v, const Rect* roi, Smem<Real>& S) {
       mse[0] = n > 0 ? sse / (double)n : 0.0;
     }
     double m0 = mse[0];
-    for (int c = 0; c < v.n_cam; ++c) mse[c] = __shfl_sync(0xffffffffu, m0, c);
+    for (int c = 0; c < NC; ++c) mse[c] = __shfl_sync(0xffffffffu, m0, c);
     __syncwarp();
   } else {
-    for (int c = 0; c < v.n_cam; ++c) {
+    for (int c = 0; c < NC; ++c) {
       Real s = part[c];
 #pragma unroll
       for (int o = 16; o > 0; o >>= 1) s += __shfl_xor_sync(0xffffffffu, s, o);
@@ -226,7 +226,7 @@ __device__ double residue(const ShakeView& v, const Rect* roi, Smem<Real>& S) {
   }
   double cost = 0.0;
   int used = 0;
-  for (int c = 0; c < v.n_cam; ++c) {
+  for (int c = 0; c < NC; ++c) {
     if (!v.cams[c].is_active) continue;
     const Rect& R = roi[c];
     const int nr = R.rmax - R.rmin, nc = R.cmax - R.cmin;
@@ -240,11 +240,11 @@ __device__ double residue(const ShakeView& v, const Rect* roi, Smem<Real>& S) {
 // Three trial points at once (the -delta / 0 / +delta evaluations of one axis):
 // lanes 3 x n_cam project point j = lane / n_cam on camera lane % n_cam; slot j of
 // the geometry arrays receives it (slot 0 is the one eval_geom uses).
-template <typename Real>
+template <typename Real, int NC>
 __device__ void eval_geom3(const ShakeView& v, const double P[3], int ax, double x0,
                            const double rel[3], Smem<Real>& S) {
   const int lane = threadIdx.x & 31;
-  const int C = v.n_cam;
+  constexpr int C = NC;
   if (lane < 3 * C) {
     const int j = lane / C, c = lane % C;
     double Q[3] = {P[0], P[1], P[2]};
@@ -263,14 +263,14 @@ __device__ void eval_geom3(const ShakeView& v, const double P[3], int ax, double
 // calShakeResidue for the three points of eval_geom3 (FP32 production path): each
 // lane visits the same pixels in the same order as three single evaluations would,
 // so the costs are the single evaluations' bit for bit; the three run interleaved.
-template <typename Real>
+template <typename Real, int NC>
 __device__ void residue3(const ShakeView& v, const Rect* roi, Smem<Real>& S, double f[3]) {
   const int lane = threadIdx.x & 31;
   const int area = v.roi_area;
-  const int C = v.n_cam;
+  constexpr int C = NC;
   double cost[3] = {0.0, 0.0, 0.0};
   int used = 0;
-#pragma unroll 1
+#pragma unroll
   for (int c = 0; c < C; ++c) {
     const Rect R = roi[c];
     if (rect_empty(R)) continue;
@@ -373,7 +373,7 @@ __device__ __forceinline__ bool in_roi(const Rect& R, double u, double w) {
   return R.cmin <= u && u < R.cmax && R.rmin <= w && w < R.rmax;
 }
 
-template <typename Real>
+template <typename Real, int NC>
 __global__ void __launch_bounds__(128, 8) shake_kernel(ShakeView v, int64_t n, double* xyz,
                                                     double* uv, const Real* otfp, double* score,
                                                     double delta, const uint8_t* active,
@@ -382,7 +382,8 @@ __global__ void __launch_bounds__(128, 8) shake_kernel(ShakeView v, int64_t n, d
   const int warp_in_blk = threadIdx.x >> 5;
   const int lane = threadIdx.x & 31;
   const int64_t o = (int64_t)blockIdx.x * (blockDim.x >> 5) + warp_in_blk;
-  const int C = v.n_cam, area = v.roi_area;
+  constexpr int C = NC;
+  const int area = v.roi_area;
   const size_t per_warp = v.smem_per_warp;
   unsigned char* base = smem_raw + per_warp * warp_in_blk;
   Smem<Real> S;
@@ -396,7 +397,7 @@ __global__ void __launch_bounds__(128, 8) shake_kernel(ShakeView v, int64_t n, d
   double P[3] = {xyz[3 * o], xyz[3 * o + 1], xyz[3 * o + 2]};
   double f_final = 0.0;
   // ---- buildROIInfo (Shake.cpp:279-328)
-  Rect roi[OLPT_MAX_CAM];
+  Rect roi[NC];
   const double* uvo = uv + o * C * 2;
   for (int c = 0; c < C; ++c) {
     roi[c] = Rect{0, 0, 0, 0};  // default-constructed PixelRange for skipped cameras
@@ -427,13 +428,13 @@ __global__ void __launch_bounds__(128, 8) shake_kernel(ShakeView v, int64_t n, d
     const double x0 = P[ax];
     const double rel[3] = {-delta, 0.0, delta};
     double f[3];
-    double su[3][OLPT_MAX_CAM], sv[3][OLPT_MAX_CAM];
-    bool sok[3][OLPT_MAX_CAM];
+    double su[3][NC], sv[3][NC];
+    bool sok[3][NC];
     if (v.exact_sums) {
       for (int j = 0; j < 3; ++j) {
         tmp[ax] = x0 + rel[j];
-        eval_geom<Real>(v, tmp, S);
-        f[j] = residue<Real>(v, roi, S);
+        eval_geom<Real, NC>(v, tmp, S);
+        f[j] = residue<Real, NC>(v, roi, S);
         for (int c = 0; c < C; ++c) {
           su[j][c] = S.uvc[2 * c];
           sv[j][c] = S.uvc[2 * c + 1];
@@ -442,8 +443,8 @@ __global__ void __launch_bounds__(128, 8) shake_kernel(ShakeView v, int64_t n, d
         __syncwarp();
       }
     } else {
-      eval_geom3<Real>(v, tmp, ax, x0, rel, S);
-      residue3<Real>(v, roi, S, f);
+      eval_geom3<Real, NC>(v, tmp, ax, x0, rel, S);
+      residue3<Real, NC>(v, roi, S, f);
       for (int j = 0; j < 3; ++j)
         for (int c = 0; c < C; ++c) {
           su[j][c] = S.uvc[2 * (j * C + c)];
@@ -476,7 +477,7 @@ __global__ void __launch_bounds__(128, 8) shake_kernel(ShakeView v, int64_t n, d
       }
     }
     if (!skip_expand && mono) {
-      double J[OLPT_MAX_CAM], M[OLPT_MAX_CAM];
+      double J[NC], M[NC];
       int nJ = 0, nM = 0;
       for (int c = 0; c < C; ++c) {
         if (sok[0][c] && sok[2][c]) {
@@ -509,7 +510,7 @@ __global__ void __launch_bounds__(128, 8) shake_kernel(ShakeView v, int64_t n, d
       if (Dp > 0.0) {
         const double dx_exp = (s >= 0 ? +Dp : -Dp);
         tmp[ax] = x0 + dx_exp;
-        eval_geom<Real>(v, tmp, S);
+        eval_geom<Real, NC>(v, tmp, S);
         bool out = false;
         for (int c = 0; c < C; ++c)
           if (!in_roi(roi[c], S.uvc[2 * c], S.uvc[2 * c + 1])) {
@@ -517,7 +518,7 @@ __global__ void __launch_bounds__(128, 8) shake_kernel(ShakeView v, int64_t n, d
             break;
           }
         if (!out) {
-          const double fexp = residue<Real>(v, roi, S);
+          const double fexp = residue<Real, NC>(v, roi, S);
           cx[nc] = dx_exp;
           cf[nc] = fexp;
           ca[nc] = x0 + dx_exp;
@@ -537,7 +538,7 @@ __global__ void __launch_bounds__(128, 8) shake_kernel(ShakeView v, int64_t n, d
       }
       if (x_hat >= xmin && x_hat <= xmax) {
         tmp[ax] = x0 + x_hat;
-        eval_geom<Real>(v, tmp, S);
+        eval_geom<Real, NC>(v, tmp, S);
         bool out = false;
         for (int c = 0; c < C; ++c)
           if (!in_roi(roi[c], S.uvc[2 * c], S.uvc[2 * c + 1])) {
@@ -545,7 +546,7 @@ __global__ void __launch_bounds__(128, 8) shake_kernel(ShakeView v, int64_t n, d
             break;
           }
         if (!out) {
-          const double fhat = residue<Real>(v, roi, S);
+          const double fhat = residue<Real, NC>(v, roi, S);
           cx[nc] = x_hat;
           cf[nc] = fhat;
           ca[nc] = x0 + x_hat;
@@ -566,10 +567,10 @@ __global__ void __launch_bounds__(128, 8) shake_kernel(ShakeView v, int64_t n, d
   }
 
   // ---- final projection + calObjectScore (Shake.cpp:668-782)
-  eval_geom<Real>(v, P, S);
-  double numer_c[OLPT_MAX_CAM], denom_c[OLPT_MAX_CAM], peak_c[OLPT_MAX_CAM];
-  Rect sr[OLPT_MAX_CAM];
-  int use[OLPT_MAX_CAM];
+  eval_geom<Real, NC>(v, P, S);
+  double numer_c[NC], denom_c[NC], peak_c[NC];
+  Rect sr[NC];
+  int use[NC];
   int n_used = 0;
   for (int c = 0; c < C; ++c) {
     use[c] = 0;
@@ -983,6 +984,32 @@ static void residual_pass(olpt_ctx* ctx, ShakeView& v, const uint8_t* flags, int
   OLPT_CUDA(cudaGetLastError());
 }
 
+// shake_kernel instantiated per camera count (per-camera arrays in registers)
+template <typename Real, int NC>
+static void launch_shake_nc(int grid, int block, size_t smem, cudaStream_t s, const ShakeView& v,
+                            int64_t n, double* xyz, double* uv, const Real* otfp, double* score,
+                            double delta, const uint8_t* active, double* resid_out) {
+  OLPT_CUDA(cudaFuncSetAttribute(shake_kernel<Real, NC>,
+                                 cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+  shake_kernel<Real, NC><<<OLPT_G(grid), block, smem, s>>>(v, n, xyz, uv, otfp, score, delta,
+                                                           active, resid_out);
+}
+
+template <typename Real>
+static void launch_shake(int C, int grid, int block, size_t smem, cudaStream_t s,
+                         const ShakeView& v, int64_t n, double* xyz, double* uv, const Real* otfp,
+                         double* score, double delta, const uint8_t* active, double* resid_out) {
+  switch (C) {
+    case 2: launch_shake_nc<Real, 2>(grid, block, smem, s, v, n, xyz, uv, otfp, score, delta, active, resid_out); break;
+    case 3: launch_shake_nc<Real, 3>(grid, block, smem, s, v, n, xyz, uv, otfp, score, delta, active, resid_out); break;
+    case 4: launch_shake_nc<Real, 4>(grid, block, smem, s, v, n, xyz, uv, otfp, score, delta, active, resid_out); break;
+    case 5: launch_shake_nc<Real, 5>(grid, block, smem, s, v, n, xyz, uv, otfp, score, delta, active, resid_out); break;
+    case 6: launch_shake_nc<Real, 6>(grid, block, smem, s, v, n, xyz, uv, otfp, score, delta, active, resid_out); break;
+    case 7: launch_shake_nc<Real, 7>(grid, block, smem, s, v, n, xyz, uv, otfp, score, delta, active, resid_out); break;
+    default: launch_shake_nc<Real, 8>(grid, block, smem, s, v, n, xyz, uv, otfp, score, delta, active, resid_out); break;
+  }
+}
+
 // n_loop shake iterations from the width delta (halved per iteration, clamped at the
 // minimum); objects with active[o] == 0 stay fixed but still enter the residual
 template <typename Real>
@@ -996,8 +1023,7 @@ static void shake_iterations(olpt_ctx* ctx, const ShakeParams& sp, ShakeView& v,
   dmin = (dmin > 0) ? dmin : sp.shake_width / 20;
   const int warps_per_blk = 4;
   const size_t smem = v.smem_per_warp * warps_per_blk;
-  OLPT_CUDA(cudaFuncSetAttribute(shake_kernel<Real>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                 (int)smem));
+
   for (int it = 0; it < n_loop; ++it) {
     residual_pass<Real>(ctx, v, nullptr, 0, 0);
     // algorithmic bytes: the augmented ROI of every active camera plus the object
@@ -1008,9 +1034,9 @@ static void shake_iterations(olpt_ctx* ctx, const ShakeParams& sp, ShakeView& v,
                                       2.0 * (3 * 8 + C * 2 * 8 + 8) + C * 5.0 * sizeof(Real));
     const int pid = ctx->prof.begin(PROF_SHAKE, s);
     if (n > 0)
-      shake_kernel<Real><<<OLPT_G(nblk(n, warps_per_blk)), 32 * warps_per_blk, smem, s>>>(
-          v, n, ctx->obj.xyz.as<double>(), ctx->obj.uv.as<double>(), W.otfp.as<Real>(),
-          ctx->obj.score.as<double>(), delta, active, resid_out);
+      launch_shake<Real>(C, nblk(n, warps_per_blk), 32 * warps_per_blk, smem, s, v, n,
+                         ctx->obj.xyz.as<double>(), ctx->obj.uv.as<double>(), W.otfp.as<Real>(),
+                         ctx->obj.score.as<double>(), delta, active, resid_out);
     ctx->prof.end(PROF_SHAKE, pid, s, bytes);
     OLPT_CUDA(cudaGetLastError());
     delta *= 0.5;
