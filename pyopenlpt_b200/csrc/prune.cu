@@ -464,9 +464,68 @@ int bit_width(uint64_t x) {
 
 // Stable LSD radix sort of (key, val) pairs on the low `bits` bits; result in
 // (key, val), scratch in (key2, val2).
+// Short lists: one CTA sorts (masked key, original position) pairs bitonically in
+// shared memory -- the same stable order as the radix passes, without their launches.
+constexpr int kSmallSort = 2048;
+
+__global__ void __launch_bounds__(1024) small_sort_kernel(const uint64_t* key, const int* val,
+                                                          int n, uint64_t mask, uint64_t* key_out,
+                                                          int* val_out) {
+  __shared__ uint64_t k[kSmallSort];
+  __shared__ int p[kSmallSort];
+  int N = 1;
+  while (N < n) N <<= 1;
+  for (int i = threadIdx.x; i < N; i += blockDim.x) {
+    if (i < n) {
+      k[i] = key[i] & mask;
+      p[i] = i;
+    } else {
+      k[i] = ~0ull;
+      p[i] = 0x7fffffff;
+    }
+  }
+  __syncthreads();
+  for (int size = 2; size <= N; size <<= 1)
+    for (int stride = size >> 1; stride > 0; stride >>= 1) {
+      for (int i = threadIdx.x; i < N; i += blockDim.x) {
+        const int j = i ^ stride;
+        if (j > i) {
+          const bool asc = (i & size) == 0;
+          const bool gt = k[i] > k[j] || (k[i] == k[j] && p[i] > p[j]);
+          if (gt == asc) {
+            const uint64_t tk = k[i];
+            k[i] = k[j];
+            k[j] = tk;
+            const int tp = p[i];
+            p[i] = p[j];
+            p[j] = tp;
+          }
+        }
+      }
+      __syncthreads();
+    }
+  for (int i = threadIdx.x; i < n; i += blockDim.x) {
+    key_out[i] = key[p[i]];
+    val_out[i] = val[p[i]];
+  }
+}
+
 void radix_sort_device(DevBuf& key, DevBuf& val, DevBuf& key2, DevBuf& val2, DevBuf& hist,
                        DevBuf& scan_tmp, int n, int bits, cudaStream_t s) {
   if (n <= 1 || bits <= 0) return;
+  if (n <= kSmallSort) {
+    key2.ensure((size_t)(n + 1) * sizeof(uint64_t), s);
+    val2.ensure((size_t)(n + 1) * sizeof(int), s);
+    // the radix passes order by the key bits below the first multiple of 8 >= bits
+    const int used = ((bits + 7) / 8) * 8;
+    const uint64_t m = used >= 64 ? ~0ull : ((1ull << used) - 1ull);
+    small_sort_kernel<<<OLPT_G(1), 1024, 0, s>>>(key.as<uint64_t>(), val.as<int>(), n, m,
+                                                key2.as<uint64_t>(), val2.as<int>());
+    OLPT_CUDA(cudaGetLastError());
+    std::swap(key, key2);
+    std::swap(val, val2);
+    return;
+  }
   const int n_blocks = (n + kRsTile - 1) / kRsTile;
   key2.ensure((size_t)(n + 1) * sizeof(uint64_t), s);
   val2.ensure((size_t)(n + 1) * sizeof(int), s);
