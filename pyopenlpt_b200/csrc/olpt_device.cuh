@@ -306,46 +306,76 @@ __device__ __forceinline__ void los_to_line2d(const CamDev& c, const Line3& L, d
 // myMATH::internal::gaussForward/gaussBackward (myMATH.h:183-289) for n = 3,
 // returning inverse(A) (gaussInverse, myMATH.h:291-301).
 __device__ __forceinline__ void gauss_inverse3(const double A[9], double R[9]) {
-  double u[9];
-  for (int i = 0; i < 9; ++i) u[i] = A[i];
-  int idx[3];
-  double maxrow[3];
+  // Rows move physically instead of through an index permutation (same operations on
+  // the same values, so the same result), which keeps every array in registers.
+  double r[3][3], mr[3];
+  int perm[3];
+#pragma unroll
   for (int x = 0; x < 3; ++x) {
-    idx[x] = x;
-    double m = u[3 * x];
-    if (u[3 * x + 1] > m) m = u[3 * x + 1];
-    if (u[3 * x + 2] > m) m = u[3 * x + 2];
-    maxrow[x] = m;
+    r[x][0] = A[3 * x];
+    r[x][1] = A[3 * x + 1];
+    r[x][2] = A[3 * x + 2];
+    double m = r[x][0];
+    if (r[x][1] > m) m = r[x][1];
+    if (r[x][2] > m) m = r[x][2];
+    mr[x] = m;
+    perm[x] = x;
   }
+#pragma unroll
   for (int y = 0; y < 2; ++y) {
     double maxp = 0;
     int t = 0;
+#pragma unroll
     for (int x = y; x < 3; ++x) {
-      double piv = fabs(u[3 * idx[x] + y] / maxrow[idx[x]]);
+      const double piv = fabs(r[x][y] / mr[x]);
       if (piv > maxp) {
         maxp = piv;
         t = x;
       }
     }
-    int tmp = idx[t];
-    idx[t] = idx[y];
-    idx[y] = tmp;
+    // swap positions y and t (t may be below y when no pivot is positive)
+#pragma unroll
+    for (int x = 0; x < 3; ++x) {
+      if (x == y || x != t) continue;
+#pragma unroll
+      for (int k = 0; k < 3; ++k) {
+        const double tmp = r[x][k];
+        r[x][k] = r[y][k];
+        r[y][k] = tmp;
+      }
+      const double tm = mr[x];
+      mr[x] = mr[y];
+      mr[y] = tm;
+      const int tp = perm[x];
+      perm[x] = perm[y];
+      perm[y] = tp;
+    }
+#pragma unroll
     for (int x = y + 1; x < 3; ++x) {
-      double m = u[3 * idx[x] + y] / u[3 * idx[y] + y];
-      u[3 * idx[x] + y] = m;
-      for (int it = y + 1; it < 3; ++it) u[3 * idx[x] + it] -= m * u[3 * idx[y] + it];
+      const double m = r[x][y] / r[y][y];
+      r[x][y] = m;
+#pragma unroll
+      for (int it = y + 1; it < 3; ++it) r[x][it] -= m * r[y][it];
     }
   }
-  double b[9] = {1, 0, 0, 0, 1, 0, 0, 0, 1};
-  for (int i = 0; i < 9; ++i) R[i] = b[i];
+  double pb[3][3];
+#pragma unroll
+  for (int x = 0; x < 3; ++x)
+#pragma unroll
+    for (int k = 0; k < 3; ++k) pb[x][k] = perm[x] == k ? 1.0 : 0.0;
+#pragma unroll
   for (int it = 0; it < 3; ++it) {
+#pragma unroll
     for (int y = 0; y < 2; ++y)
-      for (int x = y + 1; x < 3; ++x) b[3 * idx[x] + it] -= u[3 * idx[x] + y] * b[3 * idx[y] + it];
-    R[3 * 2 + it] = b[3 * idx[2] + it] / u[3 * idx[2] + 2];
+#pragma unroll
+      for (int x = y + 1; x < 3; ++x) pb[x][it] -= r[x][y] * pb[y][it];
+    R[3 * 2 + it] = pb[2][it] / r[2][2];
+#pragma unroll
     for (int x = 1; x > -1; --x) {
-      double z = b[3 * idx[x] + it];
-      for (int y = x + 1; y < 3; ++y) z -= u[3 * idx[x] + y] * R[3 * y + it];
-      R[3 * x + it] = z / u[3 * idx[x] + x];
+      double z = pb[x][it];
+#pragma unroll
+      for (int y = x + 1; y < 3; ++y) z -= r[x][y] * R[3 * y + it];
+      R[3 * x + it] = z / r[x][x];
     }
   }
 }
