@@ -197,12 +197,12 @@ __device__ double residue(const ShakeView& v, const Rect* roi, Smem<Real>& S) {
     if (row >= prmin && row < prmax && col >= pcmin && col < pcmax)
       pred = gauss<Real>(col, row, u, vv, S.otf + 5 * c);
     const Real d = S.aug[c * area + pix] - pred;
-    if (v.exact_sums)
+    if ((sizeof(Real) == 8 && v.exact_sums))
       S.dd[c * area + pix] = (double)d * (double)d;
     else
       part[c] += d * d;
   }
-  if (v.exact_sums) {
+  if ((sizeof(Real) == 8 && v.exact_sums)) {
     __syncwarp();
     if (lane < NC) {
       const Rect& R = roi[lane];
@@ -430,7 +430,7 @@ __global__ void __launch_bounds__(128, 8) shake_kernel(ShakeView v, int64_t n, d
     double f[3];
     double su[3][NC], sv[3][NC];
     bool sok[3][NC];
-    if (v.exact_sums) {
+    if ((sizeof(Real) == 8 && v.exact_sums)) {
       for (int j = 0; j < 3; ++j) {
         tmp[ax] = x0 + rel[j];
         eval_geom<Real, NC>(v, tmp, S);
