@@ -593,12 +593,50 @@ def learned_comparison(args, o: Ours):
             "speedup_particles_per_s": round(learned["particles_per_s"] / plain["particles_per_s"], 3),
             "speedup_time": round(plain["ms"] / learned["ms"], 3),
             "meets_recall_and_ghost": L.meets(learned, plain)}
+    # batched: B independent frames at once (olpt_ipr_run_batch: one context, host thread
+    # and stream per frame), wall time of the whole batch, against the same frames one
+    # at a time through the plain form
+    params = ctx.mlp_get_params()
     ctx.close()
+    B = args.learn_batch
+    ctxs = [_ffi.Context(o.local) for _ in range(B)]
+    for c in ctxs:
+        c.mlp_set_params(params)
+    scenes = [L.scene(950 + i, 0.02) for i in range(B)]
+    sk = dataclasses.replace(s, n_loop_ipr=k)
+
+    def batch_ms(sub, sset, lsx):
+        L.run_ipr_batch(sub, scenes[:len(sub)], sset, lsx)  # warm-up
+        runs = [L.run_ipr_batch(sub, scenes[:len(sub)], sset, lsx) for _ in range(args.learn_reps)]
+        best = sorted(runs, key=lambda m: m["ms"])[len(runs) // 2]
+        return {kk: round(v, 5) for kk, v in best.items()}
+
+    plain_one = [batch_ms([ctxs[i]], s, None) for i in range(B)]
+    plain_one_ms = sum(m["ms"] for m in plain_one)
+    plain_one_n = sum(m["n"] for m in plain_one)
+    plain_one_true = sum(m["true_particles_per_s"] * m["ms"] * 1e-3 for m in plain_one)
+    plain_b = batch_ms(ctxs, s, None)
+    learned_b = batch_ms(ctxs, sk, cfg)
+    for c in ctxs:
+        c.close()
+    batched = {
+        "frames": B, "ppp": 0.02,
+        "plain_one_at_a_time": {"ms_per_frame": round(plain_one_ms / B, 3),
+                                "particles_per_s": round(plain_one_n / (plain_one_ms * 1e-3)),
+                                "true_particles_per_s": round(plain_one_true / (plain_one_ms * 1e-3))},
+        "plain_batched": dict(plain_b, ms_per_frame=round(plain_b["ms"] / B, 3)),
+        "learned_batched": dict(learned_b, ms_per_frame=round(learned_b["ms"] / B, 3)),
+        "learned_batched_vs_plain": {
+            "frames_per_s": round(plain_one_ms / learned_b["ms"], 3),
+            "particles_per_s": round(learned_b["particles_per_s"] / (plain_one_n / (plain_one_ms * 1e-3)), 3),
+            "true_particles_per_s": round(learned_b["true_particles_per_s"] / (plain_one_true / (plain_one_ms * 1e-3)), 3)},
+    }
     return {
         "workload": "4 pinhole cams, 1024^2 uint8, a=200, OTF b,c ~ U[0.3,0.8], noise 2; "
                     "plain = olpt_ipr_run 4 loops x 4 shakes; learned = MLP proposal + 1 "
-                    "refine shake, calibrated loop count; device time per IPR, L2 flushed",
-        "batched": False,
+                    "refine shake, calibrated loop count; eval: device time per IPR, L2 "
+                    "flushed; batched: wall time, frames on concurrent contexts/streams",
+        "batched": batched,
         "train": {"frames": args.learn_frames, "tuples": n_tuples, "steps": len(losses),
                   "collect_s": round(t_collect, 1), "train_s": round(t_train, 1),
                   "loss_first": round(losses[0], 4),
@@ -638,6 +676,8 @@ def main():
                     help="frames of training tuples for the learned comparison (0 = skip)")
     ap.add_argument("--learn-steps", type=int, default=3000)
     ap.add_argument("--learn-reps", type=int, default=5)
+    ap.add_argument("--learn-batch", type=int, default=4,
+                    help="frames processed at once in the batched learned comparison")
     args = ap.parse_args()
     if args.warmup < 3:
         args.warmup = 3

@@ -243,6 +243,12 @@ typedef struct olpt_ipr_params {
  * tolerance growing x1.5 per loop.  The current images end as the final residual.
  * n_objects receives the number of reconstructed objects. */
 olpt_status_t olpt_ipr_run(olpt_ctx* ctx, const olpt_ipr_params* p, int64_t* n_objects);
+/* Independent frames at once (no reference counterpart): olpt_ipr_run on every
+ * context, each from its own host thread on its own stream, so the frames' kernels
+ * overlap on the device.  n_objects[i] receives context i's count; the first failing
+ * context's status is returned (its message in that context's olpt_last_error). */
+olpt_status_t olpt_ipr_run_batch(olpt_ctx* const* ctxs, int n_ctx, const olpt_ipr_params* p,
+                                 int64_t* n_objects);
 /* Objects of the last olpt_ipr_run in the reference's output order: xyz (n x 3) and
  * their 2D projections uv (n x n_cam x 2); either may be NULL. */
 olpt_status_t olpt_ipr_result(olpt_ctx* ctx, double* xyz, double* uv);

@@ -492,6 +492,22 @@ def ipr_params(settings, limit, precision: int = 0) -> IprParams:
                      n_obj2d_process_max=settings.n_obj2d_process_max)
 
 
+def ipr_run_batch(ctxs: Sequence["Context"], params: IprParams):
+    """olpt_ipr_run_batch: every context's IPR at once (one host thread and stream each);
+    returns the per-context object counts."""
+    L = lib()
+    arr = (C.c_void_p * len(ctxs))(*[c.h for c in ctxs])
+    out = np.zeros(len(ctxs), dtype=np.int64)
+    rc = L.olpt_ipr_run_batch(arr, len(ctxs), C.byref(params), _p(out, _i64p))
+    if rc != 0:
+        for c in ctxs:
+            msg = L.olpt_last_error(c.h)
+            if msg:
+                raise OlptError(rc, msg.decode())
+        raise OlptError(rc, "olpt_ipr_run_batch failed")
+    return out
+
+
 TRACK_LONG_ACTIVE, TRACK_SHORT_ACTIVE, TRACK_LONG_INACTIVE, TRACK_EXIT = 0, 1, 2, 3
 TRACK_LISTS = ("long_active", "short_active", "long_inactive", "exit")
 

@@ -7,6 +7,7 @@
 #include <cmath>
 #include <new>
 #include <string>
+#include <thread>
 #include <vector>
 
 #include "olpt_ctx.cuh"
@@ -808,6 +809,29 @@ olpt_status_t olpt_ipr_run(olpt_ctx* ctx, const olpt_ipr_params* p, int64_t* n_o
     ipr_device(ctx, to_ipr_params(p));
     if (n_objects) *n_objects = ctx->ipr.n_out;
   });
+}
+
+olpt_status_t olpt_ipr_run_batch(olpt_ctx* const* ctxs, int n_ctx, const olpt_ipr_params* p,
+                                 int64_t* n_objects) {
+  if (!ctxs || n_ctx <= 0 || !p) return OLPT_ERR_INVALID_ARG;
+  for (int i = 0; i < n_ctx; ++i)
+    for (int j = 0; j < i; ++j)
+      if (!ctxs[i] || ctxs[i] == ctxs[j]) return OLPT_ERR_INVALID_ARG;
+  std::vector<olpt_status_t> st(n_ctx, OLPT_OK);
+  std::vector<int64_t> cnt(n_ctx, 0);
+  std::vector<std::thread> th;
+  th.reserve(n_ctx);
+  for (int i = 0; i < n_ctx; ++i)
+    th.emplace_back([&, i] {
+      cudaSetDevice(ctxs[i]->device);
+      st[i] = olpt_ipr_run(ctxs[i], p, &cnt[i]);
+    });
+  for (auto& t : th) t.join();
+  for (int i = 0; i < n_ctx; ++i)
+    if (n_objects) n_objects[i] = cnt[i];
+  for (int i = 0; i < n_ctx; ++i)
+    if (st[i] != OLPT_OK) return st[i];
+  return OLPT_OK;
 }
 
 olpt_status_t olpt_ipr_result(olpt_ctx* ctx, double* xyz, double* uv) {

@@ -149,15 +149,15 @@ __global__ void __launch_bounds__(128, 1)
 }
 
 PFN_cuTensorMapEncodeTiled_v12000 encode_fn() {
-  static PFN_cuTensorMapEncodeTiled_v12000 fn = nullptr;
-  if (!fn) {
+  // thread-safe one-time lookup (contexts may run on several host threads)
+  static const PFN_cuTensorMapEncodeTiled_v12000 fn = [] {
     void* p = nullptr;
     cudaDriverEntryPointQueryResult q;
     OLPT_CUDA(cudaGetDriverEntryPoint("cuTensorMapEncodeTiled", &p, cudaEnableDefault, &q));
     OLPT_REQUIRE(q == cudaDriverEntryPointSuccess && p, OLPT_ERR_CUDA,
                  "cuTensorMapEncodeTiled is not available");
-    fn = reinterpret_cast<PFN_cuTensorMapEncodeTiled_v12000>(p);
-  }
+    return reinterpret_cast<PFN_cuTensorMapEncodeTiled_v12000>(p);
+  }();
   return fn;
 }
 
@@ -180,13 +180,8 @@ CUtensorMap tile_map(const __nv_bfloat16* base, int rows, int cols, int ld, int 
 template <int BN>
 void launch(const CUtensorMap& ta, const CUtensorMap& tb, const EpiArgs& g, dim3 grid,
             cudaStream_t s) {
-  static bool attr = false;
-  if (!attr) {
-    OLPT_CUDA(cudaFuncSetAttribute(gemm_bf16_kernel<BN>,
-                                   cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                   (int)smem_bytes<BN>()));
-    attr = true;
-  }
+  OLPT_CUDA(cudaFuncSetAttribute(gemm_bf16_kernel<BN>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                 (int)smem_bytes<BN>()));
   gemm_bf16_kernel<BN><<<OLPT_G(grid), 128, smem_bytes<BN>(), s>>>(ta, tb, g);
   OLPT_CUDA(cudaGetLastError());
 }

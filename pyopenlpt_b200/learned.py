@@ -102,6 +102,29 @@ def train(ctx: _ffi.Context, x: np.ndarray, t: np.ndarray, steps: int, batch: in
     return losses
 
 
+def run_ipr_batch(ctxs: Sequence[_ffi.Context], scenes: Sequence[synth.Scene],
+                  s: synth.IPRSettings, ls: Optional[LearnedSettings]) -> Dict[str, float]:
+    """The frames at once (olpt_ipr_run_batch, one context each): metrics summed over
+    the frames and the wall time of the whole batch."""
+    for ctx, sc in zip(ctxs, scenes):
+        bind(ctx, sc)
+        ctx.learned_configure((ls or LearnedSettings()).params(enable=ls is not None))
+    p = _ffi.ipr_params(s, scenes[0].volume)
+    t0 = time.perf_counter()
+    counts = _ffi.ipr_run_batch(ctxs, p)
+    ms = 1e3 * (time.perf_counter() - t0)
+    found = n_true = n_out = 0.0
+    for ctx, sc, n in zip(ctxs, scenes, counts):
+        xyz, _ = ctx.ipr_result(int(n))
+        m = metrics(xyz, sc.xyz)
+        found += m["recall_10"] * len(sc.xyz)
+        n_true += len(sc.xyz)
+        n_out += m["n"]
+    return {"frames": float(len(ctxs)), "n": n_out, "recall_10": found / max(n_true, 1.0),
+            "ms": ms, "particles_per_s": n_out / (ms * 1e-3),
+            "true_particles_per_s": found / (ms * 1e-3)}
+
+
 def metrics(xyz: np.ndarray, truth: np.ndarray) -> Dict[str, float]:
     """Recall and ghost rate at 0.05 and 0.1 mm, RMSE of the matched positions."""
     out: Dict[str, float] = {"n": float(len(xyz))}
