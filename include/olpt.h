@@ -363,6 +363,14 @@ olpt_status_t olpt_mlp_forward(olpt_ctx* ctx, int64_t n, const float* x, float* 
 olpt_status_t olpt_mlp_train_step(olpt_ctx* ctx, int64_t n, const float* x, const float* targets,
                                   int on_device, double lr, double ghost_weight, int update,
                                   double* loss, float* grad);
+/* Training on a device-resident dataset: x (n x OLPT_MLP_IN) and targets (n x 4), host
+ * arrays copied to the device once (or device pointers, on_device != 0); `steps` Adam
+ * steps on mini-batches of `batch` rows drawn uniformly with replacement (seeded), the
+ * learning rate decayed from lr by a cosine to 5%.  losses (host, optional): one per
+ * step. */
+olpt_status_t olpt_mlp_train(olpt_ctx* ctx, int64_t n, const float* x, const float* targets,
+                             int on_device, int batch, int steps, double lr, double ghost_weight,
+                             uint64_t seed, float* losses);
 /* Features (n_objects x OLPT_MLP_IN) of the context's objects, against a residual of
  * the current images with every object projected (4 cameras). */
 olpt_status_t olpt_mlp_features(olpt_ctx* ctx, const olpt_shake_params* p, float* x,

@@ -424,6 +424,18 @@ class Context:
                                                int(update), C.byref(loss), _p(g, _fp)))
         return (loss.value, g) if want_grad else loss.value
 
+    def mlp_train(self, x: np.ndarray, t: np.ndarray, steps: int, batch: int = 8192,
+                  lr: float = 2e-3, ghost_weight: float = 1.0, seed: int = 0) -> np.ndarray:
+        """olpt_mlp_train: the dataset goes to the device once; returns the step losses."""
+        x = np.ascontiguousarray(x, dtype=np.float32).reshape(-1, MLP_IN)
+        t = np.ascontiguousarray(t, dtype=np.float32).reshape(-1, MLP_OUT)
+        losses = np.zeros(max(steps, 1), np.float32)
+        self._check(self.L.olpt_mlp_train(self.h, C.c_int64(len(x)), _p(x, _fp), _p(t, _fp), 0,
+                                          int(batch), int(steps), C.c_double(lr),
+                                          C.c_double(ghost_weight), C.c_uint64(seed),
+                                          _p(losses, _fp)))
+        return losses[:steps]
+
     def mlp_train_step_device(self, x_ptr: int, t_ptr: int, n: int, lr: float,
                               ghost_weight: float = 1.0) -> float:
         loss = C.c_double()

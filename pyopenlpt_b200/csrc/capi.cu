@@ -1082,6 +1082,30 @@ olpt_status_t olpt_mlp_train_step(olpt_ctx* ctx, int64_t n, const float* x, cons
   });
 }
 
+olpt_status_t olpt_mlp_train(olpt_ctx* ctx, int64_t n, const float* x, const float* targets,
+                             int on_device, int batch, int steps, double lr, double ghost_weight,
+                             uint64_t seed, float* losses) {
+  return guard(ctx, [&] {
+    OLPT_REQUIRE(n > 0 && x && targets && batch > 0 && steps >= 0, OLPT_ERR_INVALID_ARG,
+                 "mlp_train: bad arguments");
+    MlpWork& W = ctx->mlp;
+    cudaStream_t s = ctx->stream;
+    const float* dx = x;
+    const float* dt = targets;
+    if (!on_device) {
+      W.ds_x.ensure((size_t)n * OLPT_MLP_IN * 4, s);
+      W.ds_t.ensure((size_t)n * kMlpOut * 4, s);
+      OLPT_CUDA(cudaMemcpyAsync(W.ds_x.p, x, (size_t)n * OLPT_MLP_IN * 4, cudaMemcpyHostToDevice, s));
+      OLPT_CUDA(cudaMemcpyAsync(W.ds_t.p, targets, (size_t)n * kMlpOut * 4, cudaMemcpyHostToDevice,
+                                s));
+      dx = W.ds_x.as<float>();
+      dt = W.ds_t.as<float>();
+    }
+    mlp_train_many(ctx, dx, dt, n, batch, steps, lr, ghost_weight, seed, losses);
+    OLPT_CUDA(cudaStreamSynchronize(s));
+  });
+}
+
 olpt_status_t olpt_mlp_features(olpt_ctx* ctx, const olpt_shake_params* p, float* x,
                                 int on_device) {
   return guard(ctx, [&] {

@@ -229,6 +229,26 @@ __global__ void adam_kernel(float* p, const float* g, float* m, float* v, int64_
   p[i] -= lr * (mi / bc1) / (sqrtf(vi / bc2) + eps);
 }
 
+// ---------------------------------------------------------------- sampling
+__device__ __forceinline__ uint64_t mix64(uint64_t z) {  // splitmix64 finaliser
+  z += 0x9e3779b97f4a7c15ull;
+  z = (z ^ (z >> 30)) * 0xbf58476d1ce4e5b9ull;
+  z = (z ^ (z >> 27)) * 0x94d049bb133111ebull;
+  return z ^ (z >> 31);
+}
+
+// mini-batch rows drawn uniformly with replacement from the resident dataset
+__global__ void sample_kernel(const float* x, const float* t, int64_t n, int batch, uint64_t seed,
+                              int64_t step, float* xb, float* tb) {
+  const int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+  if (i >= (int64_t)batch * kMlpIn) return;
+  const int64_t r = i / kMlpIn;
+  const int c = (int)(i % kMlpIn);
+  const int64_t src = (int64_t)(mix64(seed ^ ((uint64_t)step << 32) ^ (uint64_t)r) % (uint64_t)n);
+  xb[i] = x[src * kMlpIn + c];
+  if (c < kMlpOut) tb[r * kMlpOut + c] = t[src * kMlpOut + c];
+}
+
 // ---------------------------------------------------------------- features
 // one warp per object; lanes 0..3 project on their camera and evaluate the OTF there
 template <typename Real>
@@ -611,6 +631,25 @@ double mlp_train_device(olpt_ctx* ctx, const float* x_f32, const float* tgt, int
                             s));
   check_err(ctx);
   return loss;
+}
+
+void mlp_train_many(olpt_ctx* ctx, const float* x, const float* t, int64_t n, int batch, int steps,
+                    double lr, double ghost_weight, uint64_t seed, float* losses) {
+  MlpWork& W = ctx->mlp;
+  OLPT_REQUIRE(W.ready, OLPT_ERR_INVALID_ARG, "network not initialised");
+  OLPT_REQUIRE(n > 0 && batch > 0 && steps >= 0, OLPT_ERR_INVALID_ARG, "mlp_train: bad sizes");
+  cudaStream_t s = ctx->stream;
+  W.xin.ensure((size_t)batch * kMlpIn * 4, s);
+  W.tgt.ensure((size_t)batch * kMlpOut * 4, s);
+  for (int it = 0; it < steps; ++it) {
+    const double a = lr * (0.05 + 0.95 * 0.5 * (1.0 + std::cos(M_PI * it / (double)steps)));
+    sample_kernel<<<OLPT_G(nblk((int64_t)batch * kMlpIn)), 256, 0, s>>>(
+        x, t, n, batch, seed, it, W.xin.as<float>(), W.tgt.as<float>());
+    OLPT_CUDA(cudaGetLastError());
+    const double l = mlp_train_device(ctx, W.xin.as<float>(), W.tgt.as<float>(), batch, a,
+                                      ghost_weight, true);
+    if (losses) losses[it] = (float)l;
+  }
 }
 
 }  // namespace olpt

@@ -308,12 +308,12 @@ struct MlpWork {
   DevBuf master, grad, am, av, wb1, wb2, wb3, wt2, wt3;
   DevBuf x, xt, xin, tgt, z1, z2, z3, h1, h2, h3, h1t, h2t, o, dout;
   DevBuf dz1f, dz2f, dz3f, dz2b, dz3b, dz1t, dz2t, dz3t, part, hpart, loss, err;
-  DevBuf keep, pos, start_xyz, act, nres;
+  DevBuf keep, pos, start_xyz, act, nres, ds_x, ds_t;
   void release(cudaStream_t s) {
     for (DevBuf* b : {&master, &grad, &am, &av, &wb1, &wb2, &wb3, &wt2, &wt3, &x, &xt, &xin, &tgt,
                       &z1, &z2, &z3, &h1, &h2, &h3, &h1t, &h2t, &o, &dout, &dz1f, &dz2f, &dz3f,
                       &dz2b, &dz3b, &dz1t, &dz2t, &dz3t, &part, &hpart, &loss, &err, &keep, &pos,
-                      &start_xyz, &act, &nres})
+                      &start_xyz, &act, &nres, &ds_x, &ds_t})
       b->release(s);
     ready = false;
     cap = 0;
@@ -339,6 +339,10 @@ void mlp_infer_device(olpt_ctx* ctx, const __nv_bfloat16* x, int64_t n, float* o
 // one training batch: loss (mean), gradients into MlpWork::grad, Adam update when lr > 0
 double mlp_train_device(olpt_ctx* ctx, const float* x_f32, const float* tgt, int64_t n, double lr,
                         double ghost_weight, bool update);
+// steps Adam steps on uniform mini-batches of a device-resident dataset (cosine
+// learning-rate decay to 5%); losses (host, optional) per step
+void mlp_train_many(olpt_ctx* ctx, const float* x, const float* t, int64_t n, int batch, int steps,
+                    double lr, double ghost_weight, uint64_t seed, float* losses);
 // the learned shake: features -> network -> correction and ghost pruning -> short
 // plain refinement -> full plain shake for objects whose residue stays high
 void learned_shake_device(olpt_ctx* ctx, const ShakeParams& sp);

@@ -86,9 +86,18 @@ def collect(ctx: _ffi.Context, sc: synth.Scene, s: synth.IPRSettings,
 
 
 def train(ctx: _ffi.Context, x: np.ndarray, t: np.ndarray, steps: int, batch: int = 8192,
-          lr: float = 2e-3, ghost_weight: float = 1.0, seed: int = 0,
-          time_budget_s: Optional[float] = None) -> List[float]:
-    """Adam on random mini-batches, learning rate decayed by cosine to 5% of lr."""
+          lr: float = 2e-3, ghost_weight: float = 1.0, seed: int = 0) -> List[float]:
+    """Adam on uniform mini-batches of the tuples held on the device (olpt_mlp_train),
+    learning rate decayed by a cosine to 5% of lr; the step losses."""
+    return [float(v) for v in ctx.mlp_train(x, t, steps, batch=batch, lr=lr,
+                                            ghost_weight=ghost_weight, seed=seed)]
+
+
+def train_from_host(ctx: _ffi.Context, x: np.ndarray, t: np.ndarray, steps: int,
+                    batch: int = 8192, lr: float = 2e-3, ghost_weight: float = 1.0,
+                    seed: int = 0, time_budget_s: Optional[float] = None) -> List[float]:
+    """The same schedule with each mini-batch drawn on the host and copied
+    (olpt_mlp_train_step per step)."""
     rng = np.random.default_rng(seed)
     losses = []
     t0 = time.perf_counter()

@@ -173,3 +173,19 @@ def test_features_match_restatement(ctx):
         assert feats[:, :484].max() > 0.5  # the particles are in the patches
     finally:
         g.close()
+
+
+def test_resident_dataset_training(ctx):
+    """olpt_mlp_train: the dataset copied once, mini-batches sampled on the device."""
+    rng = np.random.default_rng(8)
+    ctx.mlp_init(12)
+    P = rng.normal(0, 1, (R.IN, 3)).astype(np.float32) / np.sqrt(R.IN)
+    xs = _features(rng, 20000)
+    ts = np.zeros((len(xs), 4), np.float32)
+    ts[:, :3] = np.tanh(xs @ P * 3)
+    ts[:, 3] = (xs[:, 484] > 0.2).astype(np.float32)
+    losses = ctx.mlp_train(xs, ts, steps=400, batch=2048, lr=2e-3, seed=3)
+    assert len(losses) == 400 and np.all(np.isfinite(losses))
+    first = ctx.mlp_train_step(xs[:2048], ts[:2048], lr=0.0, update=False)
+    print("resident-dataset training: loss", losses[0], "->", np.mean(losses[-20:]), "eval", first)
+    assert np.mean(losses[-20:]) < 0.35 * losses[0]
