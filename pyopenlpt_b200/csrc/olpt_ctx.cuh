@@ -192,14 +192,14 @@ struct PruneWork {
   DevBuf fl, slot_key, fcnt, slot_pct, slot_used, pct, flag;
   DevBuf f_pct, f_both, pos_pct, pos_both, pcls, ecls, newc, excl, cstart;
   DevBuf g_pts, g_cnt, g_pct, g_e, pool_e, pool_i;
-  DevBuf gkey, gstate, gfirst, gowner, sel, spos, scnt;
+  DevBuf gkey, gstate, gfirst, gowner, sel, spos, scnt, mixed;
   Csr points, gpoints;
   HostBuf pin;  // pinned staging of the greedy's input
   void release(cudaStream_t s) {
     for (DevBuf* b : {&key, &val, &key2, &val2, &hist, &scan_tmp, &ids_s, &e_s, &X_s, &fl,
                       &slot_key, &fcnt, &slot_pct, &slot_used, &pct, &flag, &f_pct, &f_both,
                       &pos_pct, &pos_both, &pcls, &ecls, &newc, &excl, &cstart, &g_pts, &g_cnt,
-                      &g_pct, &g_e, &pool_e, &pool_i, &gkey, &gstate, &gfirst, &gowner, &sel, &spos, &scnt})
+                      &g_pct, &g_e, &pool_e, &pool_i, &gkey, &gstate, &gfirst, &gowner, &sel, &spos, &scnt, &mixed})
       b->release(s);
     points.release(s);
     gpoints.release(s);

@@ -328,12 +328,30 @@ __global__ void class_assign_kernel(const int* idx, const int* newc, const int* 
   cls[idx[p]] = c;
 }
 
-__global__ void order_keys_kernel(const int* fin, const int* pos, int M, const int* cls,
-                                  uint64_t* key, int* idx) {
-  const int j = blockIdx.x * blockDim.x + threadIdx.x;
-  if (j >= M || !fin[j]) return;
-  key[pos[j]] = (uint64_t)cls[j];
-  idx[pos[j]] = j;
+// The (percentile class, e_check) order has the members of an e_check class sorted by
+// e_check value, then index; the greedy wants them by index.  Only classes whose members
+// differ in value need it: mark them, then sort each such class by index.
+__global__ void class_mixed_kernel(const int* idx, const int* newc, const int* excl, int m,
+                                   const double* val, int* mixed) {
+  const int p = blockIdx.x * blockDim.x + threadIdx.x;
+  if (p < 1 || p >= m || newc[p]) return;
+  if (val[idx[p - 1]] != val[idx[p]]) mixed[excl[p] + newc[p] - 1] = 1;
+}
+
+__global__ void class_index_sort_kernel(int* idx, const int* start, int n_cls, int m,
+                                        const int* mixed) {
+  const int c = blockIdx.x * blockDim.x + threadIdx.x;
+  if (c >= n_cls || !mixed[c]) return;
+  const int b = start[c], e = c + 1 < n_cls ? start[c + 1] : m;
+  for (int i = b + 1; i < e; ++i) {
+    const int v = idx[i];
+    int j = i - 1;
+    while (j >= b && idx[j] > v) {
+      idx[j + 1] = idx[j];
+      --j;
+    }
+    idx[j + 1] = v;
+  }
 }
 
 __global__ void gather_greedy_kernel(const int* order, int G, int n, const int* fl,
@@ -679,12 +697,16 @@ bool prune_order_device(PruneWork& W, const PruneView& pv, int M, int n, int64_t
   *G_out = G;
   if (G == 0) return true;
   // greedy order: e_check class ids already increase with the percentile class, so
-  // (class, index) is (percentile class, e_check class, index)
-  order_keys_kernel<<<OLPT_G(nblk(M)), 256, 0, s>>>(W.f_both.as<int>(), W.pos_both.as<int>(), M,
-                                                   W.ecls.as<int>(), W.key.as<uint64_t>(),
-                                                   W.val.as<int>());
-  radix_sort_device(W.key, W.val, W.key2, W.val2, W.hist, W.scan_tmp, G,
-                    bit_width((uint64_t)n_ecls), s);
+  // (class, index) is (percentile class, e_check class, index).  W.val holds the
+  // candidates in (percentile class, e_check, index) order from the class pass; only
+  // the classes whose members differ in e_check need their members re-sorted by index.
+  W.mixed.ensure((size_t)(n_ecls + 1) * sizeof(int), s);
+  OLPT_CUDA(cudaMemsetAsync(W.mixed.p, 0, (size_t)(n_ecls + 1) * sizeof(int), s));
+  class_mixed_kernel<<<OLPT_G(nblk(G)), 256, 0, s>>>(W.val.as<int>(), W.newc.as<int>(),
+                                                    W.excl.as<int>(), G, W.e_s.as<double>(),
+                                                    W.mixed.as<int>());
+  class_index_sort_kernel<<<OLPT_G(nblk(n_ecls)), 256, 0, s>>>(
+      W.val.as<int>(), W.cstart.as<int>(), n_ecls, G, W.mixed.as<int>());
   W.g_pts.ensure((size_t)(G + 1) * n * sizeof(int), s);
   W.g_cnt.ensure(G + 16, s);
   W.g_pct.ensure((size_t)(G + 1) * sizeof(double), s);
