@@ -255,6 +255,19 @@ PHASE_NAMES = {5: "detection", 6: "stereo matching (all)", 7: "candidate sort + 
                11: "sequential greedy (replacement fallback)"}
 
 
+def reduce_replicas(dist, values, device):
+    """Whole-job numbers over the replicas (one per rank): the slowest rank's times
+    (values[0] device ms, values[2] end-to-end s) and the sum of the particles
+    (values[1], values[3])."""
+    import torch
+    t = torch.tensor([float(v) for v in values], dtype=torch.float64, device=device)
+    tmax = t.clone()
+    dist.all_reduce(tmax, op=dist.ReduceOp.MAX)
+    tsum = t.clone()
+    dist.all_reduce(tsum, op=dist.ReduceOp.SUM)
+    return tmax[0].item(), tsum[1].item(), tmax[2].item(), tsum[3].item()
+
+
 class Ours:
     """One rank of our arm: device set-up, rank reduction and the JSON line."""
 
@@ -285,16 +298,9 @@ class Ours:
         return ctx
 
     def reduce(self, dev_ms, parts, e2e_s, e2e_parts):
-        torch, dist = self.torch, self.dist
-        vals = torch.tensor([dev_ms, float(parts), e2e_s, float(e2e_parts)], dtype=torch.float64,
-                            device="cuda")
         if self.world == 1:
             return dev_ms, float(parts), e2e_s, float(e2e_parts)
-        tmax = vals.clone()
-        dist.all_reduce(tmax, op=dist.ReduceOp.MAX)
-        tsum = vals.clone()
-        dist.all_reduce(tsum, op=dist.ReduceOp.SUM)
-        return tmax[0].item(), tsum[1].item(), tmax[2].item(), tsum[3].item()
+        return reduce_replicas(self.dist, [dev_ms, parts, e2e_s, e2e_parts], "cuda")
 
     def line(self, prof, dev_ms, parts, e2e_s, e2e_parts, bi, bo, launches, clk, cfg, cpu,
              extra):
