@@ -1,11 +1,11 @@
 // Tensor-core GEMM for the learned proposal's MLP (olpt_gemm.h): one CTA per
 // 128 x BN output tile, TMA-fed 4-stage shared-memory ring, tcgen05 MMAs issued by
-// one thread into a TMEM accumulator, and a fused epilogue by all four warps (warp w
-// owns TMEM lanes 32w..32w+31 = tile rows).
+// one thread into a TMEM accumulator, and a fused epilogue by all eight warps (warp w
+// owns TMEM lanes 32 (w % 4) .. + 31 = tile rows, and half of the tile's columns).
 //
 //   warp 0, lane 0: TMA producer (A tile 128 x 64, B tile BN x 64 per stage)
 //   warp 1, lane 0: MMA issuer (4 x K=16 MMAs per stage, commit frees the stage)
-//   all warps:      epilogue after the final commit
+//   all 8 warps:    epilogue after the final commit (vector stores for full chunks)
 //
 // Every mbarrier wait is bounded (umma::kWaitLimitNs); a timeout sets *err and the
 // CTA still drains its MMAs and frees its TMEM before returning.
@@ -38,7 +38,7 @@ constexpr size_t smem_bytes() {
 }
 
 template <int BN>
-__global__ void __launch_bounds__(128, 1)
+__global__ void __launch_bounds__(256, 1)
     gemm_bf16_kernel(const __grid_constant__ CUtensorMap tmA, const __grid_constant__ CUtensorMap tmB,
                      EpiArgs g) {
   using namespace umma;
@@ -111,14 +111,17 @@ __global__ void __launch_bounds__(128, 1)
   }
   fence_after_sync();
 
-  const int row = m0 + warp * 32 + lane;
+  // warp w reads TMEM lanes 32 (w % 4) .. + 31 (its rows); warps 0-3 take the first
+  // half of the tile's columns, warps 4-7 the second
+  const int quarter = warp & 3, half = warp >> 2;
+  const int row = m0 + quarter * 32 + lane;
   const bool row_ok = row < g.M;
   const GemmEpilogue& e = g.e;
   const bool partial = g.splits > 1;
-  for (int c = 0; c < BN; c += 16) {
+  for (int c = half * (BN / 2); c < (half + 1) * (BN / 2); c += 16) {
     float v[16];
     if (have) {
-      tmem_ld16(tmem + ((uint32_t)(warp * 32) << 16) + (uint32_t)c, v);
+      tmem_ld16(tmem + ((uint32_t)(quarter * 32) << 16) + (uint32_t)c, v);
     } else {
 #pragma unroll
       for (int j = 0; j < 16; ++j) v[j] = 0.0f;
@@ -128,7 +131,64 @@ __global__ void __launch_bounds__(128, 1)
     const int nv = min(16, g.N - nb);
     if (partial) {
       float* o = e.out_f32 + (size_t)blockIdx.z * g.M * e.ld_f32 + (size_t)row * e.ld_f32 + nb;
-      for (int j = 0; j < nv; ++j) o[j] = v[j];
+      if (nv == 16 && ((uintptr_t)o & 15) == 0) {
+#pragma unroll
+        for (int q = 0; q < 4; ++q)
+          reinterpret_cast<float4*>(o)[q] = make_float4(v[4 * q], v[4 * q + 1], v[4 * q + 2],
+                                                        v[4 * q + 3]);
+      } else {
+        for (int j = 0; j < nv; ++j) o[j] = v[j];
+      }
+      continue;
+    }
+    if (nv == 16) {
+      // full chunk: vector loads and stores where the addresses allow
+      if (e.bias) {
+#pragma unroll
+        for (int j = 0; j < 16; ++j) v[j] += e.bias[nb + j];
+      }
+      if (e.gelu_pre) {
+        const float* pp = e.gelu_pre + (size_t)row * e.ld_pre + nb;
+#pragma unroll
+        for (int j = 0; j < 16; ++j) v[j] *= gelu_grad_f(pp[j]);
+      }
+      if (e.out_f32) {
+        float* o = e.out_f32 + (size_t)row * e.ld_f32 + nb;
+        if (((uintptr_t)o & 15) == 0) {
+#pragma unroll
+          for (int q = 0; q < 4; ++q)
+            reinterpret_cast<float4*>(o)[q] = make_float4(v[4 * q], v[4 * q + 1], v[4 * q + 2],
+                                                          v[4 * q + 3]);
+        } else {
+#pragma unroll
+          for (int j = 0; j < 16; ++j) o[j] = v[j];
+        }
+      }
+      if (e.gelu) {
+#pragma unroll
+        for (int j = 0; j < 16; ++j) v[j] = gelu_f(v[j]);
+      }
+      if (e.out_bf16) {
+        __nv_bfloat16* o = e.out_bf16 + (size_t)row * e.ld_bf16 + nb;
+        if (((uintptr_t)o & 15) == 0) {
+          uint32_t w[8];
+#pragma unroll
+          for (int q = 0; q < 8; ++q) {
+            const __nv_bfloat162 b2 = __floats2bfloat162_rn(v[2 * q], v[2 * q + 1]);
+            w[q] = *reinterpret_cast<const uint32_t*>(&b2);
+          }
+          reinterpret_cast<uint4*>(o)[0] = make_uint4(w[0], w[1], w[2], w[3]);
+          reinterpret_cast<uint4*>(o)[1] = make_uint4(w[4], w[5], w[6], w[7]);
+        } else {
+#pragma unroll
+          for (int j = 0; j < 16; ++j) o[j] = __float2bfloat16_rn(v[j]);
+        }
+      }
+      if (e.out_bf16_t) {
+#pragma unroll
+        for (int j = 0; j < 16; ++j)
+          e.out_bf16_t[(size_t)(nb + j) * e.ld_t + row] = __float2bfloat16_rn(v[j]);
+      }
       continue;
     }
     for (int j = 0; j < nv; ++j) {
@@ -182,7 +242,7 @@ void launch(const CUtensorMap& ta, const CUtensorMap& tb, const EpiArgs& g, dim3
             cudaStream_t s) {
   OLPT_CUDA(cudaFuncSetAttribute(gemm_bf16_kernel<BN>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                  (int)smem_bytes<BN>()));
-  gemm_bf16_kernel<BN><<<OLPT_G(grid), 128, smem_bytes<BN>(), s>>>(ta, tb, g);
+  gemm_bf16_kernel<BN><<<OLPT_G(grid), 256, smem_bytes<BN>(), s>>>(ta, tb, g);
   OLPT_CUDA(cudaGetLastError());
 }
 
