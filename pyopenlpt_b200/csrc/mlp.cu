@@ -545,15 +545,35 @@ void mlp_infer_device(olpt_ctx* ctx, const __nv_bfloat16* x, int64_t n, float* o
   check_err(ctx);
 }
 
+namespace {
+// One training step enqueued on the context's stream (no synchronisation); the mean
+// loss is left on the device at the returned address.
+const double* train_enqueue(olpt_ctx* ctx, const float* x_f32, const float* tgt, int64_t n,
+                            double lr, double ghost_weight, bool update);
+}  // namespace
+
 double mlp_train_device(olpt_ctx* ctx, const float* x_f32, const float* tgt, int64_t n, double lr,
                         double ghost_weight, bool update) {
+  OLPT_REQUIRE(ctx->mlp.ready, OLPT_ERR_INVALID_ARG, "network not initialised");
+  OLPT_REQUIRE(n > 0, OLPT_ERR_INVALID_ARG, "empty batch");
+  ensure_batch(ctx, n, true);
+  OLPT_CUDA(cudaMemsetAsync(ctx->mlp.err.p, 0, 16, ctx->stream));
+  const double* d_loss = train_enqueue(ctx, x_f32, tgt, n, lr, ghost_weight, update);
+  double loss = 0.0;
+  OLPT_CUDA(cudaMemcpyAsync(&loss, d_loss, sizeof(double), cudaMemcpyDeviceToHost, ctx->stream));
+  check_err(ctx);
+  return loss;
+}
+
+namespace {
+const double* train_enqueue(olpt_ctx* ctx, const float* x_f32, const float* tgt, int64_t n,
+                            double lr, double ghost_weight, bool update) {
   MlpWork& W = ctx->mlp;
   OLPT_REQUIRE(W.ready, OLPT_ERR_INVALID_ARG, "network not initialised");
   OLPT_REQUIRE(n > 0, OLPT_ERR_INVALID_ARG, "empty batch");
   cudaStream_t s = ctx->stream;
   ensure_batch(ctx, n, true);
   const int64_t lt = round8(n);
-  OLPT_CUDA(cudaMemsetAsync(W.err.p, 0, 16, s));
   input_kernel<<<OLPT_G(nblk(n * kMlpInPad)), 256, 0, s>>>(x_f32, n, W.x.as<__nv_bfloat16>());
   {
     dim3 g((unsigned)((n + 31) / 32), kMlpInPad / 32);
@@ -626,12 +646,9 @@ double mlp_train_device(olpt_ctx* ctx, const float* x_f32, const float* tgt, int
     OLPT_CUDA(cudaGetLastError());
     pack_weights(ctx);
   }
-  double loss = 0.0;
-  OLPT_CUDA(cudaMemcpyAsync(&loss, W.loss.as<double>() + lb, sizeof(double), cudaMemcpyDeviceToHost,
-                            s));
-  check_err(ctx);
-  return loss;
+  return W.loss.as<double>() + lb;
 }
+}  // namespace
 
 void mlp_train_many(olpt_ctx* ctx, const float* x, const float* t, int64_t n, int batch, int steps,
                     double lr, double ghost_weight, uint64_t seed, float* losses) {
@@ -641,15 +658,27 @@ void mlp_train_many(olpt_ctx* ctx, const float* x, const float* t, int64_t n, in
   cudaStream_t s = ctx->stream;
   W.xin.ensure((size_t)batch * kMlpIn * 4, s);
   W.tgt.ensure((size_t)batch * kMlpOut * 4, s);
+  // the steps are enqueued back to back; the losses stay on the device until the end
+  W.loss_hist.ensure((size_t)(steps + 1) * sizeof(double), s);
+  ensure_batch(ctx, batch, true);
+  OLPT_CUDA(cudaMemsetAsync(W.err.p, 0, 16, s));
   for (int it = 0; it < steps; ++it) {
     const double a = lr * (0.05 + 0.95 * 0.5 * (1.0 + std::cos(M_PI * it / (double)steps)));
     sample_kernel<<<OLPT_G(nblk((int64_t)batch * kMlpIn)), 256, 0, s>>>(
         x, t, n, batch, seed, it, W.xin.as<float>(), W.tgt.as<float>());
     OLPT_CUDA(cudaGetLastError());
-    const double l = mlp_train_device(ctx, W.xin.as<float>(), W.tgt.as<float>(), batch, a,
-                                      ghost_weight, true);
-    if (losses) losses[it] = (float)l;
+    const double* d_loss = train_enqueue(ctx, W.xin.as<float>(), W.tgt.as<float>(), batch, a,
+                                         ghost_weight, true);
+    OLPT_CUDA(cudaMemcpyAsync(W.loss_hist.as<double>() + it, d_loss, sizeof(double),
+                              cudaMemcpyDeviceToDevice, s));
   }
+  std::vector<double> h(steps);
+  if (steps > 0)
+    OLPT_CUDA(cudaMemcpyAsync(h.data(), W.loss_hist.p, (size_t)steps * sizeof(double),
+                              cudaMemcpyDeviceToHost, s));
+  check_err(ctx);
+  if (losses)
+    for (int it = 0; it < steps; ++it) losses[it] = (float)h[it];
 }
 
 }  // namespace olpt

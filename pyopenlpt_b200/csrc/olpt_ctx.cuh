@@ -308,12 +308,12 @@ struct MlpWork {
   DevBuf master, grad, am, av, wb1, wb2, wb3, wt2, wt3;
   DevBuf x, xt, xin, tgt, z1, z2, z3, h1, h2, h3, h1t, h2t, o, dout;
   DevBuf dz1f, dz2f, dz3f, dz2b, dz3b, dz1t, dz2t, dz3t, part, hpart, loss, err;
-  DevBuf keep, pos, start_xyz, act, nres, ds_x, ds_t;
+  DevBuf keep, pos, start_xyz, act, nres, ds_x, ds_t, loss_hist;
   void release(cudaStream_t s) {
     for (DevBuf* b : {&master, &grad, &am, &av, &wb1, &wb2, &wb3, &wt2, &wt3, &x, &xt, &xin, &tgt,
                       &z1, &z2, &z3, &h1, &h2, &h3, &h1t, &h2t, &o, &dout, &dz1f, &dz2f, &dz3f,
                       &dz2b, &dz3b, &dz1t, &dz2t, &dz3t, &part, &hpart, &loss, &err, &keep, &pos,
-                      &start_xyz, &act, &nres, &ds_x, &ds_t})
+                      &start_xyz, &act, &nres, &ds_x, &ds_t, &loss_hist})
       b->release(s);
     ready = false;
     cap = 0;
