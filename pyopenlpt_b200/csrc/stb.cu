@@ -232,56 +232,86 @@ __global__ void link_kernel(const double* p_last, const int* len, int n_sa, Hash
   const double* p = p_last + 3 * (int64_t)i;
   int bk[27];
   const int nb = cell_buckets(tg, p, bk);
-  int obj_id = -1;
-  double factor = 1.0;
-  for (int step = 0; step < kLinkIters; ++step) {
-    factor = (step == 0) ? 1.0 : factor * 1.1;
-    const double r_track = (3.0 * base_r) * factor;
-    const double r_track2 = r_track * r_track;
-    int cnt = 0;
-    double mean_d2 = 0.0;
-    for (int e = 0; e < nb; ++e)
-      for (int s = tg.start[bk[e]]; s < tg.start[bk[e] + 1]; ++s) {
-        const double d2 = l2sq(p, tg.pts + 3 * (int64_t)tg.items[s]);
-        if (d2 < r_track2) {
-          ++cnt;
-          mean_d2 += d2;
+  // the radius of every step (factor 1, 1.1, 1.1 * 1.1, ...); the neighbour sums of all
+  // steps are accumulated in one scan each (same neighbour order as one scan per step,
+  // so the same sums)
+  double fac[kLinkIters], r2[kLinkIters];
+#pragma unroll
+  for (int st = 0; st < kLinkIters; ++st) {
+    fac[st] = (st == 0) ? 1.0 : fac[st - 1] * 1.1;
+    const double r_track = (3.0 * base_r) * fac[st];
+    r2[st] = r_track * r_track;
+  }
+  int cnt[kLinkIters];
+  double mean_d2[kLinkIters];
+#pragma unroll
+  for (int st = 0; st < kLinkIters; ++st) {
+    cnt[st] = 0;
+    mean_d2[st] = 0.0;
+  }
+  for (int e = 0; e < nb; ++e)
+    for (int s = tg.start[bk[e]]; s < tg.start[bk[e] + 1]; ++s) {
+      const double d2 = l2sq(p, tg.pts + 3 * (int64_t)tg.items[s]);
+#pragma unroll
+      for (int st = 0; st < kLinkIters; ++st)
+        if (d2 < r2[st]) {
+          ++cnt[st];
+          mean_d2[st] += d2;
         }
-      }
-    double vel[3] = {0.0, 0.0, 0.0};
-    if (cnt > 0) {
-      mean_d2 /= (double)cnt;
+    }
+  double beta2[kLinkIters];
+  bool any = false;
+#pragma unroll
+  for (int st = 0; st < kLinkIters; ++st) {
+    beta2[st] = 0.0;
+    if (cnt[st] > 0) {
+      any = true;
+      const double m = mean_d2[st] / (double)cnt[st];
       const double alpha = 0.8;
-      double L2 = (alpha * alpha) * mean_d2;
-      const double R = base_r * factor;
+      double L2 = (alpha * alpha) * m;
+      const double R = base_r * fac[st];
       const double Lmin2 = (0.1 * R) * (0.1 * R);
       const double Lmax2 = (0.8 * R) * (0.8 * R);
       L2 = (L2 < Lmin2) ? Lmin2 : ((Lmax2 < L2) ? Lmax2 : L2);  // std::clamp
-      const double beta2 = 1.0 / (L2 + 1e-12);
-      double sum_w = 0.0, sx = 0.0, sy = 0.0, sz = 0.0;
-      for (int e = 0; e < nb; ++e)
-        for (int s = tg.start[bk[e]]; s < tg.start[bk[e] + 1]; ++s) {
-          const int j = tg.items[s];
-          const double d2 = l2sq(p, tg.pts + 3 * (int64_t)j);
-          if (!(d2 < r_track2)) continue;
-          const double w = 1.0 / (1.0 + d2 * beta2);
-          sum_w += w;
-          sx += w * disp[3 * (int64_t)j];
-          sy += w * disp[3 * (int64_t)j + 1];
-          sz += w * disp[3 * (int64_t)j + 2];
+      beta2[st] = 1.0 / (L2 + 1e-12);
+    }
+  }
+  double sum_w[kLinkIters], sx[kLinkIters], sy[kLinkIters], sz[kLinkIters];
+#pragma unroll
+  for (int st = 0; st < kLinkIters; ++st) sum_w[st] = sx[st] = sy[st] = sz[st] = 0.0;
+  if (any)
+    for (int e = 0; e < nb; ++e)
+      for (int s = tg.start[bk[e]]; s < tg.start[bk[e] + 1]; ++s) {
+        const int j = tg.items[s];
+        const double d2 = l2sq(p, tg.pts + 3 * (int64_t)j);
+        if (!(d2 < r2[kLinkIters - 1])) continue;
+        const double dx = disp[3 * (int64_t)j], dy = disp[3 * (int64_t)j + 1],
+                     dz = disp[3 * (int64_t)j + 2];
+#pragma unroll
+        for (int st = 0; st < kLinkIters; ++st) {
+          if (cnt[st] == 0 || !(d2 < r2[st])) continue;
+          const double w = 1.0 / (1.0 + d2 * beta2[st]);
+          sum_w[st] += w;
+          sx[st] += w * dx;
+          sy[st] += w * dy;
+          sz[st] += w * dz;
         }
-      if (sum_w > 0.0) {
-        const double inv = 1.0 / sum_w;
-        vel[0] = sx * inv;
-        vel[1] = sy * inv;
-        vel[2] = sz * inv;
       }
+  int obj_id = -1;
+#pragma unroll
+  for (int st = 0; st < kLinkIters; ++st) {
+    double vel[3] = {0.0, 0.0, 0.0};
+    if (cnt[st] > 0 && sum_w[st] > 0.0) {
+      const double inv = 1.0 / sum_w[st];
+      vel[0] = sx[st] * inv;
+      vel[1] = sy[st] * inv;
+      vel[2] = sz[st] * inv;
     }
     const double est[3] = {p[0] + vel[0], p[1] + vel[1], p[2] + vel[2]};
-    const double r_obj = base_r * factor;
+    const double r_obj = base_r * fac[st];
     obj_id = grid_nearest(go, est, r_obj * r_obj);
     if (obj_id >= 0) break;
-    if (cnt == 0) {
+    if (cnt[st] == 0) {
       obj_id = grid_nearest(go, p, r_obj * r_obj);
       if (obj_id >= 0) break;
     }
