@@ -255,6 +255,22 @@ PHASE_NAMES = {5: "detection", 6: "stereo matching (all)", 7: "candidate sort + 
                11: "sequential greedy (replacement fallback)"}
 
 
+# DRAM bytes per shaken object (dram__bytes_read.sum + dram__bytes_write.sum of three
+# shake_kernel launches of the STB convergence frames, 16-19 k objects each, divided by
+# their objects), and the kernel's algorithmic bytes per object for 4 cameras in FP32:
+# 4 x 64 ROI pixels x 4 B + 2 x (24 + 4 x 16 + 8) B of state + 4 x 5 x 4 B of OTF.
+SHAKE_DRAM_BYTES_PER_OBJECT = 22_400.0
+SHAKE_ALGO_BYTES_PER_OBJECT = 1_296.0
+
+
+def shake_traffic(args, prec, dom, bytes_per_launch):
+    """DRAM traffic of an average shake launch of the STB workload, scaled from the
+    per-object figure by the objects the launch processes; None elsewhere."""
+    if dom != 3 or prec != 0 or WORKLOADS[args.workload]["kind"] != "stb":
+        return None
+    return bytes_per_launch / SHAKE_ALGO_BYTES_PER_OBJECT * SHAKE_DRAM_BYTES_PER_OBJECT
+
+
 def reduce_replicas(dist, values, device):
     """Whole-job numbers over the replicas (one per rank): the slowest rank's times
     (values[0] device ms, values[2] end-to-end s) and the sum of the particles
@@ -332,7 +348,8 @@ class Ours:
                          "peak": peak, "unit": "GB/s", "frac": achieved / peak,
                          "peak_source": peak_kind,
                          "bytes_per_launch": by / nl if nl else 0.0,
-                         "launch_ms": ms / nl if nl else 0.0, "traffic": None},
+                         "launch_ms": ms / nl if nl else 0.0,
+                         "traffic": shake_traffic(args, self.prec, dom, by / nl if nl else 0.0)},
             "cpu_baseline": cpu,
             "clocks": clk,
         }
