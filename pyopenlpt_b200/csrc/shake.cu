@@ -428,32 +428,25 @@ __global__ void __launch_bounds__(128, 8) shake_kernel(ShakeView v, int64_t n, d
     const double x0 = P[ax];
     const double rel[3] = {-delta, 0.0, delta};
     double f[3];
-    double su[3][NC], sv[3][NC];
-    bool sok[3][NC];
+    // the projections of the three trial points stay in the warp's shared slots
+    // (slot j = trial j) instead of per-lane copies
     if ((sizeof(Real) == 8 && v.exact_sums)) {
-      for (int j = 0; j < 3; ++j) {
+      for (int j = 2; j >= 0; --j) {  // slot 0 last: single evaluations write slot 0
         tmp[ax] = x0 + rel[j];
         eval_geom<Real, NC>(v, tmp, S);
         f[j] = residue<Real, NC>(v, roi, S);
-        for (int c = 0; c < C; ++c) {
-          su[j][c] = S.uvc[2 * c];
-          sv[j][c] = S.uvc[2 * c + 1];
-          sok[j][c] = in_roi(roi[c], su[j][c], sv[j][c]);
-        }
+        if (j > 0 && lane < 2 * C) S.uvc[2 * j * C + lane] = S.uvc[lane];
         __syncwarp();
       }
     } else {
       eval_geom3<Real, NC>(v, tmp, ax, x0, rel, S);
       residue3<Real, NC>(v, roi, S, f);
-      for (int j = 0; j < 3; ++j)
-        for (int c = 0; c < C; ++c) {
-          su[j][c] = S.uvc[2 * (j * C + c)];
-          sv[j][c] = S.uvc[2 * (j * C + c) + 1];
-          sok[j][c] = in_roi(roi[c], su[j][c], sv[j][c]);
-        }
       __syncwarp();
-      tmp[ax] = x0 + rel[2];  // as left by the last single evaluation
     }
+    tmp[ax] = x0 + rel[2];  // as left by the last single evaluation
+    auto su = [&](int j, int c) { return S.uvc[2 * (j * C + c)]; };
+    auto sv = [&](int j, int c) { return S.uvc[2 * (j * C + c) + 1]; };
+    auto sok = [&](int j, int c) { return in_roi(roi[c], su(j, c), sv(j, c)); };
     const double fL = f[0], f0 = f[1], fR = f[2];
     const double tol = 1e-3 * fmax(1.0, f0);
     const bool mono_dec = (fL > f0 + tol) && (f0 > fR + tol);
@@ -480,14 +473,14 @@ __global__ void __launch_bounds__(128, 8) shake_kernel(ShakeView v, int64_t n, d
       double J[NC], M[NC];
       int nJ = 0, nM = 0;
       for (int c = 0; c < C; ++c) {
-        if (sok[0][c] && sok[2][c]) {
-          const double du = su[2][c] - su[0][c], dv = sv[2][c] - sv[0][c];
+        if (sok(0, c) && sok(2, c)) {
+          const double du = su(2, c) - su(0, c), dv = sv(2, c) - sv(0, c);
           J[nJ++] = hypot(du, dv) / fmax(2.0 * delta, 1e-12);
         }
-        if (sok[1][c]) {
+        if (sok(1, c)) {
           const Rect& R = roi[c];
-          const double mu = fmin(su[1][c] - R.cmin, R.cmax - 1.0 - su[1][c]);
-          const double mv = fmin(sv[1][c] - R.rmin, R.rmax - 1.0 - sv[1][c]);
+          const double mu = fmin(su(1, c) - R.cmin, R.cmax - 1.0 - su(1, c));
+          const double mv = fmin(sv(1, c) - R.rmin, R.rmax - 1.0 - sv(1, c));
           M[nM++] = fmin(mu, mv);
         }
       }
