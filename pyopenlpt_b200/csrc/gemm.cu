@@ -208,19 +208,6 @@ __global__ void __launch_bounds__(256, 1)
   if (warp == 0) tmem_dealloc(tmem, BN);
 }
 
-PFN_cuTensorMapEncodeTiled_v12000 encode_fn() {
-  // thread-safe one-time lookup (contexts may run on several host threads)
-  static const PFN_cuTensorMapEncodeTiled_v12000 fn = [] {
-    void* p = nullptr;
-    cudaDriverEntryPointQueryResult q;
-    OLPT_CUDA(cudaGetDriverEntryPoint("cuTensorMapEncodeTiled", &p, cudaEnableDefault, &q));
-    OLPT_REQUIRE(q == cudaDriverEntryPointSuccess && p, OLPT_ERR_CUDA,
-                 "cuTensorMapEncodeTiled is not available");
-    return reinterpret_cast<PFN_cuTensorMapEncodeTiled_v12000>(p);
-  }();
-  return fn;
-}
-
 // rows x cols bf16 (row stride ld elements), box box_rows x 64, 128-byte swizzle
 CUtensorMap tile_map(const __nv_bfloat16* base, int rows, int cols, int ld, int box_rows) {
   CUtensorMap m;
@@ -228,7 +215,7 @@ CUtensorMap tile_map(const __nv_bfloat16* base, int rows, int cols, int ld, int 
   const cuuint64_t strides[1] = {(cuuint64_t)ld * 2};
   const cuuint32_t box[2] = {(cuuint32_t)kBK, (cuuint32_t)box_rows};
   const cuuint32_t estr[2] = {1, 1};
-  const CUresult r = encode_fn()(&m, CU_TENSOR_MAP_DATA_TYPE_BFLOAT16, 2, (void*)base, dims, strides,
+  const CUresult r = tensor_map_encoder()(&m, CU_TENSOR_MAP_DATA_TYPE_BFLOAT16, 2, (void*)base, dims, strides,
                                  box, estr, CU_TENSOR_MAP_INTERLEAVE_NONE,
                                  CU_TENSOR_MAP_SWIZZLE_128B, CU_TENSOR_MAP_L2_PROMOTION_L2_256B,
                                  CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
@@ -247,6 +234,19 @@ void launch(const CUtensorMap& ta, const CUtensorMap& tb, const EpiArgs& g, dim3
 }
 
 }  // namespace
+
+PFN_cuTensorMapEncodeTiled_v12000 tensor_map_encoder() {
+  // thread-safe one-time lookup (contexts may run on several host threads)
+  static const PFN_cuTensorMapEncodeTiled_v12000 fn = [] {
+    void* p = nullptr;
+    cudaDriverEntryPointQueryResult q;
+    OLPT_CUDA(cudaGetDriverEntryPoint("cuTensorMapEncodeTiled", &p, cudaEnableDefault, &q));
+    OLPT_REQUIRE(q == cudaDriverEntryPointSuccess && p, OLPT_ERR_CUDA,
+                 "cuTensorMapEncodeTiled is not available");
+    return reinterpret_cast<PFN_cuTensorMapEncodeTiled_v12000>(p);
+  }();
+  return fn;
+}
 
 void gemm_bf16(const __nv_bfloat16* A, int lda, const __nv_bfloat16* B, int ldb, int M, int N,
                int K, const GemmEpilogue& ep, int splits, int* err, cudaStream_t s) {

@@ -1,5 +1,6 @@
 // Host-side context shared by all translation units of libolpt_cuda.so.
 #pragma once
+#include <cuda.h>
 #include <cuda_runtime.h>
 
 #include <atomic>
@@ -372,8 +373,16 @@ struct olpt_ctx {
 
   // detections
   olpt::Dets dets[OLPT_MAX_CAM];
-  olpt::DevBuf det_counts;  // int64 per camera (device)
+  // int64 words: [OLPT_MAX_CAM] detection counts, then the staged detector's error
+  // word, band ticket and per-band look-back states
+  olpt::DevBuf det_counts;
   std::vector<int64_t> det_counts_h;
+  struct DetMap {  // TMA descriptor of one camera plane, re-encoded when the plane changes
+    const void* p = nullptr;
+    int dtype = -1, H = 0, W = 0, box_w = 0, box_h = 0;
+    int64_t pitch = 0;
+    CUtensorMap map;
+  } det_map[OLPT_MAX_CAM];
   olpt::DevBuf band_counts, band_offsets;
   olpt::DevBuf lut_u8, lut_u16;  // log(max(v, 1e-4)) of every integer level
 

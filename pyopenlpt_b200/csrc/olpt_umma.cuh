@@ -9,11 +9,16 @@
 // bytes.
 #pragma once
 #include <cuda.h>
+#include <cudaTypedefs.h>
 #include <cuda_runtime.h>
 
 #include <cstdint>
 
 namespace olpt {
+
+// The driver's cuTensorMapEncodeTiled, looked up once through the runtime.
+PFN_cuTensorMapEncodeTiled_v12000 tensor_map_encoder();
+
 namespace umma {
 
 // Waits give up after this long (ns of %globaltimer) and report an error instead.

@@ -4,26 +4,40 @@
 // myMATH::isLocalMax (inc/libMath/myMATH.h:399-435).
 //
 // Layout: each camera image is one HBM plane with a 16-byte aligned row pitch.  A CTA
-// owns a band of whole rows; its threads walk the band in raster order, one 16-byte
-// chunk (16 u8 / 8 u16 / 4 f32 / 2 f64 pixels) per thread per round, with the rows
-// above and below read as 16-byte vectors too.  Detection is two passes over the
-// same bands: COUNT writes one count per band, a per-camera scan turns counts into
-// offsets, EMIT re-evaluates the band and writes each detection at
-// offset + block-scan rank, which reproduces the reference's raster order exactly
-// without atomics.  The second read of a band hits L2 (a 6 x 2048^2 u16 frame is 48 MB).
+// owns a band of whole rows.
+//
+// Staged detector (detect_kernel, the production path): one read of the image.  The
+// CTA takes a band ticket, TMA-loads its band plus one halo row above and below into
+// shared memory (boxes of 256 columns, zero fill outside the image), evaluates every
+// 16-byte chunk (16 u8 / 8 u16 / 4 f32 / 2 f64 pixels) from shared memory, ranks its
+// detections in raster order with a block scan, learns the detections of the bands
+// before it by a decoupled look-back over per-band states (aggregate / inclusive
+// prefix, published with release stores), and writes each detection at prefix +
+// rank: the reference's raster order without a second pass over the image.  Tickets
+// are handed out in band order, so a band only waits on bands whose CTAs are already
+// running; every wait is bounded and a timeout is reported through an error word.
+//
+// Two-pass detector (peaks_kernel; allocation-free entry point and images too wide to
+// stage three rows of in shared memory): COUNT writes one count per band, a
+// per-camera scan turns counts into offsets, EMIT re-evaluates the band from global
+// memory and writes each detection at offset + block-scan rank.
 //
 // Exactness: integer-level images use a host-built table of ln(max(v, 1e-4)) (the
 // same libm log the reference calls); the fit then evaluates the reference's
 // expressions in the same order with no FMA contraction, so sub-pixel centres are
 // bit-identical.  Floating-point images (residuals) call CUDA's log.
+#include <cuda.h>
 #include <cuda_runtime.h>
 
+#include <algorithm>
 #include <cmath>
 #include <mutex>
 #include <string>
+#include <type_traits>
 #include <vector>
 
 #include "olpt_ctx.cuh"
+#include "olpt_umma.cuh"
 
 namespace olpt {
 namespace {
@@ -288,6 +302,453 @@ void launch_peaks(const PeakArgs& a, int n_blocks, int64_t* band_offsets, int64_
   OLPT_CUDA(cudaGetLastError());
 }
 
+
+// ---------------------------------------------------------------------------
+// Staged single-read detector.
+
+constexpr int kDetThreads = 256;
+constexpr int kBoxW = 256;  // TMA box width in elements (the hardware maximum)
+constexpr int kDetList = 2048;  // detections listed per emission round
+// det_counts words after the per-camera totals
+constexpr int kDcErr = OLPT_MAX_CAM, kDcTicket = OLPT_MAX_CAM + 1, kDcState = OLPT_MAX_CAM + 2;
+// look-back state of a band: flag in the top two bits, detection count below
+constexpr unsigned long long kStAggregate = 1ull << 62, kStPrefix = 2ull << 62;
+constexpr unsigned long long kStValue = (1ull << 62) - 1;
+
+struct DetCam {
+  int H, W;
+  int band_rows;  // R: rows per band; the staged tile holds R + 2 rows
+  int box_w;      // columns per box: 256, or the row's chunk-padded width if one box covers it
+  int n_box;      // boxes per row
+  int cpr;        // 16-byte chunks per row
+  int n_bands, band_base;
+  double* x;
+  double* y;
+  int2* rc;
+};
+
+struct DetArgs {
+  CUtensorMap map[OLPT_MAX_CAM];
+  DetCam cam[OLPT_MAX_CAM];
+  int n_cam;
+  double min_int;
+  int min_level;            // integer images: v < min_level  <=>  (double)v < min_int
+  const double* lut;        // integer images only
+  unsigned long long* dc;   // det_counts words
+};
+
+__device__ __forceinline__ unsigned long long ld_acquire_u64(const unsigned long long* p) {
+  unsigned long long v;
+  asm volatile("ld.acquire.gpu.global.u64 %0, [%1];" : "=l"(v) : "l"(p) : "memory");
+  return v;
+}
+__device__ __forceinline__ void st_release_u64(unsigned long long* p, unsigned long long v) {
+  asm volatile("st.release.gpu.global.u64 [%0], %1;" ::"l"(p), "l"(v) : "memory");
+}
+
+// Element (tile row lr, image column col) of a staged band: boxes of box_w columns,
+// each box_h rows of box_w elements, box after box.
+template <typename T>
+__device__ __forceinline__ int tile_index(const DetCam& c, int box_h, int lr, int col) {
+  return ((col >> 8) * box_h + lr) * c.box_w + (col & (kBoxW - 1));
+}
+
+// One chunk of image row r (tile row lr) from shared memory: bit j set if pixel c0 + j
+// passes eval_chunk's tests and fit.  Pixels at or past W are the TMA's zero fill, as
+// eval_chunk's loads.
+// Threshold test of one pixel: (double)v < min_int, for integer levels as the integer
+// compare v < min_level (the same outcome for every level and every min_int).
+template <typename T>
+__device__ __forceinline__ bool below(T v, double min_int, int min_level) {
+  if constexpr (std::is_integral<T>::value) {
+    return (int)v < min_level;
+  } else {
+    return (double)v < min_int;
+  }
+}
+
+template <typename T, int N>
+__device__ __forceinline__ unsigned mask_staged(const T* tile, const DetCam& c, int box_h,
+                                                double min_int, int min_level, const double* lut,
+                                                int r, int lr, int c0) {
+  if (r < 1 || r > c.H - 2) return 0u;
+  T cen[N], up[N], dn[N];
+  const int ic = tile_index<T>(c, box_h, lr, c0);
+  {
+    const uint4 q = *reinterpret_cast<const uint4*>(tile + ic);
+    const T* qt = reinterpret_cast<const T*>(&q);
+#pragma unroll
+    for (int j = 0; j < N; ++j) cen[j] = qt[j];
+  }
+  bool any = false;
+#pragma unroll
+  for (int j = 0; j < N; ++j) any |= !below<T>(cen[j], min_int, min_level);
+  if (!any) return 0u;
+  {
+    const uint4 qu = *reinterpret_cast<const uint4*>(tile + ic - c.box_w);
+    const uint4 qd = *reinterpret_cast<const uint4*>(tile + ic + c.box_w);
+    const T* tu = reinterpret_cast<const T*>(&qu);
+    const T* td = reinterpret_cast<const T*>(&qd);
+#pragma unroll
+    for (int j = 0; j < N; ++j) {
+      up[j] = tu[j];
+      dn[j] = td[j];
+    }
+  }
+  const int wpad = c.n_box * c.box_w;
+  const T left = (c0 > 0) ? tile[tile_index<T>(c, box_h, lr, c0 - 1)] : T(0);
+  const T right = (c0 + N < wpad) ? tile[tile_index<T>(c, box_h, lr, c0 + N)] : T(0);
+  unsigned cand = 0u;  // threshold and local-maximum tests
+#pragma unroll
+  for (int j = 0; j < N; ++j) {
+    const int col = c0 + j;
+    if (col < 1 || col > c.W - 2) continue;
+    const T v = cen[j];
+    if (below<T>(v, min_int, min_level)) continue;
+    const T l = (j > 0) ? cen[j - 1] : left;
+    const T rr = (j < N - 1) ? cen[j + 1] : right;
+    if (up[j] > v || l > v || dn[j] >= v || rr >= v) continue;
+    cand |= 1u << j;
+  }
+  // Integer levels: a local maximum has v >= 1 and ln(left), ln(up) <= ln(v) >
+  // ln(right), ln(down) (ln(max(x, 1e-4)) increases strictly over the integers), so
+  // both fits have a negative denominator and a finite centre: every candidate is a
+  // detection.  Floating-point levels can tie in the clamped log or be non-finite.
+  if constexpr (std::is_integral<T>::value) return cand;
+  unsigned mask = 0u;  // the fit of each candidate (one loop iteration per candidate)
+  while (cand) {
+    const int j = __ffs(cand) - 1;
+    cand &= cand - 1;
+    const int col = c0 + j;
+    const T v = tile[ic + j];
+    const T l = tile[tile_index<T>(c, box_h, lr, col - 1)];
+    const T rr = tile[tile_index<T>(c, box_h, lr, col + 1)];
+    const double lc = Ln<T>::f(v, lut);
+    double xc, yc;
+    if (!fit3(Ln<T>::f(l, lut), lc, Ln<T>::f(rr, lut), col, xc)) continue;
+    if (!fit3(Ln<T>::f(tile[ic + j - c.box_w], lut), lc, Ln<T>::f(tile[ic + j + c.box_w], lut), r,
+              yc))
+      continue;
+    mask |= 1u << j;
+  }
+  return mask;
+}
+
+
+// Integer levels, four u8 or two u16 pixels per 32-bit word: the same tests as
+// mask_staged's pixel loop with SIMD compares (0xff / 0xffff per lane that holds).
+__device__ __forceinline__ uint32_t lane_bits(uint32_t m, uint8_t) {
+  return (((m & 0x01010101u) * 0x01020408u) >> 24) & 0xfu;  // byte k -> bit k
+}
+__device__ __forceinline__ uint32_t lane_bits(uint32_t m, uint16_t) {
+  return (m & 1u) | ((m >> 15) & 2u);  // half k -> bit k
+}
+__device__ __forceinline__ uint32_t vge(uint32_t a, uint32_t b, uint8_t) { return __vcmpgeu4(a, b); }
+__device__ __forceinline__ uint32_t vgt(uint32_t a, uint32_t b, uint8_t) { return __vcmpgtu4(a, b); }
+__device__ __forceinline__ uint32_t vge(uint32_t a, uint32_t b, uint16_t) { return __vcmpgeu2(a, b); }
+__device__ __forceinline__ uint32_t vgt(uint32_t a, uint32_t b, uint16_t) { return __vcmpgtu2(a, b); }
+
+template <typename T>
+__device__ __forceinline__ unsigned mask_staged_int(const T* tile, const DetCam& c, int box_h,
+                                                    int min_level, int r, int lr, int c0) {
+  constexpr int N = 16 / sizeof(T), PW = 4 / sizeof(T);  // pixels per chunk, per word
+  constexpr int kMaxLevel = sizeof(T) == 1 ? 255 : 65535;
+  if (r < 1 || r > c.H - 2 || min_level > kMaxLevel) return 0u;
+  const uint32_t thr = sizeof(T) == 1 ? (uint32_t)min_level * 0x01010101u
+                                      : (uint32_t)min_level * 0x00010001u;
+  const int ic = tile_index<T>(c, box_h, lr, c0);
+  const uint4 qc = *reinterpret_cast<const uint4*>(tile + ic);
+  const uint32_t C[4] = {qc.x, qc.y, qc.z, qc.w};
+  uint32_t keep[4];
+  uint32_t any = 0u;
+#pragma unroll
+  for (int k = 0; k < 4; ++k) {
+    keep[k] = vge(C[k], thr, T());
+    any |= keep[k];
+  }
+  if (!any) return 0u;
+  const uint4 qu = *reinterpret_cast<const uint4*>(tile + ic - c.box_w);
+  const uint4 qd = *reinterpret_cast<const uint4*>(tile + ic + c.box_w);
+  const uint32_t U[4] = {qu.x, qu.y, qu.z, qu.w};
+  const uint32_t D[4] = {qd.x, qd.y, qd.z, qd.w};
+  const int wpad = c.n_box * c.box_w;
+  const uint32_t left = (c0 > 0) ? (uint32_t)tile[tile_index<T>(c, box_h, lr, c0 - 1)] : 0u;
+  const uint32_t right = (c0 + N < wpad) ? (uint32_t)tile[tile_index<T>(c, box_h, lr, c0 + N)] : 0u;
+  // the word of left / right neighbours of word k's pixels
+  const uint32_t lw0 = left << (32 - 8 * sizeof(T));
+  unsigned mask = 0u;
+#pragma unroll
+  for (int k = 0; k < 4; ++k) {
+    const uint32_t prev = k > 0 ? C[k - 1] : lw0;
+    const uint32_t next = k < 3 ? C[k + 1] : right;
+    const uint32_t L = sizeof(T) == 1 ? __byte_perm(prev, C[k], 0x6543) : __byte_perm(prev, C[k], 0x5432);
+    const uint32_t R = sizeof(T) == 1 ? __byte_perm(C[k], next, 0x4321) : __byte_perm(C[k], next, 0x5432);
+    // isLocalMax: up / left reject if strictly greater, down / right if >=
+    const uint32_t m = keep[k] & vge(C[k], U[k], T()) & vge(C[k], L, T()) & vgt(C[k], D[k], T()) &
+                       vgt(C[k], R, T());
+    mask |= lane_bits(m, T()) << (PW * k);
+  }
+  // border columns are never peaks
+  const int lo = max(0, 1 - c0), hi = min(N - 1, c.W - 2 - c0);
+  if (hi < lo) return 0u;
+  const unsigned cols = ((hi >= 31 ? 0xffffffffu : ((1u << (hi + 1)) - 1u))) & ~((1u << lo) - 1u);
+  return mask & cols;
+}
+
+// The sub-pixel centre of a pixel that mask_staged accepted (same operations, same
+// operands, so the same values).
+template <typename T>
+__device__ __forceinline__ void fit_staged(const T* tile, const DetCam& c, int box_h,
+                                           const double* lut, int r, int lr, int col, double& xc,
+                                           double& yc) {
+  const int ic = tile_index<T>(c, box_h, lr, col);
+  const double lc = Ln<T>::f(tile[ic], lut);
+  fit3(Ln<T>::f(tile[tile_index<T>(c, box_h, lr, col - 1)], lut), lc,
+       Ln<T>::f(tile[tile_index<T>(c, box_h, lr, col + 1)], lut), col, xc);
+  fit3(Ln<T>::f(tile[ic - c.box_w], lut), lc, Ln<T>::f(tile[ic + c.box_w], lut), r, yc);
+}
+
+template <typename T>
+__global__ void __launch_bounds__(kDetThreads, 3) detect_kernel(const __grid_constant__ DetArgs a) {
+  constexpr int N = 16 / sizeof(T);
+  // declared with the alignment the runtime guarantees (dynamic shared memory follows
+  // the static variables), so the rounding below is computed, not assumed away
+  extern __shared__ __align__(16) unsigned char det_smem[];
+  __shared__ uint64_t bar;
+  __shared__ int s_ticket, s_ok;
+  __shared__ int s_warp[kDetThreads / 32];
+  __shared__ long long s_prefix;
+  __shared__ int s_total;
+  const int tid = threadIdx.x, lane = tid & 31, wid = tid >> 5;
+  unsigned long long* dc = a.dc;
+
+  if (tid == 0) {
+    umma::mbar_init(&bar, 1);
+    umma::fence_barrier_init();
+    s_ticket = (int)atomicAdd(dc + kDcTicket, 1ull);
+  }
+  __syncthreads();
+  const int tk = s_ticket;
+  int cam = 0;
+  for (int i = 0; i < a.n_cam; ++i)
+    if (tk >= a.cam[i].band_base && tk < a.cam[i].band_base + a.cam[i].n_bands) cam = i;
+  const DetCam& c = a.cam[cam];
+  const int band = tk - c.band_base;
+  const int box_h = c.band_rows + 2;
+  const int r0 = band * c.band_rows;
+  const int rows = min(c.band_rows, c.H - r0);
+  // TMA destinations are 128-byte aligned (every box is a multiple of 128 bytes)
+  unsigned char* base = det_smem + ((128u - (umma::smem_u32(det_smem) & 127u)) & 127u);
+  T* tile = reinterpret_cast<T*>(base);
+  const int tile_elems = c.n_box * box_h * c.box_w;
+  uint16_t* masks = reinterpret_cast<uint16_t*>(base + (size_t)tile_elems * sizeof(T));
+
+  // stage the band with its halo rows (row r0 - 1 may be -1: zero fill)
+  if (tid == 0) {
+    const uint32_t box_bytes = (uint32_t)(box_h * c.box_w * (int)sizeof(T));
+    umma::mbar_arrive_expect_tx(&bar, box_bytes * (uint32_t)c.n_box);
+    for (int b = 0; b < c.n_box; ++b)
+      umma::tma_load_2d(tile + (size_t)b * box_h * c.box_w, &a.map[cam], &bar, b * kBoxW, r0 - 1);
+  }
+  const bool staged = __syncthreads_and(umma::mbar_wait(&bar, 0)) != 0;
+  unsigned long long* state = dc + kDcState + tk;
+  if (!staged) {
+    if (tid == 0) {
+      atomicOr(dc + kDcErr, 1ull);
+      umma::mbar_wait(&bar, 0);              // the copies must land before the CTA exits
+      st_release_u64(state, kStPrefix);      // successors go on (results are void)
+    }
+    return;
+  }
+
+  // 1. evaluate every chunk of the band (coalesced over threads), keep the masks
+  const int cpr = c.cpr;
+  const int n_chunks = rows * cpr;
+  for (int i = tid; i < n_chunks; i += kDetThreads) {
+    const int lr = 1 + i / cpr;
+    if constexpr (std::is_integral<T>::value)
+      masks[i] = (uint16_t)mask_staged_int<T>(tile, c, box_h, a.min_level, r0 + lr - 1, lr,
+                                              (i % cpr) * N);
+    else
+      masks[i] = (uint16_t)mask_staged<T, N>(tile, c, box_h, a.min_int, a.min_level, a.lut,
+                                             r0 + lr - 1, lr, (i % cpr) * N);
+  }
+  __syncthreads();
+
+  // 2. raster-order ranks: thread t owns chunks [t K, t K + K)
+  const int K = (n_chunks + kDetThreads - 1) / kDetThreads;
+  const int i0 = min(tid * K, n_chunks), i1 = min(i0 + K, n_chunks);
+  int n = 0;
+  for (int i = i0; i < i1; ++i) n += __popc((unsigned)masks[i]);
+  int incl = n;
+#pragma unroll
+  for (int o = 1; o < 32; o <<= 1) {
+    const int t = __shfl_up_sync(0xffffffffu, incl, o);
+    if (lane >= o) incl += t;
+  }
+  if (lane == 31) s_warp[wid] = incl;
+  __syncthreads();
+  if (wid == 0) {
+    int acc = 0;
+    if (lane == 0) {
+      for (int w = 0; w < kDetThreads / 32; ++w) {
+        const int t = s_warp[w];
+        s_warp[w] = acc;
+        acc += t;
+      }
+    }
+    const unsigned long long total = (unsigned long long)__shfl_sync(0xffffffffu, acc, 0);
+    if (lane == 0) s_total = acc;
+    if (lane == 0) st_release_u64(state, (band == 0 ? kStPrefix : kStAggregate) | total);
+    // 3. look-back over windows of 32 earlier bands: sum the aggregates down to the
+    //    nearest published prefix (bands before the camera's first count as an empty
+    //    prefix); wait while a band of the window has published nothing yet
+    unsigned long long prefix = 0;
+    int ok = 1;
+    if (band > 0) {
+      int top = tk - 1;
+      uint64_t t0 = 0;
+      while (true) {
+        const int idx = top - 31 + lane;
+        const unsigned long long w =
+            idx >= c.band_base ? ld_acquire_u64(dc + kDcState + idx) : kStPrefix;
+        const unsigned long long flag = w & ~kStValue;
+        if (__any_sync(0xffffffffu, flag == 0)) {
+          int expired = 0;
+          if (lane == 0) {
+            const uint64_t now = umma::global_timer();
+            if (t0 == 0) t0 = now;
+            else if (now - t0 > umma::kWaitLimitNs) expired = 1;
+          }
+          if (__shfl_sync(0xffffffffu, expired, 0)) {
+            if (lane == 0) atomicOr(dc + kDcErr, 2ull);
+            ok = 0;
+            break;
+          }
+          __nanosleep(64);
+          continue;
+        }
+        const unsigned pmask = __ballot_sync(0xffffffffu, flag == kStPrefix);
+        const int nearest = pmask ? 31 - __clz(pmask) : 0;  // highest lane with a prefix
+        unsigned long long v = lane >= nearest ? (w & kStValue) : 0ull;
+#pragma unroll
+        for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
+        prefix += v;
+        if (pmask) break;
+        top -= 32;
+      }
+      if (lane == 0) st_release_u64(state, kStPrefix | (prefix + total));
+    }
+    if (lane == 0) {
+      if (band == c.n_bands - 1) dc[cam] = prefix + total;
+      s_prefix = (long long)prefix;
+      s_ok = ok;
+    }
+  }
+  __syncthreads();
+  if (!s_ok) return;
+
+  // 4. write the detections at prefix + rank, kDetList at a time: the block's
+  //    detections are listed in rank order in shared memory, then fitted and written
+  //    one per thread (coalesced stores, the fits spread over all threads)
+  uint32_t* dlist = reinterpret_cast<uint32_t*>(
+      base + (((size_t)tile_elems * sizeof(T) + (size_t)c.band_rows * cpr * sizeof(uint16_t) + 3) &
+              ~(size_t)3));
+  const int my0 = s_warp[wid] + incl - n;  // this thread's first rank in the block
+  const int block_total = s_total;
+  for (int lo = 0; lo < block_total; lo += kDetList) {
+    if (my0 < lo + kDetList && my0 + n > lo) {
+      int rank = my0;
+      for (int i = i0; i < i1 && rank < lo + kDetList; ++i) {
+        unsigned m = masks[i];
+        while (m) {
+          const int j = __ffs(m) - 1;
+          m &= m - 1;
+          if (rank >= lo && rank < lo + kDetList) dlist[rank - lo] = (uint32_t)i * 16u + (uint32_t)j;
+          ++rank;
+        }
+      }
+    }
+    __syncthreads();
+    const int cnt = min(kDetList, block_total - lo);
+    const int64_t base = s_prefix + lo;
+    for (int k = tid; k < cnt; k += kDetThreads) {
+      const uint32_t code = dlist[k];
+      const int i = (int)(code >> 4);
+      const int lr = 1 + i / cpr;
+      const int r = r0 + lr - 1;
+      const int col = (i % cpr) * N + (int)(code & 15u);
+      double xc, yc;
+      fit_staged<T>(tile, c, box_h, a.lut, r, lr, col, xc, yc);
+      c.x[base + k] = xc;
+      c.y[base + k] = yc;
+      c.rc[base + k] = make_int2(r, col);
+    }
+    __syncthreads();
+  }
+}
+
+// Dynamic shared memory of detect_kernel<T> raised to at least `bytes` (once per size).
+template <typename T>
+void detect_smem_attr(size_t bytes) {
+  static std::mutex mu;
+  static size_t set = 48 * 1024;
+  std::lock_guard<std::mutex> lk(mu);
+  if (bytes <= set) return;
+  OLPT_CUDA(cudaFuncSetAttribute(detect_kernel<T>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                 (int)bytes));
+  set = bytes;
+}
+
+template <typename T>
+void launch_detect(const DetArgs& a, int n_blocks, size_t smem, cudaStream_t s) {
+  detect_smem_attr<T>(smem);
+  detect_kernel<T><<<OLPT_G(n_blocks), kDetThreads, smem, s>>>(a);
+  OLPT_CUDA(cudaGetLastError());
+}
+
+CUtensorMapDataType tma_dtype(int dtype) {
+  switch (dtype) {
+    case OLPT_U8: return CU_TENSOR_MAP_DATA_TYPE_UINT8;
+    case OLPT_U16: return CU_TENSOR_MAP_DATA_TYPE_UINT16;
+    case OLPT_F32: return CU_TENSOR_MAP_DATA_TYPE_FLOAT32;
+    default: return CU_TENSOR_MAP_DATA_TYPE_FLOAT64;
+  }
+}
+
+// Shared memory of one staged band: 64 KB (three CTAs per SM), up to 200 KB when a
+// row is so wide that fewer than four rows would fit.
+constexpr size_t kDetTileBudget = 64 * 1024, kDetTileBudgetMax = 200 * 1024;
+
+struct DetGeom {
+  int cpr, n_box, box_w;
+  size_t row_img, row_mask;
+};
+
+DetGeom det_geom(int W, int esz) {
+  DetGeom g;
+  const int N = 16 / esz;
+  g.cpr = (W + N - 1) / N;
+  g.n_box = (W + kBoxW - 1) / kBoxW;
+  g.box_w = g.n_box > 1 ? kBoxW : g.cpr * N;  // a multiple of N, at most 256
+  g.row_img = (size_t)g.n_box * g.box_w * esz;
+  g.row_mask = (size_t)g.cpr * sizeof(uint16_t);
+  return g;
+}
+
+// Rows per band that fit `budget` bytes: (R + 2) image rows, R mask rows, the
+// detection list, alignment.
+int det_rows_fitting(const DetGeom& g, size_t budget) {
+  const size_t fixed = 128 + 2 * g.row_img + 8 + kDetList * sizeof(uint32_t);
+  if (budget <= fixed) return 0;
+  return (int)std::min<size_t>((budget - fixed) / (g.row_img + g.row_mask), 254);
+}
+
+size_t det_smem_bytes(const DetGeom& g, int R) {
+  return 128 + (size_t)(R + 2) * g.row_img + (size_t)R * g.row_mask + 8 +
+         kDetList * sizeof(uint32_t);
+}
+
 }  // namespace
 
 void ensure_log_luts(olpt_ctx* ctx) {
@@ -315,75 +776,159 @@ void ensure_det_capacity(olpt_ctx* ctx, int cam, int64_t cap) {
   d.cap = cap;
 }
 
+// The two-pass detector on the context's images (images too wide to stage).
+template <typename T>
+void two_pass(olpt_ctx* ctx, PeakArgs& a, int blocks, int64_t* tot) {
+  ctx->band_counts.ensure(blocks * sizeof(int), ctx->stream);
+  ctx->band_offsets.ensure(blocks * sizeof(int64_t), ctx->stream);
+  a.band_counts = ctx->band_counts.as<int>();
+  launch_peaks<T>(a, blocks, ctx->band_offsets.as<int64_t>(), tot, ctx->stream);
+}
+
 // Detect on the current images; counts stay on the device in ctx->det_counts and are
 // mirrored to det_counts_h when `sync_counts`.
 void find_peaks_device(olpt_ctx* ctx, double min_int, bool sync_counts) {
   OLPT_REQUIRE(ctx->n_cam > 0, OLPT_ERR_INVALID_ARG, "no cameras uploaded");
   ensure_log_luts(ctx);
-  PeakArgs a{};
-  a.n_cam = ctx->n_cam;
-  a.min_int = min_int;
   int dtype = -1;
-  int blocks = 0;
+  int64_t active_rows = 0;
   for (int c = 0; c < ctx->n_cam; ++c) {
     ImagePlane& im = ctx->img[c];
     OLPT_REQUIRE(im.buf.p != nullptr, OLPT_ERR_INVALID_ARG, "no image uploaded for camera");
     if (dtype < 0) dtype = im.dtype;
     OLPT_REQUIRE(im.dtype == dtype, OLPT_ERR_INVALID_ARG, "all cameras must share one dtype");
-    const int esz = dtype == OLPT_U8 ? 1 : dtype == OLPT_U16 ? 2 : dtype == OLPT_F32 ? 4 : 8;
-    const int N = 16 / esz;
-    const int cpr = (im.W + N - 1) / N;
-    int band_rows = (2048 + cpr - 1) / cpr;
-    if (band_rows < 1) band_rows = 1;
-    PeakCam& pc = a.cam[c];
-    pc.img = im.buf.as<unsigned char>();
-    pc.pitch = im.pitch;
-    pc.H = im.H;
-    pc.W = im.W;
-    pc.band_rows = band_rows;
-    pc.n_bands = (im.H + band_rows - 1) / band_rows;
-    pc.band_base = blocks;
-    pc.active = ctx->cams_h[c].is_active;
-    blocks += pc.n_bands;
+    if (ctx->cams_h[c].is_active) active_rows += im.H;
     ensure_det_capacity(ctx, c, ((int64_t)im.H * im.W + 1) / 2 + 1);
-    pc.x = ctx->dets[c].x.as<double>();
-    pc.y = ctx->dets[c].y.as<double>();
-    pc.rc = ctx->dets[c].rc.as<int2>();
   }
-  ctx->band_counts.ensure(blocks * sizeof(int), ctx->stream);
-  ctx->band_offsets.ensure(blocks * sizeof(int64_t), ctx->stream);
-  ctx->det_counts.ensure(OLPT_MAX_CAM * sizeof(int64_t), ctx->stream);
-  a.band_counts = ctx->band_counts.as<int>();
-  int64_t* offs = ctx->band_offsets.as<int64_t>();
-  int64_t* tot = ctx->det_counts.as<int64_t>();
+  const int esz = dtype == OLPT_U8 ? 1 : dtype == OLPT_U16 ? 2 : dtype == OLPT_F32 ? 4 : 8;
+  const double* lut = dtype == OLPT_U8    ? ctx->lut_u8.as<double>()
+                      : dtype == OLPT_U16 ? ctx->lut_u16.as<double>()
+                                          : nullptr;
   double img_bytes = 0;
   for (int c = 0; c < ctx->n_cam; ++c)
-    if (a.cam[c].active)
-      img_bytes += (double)a.cam[c].H * a.cam[c].W *
-                   (dtype == OLPT_U8 ? 1 : dtype == OLPT_U16 ? 2 : dtype == OLPT_F32 ? 4 : 8);
+    if (ctx->cams_h[c].is_active) img_bytes += (double)ctx->img[c].H * ctx->img[c].W * esz;
+
+  // staged geometry: bands of R rows, R small enough for about three CTAs per SM over
+  // all cameras' rows and for the shared-memory budget
+  const int rows_fill = (int)std::max<int64_t>(4, active_rows / (3 * 148));
+  bool staged = true;
+  DetGeom geo[OLPT_MAX_CAM];
+  int band_rows[OLPT_MAX_CAM];
+  size_t smem = 0;
+  for (int c = 0; c < ctx->n_cam; ++c) {
+    geo[c] = det_geom(ctx->img[c].W, esz);
+    int R = det_rows_fitting(geo[c], kDetTileBudget);
+    if (R < 4) R = det_rows_fitting(geo[c], kDetTileBudgetMax);
+    if (R < 1) staged = false;
+    band_rows[c] = std::max(1, std::min(R, rows_fill));
+    if (ctx->cams_h[c].is_active) smem = std::max(smem, det_smem_bytes(geo[c], band_rows[c]));
+  }
+
   const int pid = ctx->prof.begin(PROF_PEAKS, ctx->stream);
-  switch (dtype) {
-    case OLPT_U8:
-      a.lut = ctx->lut_u8.as<double>();
-      launch_peaks<uint8_t>(a, blocks, offs, tot, ctx->stream);
-      break;
-    case OLPT_U16:
-      a.lut = ctx->lut_u16.as<double>();
-      launch_peaks<uint16_t>(a, blocks, offs, tot, ctx->stream);
-      break;
-    case OLPT_F32:
-      launch_peaks<float>(a, blocks, offs, tot, ctx->stream);
-      break;
-    default:
-      launch_peaks<double>(a, blocks, offs, tot, ctx->stream);
-      break;
+  if (staged) {
+    DetArgs a{};
+    a.n_cam = ctx->n_cam;
+    a.min_int = min_int;
+    // levels are 0 .. 65535: NaN or <= 0 rejects none, above 65535 rejects all
+    a.min_level = !(min_int > 0.0) ? 0 : min_int > 65535.0 ? 65536 : (int)std::ceil(min_int);
+    a.lut = lut;
+    int blocks = 0;
+    for (int c = 0; c < ctx->n_cam; ++c) {
+      ImagePlane& im = ctx->img[c];
+      DetCam& dc = a.cam[c];
+      dc.H = im.H;
+      dc.W = im.W;
+      dc.band_rows = band_rows[c];
+      dc.box_w = geo[c].box_w;
+      dc.n_box = geo[c].n_box;
+      dc.cpr = geo[c].cpr;
+      dc.n_bands = ctx->cams_h[c].is_active ? (im.H + dc.band_rows - 1) / dc.band_rows : 0;
+      dc.band_base = blocks;
+      dc.x = ctx->dets[c].x.as<double>();
+      dc.y = ctx->dets[c].y.as<double>();
+      dc.rc = ctx->dets[c].rc.as<int2>();
+      blocks += dc.n_bands;
+      olpt_ctx::DetMap& m = ctx->det_map[c];
+      if (m.p != im.buf.p || m.dtype != dtype || m.H != im.H || m.W != im.W ||
+          m.pitch != im.pitch || m.box_w != dc.box_w || m.box_h != dc.band_rows + 2) {
+        const cuuint64_t dims[2] = {(cuuint64_t)im.W, (cuuint64_t)im.H};
+        const cuuint64_t strides[1] = {(cuuint64_t)im.pitch};
+        const cuuint32_t box[2] = {(cuuint32_t)dc.box_w, (cuuint32_t)(dc.band_rows + 2)};
+        const cuuint32_t estr[2] = {1, 1};
+        const CUresult r = tensor_map_encoder()(
+            &m.map, tma_dtype(dtype), 2, im.buf.p, dims, strides, box, estr,
+            CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_NONE,
+            CU_TENSOR_MAP_L2_PROMOTION_L2_256B, CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
+        OLPT_REQUIRE(r == CUDA_SUCCESS, OLPT_ERR_CUDA,
+                     "cuTensorMapEncodeTiled failed for a camera image (" +
+                         std::to_string((int)r) + ")");
+        m.p = im.buf.p;
+        m.dtype = dtype;
+        m.H = im.H;
+        m.W = im.W;
+        m.pitch = im.pitch;
+        m.box_w = dc.box_w;
+        m.box_h = dc.band_rows + 2;
+      }
+      a.map[c] = m.map;
+    }
+    const size_t words = (size_t)kDcState + blocks;
+    ctx->det_counts.ensure(words * sizeof(int64_t), ctx->stream);
+    a.dc = ctx->det_counts.as<unsigned long long>();
+    // totals, error word, ticket and band states start at zero
+    OLPT_CUDA(cudaMemsetAsync(ctx->det_counts.p, 0, words * sizeof(int64_t), ctx->stream));
+    if (blocks > 0) {
+      switch (dtype) {
+        case OLPT_U8: launch_detect<uint8_t>(a, blocks, smem, ctx->stream); break;
+        case OLPT_U16: launch_detect<uint16_t>(a, blocks, smem, ctx->stream); break;
+        case OLPT_F32: launch_detect<float>(a, blocks, smem, ctx->stream); break;
+        default: launch_detect<double>(a, blocks, smem, ctx->stream); break;
+      }
+    }
+  } else {
+    PeakArgs a{};
+    a.n_cam = ctx->n_cam;
+    a.min_int = min_int;
+    a.lut = lut;
+    int blocks = 0;
+    for (int c = 0; c < ctx->n_cam; ++c) {
+      ImagePlane& im = ctx->img[c];
+      const int N = 16 / esz;
+      const int cpr = (im.W + N - 1) / N;
+      PeakCam& pc = a.cam[c];
+      pc.img = im.buf.as<unsigned char>();
+      pc.pitch = im.pitch;
+      pc.H = im.H;
+      pc.W = im.W;
+      pc.band_rows = std::max(1, (2048 + cpr - 1) / cpr);
+      pc.n_bands = (im.H + pc.band_rows - 1) / pc.band_rows;
+      pc.band_base = blocks;
+      pc.active = ctx->cams_h[c].is_active;
+      blocks += pc.n_bands;
+      pc.x = ctx->dets[c].x.as<double>();
+      pc.y = ctx->dets[c].y.as<double>();
+      pc.rc = ctx->dets[c].rc.as<int2>();
+    }
+    ctx->det_counts.ensure((size_t)(kDcErr + 1) * sizeof(int64_t), ctx->stream);
+    int64_t* tot = ctx->det_counts.as<int64_t>();
+    OLPT_CUDA(cudaMemsetAsync(tot, 0, (size_t)(kDcErr + 1) * sizeof(int64_t), ctx->stream));
+    switch (dtype) {
+      case OLPT_U8: two_pass<uint8_t>(ctx, a, blocks, tot); break;
+      case OLPT_U16: two_pass<uint16_t>(ctx, a, blocks, tot); break;
+      case OLPT_F32: two_pass<float>(ctx, a, blocks, tot); break;
+      default: two_pass<double>(ctx, a, blocks, tot); break;
+    }
   }
   ctx->prof.end(PROF_PEAKS, pid, ctx->stream, img_bytes);
   ctx->det_counts_h.assign(ctx->n_cam, 0);
   if (sync_counts) {
-    OLPT_CUDA(cudaMemcpyAsync(ctx->det_counts_h.data(), tot, ctx->n_cam * sizeof(int64_t),
-                              cudaMemcpyDeviceToHost, ctx->stream));
+    int64_t h[kDcErr + 1];
+    OLPT_CUDA(cudaMemcpyAsync(h, ctx->det_counts.p, sizeof(h), cudaMemcpyDeviceToHost,
+                              ctx->stream));
     OLPT_CUDA(cudaStreamSynchronize(ctx->stream));
+    OLPT_REQUIRE(h[kDcErr] == 0, OLPT_ERR_TIMEOUT,
+                 "peak detection: a staging or look-back wait timed out");
+    for (int c = 0; c < ctx->n_cam; ++c) ctx->det_counts_h[c] = h[c];
   }
 }
 
