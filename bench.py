@@ -357,7 +357,7 @@ class Ours:
         print(json.dumps(line), flush=True)
 
 
-def run_ours_ipr(args, o: Ours, learned=None):
+def run_ours_ipr(args, o: Ours, pre):
     from pyopenlpt_b200 import _ffi
     torch = o.torch
     sc, s = build_scene(args.workload, 1234 + o.rank)
@@ -430,12 +430,11 @@ def run_ours_ipr(args, o: Ours, learned=None):
                    "sample": "one whole frame of the same workload (IPR::runIPR compiled "
                              "from the reference sources, OpenMP)"}
         o.line(prof, dev_ms, parts, e2e_s, e2e_parts, bi, bo // max(1, args.steps), launches,
-               clk, workload_config(args.workload, s, sc=sc), cpu,
-               {} if learned is None else {"learned": learned})
+               clk, workload_config(args.workload, s, sc=sc), cpu, dict(pre))
     ctx.close()
 
 
-def run_ours_stb(args, o: Ours, learned=None):
+def run_ours_stb(args, o: Ours, pre):
     from pyopenlpt_b200 import _ffi
     torch = o.torch
     nf = N_INIT + args.warmup + args.steps
@@ -538,8 +537,7 @@ def run_ours_stb(args, o: Ours, learned=None):
         extra = {"initial_phase_ms_per_frame": [round(x, 1) for x in init_ms],
                  "extended_plus_new_per_step": ext_new / args.steps,
                  "track_lists_after": dict(zip(_ffi.TRACK_LISTS, lists))}
-        if learned is not None:
-            extra["learned"] = learned
+        extra.update(pre)
         o.line(prof, dev_ms, parts, e2e_s, e2e_parts, bi, bo // max(1, args.steps), launches,
                clk, workload_config(args.workload, s, seq=seq, st=st), cpu, extra)
 
@@ -671,16 +669,78 @@ def learned_comparison(args, o: Ours):
     }
 
 
+# ----------------------------------------------------------------------------- detection
+DET_SIZE, DET_CAMS, DET_PPP = 2048, 6, 0.1
+
+
+def render_spots(rng, H, W, n, amp=3000.0, noise=20.0, bits=12):
+    """n Gaussian spots (a exp(-0.5 (dx^2 + dy^2)), 7 x 7 window, fused by max) on
+    Gaussian noise, rounded and clipped to `bits` bits, uint16."""
+    im = np.zeros((H, W))
+    ys, xs = rng.uniform(-3, H + 3, n), rng.uniform(-3, W + 3, n)
+    for dy in range(-3, 4):
+        for dx in range(-3, 4):
+            r = np.floor(ys).astype(np.int64) + dy
+            c = np.floor(xs).astype(np.int64) + dx
+            ok = (r >= 0) & (r < H) & (c >= 0) & (c < W)
+            v = amp * np.exp(-0.5 * ((r - ys) ** 2 + (c - xs) ** 2))
+            np.maximum.at(im, (r[ok], c[ok]), v[ok])
+    im += rng.normal(0, noise, im.shape)
+    return np.clip(np.round(im), 0, 2 ** bits - 1).astype(np.uint16)
+
+
+def detection_roofline(args, o: Ours):
+    """The detection kernel alone at the image size of the 6-camera 2048^2 uint16
+    configuration (0.1 ppp of seeded spots per image): device time per launch with the
+    L2 flushed before each launch (the flush is queued on the library stream just
+    before the launch, so the events time the device work only), against HBM."""
+    from pyopenlpt_b200 import _ffi
+    torch = o.torch
+    rng = np.random.default_rng(2024)
+    n_spots = int(DET_PPP * DET_SIZE * DET_SIZE)
+    imgs = [render_spots(rng, DET_SIZE, DET_SIZE, n_spots) for _ in range(DET_CAMS)]
+    sc = synth.make_scene(n_particles=10, size=512, focal=2500.0, seed=1)
+    ctx = _ffi.Context(o.local)
+    ctx.upload_cameras([_ffi.camera_desc_from_pinhole(sc.cams[0])] * DET_CAMS)
+    ctx.upload_images(imgs)
+    stream = torch.cuda.ExternalStream(ctx.stream())
+    for _ in range(args.warmup):
+        counts = ctx.find_peaks(300)
+    ctx.profile(True)
+    for _ in range(args.steps):
+        with torch.cuda.stream(stream):
+            o.flush.zero_()
+        counts = ctx.find_peaks(300)
+    ms, n, img_bytes = ctx.profile_read(_ffi.PROF_PEAKS)
+    ctx.profile(False)
+    ctx.close()
+    peak, peak_kind = measured_peak_hbm()
+    dets = int(counts.sum())
+    algo = img_bytes / n + 24.0 * dets  # image read + detections written (x, y f64, row/col i32)
+    achieved = algo / (ms / n * 1e-3) / 1e9
+    return {"kernel": "detect_kernel<uint16_t> (staged single read)",
+            "images": f"{DET_CAMS} x {DET_SIZE}x{DET_SIZE} uint16 (12-bit), {n_spots} spots "
+                      f"each (0.1 ppp), noise sigma 20, threshold 300",
+            "detections_per_launch": dets, "launch_us": round(ms / n * 1e3, 2),
+            "bytes_per_launch": algo, "achieved": achieved, "peak": peak, "unit": "GB/s",
+            "frac": achieved / peak, "peak_source": peak_kind, "launches": n,
+            "timing": "CUDA events on the library stream, L2 flushed before each launch"}
+
+
 def run_ours(args):
     o = Ours(args)
     learned = None
     if o.world == 1 and args.learn_frames > 0:
         learned = learned_comparison(args, o)
         o.torch.cuda.synchronize()
+    pre = {} if learned is None else {"learned": learned}
+    if o.world == 1 and not args.no_detection_roofline:
+        pre["detection_roofline"] = detection_roofline(args, o)
+        o.torch.cuda.synchronize()
     if WORKLOADS[args.workload]["kind"] == "ipr":
-        run_ours_ipr(args, o, learned)
+        run_ours_ipr(args, o, pre)
     else:
-        run_ours_stb(args, o, learned)
+        run_ours_stb(args, o, pre)
     if o.world > 1:
         o.dist.destroy_process_group()
     return 0
@@ -695,6 +755,8 @@ def main():
     ap.add_argument("--workload", choices=sorted(WORKLOADS), default=DEFAULT_WORKLOAD)
     ap.add_argument("--precision", choices=["fp32", "fp64"], default="fp32")
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--no-detection-roofline", action="store_true",
+                    help="skip the detection kernel's roofline measurement")
     ap.add_argument("--learn-frames", type=int, default=24,
                     help="frames of training tuples for the learned comparison (0 = skip)")
     ap.add_argument("--learn-steps", type=int, default=3000)

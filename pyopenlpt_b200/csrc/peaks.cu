@@ -70,11 +70,13 @@ template <typename T>
 struct Ln;
 template <>
 struct Ln<uint8_t> {
-  static __device__ __forceinline__ double f(uint8_t v, const double* lut) { return lut[v]; }
+  static __device__ __forceinline__ double f(uint8_t v, const double* lut) { return __ldg(lut + v); }
 };
 template <>
 struct Ln<uint16_t> {
-  static __device__ __forceinline__ double f(uint16_t v, const double* lut) { return lut[v]; }
+  static __device__ __forceinline__ double f(uint16_t v, const double* lut) {
+    return __ldg(lut + v);
+  }
 };
 template <>
 struct Ln<float> {
@@ -337,9 +339,11 @@ struct DetArgs {
   unsigned long long* dc;   // det_counts words
 };
 
-__device__ __forceinline__ unsigned long long ld_acquire_u64(const unsigned long long* p) {
+// A band state is read as one word (flag and count together), so a relaxed load is
+// enough: nothing else that the publishing CTA wrote is read through it.
+__device__ __forceinline__ unsigned long long ld_relaxed_u64(const unsigned long long* p) {
   unsigned long long v;
-  asm volatile("ld.acquire.gpu.global.u64 %0, [%1];" : "=l"(v) : "l"(p) : "memory");
+  asm volatile("ld.relaxed.gpu.global.u64 %0, [%1];" : "=l"(v) : "l"(p) : "memory");
   return v;
 }
 __device__ __forceinline__ void st_release_u64(unsigned long long* p, unsigned long long v) {
@@ -435,77 +439,35 @@ __device__ __forceinline__ unsigned mask_staged(const T* tile, const DetCam& c, 
 }
 
 
-// Integer levels, four u8 or two u16 pixels per 32-bit word: the same tests as
-// mask_staged's pixel loop with SIMD compares (0xff / 0xffff per lane that holds).
-__device__ __forceinline__ uint32_t lane_bits(uint32_t m, uint8_t) {
-  return (((m & 0x01010101u) * 0x01020408u) >> 24) & 0xfu;  // byte k -> bit k
-}
-__device__ __forceinline__ uint32_t lane_bits(uint32_t m, uint16_t) {
-  return (m & 1u) | ((m >> 15) & 2u);  // half k -> bit k
-}
-__device__ __forceinline__ uint32_t vge(uint32_t a, uint32_t b, uint8_t) { return __vcmpgeu4(a, b); }
-__device__ __forceinline__ uint32_t vgt(uint32_t a, uint32_t b, uint8_t) { return __vcmpgtu4(a, b); }
-__device__ __forceinline__ uint32_t vge(uint32_t a, uint32_t b, uint16_t) { return __vcmpgeu2(a, b); }
-__device__ __forceinline__ uint32_t vgt(uint32_t a, uint32_t b, uint16_t) { return __vcmpgtu2(a, b); }
-
+// One chunk of integer levels: bit j set if pixel c0 + j passes the threshold and the
+// isLocalMax tie rule (up / left reject if strictly greater, down / right if >=).
+// qc: the chunk (the chunks above and below are read only if a pixel passes the
+// threshold); left / right: the pixels beside it (0 outside the image, as the zero
+// fill); cols: the interior-column bits.
 template <typename T>
-__device__ __forceinline__ unsigned mask_staged_int(const T* tile, const DetCam& c, int box_h,
-                                                    int min_level, int r, int lr, int c0) {
-  constexpr int N = 16 / sizeof(T), PW = 4 / sizeof(T);  // pixels per chunk, per word
-  constexpr int kMaxLevel = sizeof(T) == 1 ? 255 : 65535;
-  if (r < 1 || r > c.H - 2 || min_level > kMaxLevel) return 0u;
-  const uint32_t thr = sizeof(T) == 1 ? (uint32_t)min_level * 0x01010101u
-                                      : (uint32_t)min_level * 0x00010001u;
-  const int ic = tile_index<T>(c, box_h, lr, c0);
-  const uint4 qc = *reinterpret_cast<const uint4*>(tile + ic);
-  const uint32_t C[4] = {qc.x, qc.y, qc.z, qc.w};
-  uint32_t keep[4];
-  uint32_t any = 0u;
+__device__ __forceinline__ unsigned mask_int(const uint4& qc, const T* tile, int ic, int box_w,
+                                             uint32_t left, uint32_t right, int min_level,
+                                             unsigned cols) {
+  constexpr int N = 16 / sizeof(T);  // pixels per chunk
+  const T* cen = reinterpret_cast<const T*>(&qc);
+  unsigned cand = 0u;
 #pragma unroll
-  for (int k = 0; k < 4; ++k) {
-    keep[k] = vge(C[k], thr, T());
-    any |= keep[k];
-  }
-  if (!any) return 0u;
-  const uint4 qu = *reinterpret_cast<const uint4*>(tile + ic - c.box_w);
-  const uint4 qd = *reinterpret_cast<const uint4*>(tile + ic + c.box_w);
-  const uint32_t U[4] = {qu.x, qu.y, qu.z, qu.w};
-  const uint32_t D[4] = {qd.x, qd.y, qd.z, qd.w};
-  const int wpad = c.n_box * c.box_w;
-  const uint32_t left = (c0 > 0) ? (uint32_t)tile[tile_index<T>(c, box_h, lr, c0 - 1)] : 0u;
-  const uint32_t right = (c0 + N < wpad) ? (uint32_t)tile[tile_index<T>(c, box_h, lr, c0 + N)] : 0u;
-  // the word of left / right neighbours of word k's pixels
-  const uint32_t lw0 = left << (32 - 8 * sizeof(T));
+  for (int j = 0; j < N; ++j) cand |= (unsigned)((int)cen[j] >= min_level) << j;
+  cand &= cols;
+  if (!cand) return 0u;
+  const uint4 qu = *reinterpret_cast<const uint4*>(tile + ic - box_w);
+  const uint4 qd = *reinterpret_cast<const uint4*>(tile + ic + box_w);
+  const T* up = reinterpret_cast<const T*>(&qu);
+  const T* dn = reinterpret_cast<const T*>(&qd);
   unsigned mask = 0u;
 #pragma unroll
-  for (int k = 0; k < 4; ++k) {
-    const uint32_t prev = k > 0 ? C[k - 1] : lw0;
-    const uint32_t next = k < 3 ? C[k + 1] : right;
-    const uint32_t L = sizeof(T) == 1 ? __byte_perm(prev, C[k], 0x6543) : __byte_perm(prev, C[k], 0x5432);
-    const uint32_t R = sizeof(T) == 1 ? __byte_perm(C[k], next, 0x4321) : __byte_perm(C[k], next, 0x5432);
-    // isLocalMax: up / left reject if strictly greater, down / right if >=
-    const uint32_t m = keep[k] & vge(C[k], U[k], T()) & vge(C[k], L, T()) & vgt(C[k], D[k], T()) &
-                       vgt(C[k], R, T());
-    mask |= lane_bits(m, T()) << (PW * k);
+  for (int j = 0; j < N; ++j) {
+    const uint32_t v = cen[j];
+    const uint32_t l = j > 0 ? (uint32_t)cen[j - 1] : left;
+    const uint32_t rr = j < N - 1 ? (uint32_t)cen[j + 1] : right;
+    mask |= (unsigned)((uint32_t)up[j] <= v && l <= v && (uint32_t)dn[j] < v && rr < v) << j;
   }
-  // border columns are never peaks
-  const int lo = max(0, 1 - c0), hi = min(N - 1, c.W - 2 - c0);
-  if (hi < lo) return 0u;
-  const unsigned cols = ((hi >= 31 ? 0xffffffffu : ((1u << (hi + 1)) - 1u))) & ~((1u << lo) - 1u);
-  return mask & cols;
-}
-
-// The sub-pixel centre of a pixel that mask_staged accepted (same operations, same
-// operands, so the same values).
-template <typename T>
-__device__ __forceinline__ void fit_staged(const T* tile, const DetCam& c, int box_h,
-                                           const double* lut, int r, int lr, int col, double& xc,
-                                           double& yc) {
-  const int ic = tile_index<T>(c, box_h, lr, col);
-  const double lc = Ln<T>::f(tile[ic], lut);
-  fit3(Ln<T>::f(tile[tile_index<T>(c, box_h, lr, col - 1)], lut), lc,
-       Ln<T>::f(tile[tile_index<T>(c, box_h, lr, col + 1)], lut), col, xc);
-  fit3(Ln<T>::f(tile[ic - c.box_w], lut), lc, Ln<T>::f(tile[ic + c.box_w], lut), r, yc);
+  return mask & cand;
 }
 
 template <typename T>
@@ -564,14 +526,56 @@ __global__ void __launch_bounds__(kDetThreads, 3) detect_kernel(const __grid_con
   // 1. evaluate every chunk of the band (coalesced over threads), keep the masks
   const int cpr = c.cpr;
   const int n_chunks = rows * cpr;
-  for (int i = tid; i < n_chunks; i += kDetThreads) {
-    const int lr = 1 + i / cpr;
-    if constexpr (std::is_integral<T>::value)
-      masks[i] = (uint16_t)mask_staged_int<T>(tile, c, box_h, a.min_level, r0 + lr - 1, lr,
-                                              (i % cpr) * N);
-    else
+  if constexpr (std::is_integral<T>::value) {
+    // chunk i = (lr - 1) * cpr + ci, stepped without divisions; a warp's lanes hold
+    // consecutive chunks, so the pixels beside a chunk come from the neighbour lanes
+    constexpr int kShift = 32 - 8 * (int)sizeof(T);
+    constexpr uint32_t kLow = sizeof(T) == 1 ? 0xffu : 0xffffu;
+    const int kMaxLevel = sizeof(T) == 1 ? 255 : 65535;
+    int lr = 1 + tid / cpr, ci = tid % cpr;
+    const int step_r = kDetThreads / cpr, step_c = kDetThreads % cpr;
+    for (int i = tid; i - lane < n_chunks; i += kDetThreads) {  // warp-uniform condition
+      const bool act = i < n_chunks;
+      const int c0 = ci * N;
+      const int ic = act ? tile_index<T>(c, box_h, lr, c0) : 0;
+      const uint4 qc = act ? *reinterpret_cast<const uint4*>(tile + ic) : make_uint4(0, 0, 0, 0);
+      const uint32_t prev = __shfl_up_sync(0xffffffffu, qc.w, 1);
+      const uint32_t next = __shfl_down_sync(0xffffffffu, qc.x, 1);
+      if (act) {
+        const int r = r0 + lr - 1;
+        unsigned m = 0u;
+        if (r >= 1 && r <= c.H - 2 && a.min_level <= kMaxLevel) {
+          uint32_t left = 0u, right = 0u;
+          if (ci > 0)
+            left = lane > 0 ? prev >> kShift : (uint32_t)tile[tile_index<T>(c, box_h, lr, c0 - 1)];
+          if (ci + 1 < cpr)
+            right = lane < 31 ? next & kLow : (uint32_t)tile[tile_index<T>(c, box_h, lr, c0 + N)];
+          const int lo = max(0, 1 - c0), hi = min(N - 1, c.W - 2 - c0);
+          const unsigned cols = hi < lo ? 0u : (((1u << (hi + 1)) - 1u) & ~((1u << lo) - 1u));
+          m = cols ? mask_int<T>(qc, tile, ic, c.box_w, left, right, a.min_level, cols) : 0u;
+        }
+        masks[i] = (uint16_t)m;
+      }
+      lr += step_r;
+      ci += step_c;
+      if (ci >= cpr) {
+        ci -= cpr;
+        ++lr;
+      }
+    }
+  } else {
+    int lr = 1 + tid / cpr, ci = tid % cpr;
+    const int step_r = kDetThreads / cpr, step_c = kDetThreads % cpr;
+    for (int i = tid; i < n_chunks; i += kDetThreads) {
       masks[i] = (uint16_t)mask_staged<T, N>(tile, c, box_h, a.min_int, a.min_level, a.lut,
-                                             r0 + lr - 1, lr, (i % cpr) * N);
+                                             r0 + lr - 1, lr, ci * N);
+      lr += step_r;
+      ci += step_c;
+      if (ci >= cpr) {
+        ci -= cpr;
+        ++lr;
+      }
+    }
   }
   __syncthreads();
 
@@ -602,7 +606,7 @@ __global__ void __launch_bounds__(kDetThreads, 3) detect_kernel(const __grid_con
     if (lane == 0) st_release_u64(state, (band == 0 ? kStPrefix : kStAggregate) | total);
     // 3. look-back over windows of 32 earlier bands: sum the aggregates down to the
     //    nearest published prefix (bands before the camera's first count as an empty
-    //    prefix); wait while a band of the window has published nothing yet
+    //    prefix); wait while a band above that prefix has published nothing yet
     unsigned long long prefix = 0;
     int ok = 1;
     if (band > 0) {
@@ -611,9 +615,11 @@ __global__ void __launch_bounds__(kDetThreads, 3) detect_kernel(const __grid_con
       while (true) {
         const int idx = top - 31 + lane;
         const unsigned long long w =
-            idx >= c.band_base ? ld_acquire_u64(dc + kDcState + idx) : kStPrefix;
+            idx >= c.band_base ? ld_relaxed_u64(dc + kDcState + idx) : kStPrefix;
         const unsigned long long flag = w & ~kStValue;
-        if (__any_sync(0xffffffffu, flag == 0)) {
+        const unsigned pmask = __ballot_sync(0xffffffffu, flag == kStPrefix);
+        const int nearest = pmask ? 31 - __clz(pmask) : 0;  // highest lane with a prefix
+        if (__any_sync(0xffffffffu, flag == 0 && lane > nearest - (pmask ? 0 : 1))) {
           int expired = 0;
           if (lane == 0) {
             const uint64_t now = umma::global_timer();
@@ -628,8 +634,6 @@ __global__ void __launch_bounds__(kDetThreads, 3) detect_kernel(const __grid_con
           __nanosleep(64);
           continue;
         }
-        const unsigned pmask = __ballot_sync(0xffffffffu, flag == kStPrefix);
-        const int nearest = pmask ? 31 - __clz(pmask) : 0;  // highest lane with a prefix
         unsigned long long v = lane >= nearest ? (w & kStValue) : 0ull;
 #pragma unroll
         for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
@@ -659,30 +663,56 @@ __global__ void __launch_bounds__(kDetThreads, 3) detect_kernel(const __grid_con
   for (int lo = 0; lo < block_total; lo += kDetList) {
     if (my0 < lo + kDetList && my0 + n > lo) {
       int rank = my0;
+      int lr = 1 + i0 / cpr, ci = i0 % cpr;
       for (int i = i0; i < i1 && rank < lo + kDetList; ++i) {
         unsigned m = masks[i];
         while (m) {
           const int j = __ffs(m) - 1;
           m &= m - 1;
-          if (rank >= lo && rank < lo + kDetList) dlist[rank - lo] = (uint32_t)i * 16u + (uint32_t)j;
+          if (rank >= lo && rank < lo + kDetList)
+            dlist[rank - lo] = ((uint32_t)lr << 16) | (uint32_t)(ci * N + j);  // tile row, column
           ++rank;
+        }
+        if (++ci == cpr) {
+          ci = 0;
+          ++lr;
         }
       }
     }
     __syncthreads();
     const int cnt = min(kDetList, block_total - lo);
     const int64_t base = s_prefix + lo;
-    for (int k = tid; k < cnt; k += kDetThreads) {
-      const uint32_t code = dlist[k];
-      const int i = (int)(code >> 4);
-      const int lr = 1 + i / cpr;
-      const int r = r0 + lr - 1;
-      const int col = (i % cpr) * N + (int)(code & 15u);
-      double xc, yc;
-      fit_staged<T>(tile, c, box_h, a.lut, r, lr, col, xc, yc);
-      c.x[base + k] = xc;
-      c.y[base + k] = yc;
-      c.rc[base + k] = make_int2(r, col);
+    // three detections per thread at a time: their log lookups are in flight together
+    constexpr int U = 3;
+    for (int k0 = tid; k0 < cnt; k0 += U * kDetThreads) {
+      int rr[U], cc[U];
+      double ln[U][5];
+#pragma unroll
+      for (int u = 0; u < U; ++u) {
+        const int k = min(k0 + u * kDetThreads, cnt - 1);  // past the end: a repeat, not stored
+        const uint32_t code = dlist[k];
+        const int lr = (int)(code >> 16);
+        rr[u] = r0 + lr - 1;
+        cc[u] = (int)(code & 0xffffu);
+        const int ic = tile_index<T>(c, box_h, lr, cc[u]);
+        ln[u][0] = Ln<T>::f(tile[tile_index<T>(c, box_h, lr, cc[u] - 1)], a.lut);
+        ln[u][1] = Ln<T>::f(tile[ic], a.lut);
+        ln[u][2] = Ln<T>::f(tile[tile_index<T>(c, box_h, lr, cc[u] + 1)], a.lut);
+        ln[u][3] = Ln<T>::f(tile[ic - c.box_w], a.lut);
+        ln[u][4] = Ln<T>::f(tile[ic + c.box_w], a.lut);
+      }
+#pragma unroll
+      for (int u = 0; u < U; ++u) {
+        const int k = k0 + u * kDetThreads;
+        if (k >= cnt) break;
+        // the two fits of eval_chunk / mask_staged: same operands, same operations
+        double xc, yc;
+        fit3(ln[u][0], ln[u][1], ln[u][2], cc[u], xc);
+        fit3(ln[u][3], ln[u][1], ln[u][4], rr[u], yc);
+        c.x[base + k] = xc;
+        c.y[base + k] = yc;
+        c.rc[base + k] = make_int2(rr[u], cc[u]);
+      }
     }
     __syncthreads();
   }
@@ -819,7 +849,7 @@ void find_peaks_device(olpt_ctx* ctx, double min_int, bool sync_counts) {
     geo[c] = det_geom(ctx->img[c].W, esz);
     int R = det_rows_fitting(geo[c], kDetTileBudget);
     if (R < 4) R = det_rows_fitting(geo[c], kDetTileBudgetMax);
-    if (R < 1) staged = false;
+    if (R < 1 || ctx->img[c].W > 65535) staged = false;  // detection codes hold 16-bit columns
     band_rows[c] = std::max(1, std::min(R, rows_fill));
     if (ctx->cams_h[c].is_active) smem = std::max(smem, det_smem_bytes(geo[c], band_rows[c]));
   }
