@@ -718,16 +718,20 @@ __global__ void __launch_bounds__(kDetThreads, 3) detect_kernel(const __grid_con
   }
 }
 
-// Dynamic shared memory of detect_kernel<T> raised to at least `bytes` (once per size).
+// Dynamic shared memory of detect_kernel<T> on the current device raised to at least
+// `bytes` (the attribute is per device; set once per device and size).
 template <typename T>
 void detect_smem_attr(size_t bytes) {
   static std::mutex mu;
-  static size_t set = 48 * 1024;
+  static size_t set[64] = {};
+  int dev = 0;
+  OLPT_CUDA(cudaGetDevice(&dev));
+  OLPT_REQUIRE(dev >= 0 && dev < 64, OLPT_ERR_INVALID_ARG, "device ordinal out of range");
   std::lock_guard<std::mutex> lk(mu);
-  if (bytes <= set) return;
+  if (bytes <= 48 * 1024 || bytes <= set[dev]) return;
   OLPT_CUDA(cudaFuncSetAttribute(detect_kernel<T>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                  (int)bytes));
-  set = bytes;
+  set[dev] = bytes;
 }
 
 template <typename T>
