@@ -174,10 +174,20 @@ __device__ void eval_geom(const ShakeView& v, const double P[3], Smem<Real>& S) 
   __syncwarp();
 }
 
+template <typename Real, int NC, int K>
+__device__ void residueK(const ShakeView& v, const Rect* roi, Smem<Real>& S, double f[K]);
+
 // TracerShakeStrategy::calShakeResidue (Shake.cpp:951-1045) for the point whose
-// geometry is in S (eval_geom), against the staged augmented ROIs.
+// geometry is in S (eval_geom), against the staged augmented ROIs.  The production
+// path is residueK with one point; the FP64 parity path stages the squared
+// differences and sums them per camera in row-major order.
 template <typename Real, int NC>
 __device__ double residue(const ShakeView& v, const Rect* roi, Smem<Real>& S) {
+  if (!(sizeof(Real) == 8 && v.exact_sums)) {
+    double f1[1];
+    residueK<Real, NC, 1>(v, roi, S, f1);
+    return f1[0];
+  }
   const int lane = threadIdx.x & 31;
   const int area = v.roi_area;
   double mse[NC];
@@ -260,26 +270,32 @@ __device__ void eval_geom3(const ShakeView& v, const double P[3], int ax, double
   __syncwarp();
 }
 
-// calShakeResidue for the three points of eval_geom3 (FP32 production path): each
-// lane visits the same pixels in the same order as three single evaluations would,
-// so the costs are the single evaluations' bit for bit; the three run interleaved.
-template <typename Real, int NC>
-__device__ void residue3(const ShakeView& v, const Rect* roi, Smem<Real>& S, double f[3]) {
+// calShakeResidue for the K points in the geometry slots 0 .. K - 1 (K = 3: the points
+// of eval_geom3; K = 1: the point of eval_geom), production path: per camera, each
+// lane visits the pixels q = lane, lane + 32, ... of the reference loop over all
+// cameras' ROI pixels, in that order, so the sums are those of single evaluations bit
+// for bit; the K points run interleaved.
+template <typename Real, int NC, int K>
+__device__ void residueK(const ShakeView& v, const Rect* roi, Smem<Real>& S, double f[K]) {
   const int lane = threadIdx.x & 31;
   const int area = v.roi_area;
   constexpr int C = NC;
-  double cost[3] = {0.0, 0.0, 0.0};
-  int used = 0;
+  double cost[K];
 #pragma unroll
+  for (int j = 0; j < K; ++j) cost[j] = 0.0;
+  int used = 0;
+  // kept rolled: one copy of the pixel loop instead of one per camera (the kernel is
+  // bound by instruction fetch; the unrolled form measured 10% slower)
+#pragma unroll 1
   for (int c = 0; c < C; ++c) {
     const Rect R = roi[c];
     if (rect_empty(R)) continue;
     const int w = R.cmax - R.cmin, h = R.rmax - R.rmin;
     if (w <= 0 || h <= 0) continue;
-    double u[3], vv[3];
-    int prmin[3], prmax[3], pcmin[3], pcmax[3];
+    double u[K], vv[K];
+    int prmin[K], prmax[K], pcmin[K], pcmax[K];
 #pragma unroll
-    for (int j = 0; j < 3; ++j) {
+    for (int j = 0; j < K; ++j) {
       u[j] = S.uvc[2 * (j * C + c)];
       vv[j] = S.uvc[2 * (j * C + c) + 1];
       prmin[j] = (int)floor(vv[j] - v.r_px);
@@ -291,13 +307,15 @@ __device__ void residue3(const ShakeView& v, const Rect* roi, Smem<Real>& S, dou
     // over q = lane, lane + 32, ... < C * area, in the same order
     int first = lane - (c * area) % 32;
     if (first < 0) first += 32;
-    Real part[3] = {(Real)0, (Real)0, (Real)0};
+    Real part[K];
+#pragma unroll
+    for (int j = 0; j < K; ++j) part[j] = (Real)0;
     for (int pix = first; pix < area; pix += 32) {
       if (pix >= w * h) continue;
       const int row = R.rmin + pix / w, col = R.cmin + pix % w;
       const Real a = S.aug[c * area + pix];
 #pragma unroll
-      for (int j = 0; j < 3; ++j) {
+      for (int j = 0; j < K; ++j) {
         Real pred = (Real)0;
         if (row >= prmin[j] && row < prmax[j] && col >= pcmin[j] && col < pcmax[j])
           pred = gauss<Real>(col, row, u[j], vv[j], S.otf + 5 * (j * C + c));
@@ -306,17 +324,17 @@ __device__ void residue3(const ShakeView& v, const Rect* roi, Smem<Real>& S, dou
       }
     }
 #pragma unroll
-    for (int j = 0; j < 3; ++j)
+    for (int j = 0; j < K; ++j)
 #pragma unroll
       for (int o = 16; o > 0; o >>= 1) part[j] += __shfl_xor_sync(0xffffffffu, part[j], o);
     if (!v.cams[c].is_active) continue;
     const int n = w * h;
 #pragma unroll
-    for (int j = 0; j < 3; ++j) cost[j] += (double)part[j] / (double)n;
+    for (int j = 0; j < K; ++j) cost[j] += (double)part[j] / (double)n;
     ++used;
   }
 #pragma unroll
-  for (int j = 0; j < 3; ++j)
+  for (int j = 0; j < K; ++j)
     f[j] = used > 1 ? cost[j] / (double)used : __longlong_as_double(0x7ff0000000000000LL);
 }
 
@@ -440,7 +458,7 @@ __global__ void __launch_bounds__(128, 8) shake_kernel(ShakeView v, int64_t n, d
       }
     } else {
       eval_geom3<Real, NC>(v, tmp, ax, x0, rel, S);
-      residue3<Real, NC>(v, roi, S, f);
+      residueK<Real, NC, 3>(v, roi, S, f);
       __syncwarp();
     }
     tmp[ax] = x0 + rel[2];  // as left by the last single evaluation
