@@ -259,7 +259,7 @@ PHASE_NAMES = {5: "detection", 6: "stereo matching (all)", 7: "candidate sort + 
 # shake_kernel launches of the STB convergence frames, 16-19 k objects each, divided by
 # their objects), and the kernel's algorithmic bytes per object for 4 cameras in FP32:
 # 4 x 64 ROI pixels x 4 B + 2 x (24 + 4 x 16 + 8) B of state + 4 x 5 x 4 B of OTF.
-SHAKE_DRAM_BYTES_PER_OBJECT = 22_400.0
+SHAKE_DRAM_BYTES_PER_OBJECT = 7_300.0
 SHAKE_ALGO_BYTES_PER_OBJECT = 1_296.0
 
 
