@@ -116,7 +116,9 @@ olpt_status_t olpt_image_download(olpt_ctx* ctx, int cam, olpt_dtype_t dtype, vo
 
 /* ------------------------------------------------------------------ 2D detection */
 /* ObjectFinder2D::findObject2D -> findTracer2D (src/srcObject/ObjectFinder.cpp:6-111) on the
- * current image of every active camera, keeping detections on the device.
+ * current image of every active camera, keeping detections on the device (raster order,
+ * as the reference).  One read of each image; OLPT_ERR_TIMEOUT if one of the kernel's
+ * bounded device waits (tile staging, ordering between row bands) ran out.
  * counts (host, n_cam) receives the number of detections per camera. */
 olpt_status_t olpt_find_peaks(olpt_ctx* ctx, double min_obj_int, int64_t* counts);
 /* Download detections of one camera in raster order: xy (n x 2, x = col, y = row) and
@@ -131,9 +133,9 @@ olpt_status_t olpt_detections_upload(olpt_ctx* ctx, int n_cam, const int64_t* co
  * memory -- code that runs inside another framework's memory arena or caching
  * allocator, or a plug-in host that budgets the device memory itself -- so it needs
  * no context and calls no cudaMalloc/cudaFree or allocating library routine.  Same
- * kernels and results as olpt_find_peaks; its scratch (per-band counts and offsets)
- * and the log table live in library-owned static device arrays that every GPU
- * loading this library holds until exit.
+ * results as olpt_find_peaks (through the two-pass kernels: count, scan, emit); its
+ * scratch (per-band counts and offsets) and the log table live in library-owned
+ * static device arrays that every GPU loading this library holds until exit.
  *   d_img       device image, H x W elements of `dtype`, rows pitch_bytes apart
  *               (pitch and pointer 16-byte aligned); H, W at most 16384
  *   d_x, d_y    device outputs (capacity doubles each), d_rc device output
