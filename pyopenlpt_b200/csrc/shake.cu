@@ -423,20 +423,25 @@ __global__ void __launch_bounds__(128, 8) shake_kernel(ShakeView v, int64_t n, d
     roi[c] = roi_bound(v.cams[c].n_row, v.cams[c].n_col, uvo[2 * c], uvo[2 * c + 1],
                        v.r_px * v.ratio, v.r_px * v.ratio);
   }
-  for (int q = lane; q < C * area; q += 32) {
-    const int c = q / area, pix = q % area;
-    const Rect& R = roi[c];
+  // per camera: the projection window once, then the ROI's pixels over the lanes (each
+  // pixel is independent, so the lane mapping does not change the values)
+#pragma unroll 1
+  for (int c = 0; c < C; ++c) {
+    const Rect R = roi[c];
     if (!v.cams[c].is_active || rect_empty(R)) continue;
     const int w = R.cmax - R.cmin, h = R.rmax - R.rmin;
-    if (pix >= w * h) continue;
-    const int row = R.rmin + pix / w, col = R.cmin + pix % w;
-    const Rect pr = roi_bound(v.cams[c].n_row, v.cams[c].n_col, uvo[2 * c], uvo[2 * c + 1],
-                              v.r_px, v.r_px);
+    const double u = uvo[2 * c], vv = uvo[2 * c + 1];
+    const Rect pr = roi_bound(v.cams[c].n_row, v.cams[c].n_col, u, vv, v.r_px, v.r_px);
     const Real* res = reinterpret_cast<const Real*>(v.res[c].p);
-    Real a = res[(int64_t)row * (v.res[c].pitch / (int64_t)sizeof(Real)) + col];
-    if (row >= pr.rmin && row < pr.rmax && col >= pr.cmin && col < pr.cmax)
-      a += gauss<Real>(col, row, uvo[2 * c], uvo[2 * c + 1], otfp + (o * C + c) * 5);
-    S.aug[c * area + pix] = a > (Real)0 ? a : (Real)0;
+    const int64_t rp = v.res[c].pitch / (int64_t)sizeof(Real);
+    const Real* q5 = otfp + (o * C + c) * 5;
+    for (int pix = lane; pix < w * h; pix += 32) {
+      const int row = R.rmin + pix / w, col = R.cmin + pix % w;
+      Real a = res[(int64_t)row * rp + col];
+      if (row >= pr.rmin && row < pr.rmax && col >= pr.cmin && col < pr.cmax)
+        a += gauss<Real>(col, row, u, vv, q5);
+      S.aug[c * area + pix] = a > (Real)0 ? a : (Real)0;
+    }
   }
   __syncwarp();
 
