@@ -3,7 +3,20 @@
 
 Metric: particles/s (IPR+shake).
 
-* stb_1280x800_u16_51k (default): the Shake-the-Box sequence -- 4 pinhole cameras
+* stb_2048_u16_6cam_poly_419k (default): the high-density Shake-the-Box sequence --
+  6 cubic polynomial cameras (seeded, up to 2 px of distortion at the corners) on a
+  45 deg ring of radius 500 mm tilted 30 deg, 2048^2 12-bit images (uint16), 0.1 ppp
+  = 419,430 particles in 80x80x40 mm advected by ABC flow (A = B = C = 1, wavelength
+  40 mm, at most 4 px/frame), a seeded 5x5x5 OTF grid (a in [2400, 3600], b and c in
+  [0.3, 0.9]), noise sigma 20.  After the 4-frame initial phase, one step = one
+  convergence-phase STB::processFrame.  The line compares the plain GPU form with the
+  learned form on the same frames, at their recall and ghost rate against the
+  generator's ground truth, and reports the FP32 path's position error against the
+  FP64 mode.  The reference's CPU path cannot finish this workload in a bench run
+  (its initial phase alone is hours of CPU time); its arm times the same generator
+  at 256^2 (stb_256_u16_6cam_poly_6.5k: same rig, ppp, flow, OTF and settings in
+  pixels, 1/64 of the particles, epipolar strips 1/8 as long).
+* stb_1280x800_u16_51k: the Shake-the-Box sequence -- 4 pinhole cameras
   (f = 5000 px, 45 deg ring of radius 500 mm, 30 deg tilt), 1280x800 12-bit images,
   51,000 particles in 60x40x30 mm advected by a Burgers vortex plus drift.  After the
   4-frame initial phase, one step = one convergence-phase STB::processFrame (predict,
@@ -54,7 +67,22 @@ WORKLOADS = {
                                                    noise=2.0, bits=8),
                             settings=dict()),
 }
-DEFAULT_WORKLOAD = "stb_1280x800_u16_51k"
+# High-density polynomial-camera STB: settings in pixels of the rig (shake width
+# 0.25 px, tol_3d 0.6 px, link radii 10 px, field radius 30 px, threshold 300 on the
+# 12-bit images); every camera in the build (match_cam_count = 6: with check
+# cameras the reference's StereoMatch aborts, StereoMatch.cpp:120-127).
+POLY_PX = dict(shake_width=0.25, tol_3d=0.6, link=10.0, pf_r=30.0)
+WORKLOADS["stb_2048_u16_6cam_poly_419k"] = dict(
+    kind="stb", gen="poly", seq=dict(ppp=0.1, n_cam=6, size=2048,
+                                     volume=(-40.0, 40.0, -40.0, 40.0, -20.0, 20.0), bits=12),
+    settings=dict(min_obj_int=300), stb=dict(pf_nx=11, pf_ny=11, pf_nz=6))
+WORKLOADS["stb_256_u16_6cam_poly_6.5k"] = dict(
+    kind="stb", gen="poly", seq=dict(ppp=0.1, n_cam=6, size=256,
+                                     volume=(-5.0, 5.0, -5.0, 5.0, -2.5, 2.5), bits=12),
+    settings=dict(min_obj_int=300), stb=dict(pf_nx=11, pf_ny=11, pf_nz=6))
+# the reference arm's sample of each workload (a workload the CPU path finishes)
+REFERENCE_SAMPLE = {"stb_2048_u16_6cam_poly_419k": "stb_256_u16_6cam_poly_6.5k"}
+DEFAULT_WORKLOAD = "stb_2048_u16_6cam_poly_419k"
 
 
 def ipr_settings(name: str, n_cam: int):
@@ -68,9 +96,22 @@ def build_scene(name: str, seed: int):
     return sc, ipr_settings(name, sc.n_cam)
 
 
-def build_sequence(name: str, seed: int, n_frames: int):
-    seq = synth.make_sequence(n_frames=n_frames, seed=seed, **WORKLOADS[name]["seq"])
-    return seq, ipr_settings(name, seq.n_cam), synth.STBSettings(**WORKLOADS[name]["stb"])
+def build_sequence(name: str, seed: int, n_frames: int, device="cpu", with_images=True):
+    w = WORKLOADS[name]
+    if w.get("gen") == "poly":
+        seq = synth.make_poly_sequence(n_frames=n_frames, seed=seed, device=device,
+                                       with_images=with_images, **w["seq"])
+        mm_px = 1.0 / max(synth.px_per_mm(c, np.zeros(3)) for c in seq.cams)
+        s = synth.IPRSettings(**w["settings"])
+        s.match_cam_count = seq.n_cam
+        s.shake_width = POLY_PX["shake_width"] * mm_px
+        s.tol_3d_mm = POLY_PX["tol_3d"] * mm_px
+        st = synth.STBSettings(radius_search_obj=POLY_PX["link"] * mm_px,
+                               radius_search_track=POLY_PX["link"] * mm_px,
+                               pf_r=POLY_PX["pf_r"] * mm_px, **w["stb"])
+        return seq, s, st
+    seq = synth.make_sequence(n_frames=n_frames, seed=seed, with_images=with_images, **w["seq"])
+    return seq, ipr_settings(name, seq.n_cam), synth.STBSettings(**w["stb"])
 
 
 # ----------------------------------------------------------------------------- clocks
@@ -173,6 +214,34 @@ def reference_ipr_time(sc, s, threads: int, images=None):
 REF_STB_BUDGET_S = 240.0  # convergence frames of the reference arm stop after this
 
 
+def reference_stb(name, threads, warmup, steps, budget_s):
+    """The reference STB (compiled from its sources) on the workload's CPU sample:
+    N_INIT initial-phase and ``warmup`` convergence-phase frames untimed, then up to
+    ``steps`` convergence frames timed (wall clock), stopping once ``budget_s`` has
+    passed.  Particles per frame = track points the frame adds over the four lists."""
+    from oracle.ref import RefSTB
+    sample_name = REFERENCE_SAMPLE.get(name, name)
+    nf = N_INIT + warmup + steps
+    seq, s, st = build_sequence(sample_name, 1234, nf)
+    times, counts = [], []
+    with _MuteStdout():
+        ref = RefSTB(seq, s, st, threads=threads, match_cam_count=s.match_cam_count)
+        t_start = time.perf_counter()
+        for t in range(nf):
+            a = time.perf_counter()
+            ref.frame(t)
+            dt = time.perf_counter() - a
+            if t >= N_INIT + warmup:
+                rows = ref.tracks()
+                times.append(dt)
+                counts.append(sum(int(np.count_nonzero(v[:, 1] == t)) for v in rows.values()
+                                  if len(v)))
+                if time.perf_counter() - t_start > budget_s:
+                    break
+        ref.close()
+    return times, counts, seq, s, st, sample_name
+
+
 def run_reference(args):
     rank = int(os.environ.get("RANK", "0"))
     if rank != 0:
@@ -190,28 +259,18 @@ def run_reference(args):
         cfg = workload_config(args.workload, s, sc=sc)
         sample = "whole frame per step (IPR::runIPR, OpenMP, all host threads)"
     else:
-        from oracle.ref import RefSTB
-        nf = N_INIT + args.steps
-        seq, s, st = build_sequence(args.workload, 1234, nf)
-        with _MuteStdout():
-            ref = RefSTB(seq, s, st, threads=threads)
-            t_start = time.perf_counter()
-            for t in range(nf):
-                a = time.perf_counter()
-                ref.frame(t)
-                dt = time.perf_counter() - a
-                if t >= N_INIT:
-                    rows = ref.tracks()
-                    times.append(dt)
-                    counts.append(sum(int(np.count_nonzero(v[:, 1] == t)) for v in rows.values()
-                                      if len(v)))
-                    if time.perf_counter() - t_start > REF_STB_BUDGET_S:
-                        break
-            ref.close()
-        cfg = workload_config(args.workload, s, seq=seq, st=st)
-        sample = (f"STB::processFrame: {N_INIT} initial-phase frames untimed, then "
-                  f"{len(times)} convergence-phase frames timed (stops after "
-                  f"{REF_STB_BUDGET_S:.0f} s); OpenMP, all host threads")
+        times, counts, seq, s, st, sample_name = reference_stb(
+            args.workload, threads, args.warmup, args.steps, REF_STB_BUDGET_S)
+        if sample_name != args.workload:
+            main = build_sequence(args.workload, 1234, 1, with_images=False)
+            cfg = workload_config(args.workload, main[1], seq=main[0], st=main[2])
+            cfg["reference_sample"] = workload_config(sample_name, s, seq=seq, st=st)
+        else:
+            cfg = workload_config(args.workload, s, seq=seq, st=st)
+        sample = (f"STB::processFrame on {sample_name}: {N_INIT} initial-phase and "
+                  f"{args.warmup} convergence-phase frames untimed, then {len(times)} "
+                  f"convergence-phase frames timed (the same frame indices as the GPU arm; "
+                  f"stops after {REF_STB_BUDGET_S:.0f} s); OpenMP, all host threads")
     value = sum(counts) / sum(times)
     line = {
         "impl": "reference", "metric": METRIC, "value": value, "unit": "particles/s",
@@ -238,12 +297,21 @@ def workload_config(name, s, sc=None, seq=None, st=None):
         base.update(particles=int(len(sc.xyz)), cameras=sc.n_cam,
                     image=f"{H}x{W} {sc.images[0].dtype}")
     else:
-        H, W = seq.frames[0][0].shape
+        H, W = seq.cams[0].n_row, seq.cams[0].n_col
+        dt = "uint8" if seq.max_val <= 255 else "uint16"
         base.update(particles=int(len(seq.truth[0])), cameras=seq.n_cam,
-                    image=f"{H}x{W} {seq.frames[0][0].dtype} ({int(seq.max_val).bit_length()}-bit)",
+                    image=f"{H}x{W} {dt} ({int(seq.max_val).bit_length()}-bit)",
+                    ppp=round(len(seq.truth[0]) / (H * W), 4),
                     initial_frames=N_INIT, link_radius_mm=st.radius_search_track,
                     pred_field=f"{st.pf_nx}x{st.pf_ny}x{st.pf_nz} r {st.pf_r} mm",
+                    match_cam_count=s.match_cam_count,
+                    detection_cap=s.n_obj2d_process_max,
                     step="one convergence-phase frame")
+        if isinstance(seq, synth.PolySequence):
+            base.update(camera_model="cubic polynomial (20 terms), <= 2 px corner distortion",
+                        otf=f"{'x'.join(map(str, seq.otf_n))} grid, a in [2400, 3600], "
+                            "b, c in [0.3, 0.9]",
+                        flow="ABC (A = B = C = 1, wavelength 40 mm), <= 4 px/frame")
     return base
 
 
@@ -306,11 +374,16 @@ class Ours:
         if self.world > 1:
             self.dist.barrier()
 
-    def context(self, cams, volume, otf_abc):
+    def context(self, sc):
+        """A context with the rig of a scene or sequence: its cameras (pinhole or
+        polynomial) and its OTF (uniform 2x2x2, or the sequence's grid)."""
         from pyopenlpt_b200 import _ffi
         ctx = _ffi.Context(self.local)
-        ctx.upload_cameras([_ffi.camera_desc_from_pinhole(c) for c in cams])
-        ctx.upload_otf(2, 2, 2, volume, synth.otf_table_array(len(cams), otf_abc))
+        ctx.upload_cameras([_ffi.camera_desc(c) for c in sc.cams])
+        if getattr(sc, "otf_table", None) is not None:
+            ctx.upload_otf(*sc.otf_n, sc.volume, sc.otf_table)
+        else:
+            ctx.upload_otf(2, 2, 2, sc.volume, synth.otf_table_array(len(sc.cams), sc.otf_abc))
         return ctx
 
     def reduce(self, dev_ms, parts, e2e_s, e2e_parts):
@@ -361,7 +434,7 @@ def run_ours_ipr(args, o: Ours, pre):
     from pyopenlpt_b200 import _ffi
     torch = o.torch
     sc, s = build_scene(args.workload, 1234 + o.rank)
-    ctx = o.context(sc.cams, sc.volume, sc.otf_abc)
+    ctx = o.context(sc)
     params = _ffi.ipr_params(s, sc.volume, o.prec)
     H, W = sc.images[0].shape
     dtype = _ffi._DTYPES[sc.images[0].dtype]
@@ -434,39 +507,65 @@ def run_ours_ipr(args, o: Ours, pre):
     ctx.close()
 
 
+def recall_ghost(found, truth, radius):
+    """Fraction of true particles with an output within radius, and fraction of
+    outputs with no true particle within radius."""
+    from scipy.spatial import cKDTree
+    if len(found) == 0:
+        return 0.0, 0.0
+    d_gt, _ = cKDTree(found).query(truth)
+    d_f, _ = cKDTree(truth).query(found)
+    return float(np.mean(d_gt <= radius)), float(np.mean(d_f > radius))
+
+
+def frame_quality(xyz, truth):
+    r05, g05 = recall_ghost(xyz, truth, 0.05)
+    r10, g10 = recall_ghost(xyz, truth, 0.1)
+    return {"n": int(len(xyz)), "recall_05": r05, "ghost_05": g05, "recall_10": r10,
+            "ghost_10": g10}
+
+
+def mean_quality(qs):
+    keys = ("recall_05", "ghost_05", "recall_10", "ghost_10")
+    return {k: round(float(np.mean([q[k] for q in qs])), 5) for k in keys}
+
+
 def run_ours_stb(args, o: Ours, pre):
     from pyopenlpt_b200 import _ffi
     torch = o.torch
     nf = N_INIT + args.warmup + args.steps
-    seq, s, st = build_sequence(args.workload, 1234 + o.rank, nf)
-    H, W = seq.frames[0][0].shape
+    t_gen = time.perf_counter()
+    seq, s, st = build_sequence(args.workload, 1234 + o.rank, nf, device=f"cuda:{o.local}")
+    t_gen = time.perf_counter() - t_gen
+    H, W = seq.cams[0].n_row, seq.cams[0].n_col
     C = seq.n_cam
-    dtype = _ffi._DTYPES[seq.frames[0][0].dtype]
-    dev_frames = [torch.from_numpy(np.stack(f)).cuda() for f in seq.frames]
-    host_frames = [torch.from_numpy(np.stack(f)).pin_memory() for f in seq.frames]
+    frames = [np.ascontiguousarray(np.stack(f)) for f in seq.frames]
+    dtype = _ffi._DTYPES[frames[0].dtype]
+    dev_frames = [torch.from_numpy(f).cuda() for f in frames]
+    host_frames = [torch.from_numpy(f).pin_memory() for f in frames]
     params = _ffi.stb_params(s, st, seq.volume, 0, nf - 1, o.prec)
+    t0_frame = N_INIT + args.warmup
 
-    def new_ctx():
-        ctx = o.context(seq.cams, seq.volume, seq.otf_abc)
-        ctx.stb_configure(params)
+    def new_ctx(prec=o.prec):
+        ctx = o.context(seq)
+        ctx.stb_configure(_ffi.stb_params(s, st, seq.volume, 0, nf - 1, prec))
         return ctx
 
-    ctx = new_ctx()
-    stream = torch.cuda.ExternalStream(ctx.stream())
-    torch.cuda.synchronize()
-
-    def frame_device(t):
+    def frame_device(ctx, t):
         ctx.upload_images_device([dev_frames[t][c].data_ptr() for c in range(C)], dtype,
                                  [H] * C, [W] * C)
         ctx.stb_process_frame(t)
 
+    ctx = new_ctx()
+    stream = torch.cuda.ExternalStream(ctx.stream())
+    torch.cuda.synchronize()
     init_ms = []
     for t in range(N_INIT):
         a = time.perf_counter()
-        frame_device(t)
+        frame_device(ctx, t)
         init_ms.append(1e3 * (time.perf_counter() - a))
-    for t in range(N_INIT, N_INIT + args.warmup):
-        frame_device(t)
+    for t in range(N_INIT, t0_frame):
+        frame_device(ctx, t)
     torch.cuda.synchronize()
 
     clocks = ClockSampler(o.local)
@@ -476,20 +575,26 @@ def run_ours_stb(args, o: Ours, pre):
     torch.cuda.synchronize()
     launches0 = _ffi.launch_count()
     dev_ms, parts, ext_new = 0.0, 0, 0
-    t0_frame = N_INIT + args.warmup
+    quality, plain_objs = [], {}
     for t in range(t0_frame, nf):
         with torch.cuda.stream(stream):
             o.flush.zero_()
             e0 = torch.cuda.Event(enable_timing=True)
             e1 = torch.cuda.Event(enable_timing=True)
             e0.record(stream)
-        frame_device(t)
+        frame_device(ctx, t)
         e1.record(stream)
         e1.synchronize()
         dev_ms += e0.elapsed_time(e1)
         parts += ctx.stb_frame_points(t)
         _, ne, nn = ctx.stb_counts()
         ext_new += ne + nn
+        # outside the events: the frame's particles against the ground truth
+        launches_q = _ffi.launch_count()
+        xyz = ctx.stb_frame_objects()
+        plain_objs[t] = xyz
+        quality.append(frame_quality(xyz, seq.truth[t]))
+        launches0 += _ffi.launch_count() - launches_q
     torch.cuda.synchronize()
     o.barrier()
     launches = _ffi.launch_count() - launches0
@@ -497,6 +602,7 @@ def run_ours_stb(args, o: Ours, pre):
     ctx.profile(False)
     clk = clocks.stop()
     lists, _, _ = ctx.stb_counts()
+    res32 = ctx.stb_frame_image(0, H, W) if o.world == 1 and o.prec == 0 else None
     ctx.close()
 
     # end to end through the C ABI with host (pinned) images: a second tracker over the
@@ -522,24 +628,64 @@ def run_ours_stb(args, o: Ours, pre):
         bo += xyz.nbytes
     o.barrier()
     ctx.close()
-    bi = C * H * W * seq.frames[0][0].itemsize
+    bi = C * H * W * frames[0].itemsize
     dev_ms, parts, e2e_s, e2e_parts = o.reduce(dev_ms, parts, e2e_s, e2e_parts)
     if o.rank == 0:
         cpu = None
-        if o.world == 1 and not args.no_cpu_baseline:
-            threads = os.cpu_count() or 1
-            ncpu, tcpu = reference_ipr_time(seq, s, threads, images=seq.frames[0])
-            cpu = {"value": ncpu / tcpu, "unit": "particles/s", "cores": threads,
-                   "kind": "reference",
-                   "sample": "IPR::runIPR on frame 0 of the same sequence (the work of an "
-                             "initial-phase STB::processFrame), compiled from the reference "
-                             "sources, OpenMP"}
         extra = {"initial_phase_ms_per_frame": [round(x, 1) for x in init_ms],
                  "extended_plus_new_per_step": ext_new / args.steps,
-                 "track_lists_after": dict(zip(_ffi.TRACK_LISTS, lists))}
+                 "track_lists_after": dict(zip(_ffi.TRACK_LISTS, lists)),
+                 "quality_vs_truth": mean_quality(quality),
+                 "generation_s": round(t_gen, 1)}
+        if o.world == 1 and o.prec == 0 and not args.no_fp64_check:
+            extra["fp64_check"] = fp64_check(args, o, seq, s, st, nf, t0_frame, new_ctx,
+                                             frame_device, plain_objs, res32, H, W)
+        if o.world == 1 and not args.no_cpu_baseline:
+            threads = os.cpu_count() or 1
+            times, counts, rseq, _, _, sname = reference_stb(args.workload, threads, 0, 2, 60.0)
+            cpu = {"value": sum(counts) / sum(times), "unit": "particles/s", "cores": threads,
+                   "kind": "reference",
+                   "sample": f"STB::processFrame compiled from the reference sources (OpenMP) "
+                             f"on {sname}: {N_INIT} initial-phase frames untimed, then "
+                             f"{len(times)} convergence-phase frames timed"}
         extra.update(pre)
         o.line(prof, dev_ms, parts, e2e_s, e2e_parts, bi, bo // max(1, args.steps), launches,
                clk, workload_config(args.workload, s, seq=seq, st=st), cpu, extra)
+
+
+def fp64_check(args, o, seq, s, st, nf, t0_frame, new_ctx, frame_device, objs32, res32, H, W):
+    """The FP32 production path against the library's FP64 mode (the reference's
+    arithmetic) on the same frames: position differences of the frame's particles
+    matched one to one (nearest within 1e-3 mm), their reprojection differences, and
+    the residual image of camera 0 after the last frame."""
+    from scipy.spatial import cKDTree
+    ctx = new_ctx(1)
+    d_all, r_all, unmatched = [], [], 0
+    for t in range(nf):
+        frame_device(ctx, t)
+        if t in objs32:
+            x64 = ctx.stb_frame_objects()
+            x32 = objs32[t]
+            if len(x64) and len(x32):
+                d, j = cKDTree(x64).query(x32)
+                ok = d <= 1e-3
+                unmatched += int(np.sum(~ok)) + max(0, len(x64) - int(np.sum(ok)))
+                d_all.append(d[ok])
+                for c in range(len(seq.cams)):
+                    r_all.append(np.abs(ctx.project(c, x32[ok]) - ctx.project(c, x64[j[ok]])).max(1))
+    res64 = ctx.stb_frame_image(0, H, W)
+    ctx.close()
+    d = np.concatenate(d_all) if d_all else np.zeros(0)
+    r = np.concatenate(r_all) if r_all else np.zeros(0)
+    return {"frames": len(objs32), "matched": int(len(d)), "unmatched": unmatched,
+            "position_mm": {"median": float(np.median(d)) if len(d) else None,
+                            "p99": float(np.quantile(d, 0.99)) if len(d) else None,
+                            "max": float(d.max()) if len(d) else None,
+                            "frac_le_1e-4": float(np.mean(d <= 1e-4)) if len(d) else None},
+            "reprojection_px": {"median": float(np.median(r)) if len(r) else None,
+                                "max": float(r.max()) if len(r) else None},
+            "residual_cam0_max_abs": float(np.max(np.abs(res32 - res64))) if res32 is not None
+            else None}
 
 
 # ----------------------------------------------------------------------------- learned
@@ -755,6 +901,8 @@ def main():
     ap.add_argument("--workload", choices=sorted(WORKLOADS), default=DEFAULT_WORKLOAD)
     ap.add_argument("--precision", choices=["fp32", "fp64"], default="fp32")
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--no-fp64-check", action="store_true",
+                    help="skip the FP32-vs-FP64 comparison of the STB workload")
     ap.add_argument("--no-detection-roofline", action="store_true",
                     help="skip the detection kernel's roofline measurement")
     ap.add_argument("--learn-frames", type=int, default=24,

@@ -144,9 +144,10 @@ olpt_status_t olpt_detections_upload(olpt_ctx* ctx, int n_cam, const int64_t* co
  *   d_count     device int64 receiving the number of detections
  *   stream      cudaStream_t to launch on (NULL = default stream); the call returns
  *               without synchronising.
- * The first call on a device does a one-time, synchronous set-up (resolving the
- * static arrays' device addresses and filling the log table), so make it before
- * any stream capture.  All calls share the static scratch: calls that overlap on
+ * Every call resolves the static arrays' device addresses; the first call in each
+ * CUDA context of a device (the first on the device, and the first after a
+ * cudaDeviceReset) also fills the log table with a synchronous copy, so make it
+ * before any stream capture.  All calls share the static scratch: calls that overlap on
  * the GPU (different streams, host threads) race; serialise them.  Error text:
  * olpt_find_peaks_noalloc_error(). */
 olpt_status_t olpt_find_peaks_noalloc(const void* d_img, olpt_dtype_t dtype, int H, int W,
@@ -172,6 +173,31 @@ typedef struct olpt_sm_params {
  * candidate set (before the prune); n_matches: number of objects. */
 olpt_status_t olpt_stereo_match(olpt_ctx* ctx, const olpt_sm_params* p, int64_t* n_candidates,
                                 int64_t* n_matches);
+
+/* Near-tolerance decision log of stereo matching (no counterpart in the reference,
+ * which decides with the same tests without recording them).  The 2D tests of
+ * IDMap::visitPointsInRowSpans (|(q - p) x u|^2 > tol^2, StereoMatch.cpp:1582-1615)
+ * and StereoMatch::checkBackProjection (StereoMatch.cpp:1214-1223) whose distance
+ * lies within band_px of tol_2d_px are appended to a device log by every
+ * subsequent olpt_stereo_match (and every stereo step inside olpt_ipr_run and
+ * olpt_stb_process_frame), so that a decision that rounding could flip is visible.
+ * enable: band_px > 0 turns the log on with room for `capacity` records and clears
+ * it; band_px = 0 turns it off.  read: copies up to `cap` records (in append order,
+ * which is not deterministic) and the number of near-tolerance tests seen since the
+ * last enable or reset (records beyond the capacity are counted, not stored). */
+typedef struct olpt_near_record {
+  int32_t kind;      /* 0 = strip test: the target detection against a chosen point's
+                        image line; 1 = back-projection: the chosen point against the
+                        target detection's image line on the chosen camera */
+  int32_t n_chosen;  /* cameras in the partial match when the test ran */
+  int32_t cam, id;   /* the tested detection on the target camera */
+  int32_t other_cam, other_id; /* the chosen detection it was tested against */
+  double margin_px;  /* |distance| - tol_2d_px (negative: accepted side) */
+} olpt_near_record;
+olpt_status_t olpt_stereo_near_log_enable(olpt_ctx* ctx, double band_px, int64_t capacity);
+olpt_status_t olpt_stereo_near_log_read(olpt_ctx* ctx, olpt_near_record* out, int64_t cap,
+                                        int64_t* n_total);
+olpt_status_t olpt_stereo_near_log_reset(olpt_ctx* ctx);
 /* Candidate set of the last match in the reference's order (sorted by ids):
  * ids n_candidates x n_cam (-1 = unused camera), e_check, triangulated xyz. */
 olpt_status_t olpt_get_candidates(olpt_ctx* ctx, int32_t* ids, double* e_check, double* xyz);
@@ -325,16 +351,20 @@ olpt_status_t olpt_stb_load_tracks(olpt_ctx* ctx, int which, const char* path);
 
 /* ------------------------------------------------------------------ learned proposal */
 /* No reference counterpart: a small MLP that reads, for each candidate after stereo
- * matching, 4 cameras x 11 x 11 patches of max(0, residual + own projection) divided
- * by the candidate's OTF amplitude, the 8 sub-pixel offsets of its projections and a
- * constant 1 (OLPT_MLP_IN values, camera-major, patches row-major), and predicts a 3D
- * correction (units of out_scale_mm) and a ghost logit.  Layers 493 -> 256 -> 256 ->
- * 256 (GELU, erf form) -> 4; bf16 weights and activations on tcgen05 GEMMs with f32
- * accumulation.  Parameters are one flat f32 array: W1[256][493], b1[256],
- * W2[256][256], b2[256], W3[256][256], b3[256], W4[4][256], b4[4]. */
+ * matching, C cameras x 11 x 11 patches of max(0, residual + own projection) divided
+ * by the candidate's OTF amplitude, the 2 C sub-pixel offsets of its projections and
+ * a constant 1 (n_in = 121 C + 2 C + 1 values, camera-major, patches row-major), and
+ * predicts a 3D correction (units of out_scale_mm) and a ghost logit.  Layers n_in ->
+ * 256 -> 256 -> 256 (GELU, erf form) -> 4; bf16 weights and activations on tcgen05
+ * GEMMs with f32 accumulation.  Parameters are one flat f32 array: W1[256][n_in],
+ * b1[256], W2[256][256], b2[256], W3[256][256], b3[256], W4[4][256], b4[4].  C is the
+ * context's camera count when the network is initialised or set (2..8; 4 when no
+ * cameras are uploaded yet); OLPT_MLP_IN / OLPT_MLP_PARAMS are the 4-camera sizes. */
 #define OLPT_MLP_IN 493
 #define OLPT_MLP_OUT 4
 #define OLPT_MLP_PARAMS 259076
+/* Input width and parameter count of the network for a rig of n_cam cameras. */
+olpt_status_t olpt_mlp_dims(int n_cam, int* n_in, int64_t* n_params);
 
 /* The learned shake used by olpt_ipr_run (and the IPR inside the STB frame loop) when
  * enable != 0, in place of the plain runShake: the network corrects every candidate
@@ -355,17 +385,17 @@ typedef struct olpt_learned_params {
 olpt_status_t olpt_mlp_init(olpt_ctx* ctx, uint64_t seed);
 olpt_status_t olpt_mlp_set_params(olpt_ctx* ctx, const float* params);
 olpt_status_t olpt_mlp_get_params(olpt_ctx* ctx, float* params);
-/* out (n x 4) = network(x (n x OLPT_MLP_IN)); host or device pointers (on_device). */
+/* out (n x 4) = network(x (n x n_in)); host or device pointers (on_device). */
 olpt_status_t olpt_mlp_forward(olpt_ctx* ctx, int64_t n, const float* x, float* out,
                                int on_device);
 /* One training step on a batch: targets n x 4 (dx, dy, dz in units of out_scale_mm,
  * ghost label 0/1); loss = mean[(1 - ghost) * mean_d (o_d - t_d)^2 + ghost_weight *
- * BCE(o_3, ghost)].  Gradients of the mean loss go to grad (host, OLPT_MLP_PARAMS,
+ * BCE(o_3, ghost)].  Gradients of the mean loss go to grad (host, n_params floats,
  * optional); update != 0 applies Adam (lr, 0.9, 0.999, 1e-8). */
 olpt_status_t olpt_mlp_train_step(olpt_ctx* ctx, int64_t n, const float* x, const float* targets,
                                   int on_device, double lr, double ghost_weight, int update,
                                   double* loss, float* grad);
-/* Training on a device-resident dataset: x (n x OLPT_MLP_IN) and targets (n x 4), host
+/* Training on a device-resident dataset: x (n x n_in) and targets (n x 4), host
  * arrays copied to the device once (or device pointers, on_device != 0); `steps` Adam
  * steps on mini-batches of `batch` rows drawn uniformly with replacement (seeded), the
  * learning rate decayed from lr by a cosine to 5%.  losses (host, optional): one per
@@ -373,8 +403,8 @@ olpt_status_t olpt_mlp_train_step(olpt_ctx* ctx, int64_t n, const float* x, cons
 olpt_status_t olpt_mlp_train(olpt_ctx* ctx, int64_t n, const float* x, const float* targets,
                              int on_device, int batch, int steps, double lr, double ghost_weight,
                              uint64_t seed, float* losses);
-/* Features (n_objects x OLPT_MLP_IN) of the context's objects, against a residual of
- * the current images with every object projected (4 cameras). */
+/* Features (n_objects x n_in) of the context's objects, against a residual of the
+ * current images with every object projected. */
 olpt_status_t olpt_mlp_features(olpt_ctx* ctx, const olpt_shake_params* p, float* x,
                                 int on_device);
 olpt_status_t olpt_learned_configure(olpt_ctx* ctx, const olpt_learned_params* p);

@@ -8,8 +8,9 @@ dZ operands of the weight gradients), f32 accumulation, and the same loss.
 ``fd_check`` pins the analytic gradients of the model itself against central finite
 differences (with bf16 rounding switched off).
 
-Parameter layout (flat f32): W1[256][493], b1[256], W2[256][256], b2, W3[256][256],
-b3, W4[4][256], b4[4].  Nothing in the product imports this module.
+Parameter layout (flat f32): W1[256][n_in], b1[256], W2[256][256], b2, W3[256][256],
+b3, W4[4][256], b4[4], with n_in = 121 C + 2 C + 1 for C cameras (493 for 4; the
+functions take n_in from the flat size).  Nothing in the product imports this module.
 """
 from __future__ import annotations
 
@@ -17,14 +18,30 @@ import numpy as np
 from scipy.special import erf
 
 IN, HID, OUT = 493, 256, 4
-SHAPES = [("W1", (HID, IN)), ("b1", (HID,)), ("W2", (HID, HID)), ("b2", (HID,)),
-          ("W3", (HID, HID)), ("b3", (HID,)), ("W4", (OUT, HID)), ("b4", (OUT,))]
+
+
+def n_in(n_cam: int) -> int:
+    return 121 * n_cam + 2 * n_cam + 1
+
+
+def shapes(n_in_: int = IN):
+    return [("W1", (HID, n_in_)), ("b1", (HID,)), ("W2", (HID, HID)), ("b2", (HID,)),
+            ("W3", (HID, HID)), ("b3", (HID,)), ("W4", (OUT, HID)), ("b4", (OUT,))]
+
+
+SHAPES = shapes(IN)
 N_PARAMS = sum(int(np.prod(s)) for _, s in SHAPES)
+_REST = N_PARAMS - HID * IN
+
+
+def shapes_of(flat) -> list:
+    """The layer shapes of a flat parameter array (its first layer's width from its size)."""
+    return shapes((len(flat) - _REST) // HID)
 
 
 def unpack(flat: np.ndarray) -> dict:
     out, off = {}, 0
-    for name, shp in SHAPES:
+    for name, shp in shapes_of(flat):
         k = int(np.prod(shp))
         out[name] = flat[off:off + k].reshape(shp).astype(np.float32)
         off += k
@@ -32,7 +49,8 @@ def unpack(flat: np.ndarray) -> dict:
 
 
 def pack(p: dict) -> np.ndarray:
-    return np.concatenate([p[name].ravel() for name, _ in SHAPES]).astype(np.float32)
+    return np.concatenate([p[name].ravel() for name, _ in shapes(p["W1"].shape[1])]).astype(
+        np.float32)
 
 
 def bf16(a: np.ndarray) -> np.ndarray:
@@ -64,7 +82,7 @@ def forward(flat: np.ndarray, x: np.ndarray, rounding: bool = True):
     p = {k: v.astype(dt) for k, v in unpack(np.asarray(flat, np.float64)).items()}
     if not rounding:  # unpack rounds to f32; take the float64 values
         off = 0
-        for name, shp in SHAPES:
+        for name, shp in shapes_of(flat):
             k = int(np.prod(shp))
             p[name] = np.asarray(flat[off:off + k], np.float64).reshape(shp)
             off += k
@@ -113,7 +131,7 @@ def backward(flat: np.ndarray, x: np.ndarray, t: np.ndarray, ghost_weight: float
     dz1 = (r(dz2) @ c["W2"]) * gelu_grad(c["z1"])
     g["W1"] = r(dz1).T @ c["xb"]
     g["b1"] = dz1.sum(0)
-    return loss, np.concatenate([g[name].ravel() for name, _ in SHAPES])
+    return loss, np.concatenate([g[name].ravel() for name, _ in shapes_of(flat)])
 
 
 def adam(flat, grad, m, v, t, lr, b1=0.9, b2=0.999, eps=1e-8):
@@ -123,10 +141,10 @@ def adam(flat, grad, m, v, t, lr, b1=0.9, b2=0.999, eps=1e-8):
     return flat.astype(np.float32), m, v
 
 
-def init(seed: int = 0) -> np.ndarray:
+def init(seed: int = 0, n_in_: int = IN) -> np.ndarray:
     rng = np.random.default_rng(seed)
     p = {}
-    for name, shp in SHAPES:
+    for name, shp in shapes(n_in_):
         if name.startswith("b"):
             p[name] = np.zeros(shp, np.float32)
         else:

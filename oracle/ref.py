@@ -86,6 +86,8 @@ class RefOracle:
             raise RuntimeError(lib.oref_last_error().decode())
         s = settings
         lim = limit if limit is not None else scene.volume
+        if otf is None and getattr(scene, "otf_table", None) is not None:
+            otf, otf_n = scene.otf_table, scene.otf_n
         self.otf = otf if otf is not None else otf_table(self.n_cam, scene.otf_abc, n=otf_n)
         self.otf = np.ascontiguousarray(self.otf, dtype=np.float64)
         cfg = _Cfg(n_cam=self.n_cam, min_obj_int=s.min_obj_int, radius_obj=s.radius_obj,
@@ -128,6 +130,10 @@ class RefOracle:
         H = (C.c_int * len(d))(*[im.shape[0] for im in d])
         W = (C.c_int * len(d))(*[im.shape[1] for im in d])
         return d, _ptr_array(d), H, W
+
+    def srand(self, seed: int):
+        """Seed the C library's rand() (the polynomial camera's Newton start points)."""
+        self.lib.oref_srand(C.c_uint(seed))
 
     def set_active(self, active: Sequence[int]):
         a = (C.c_int * self.n_cam)(*[int(x) for x in active])
@@ -227,7 +233,8 @@ class RefSTB:
     reference-format config files written by synth.write_stb_config."""
 
     def __init__(self, seq, ipr_settings, stb_settings, workdir: Optional[str] = None,
-                 threads: int = 0, n_frames: Optional[int] = None, otf_override: bool = True):
+                 threads: int = 0, n_frames: Optional[int] = None, otf_override: bool = True,
+                 match_cam_count: Optional[int] = None):
         from pyopenlpt_b200.synth import write_stb_config
         self.lib = lib = C.CDLL(REF_SO)
         lib.oref_stb_new.restype = C.c_void_p
@@ -246,6 +253,8 @@ class RefSTB:
         self.h = lib.oref_stb_new(main.encode(), otf.encode())
         if not self.h:
             raise RuntimeError(lib.oref_last_error().decode())
+        if match_cam_count is not None:
+            lib.oref_stb_set_match_cam_count(C.c_void_p(self.h), int(match_cam_count))
 
     def frame(self, t: int, imgs=None):
         imgs = imgs if imgs is not None else self.seq.frames[t]

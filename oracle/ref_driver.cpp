@@ -132,6 +132,9 @@ extern "C" {
 
 const char* oref_last_error() { return g_last_error.c_str(); }
 void oref_set_threads(int n) { omp_set_num_threads(n > 0 ? n : omp_get_num_procs()); }
+// Seeds the C library's rand(), which Camera::polyImgToWorld draws its Newton start
+// point from (src/srcMath/Camera.cpp:1176-1180).
+void oref_srand(unsigned seed) { srand(seed); }
 int oref_max_threads() { return omp_get_max_threads(); }
 
 // ---------------------------------------------------------------- results
@@ -512,6 +515,13 @@ void* oref_stb_new(const char* main_cfg, const char* otf_file) {
 }
 
 void oref_stb_free(void* h) { delete static_cast<RefStb*>(h); }
+
+// SMParam::match_cam_count after the config is read (the tracer config file has no
+// line for it; readCommonConfig caps the default of 4 at n_cam, Config.cpp:222-224).
+void oref_stb_set_match_cam_count(void* h, int n) {
+  auto* r = static_cast<RefStb*>(h);
+  DebugAccess_STB::cfg(*r->stb)._sm_param.match_cam_count = n;
+}
 
 // The tracer config's OTF table [4][n_cam][n_grid] (a, b, c, alpha); returns n_grid.
 int oref_stb_otf(void* h, double* out) {

@@ -24,7 +24,11 @@ _u16p = C.POINTER(C.c_uint16)
 _i64p = C.POINTER(C.c_int64)
 _i32p = C.POINTER(C.c_int32)
 
-MLP_IN, MLP_OUT, MLP_PARAMS = 493, 4, 259076
+MLP_IN, MLP_OUT, MLP_PARAMS = 493, 4, 259076   # the network of a 4-camera rig
+
+# olpt_near_record: one near-tolerance 2D test of stereo matching
+NEAR_RECORD = np.dtype([("kind", "<i4"), ("n_chosen", "<i4"), ("cam", "<i4"), ("id", "<i4"),
+                        ("other_cam", "<i4"), ("other_id", "<i4"), ("margin_px", "<f8")])
 
 
 class LearnedParams(C.Structure):
@@ -93,6 +97,16 @@ def lib():
     return _lib
 
 
+def mlp_dims(n_cam: int):
+    """(n_in, n_params) of the learned proposal's network for a rig of n_cam cameras."""
+    n_in = C.c_int()
+    n_p = C.c_int64()
+    rc = lib().olpt_mlp_dims(int(n_cam), C.byref(n_in), C.byref(n_p))
+    if rc:
+        raise OlptError(rc, f"mlp_dims: unsupported camera count {n_cam}")
+    return n_in.value, n_p.value
+
+
 def launch_count() -> int:
     """Kernel launches issued by libolpt_cuda.so in this process."""
     L = lib()
@@ -123,6 +137,29 @@ def camera_desc_from_pinhole(cam, active: bool = True) -> CameraDesc:
         d.t_vec[i] = T[i]
         d.t_inv[i] = Ti[i]
     return d
+
+
+def camera_desc_from_poly(cam, active: bool = True) -> CameraDesc:
+    """A POLYNOMIAL camera (n_coeff x 4 tables of coefficient, x, y, z powers); the
+    descriptor keeps its coefficient arrays alive."""
+    d = CameraDesc()
+    d.type = 1
+    d.n_row, d.n_col, d.is_active = cam.n_row, cam.n_col, int(active)
+    d.ref_plane = int(cam.ref_plane)
+    d.plane[0], d.plane[1] = float(cam.plane[0]), float(cam.plane[1])
+    u = np.ascontiguousarray(cam.u_coeffs, dtype=np.float64)
+    v = np.ascontiguousarray(cam.v_coeffs, dtype=np.float64)
+    d.n_coeff = len(u)
+    d.u_coeffs, d.v_coeffs = _p(u), _p(v)
+    d._keep = (u, v)
+    return d
+
+
+def camera_desc(cam, active: bool = True) -> CameraDesc:
+    """Descriptor of a synth camera of either model."""
+    if hasattr(cam, "u_coeffs"):
+        return camera_desc_from_poly(cam, active)
+    return camera_desc_from_pinhole(cam, active)
 
 
 class Context:
@@ -247,6 +284,23 @@ class Context:
         nm = C.c_int64()
         self._check(self.L.olpt_stereo_match(self.h, C.byref(params), C.byref(nc), C.byref(nm)))
         return nc.value, nm.value
+
+    def near_log_enable(self, band_px: float, capacity: int = 1 << 20):
+        """Log every stereo 2D test whose distance is within band_px of tol_2d_px."""
+        self._check(self.L.olpt_stereo_near_log_enable(self.h, C.c_double(band_px),
+                                                       C.c_int64(capacity)))
+
+    def near_log(self, cap: int = 1 << 20):
+        """(records, total): the logged near-tolerance tests (NEAR_RECORD array) and how
+        many were seen since the last enable / reset."""
+        out = np.zeros(cap, dtype=NEAR_RECORD)
+        n = C.c_int64()
+        self._check(self.L.olpt_stereo_near_log_read(self.h, out.ctypes.data_as(C.c_void_p),
+                                                     C.c_int64(cap), C.byref(n)))
+        return out[:min(cap, n.value)], n.value
+
+    def near_log_reset(self):
+        self._check(self.L.olpt_stereo_near_log_reset(self.h))
 
     def candidates(self, n: int):
         ids = np.empty((n, self.n_cam), dtype=np.int32)
@@ -389,21 +443,26 @@ class Context:
         return s.value or 0
 
     # ---------------------------------------------------------------- learned proposal
+    def mlp_dims(self):
+        """(n_in, n_params) of the network for this context's camera count."""
+        cams = getattr(self, "n_cam", 0)
+        return mlp_dims(cams if cams >= 2 else 4)
+
     def mlp_init(self, seed: int = 0):
         self._check(self.L.olpt_mlp_init(self.h, C.c_uint64(seed)))
 
     def mlp_set_params(self, flat: np.ndarray):
         flat = np.ascontiguousarray(flat, dtype=np.float32)
-        assert flat.size == MLP_PARAMS
+        assert flat.size == self.mlp_dims()[1]
         self._check(self.L.olpt_mlp_set_params(self.h, _p(flat, _fp)))
 
     def mlp_get_params(self) -> np.ndarray:
-        out = np.empty(MLP_PARAMS, np.float32)
+        out = np.empty(self.mlp_dims()[1], np.float32)
         self._check(self.L.olpt_mlp_get_params(self.h, _p(out, _fp)))
         return out
 
     def mlp_forward(self, x: np.ndarray) -> np.ndarray:
-        x = np.ascontiguousarray(x, dtype=np.float32).reshape(-1, MLP_IN)
+        x = np.ascontiguousarray(x, dtype=np.float32).reshape(-1, self.mlp_dims()[0])
         out = np.empty((len(x), MLP_OUT), np.float32)
         self._check(self.L.olpt_mlp_forward(self.h, C.c_int64(len(x)), _p(x, _fp), _p(out, _fp), 0))
         return out
@@ -415,10 +474,10 @@ class Context:
 
     def mlp_train_step(self, x: np.ndarray, t: np.ndarray, lr: float = 1e-3,
                        ghost_weight: float = 1.0, update: bool = True, want_grad: bool = False):
-        x = np.ascontiguousarray(x, dtype=np.float32).reshape(-1, MLP_IN)
+        x = np.ascontiguousarray(x, dtype=np.float32).reshape(-1, self.mlp_dims()[0])
         t = np.ascontiguousarray(t, dtype=np.float32).reshape(-1, MLP_OUT)
         loss = C.c_double()
-        g = np.empty(MLP_PARAMS, np.float32) if want_grad else None
+        g = np.empty(self.mlp_dims()[1], np.float32) if want_grad else None
         self._check(self.L.olpt_mlp_train_step(self.h, C.c_int64(len(x)), _p(x, _fp), _p(t, _fp), 0,
                                                C.c_double(lr), C.c_double(ghost_weight),
                                                int(update), C.byref(loss), _p(g, _fp)))
@@ -427,7 +486,7 @@ class Context:
     def mlp_train(self, x: np.ndarray, t: np.ndarray, steps: int, batch: int = 8192,
                   lr: float = 2e-3, ghost_weight: float = 1.0, seed: int = 0) -> np.ndarray:
         """olpt_mlp_train: the dataset goes to the device once; returns the step losses."""
-        x = np.ascontiguousarray(x, dtype=np.float32).reshape(-1, MLP_IN)
+        x = np.ascontiguousarray(x, dtype=np.float32).reshape(-1, self.mlp_dims()[0])
         t = np.ascontiguousarray(t, dtype=np.float32).reshape(-1, MLP_OUT)
         losses = np.zeros(max(steps, 1), np.float32)
         self._check(self.L.olpt_mlp_train(self.h, C.c_int64(len(x)), _p(x, _fp), _p(t, _fp), 0,
@@ -446,7 +505,7 @@ class Context:
 
     def mlp_features(self, params: ShakeParams) -> np.ndarray:
         n = self.n_objects()
-        x = np.zeros((n, MLP_IN), np.float32)
+        x = np.zeros((n, self.mlp_dims()[0]), np.float32)
         if n:
             self._check(self.L.olpt_mlp_features(self.h, C.byref(params), _p(x, _fp), 0))
         return x

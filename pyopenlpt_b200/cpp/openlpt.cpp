@@ -774,6 +774,16 @@ bool TracerConfig::readConfig(const std::string& filepath, BasicSetting& setting
   return true;
 }
 
+const TracerConfig& tracer_config(const ObjectConfig& cfg) {
+  if (cfg.kind() != ObjectKind::Tracer)
+    throw FatalError(OLPT_ERR_UNSUPPORTED, "only tracer objects are supported by this library");
+  return static_cast<const TracerConfig&>(cfg);
+}
+
+TracerConfig& tracer_config(ObjectConfig& cfg) {
+  return const_cast<TracerConfig&>(tracer_config(static_cast<const ObjectConfig&>(cfg)));
+}
+
 std::unique_ptr<Object3D> TracerConfig::creatObject3D(const Pt3D& center) const {
   auto t = std::make_unique<Tracer3D>();
   t->_pt_center = center;
@@ -808,7 +818,8 @@ olpt_ipr_params TracerConfig::iprParams() const {
 
 // ---------------------------------------------------------------- hot path
 std::vector<std::unique_ptr<Object2D>> ObjectFinder2D::findObject2D(const Image& img,
-                                                                    const TracerConfig& cfg) {
+                                                                    const ObjectConfig& ocfg) {
+  const TracerConfig& cfg = tracer_config(ocfg);
   olpt_ctx* ctx = default_context();
   olpt_camera_desc d = dummy_camera(img.getDimRow(), img.getDimCol());
   check(ctx, olpt_cameras_upload(ctx, &d, 1));
@@ -830,8 +841,8 @@ std::vector<std::unique_ptr<Object2D>> ObjectFinder2D::findObject2D(const Image&
 
 StereoMatch::StereoMatch(const std::vector<Camera>& cams,
                          const std::vector<std::vector<std::unique_ptr<Object2D>>>& obj2d_list,
-                         const TracerConfig& cfg)
-    : cams_(cams), obj2d_(obj2d_list), cfg_(cfg) {
+                         const ObjectConfig& cfg)
+    : cams_(cams), obj2d_(obj2d_list), cfg_(tracer_config(cfg)) {
   if (obj2d_list.size() != cams.size())
     throw FatalError(OLPT_ERR_INVALID_ARG, "StereoMatch: obj2d_list size must equal n_cams");
 }
@@ -945,7 +956,8 @@ std::vector<Image> Shake::calResidualImage(const std::vector<std::unique_ptr<Obj
   return residual_images(ctx, img_orig);
 }
 
-std::vector<std::unique_ptr<Object3D>> IPR::runIPR(TracerConfig& cfg, std::vector<Image> images) {
+std::vector<std::unique_ptr<Object3D>> IPR::runIPR(ObjectConfig& ocfg, std::vector<Image> images) {
+  const TracerConfig& cfg = tracer_config(ocfg);
   olpt_ctx* ctx = default_context();
   upload_rig(ctx, cams_, &cfg._otf);
   upload_images(ctx, images);
@@ -975,7 +987,7 @@ std::vector<std::unique_ptr<Object3D>> IPR::runIPR(TracerConfig& cfg, std::vecto
 // Error and Ncam columns the rows do not have), then Tracer3D::saveObject3D rows in
 // the stream's default format.
 void IPR::saveObjInfo(const std::string& file, const std::vector<std::unique_ptr<Object3D>>& objs,
-                      const TracerConfig&) const {
+                      const ObjectConfig&) const {
   std::ofstream out(file);
   if (!out) throw FatalError(OLPT_ERR_INVALID_ARG, "Cannot open file " + file);
   out << "WorldX,WorldY,WorldZ,Error,Ncam";

@@ -205,35 +205,53 @@ struct IPRParam {
   int64_t n_obj2d_process_max = 200000;
 };
 
-// TracerConfig (inc/libSTB/Config.h:182-205): readCommonConfig + tracer fields; the
-// OTF is estimated from the first frames as in TracerConfig::readConfig.
-struct TracerConfig {
+enum class ObjectKind { Tracer = 0, Bubble = 1 };
+
+// ObjectConfig (inc/libSTB/Config.h:154-189): the parameters every object type
+// shares (STB, shake, predictive field, IPR, stereo matching).  The hot-path classes
+// take it by reference as the reference's do; only tracers are built here, so they
+// check the kind and throw FatalError(OLPT_ERR_UNSUPPORTED) for any other.
+struct ObjectConfig {
   STBParam _stb_param;
   ShakeParam _shake_param;
   PFParam _pf_param;
   SMParam _sm_param;
   IPRParam _ipr_param;
+  // precision of the shake and residual: 0 = FP32 (default), 1 = FP64 (the reference's)
+  int precision = 0;
+  virtual ~ObjectConfig() = default;
+  virtual bool readConfig(const std::string& filepath, BasicSetting& settings) = 0;
+  virtual ObjectKind kind() const = 0;
+  virtual std::unique_ptr<Object3D> creatObject3D(const Pt3D& center) const = 0;
+};
+
+// TracerConfig (inc/libSTB/Config.h:191-205): readCommonConfig + tracer fields; the
+// OTF is estimated from the first frames as in TracerConfig::readConfig.
+struct TracerConfig : ObjectConfig {
   int _min_obj_int = 30;
   double _radius_obj = 2;
   OTF _otf;
-  bool readConfig(const std::string& filepath, BasicSetting& settings);
-  std::unique_ptr<Object3D> creatObject3D(const Pt3D& center) const;
-  // precision of the shake and residual: 0 = FP32 (default), 1 = FP64
-  int precision = 0;
+  bool readConfig(const std::string& filepath, BasicSetting& settings) override;
+  ObjectKind kind() const override { return ObjectKind::Tracer; }
+  std::unique_ptr<Object3D> creatObject3D(const Pt3D& center) const override;
   olpt_ipr_params iprParams() const;
 };
+
+// The tracer configuration behind an ObjectConfig reference; FatalError for other kinds.
+const TracerConfig& tracer_config(const ObjectConfig& cfg);
+TracerConfig& tracer_config(ObjectConfig& cfg);
 
 // ---------------------------------------------------------------- hot path
 class ObjectFinder2D {
  public:
-  std::vector<std::unique_ptr<Object2D>> findObject2D(const Image& img, const TracerConfig& cfg);
+  std::vector<std::unique_ptr<Object2D>> findObject2D(const Image& img, const ObjectConfig& cfg);
 };
 
 class StereoMatch {
  public:
   StereoMatch(const std::vector<Camera>& cams,
               const std::vector<std::vector<std::unique_ptr<Object2D>>>& obj2d_list,
-              const TracerConfig& cfg);
+              const ObjectConfig& cfg);
   std::vector<std::unique_ptr<Object3D>> match() const;
 
  private:
@@ -244,7 +262,8 @@ class StereoMatch {
 
 class Shake {
  public:
-  Shake(const std::vector<Camera>& cams, const TracerConfig& cfg) : cams_(cams), cfg_(cfg) {}
+  Shake(const std::vector<Camera>& cams, const ObjectConfig& cfg)
+      : cams_(cams), cfg_(tracer_config(cfg)) {}
   std::vector<ObjFlag> runShake(std::vector<std::unique_ptr<Object3D>>& objs,
                                 const std::vector<Image>& img_orig);
   std::vector<Image> calResidualImage(const std::vector<std::unique_ptr<Object3D>>& objs,
@@ -259,9 +278,9 @@ class Shake {
 class IPR {
  public:
   explicit IPR(std::vector<Camera>& cams) : cams_(cams) {}
-  std::vector<std::unique_ptr<Object3D>> runIPR(TracerConfig& cfg, std::vector<Image> images);
+  std::vector<std::unique_ptr<Object3D>> runIPR(ObjectConfig& cfg, std::vector<Image> images);
   void saveObjInfo(const std::string& file, const std::vector<std::unique_ptr<Object3D>>& objs,
-                   const TracerConfig& cfg) const;
+                   const ObjectConfig& cfg) const;
 
  private:
   std::vector<Camera>& cams_;

@@ -1,6 +1,6 @@
-// Python module of the drop-in classes (module pyopenlpt_b200._openlpt; the shim
-// pyopenlpt_b200/openlpt.py re-exports it like the reference's openlpt.py does for
-// pyopenlpt).  Class and method names follow the reference's bindings
+// Python module of the drop-in classes, under the reference's module name pyopenlpt
+// (built as pyopenlpt_b200/pyopenlpt*.so; the shim pyopenlpt_b200/openlpt.py
+// re-exports it as the reference's openlpt.py does).  Class and method names follow the reference's bindings
 // (src/pybind_OpenLPT/py*.cpp) for the reconstruction path: Camera, OTF, Image,
 // ImageIO, Pt2D, Pt3D, Tracer2D, Tracer3D, ObjFlag, BasicSetting, TracerConfig (+
 // parameter structs), ObjectFinder2D, StereoMatch, Shake (runShake returns
@@ -114,7 +114,7 @@ struct PyIPR {
 
 }  // namespace
 
-PYBIND11_MODULE(_openlpt, m) {
+PYBIND11_MODULE(pyopenlpt, m) {
   m.doc() = "B200 drop-in for the OpenLPT reconstruction path (IPR + Shake-the-Box)";
   py::register_exception<FatalError>(m, "FatalError", PyExc_RuntimeError);
 
@@ -293,18 +293,23 @@ PYBIND11_MODULE(_openlpt, m) {
       .def_readwrite("n_loop_ipr", &IPRParam::n_loop_ipr)
       .def_readwrite("n_loop_ipr_reduced", &IPRParam::n_loop_ipr_reduced)
       .def_readwrite("n_obj2d_process_max", &IPRParam::n_obj2d_process_max);
-  py::class_<TracerConfig>(m, "TracerConfig")
+  py::enum_<ObjectKind>(m, "ObjectKind")
+      .value("Tracer", ObjectKind::Tracer)
+      .value("Bubble", ObjectKind::Bubble);
+  py::class_<ObjectConfig>(m, "ObjectConfig")
+      .def("kind", &ObjectConfig::kind)
+      .def_readwrite("_stb_param", &ObjectConfig::_stb_param)
+      .def_readwrite("_shake_param", &ObjectConfig::_shake_param)
+      .def_readwrite("_pf_param", &ObjectConfig::_pf_param)
+      .def_readwrite("_sm_param", &ObjectConfig::_sm_param)
+      .def_readwrite("_ipr_param", &ObjectConfig::_ipr_param)
+      .def_readwrite("precision", &ObjectConfig::precision);
+  py::class_<TracerConfig, ObjectConfig>(m, "TracerConfig")
       .def(py::init<>())
       .def("readConfig", &TracerConfig::readConfig, py::arg("filepath"), py::arg("settings"))
-      .def_readwrite("_stb_param", &TracerConfig::_stb_param)
-      .def_readwrite("_shake_param", &TracerConfig::_shake_param)
-      .def_readwrite("_pf_param", &TracerConfig::_pf_param)
-      .def_readwrite("_sm_param", &TracerConfig::_sm_param)
-      .def_readwrite("_ipr_param", &TracerConfig::_ipr_param)
       .def_readwrite("_min_obj_int", &TracerConfig::_min_obj_int)
       .def_readwrite("_radius_obj", &TracerConfig::_radius_obj)
-      .def_readwrite("_otf", &TracerConfig::_otf)
-      .def_readwrite("precision", &TracerConfig::precision);
+      .def_readwrite("_otf", &TracerConfig::_otf);
 
   py::class_<ObjectFinder2D>(m, "ObjectFinder2D")
       .def(py::init<>())

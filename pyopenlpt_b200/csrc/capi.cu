@@ -580,6 +580,51 @@ olpt_status_t olpt_stereo_match(olpt_ctx* ctx, const olpt_sm_params* p, int64_t*
   });
 }
 
+olpt_status_t olpt_stereo_near_log_enable(olpt_ctx* ctx, double band_px, int64_t capacity) {
+  return guard(ctx, [&] {
+    OLPT_REQUIRE(band_px >= 0.0 && capacity >= 0, OLPT_ERR_INVALID_ARG,
+                 "band_px and capacity must be non-negative");
+    StereoWork& W = ctx->sm;
+    W.near_band = band_px;
+    W.near_cap = band_px > 0.0 ? capacity : 0;
+    if (band_px > 0.0) {
+      W.near_rec.ensure(sizeof(olpt_near_record) * (size_t)(capacity + 1), ctx->stream);
+      W.near_count.ensure(sizeof(unsigned long long), ctx->stream);
+      OLPT_CUDA(cudaMemsetAsync(W.near_count.p, 0, sizeof(unsigned long long), ctx->stream));
+      OLPT_CUDA(cudaStreamSynchronize(ctx->stream));
+    }
+  });
+}
+
+olpt_status_t olpt_stereo_near_log_reset(olpt_ctx* ctx) {
+  return guard(ctx, [&] {
+    if (ctx->sm.near_band > 0.0) {
+      OLPT_CUDA(cudaMemsetAsync(ctx->sm.near_count.p, 0, sizeof(unsigned long long), ctx->stream));
+      OLPT_CUDA(cudaStreamSynchronize(ctx->stream));
+    }
+  });
+}
+
+olpt_status_t olpt_stereo_near_log_read(olpt_ctx* ctx, olpt_near_record* out, int64_t cap,
+                                        int64_t* n_total) {
+  return guard(ctx, [&] {
+    OLPT_REQUIRE(cap >= 0 && (cap == 0 || out), OLPT_ERR_INVALID_ARG, "null output");
+    StereoWork& W = ctx->sm;
+    unsigned long long n = 0;
+    if (W.near_band > 0.0) {
+      OLPT_CUDA(cudaMemcpyAsync(&n, W.near_count.p, sizeof(n), cudaMemcpyDeviceToHost, ctx->stream));
+      OLPT_CUDA(cudaStreamSynchronize(ctx->stream));
+      const int64_t k = std::min<int64_t>({(int64_t)n, W.near_cap, cap});
+      if (k > 0) {
+        OLPT_CUDA(cudaMemcpyAsync(out, W.near_rec.p, sizeof(olpt_near_record) * (size_t)k,
+                                  cudaMemcpyDeviceToHost, ctx->stream));
+        OLPT_CUDA(cudaStreamSynchronize(ctx->stream));
+      }
+    }
+    if (n_total) *n_total = (int64_t)n;
+  });
+}
+
 olpt_status_t olpt_get_candidates(olpt_ctx* ctx, int32_t* ids, double* e_check, double* xyz) {
   return guard(ctx, [&] {
     StereoResult& r = ctx->sm_result;
@@ -1012,6 +1057,14 @@ olpt_status_t olpt_stb_load_tracks(olpt_ctx* ctx, int which, const char* path) {
 
 
 // ---------------------------------------------------------------- learned proposal
+olpt_status_t olpt_mlp_dims(int n_cam, int* n_in, int64_t* n_params) {
+  if (n_cam < 2 || n_cam > kMlpMaxCams) return OLPT_ERR_INVALID_ARG;
+  const MlpDims d = mlp_dims(n_cam);
+  if (n_in) *n_in = d.in;
+  if (n_params) *n_params = d.params;
+  return OLPT_OK;
+}
+
 olpt_status_t olpt_mlp_init(olpt_ctx* ctx, uint64_t seed) {
   return guard(ctx, [&] { mlp_init(ctx, seed); });
 }
@@ -1040,11 +1093,11 @@ olpt_status_t olpt_mlp_forward(olpt_ctx* ctx, int64_t n, const float* x, float* 
     cudaStream_t s = ctx->stream;
     const float* dx = x;
     if (!on_device) {
-      W.xin.ensure((size_t)n * OLPT_MLP_IN * 4, s);
-      OLPT_CUDA(cudaMemcpyAsync(W.xin.p, x, (size_t)n * OLPT_MLP_IN * 4, cudaMemcpyHostToDevice, s));
+      W.xin.ensure((size_t)n * ctx->mlp.dims.in * 4, s);
+      OLPT_CUDA(cudaMemcpyAsync(W.xin.p, x, (size_t)n * ctx->mlp.dims.in * 4, cudaMemcpyHostToDevice, s));
       dx = W.xin.as<float>();
     }
-    W.x.ensure((size_t)n * kMlpInPad * 2, s);
+    W.x.ensure((size_t)n * ctx->mlp.dims.in_pad * 2, s);
     W.o.ensure((size_t)n * kMlpOut * 4, s);
     mlp_input_device(ctx, dx, n, W.x.as<__nv_bfloat16>());
     mlp_infer_device(ctx, W.x.as<__nv_bfloat16>(), n, W.o.as<float>());
@@ -1065,9 +1118,9 @@ olpt_status_t olpt_mlp_train_step(olpt_ctx* ctx, int64_t n, const float* x, cons
     const float* dx = x;
     const float* dt = targets;
     if (!on_device) {
-      W.xin.ensure((size_t)n * OLPT_MLP_IN * 4, s);
+      W.xin.ensure((size_t)n * ctx->mlp.dims.in * 4, s);
       W.tgt.ensure((size_t)n * kMlpOut * 4, s);
-      OLPT_CUDA(cudaMemcpyAsync(W.xin.p, x, (size_t)n * OLPT_MLP_IN * 4, cudaMemcpyHostToDevice, s));
+      OLPT_CUDA(cudaMemcpyAsync(W.xin.p, x, (size_t)n * ctx->mlp.dims.in * 4, cudaMemcpyHostToDevice, s));
       OLPT_CUDA(cudaMemcpyAsync(W.tgt.p, targets, (size_t)n * kMlpOut * 4, cudaMemcpyHostToDevice,
                                 s));
       dx = W.xin.as<float>();
@@ -1076,7 +1129,7 @@ olpt_status_t olpt_mlp_train_step(olpt_ctx* ctx, int64_t n, const float* x, cons
     const double l = mlp_train_device(ctx, dx, dt, n, lr, ghost_weight, update != 0);
     if (loss) *loss = l;
     if (grad) {
-      OLPT_CUDA(cudaMemcpyAsync(grad, W.grad.p, (size_t)kMlpParams * 4, cudaMemcpyDeviceToHost, s));
+      OLPT_CUDA(cudaMemcpyAsync(grad, W.grad.p, (size_t)ctx->mlp.dims.params * 4, cudaMemcpyDeviceToHost, s));
       OLPT_CUDA(cudaStreamSynchronize(s));
     }
   });
@@ -1093,9 +1146,9 @@ olpt_status_t olpt_mlp_train(olpt_ctx* ctx, int64_t n, const float* x, const flo
     const float* dx = x;
     const float* dt = targets;
     if (!on_device) {
-      W.ds_x.ensure((size_t)n * OLPT_MLP_IN * 4, s);
+      W.ds_x.ensure((size_t)n * ctx->mlp.dims.in * 4, s);
       W.ds_t.ensure((size_t)n * kMlpOut * 4, s);
-      OLPT_CUDA(cudaMemcpyAsync(W.ds_x.p, x, (size_t)n * OLPT_MLP_IN * 4, cudaMemcpyHostToDevice, s));
+      OLPT_CUDA(cudaMemcpyAsync(W.ds_x.p, x, (size_t)n * ctx->mlp.dims.in * 4, cudaMemcpyHostToDevice, s));
       OLPT_CUDA(cudaMemcpyAsync(W.ds_t.p, targets, (size_t)n * kMlpOut * 4, cudaMemcpyHostToDevice,
                                 s));
       dx = W.ds_x.as<float>();
@@ -1117,15 +1170,15 @@ olpt_status_t olpt_mlp_features(olpt_ctx* ctx, const olpt_shake_params* p, float
     residual_all_device(ctx, sp);
     MlpWork& W = ctx->mlp;
     cudaStream_t s = ctx->stream;
-    W.x.ensure((size_t)n * kMlpInPad * 2, s);
+    W.x.ensure((size_t)n * ctx->mlp.dims.in_pad * 2, s);
     float* f = x;
     if (!on_device) {
-      W.xin.ensure((size_t)n * OLPT_MLP_IN * 4, s);
+      W.xin.ensure((size_t)n * ctx->mlp.dims.in * 4, s);
       f = W.xin.as<float>();
     }
     mlp_features_device(ctx, sp, W.x.as<__nv_bfloat16>(), f);
     if (!on_device)
-      OLPT_CUDA(cudaMemcpyAsync(x, f, (size_t)n * OLPT_MLP_IN * 4, cudaMemcpyDeviceToHost, s));
+      OLPT_CUDA(cudaMemcpyAsync(x, f, (size_t)n * ctx->mlp.dims.in * 4, cudaMemcpyDeviceToHost, s));
     OLPT_CUDA(cudaStreamSynchronize(s));
   });
 }

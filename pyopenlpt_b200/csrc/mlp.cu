@@ -24,11 +24,11 @@ inline int nblk(int64_t n, int t = 256) { return (int)((n + t - 1) / t); }
 inline int64_t round8(int64_t n) { return (n + 7) / 8 * 8; }
 
 // ---------------------------------------------------------------- weights
-__global__ void pack_w1_kernel(const float* master, __nv_bfloat16* wb1) {
+__global__ void pack_w1_kernel(const float* w1, int in, int in_pad, __nv_bfloat16* wb1) {
   const int i = blockIdx.x * blockDim.x + threadIdx.x;
-  if (i >= kMlpHid * kMlpInPad) return;
-  const int r = i / kMlpInPad, c = i % kMlpInPad;
-  wb1[i] = __float2bfloat16_rn(c < kMlpIn ? master[kOffW1 + (int64_t)r * kMlpIn + c] : 0.0f);
+  if (i >= kMlpHid * in_pad) return;
+  const int r = i / in_pad, c = i % in_pad;
+  wb1[i] = __float2bfloat16_rn(c < in ? w1[(int64_t)r * in + c] : 0.0f);
 }
 
 __global__ void pack_sq_kernel(const float* w, __nv_bfloat16* wb, __nv_bfloat16* wt) {
@@ -41,13 +41,13 @@ __global__ void pack_sq_kernel(const float* w, __nv_bfloat16* wb, __nv_bfloat16*
 }
 
 // ---------------------------------------------------------------- inputs
-// f32 rows of kMlpIn -> bf16 rows of kMlpInPad (zero padded)
-__global__ void input_kernel(const float* xin, int64_t n, __nv_bfloat16* x) {
+// f32 rows of `in` values -> bf16 rows of in_pad (zero padded)
+__global__ void input_kernel(const float* xin, int64_t n, int in, int in_pad, __nv_bfloat16* x) {
   const int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
-  if (i >= n * kMlpInPad) return;
-  const int64_t r = i / kMlpInPad;
-  const int c = (int)(i % kMlpInPad);
-  x[i] = __float2bfloat16_rn(c < kMlpIn ? xin[r * kMlpIn + c] : 0.0f);
+  if (i >= n * in_pad) return;
+  const int64_t r = i / in_pad;
+  const int c = (int)(i % in_pad);
+  x[i] = __float2bfloat16_rn(c < in ? xin[r * in + c] : 0.0f);
 }
 
 // out[c][r] = in[r][c] for r < rows, c < cols (32 x 32 tiles through shared memory)
@@ -71,11 +71,11 @@ __global__ void transpose_kernel(const __nv_bfloat16* in, int64_t rows, int cols
 
 // ---------------------------------------------------------------- head (256 -> 4)
 // one warp per row: o = W4 h3 + b4
-__global__ void head_fwd_kernel(const __nv_bfloat16* h3, int64_t n, const float* master, float* o) {
+__global__ void head_fwd_kernel(const __nv_bfloat16* h3, int64_t n, const float* W4,
+                                const float* b4, float* o) {
   const int64_t row = (blockIdx.x * (int64_t)blockDim.x + threadIdx.x) >> 5;
   const int lane = threadIdx.x & 31;
   if (row >= n) return;
-  const float* W4 = master + kOffW4;
   float acc[kMlpOut] = {0, 0, 0, 0};
   for (int k = lane; k < kMlpHid; k += 32) {
     const float h = __bfloat162float(h3[row * kMlpHid + k]);
@@ -88,7 +88,7 @@ __global__ void head_fwd_kernel(const __nv_bfloat16* h3, int64_t n, const float*
     for (int off = 16; off > 0; off >>= 1) v += __shfl_xor_sync(0xffffffffu, v, off);
     acc[j] = v;
   }
-  if (lane < kMlpOut) o[row * kMlpOut + lane] = acc[lane] + master[kOffB4 + lane];
+  if (lane < kMlpOut) o[row * kMlpOut + lane] = acc[lane] + b4[lane];
 }
 
 // loss per row: (1 - ghost) * mean_d (o_d - t_d)^2 + w * BCE(o_3, ghost); dout = dL/do / n.
@@ -134,12 +134,11 @@ __global__ void sum_double_kernel(const double* part, int n, double* out, double
 
 // dZ3 = (dout W4) * gelu'(z3): 32 rows per block, 256 threads (one per column);
 // writes f32 and bf16 rows and the bf16 transpose (ld_t)
-__global__ void head_bwd_kernel(const float* dout, const float* master, const float* z3, int64_t n,
+__global__ void head_bwd_kernel(const float* dout, const float* W4, const float* z3, int64_t n,
                                 float* dzf, __nv_bfloat16* dzb, __nv_bfloat16* dzt, int64_t ld_t) {
   __shared__ __nv_bfloat16 tile[32][kMlpHid + 8];
   const int k = threadIdx.x;
   const int64_t r0 = (int64_t)blockIdx.x * 32;
-  const float* W4 = master + kOffW4;
   const float w0 = W4[k], w1 = W4[kMlpHid + k], w2 = W4[2 * kMlpHid + k], w3 = W4[3 * kMlpHid + k];
   for (int rr = 0; rr < 32; ++rr) {
     const int64_t r = r0 + rr;
@@ -238,37 +237,41 @@ __device__ __forceinline__ uint64_t mix64(uint64_t z) {  // splitmix64 finaliser
 }
 
 // mini-batch rows drawn uniformly with replacement from the resident dataset
-__global__ void sample_kernel(const float* x, const float* t, int64_t n, int batch, uint64_t seed,
-                              int64_t step, float* xb, float* tb) {
+__global__ void sample_kernel(const float* x, const float* t, int64_t n, int in, int batch,
+                              uint64_t seed, int64_t step, float* xb, float* tb) {
   const int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
-  if (i >= (int64_t)batch * kMlpIn) return;
-  const int64_t r = i / kMlpIn;
-  const int c = (int)(i % kMlpIn);
+  if (i >= (int64_t)batch * in) return;
+  const int64_t r = i / in;
+  const int c = (int)(i % in);
   const int64_t src = (int64_t)(mix64(seed ^ ((uint64_t)step << 32) ^ (uint64_t)r) % (uint64_t)n);
-  xb[i] = x[src * kMlpIn + c];
+  xb[i] = x[src * in + c];
   if (c < kMlpOut) tb[r * kMlpOut + c] = t[src * kMlpOut + c];
 }
 
 // ---------------------------------------------------------------- features
-// one warp per object; lanes 0..3 project on their camera and evaluate the OTF there
+// the residual planes of every camera, by value
+struct PlaneSet {
+  PlaneView p[kMlpMaxCams];
+};
+
+// one warp per object; lanes 0..C-1 project on their camera and evaluate the OTF there
 template <typename Real>
 __global__ void features_kernel(const CamDev* cams, OtfView otf, const double* xyz, int64_t n,
-                                PlaneView r0, PlaneView r1, PlaneView r2, PlaneView r3, double r_px,
-                                __nv_bfloat16* x, float* f32) {
+                                const PlaneSet planes, int n_cams, int in, int in_pad,
+                                double r_px, __nv_bfloat16* x, float* f32) {
   const int64_t o = (blockIdx.x * (int64_t)blockDim.x + threadIdx.x) >> 5;
   const int lane = threadIdx.x & 31;
   if (o >= n) return;
   const double X = xyz[3 * o], Y = xyz[3 * o + 1], Z = xyz[3 * o + 2];
   double u = 0, w = 0, q[5] = {0, 0, 0, 1, 0};
-  if (lane < kMlpCams) {
+  if (lane < n_cams) {
     cam_project(cams[lane], X, Y, Z, u, w);
     otf_param(otf, lane, X, Y, Z, q);
   }
-  const PlaneView planes[kMlpCams] = {r0, r1, r2, r3};
-  constexpr int kArea = kMlpPatch * kMlpPatch;
-  __nv_bfloat16* xo = x + o * kMlpInPad;
-  float* fo = f32 ? f32 + o * kMlpIn : nullptr;
-  for (int c = 0; c < kMlpCams; ++c) {
+  constexpr int kArea = kMlpArea;
+  __nv_bfloat16* xo = x + o * in_pad;
+  float* fo = f32 ? f32 + o * in : nullptr;
+  for (int c = 0; c < n_cams; ++c) {
     const double uc = __shfl_sync(0xffffffffu, u, c), wc = __shfl_sync(0xffffffffu, w, c);
     Real qc[5];
     for (int k = 0; k < 5; ++k) qc[k] = (Real)__shfl_sync(0xffffffffu, q[k], c);
@@ -277,7 +280,7 @@ __global__ void features_kernel(const CamDev* cams, OtfView otf, const double* x
     const bool finite = isfinite(uc) && isfinite(wc) && fabs(uc) < 1e6 && fabs(wc) < 1e6;
     const int cu = finite ? (int)ru : -100000, cw = finite ? (int)rw : -100000;
     const Rect pr = finite ? roi_bound(cm.n_row, cm.n_col, uc, wc, r_px, r_px) : Rect{1, 0, 1, 0};
-    const PlaneView& P = planes[c];
+    const PlaneView& P = planes.p[c];
     const Real* res = reinterpret_cast<const Real*>(P.p);
     const int64_t rp = P.pitch / (int64_t)sizeof(Real);
     const Real inv_a = (Real)1 / (qc[0] > (Real)1e-6 ? qc[0] : (Real)1e-6);
@@ -296,7 +299,7 @@ __global__ void features_kernel(const CamDev* cams, OtfView otf, const double* x
     }
     if (lane == 0) {
       const float du = finite ? (float)(uc - ru) : 0.0f, dw = finite ? (float)(wc - rw) : 0.0f;
-      const int b = kMlpCams * kArea + 2 * c;
+      const int b = n_cams * kArea + 2 * c;
       xo[b] = __float2bfloat16_rn(du);
       xo[b + 1] = __float2bfloat16_rn(dw);
       if (fo) {
@@ -305,30 +308,31 @@ __global__ void features_kernel(const CamDev* cams, OtfView otf, const double* x
       }
     }
   }
-  for (int k = kMlpIn - 1 + lane; k < kMlpInPad; k += 32) {
-    const float val = k == kMlpIn - 1 ? 1.0f : 0.0f;
+  for (int k = in - 1 + lane; k < in_pad; k += 32) {
+    const float val = k == in - 1 ? 1.0f : 0.0f;
     xo[k] = __float2bfloat16_rn(val);
-    if (fo && k == kMlpIn - 1) fo[k] = val;
+    if (fo && k == in - 1) fo[k] = val;
   }
 }
 
 // ---------------------------------------------------------------- host helpers
 void ensure_batch(olpt_ctx* ctx, int64_t n, bool training) {
   MlpWork& W = ctx->mlp;
+  const MlpDims& D = W.dims;
   cudaStream_t s = ctx->stream;
   const int64_t m = std::max<int64_t>(n, 1);
   const int64_t lt = round8(m);
   const size_t hb = (size_t)m * kMlpHid;
-  W.x.ensure((size_t)m * kMlpInPad * 2, s);
+  W.x.ensure((size_t)m * D.in_pad * 2, s);
   W.h1.ensure(hb * 2, s);
   W.h2.ensure(hb * 2, s);
   W.h3.ensure(hb * 2, s);
   W.o.ensure((size_t)m * kMlpOut * 4, s);
   W.err.ensure(16, s);
   if (!training) return;
-  W.xin.ensure((size_t)m * kMlpIn * 4, s);
+  W.xin.ensure((size_t)m * D.in * 4, s);
   W.tgt.ensure((size_t)m * kMlpOut * 4, s);
-  W.xt.ensure((size_t)kMlpInPad * lt * 2, s);
+  W.xt.ensure((size_t)D.in_pad * lt * 2, s);
   for (DevBuf* b : {&W.z1, &W.z2, &W.z3, &W.dz1f, &W.dz2f, &W.dz3f}) b->ensure(hb * 4, s);
   for (DevBuf* b : {&W.dz2b, &W.dz3b}) b->ensure(hb * 2, s);
   for (DevBuf* b : {&W.h1t, &W.h2t, &W.dz1t, &W.dz2t, &W.dz3t})
@@ -339,22 +343,25 @@ void ensure_batch(olpt_ctx* ctx, int64_t n, bool training) {
 
 void pack_weights(olpt_ctx* ctx) {
   MlpWork& W = ctx->mlp;
+  const MlpDims& D = W.dims;
   cudaStream_t s = ctx->stream;
   const float* M = W.master.as<float>();
-  pack_w1_kernel<<<OLPT_G(nblk(kMlpHid * kMlpInPad)), 256, 0, s>>>(M, W.wb1.as<__nv_bfloat16>());
+  pack_w1_kernel<<<OLPT_G(nblk(kMlpHid * D.in_pad)), 256, 0, s>>>(M + D.off_w1, D.in, D.in_pad,
+                                                                  W.wb1.as<__nv_bfloat16>());
   pack_sq_kernel<<<OLPT_G(nblk(kMlpHid * kMlpHid)), 256, 0, s>>>(
-      M + kOffW2, W.wb2.as<__nv_bfloat16>(), W.wt2.as<__nv_bfloat16>());
+      M + D.off_w2, W.wb2.as<__nv_bfloat16>(), W.wt2.as<__nv_bfloat16>());
   pack_sq_kernel<<<OLPT_G(nblk(kMlpHid * kMlpHid)), 256, 0, s>>>(
-      M + kOffW3, W.wb3.as<__nv_bfloat16>(), W.wt3.as<__nv_bfloat16>());
+      M + D.off_w3, W.wb3.as<__nv_bfloat16>(), W.wt3.as<__nv_bfloat16>());
   OLPT_CUDA(cudaGetLastError());
 }
 
 void alloc_params(olpt_ctx* ctx) {
   MlpWork& W = ctx->mlp;
+  const MlpDims& D = W.dims;
   cudaStream_t s = ctx->stream;
-  const size_t pb = (size_t)kMlpParams * 4;
+  const size_t pb = (size_t)D.params * 4;
   for (DevBuf* b : {&W.master, &W.grad, &W.am, &W.av}) b->ensure(pb, s);
-  W.wb1.ensure((size_t)kMlpHid * kMlpInPad * 2, s);
+  W.wb1.ensure((size_t)kMlpHid * D.in_pad * 2, s);
   for (DevBuf* b : {&W.wb2, &W.wb3, &W.wt2, &W.wt3}) b->ensure((size_t)kMlpHid * kMlpHid * 2, s);
   OLPT_CUDA(cudaMemsetAsync(W.am.p, 0, pb, s));
   OLPT_CUDA(cudaMemsetAsync(W.av.p, 0, pb, s));
@@ -375,12 +382,13 @@ int check_err(olpt_ctx* ctx) {
 // and the transposed activations for the weight gradients
 void forward(olpt_ctx* ctx, int64_t n, bool training) {
   MlpWork& W = ctx->mlp;
+  const MlpDims& D = W.dims;
   cudaStream_t s = ctx->stream;
   const int lt = (int)round8(n);
   const float* M = W.master.as<float>();
   int* err = W.err.as<int>();
   GemmEpilogue e1;
-  e1.bias = M + kOffB1;
+  e1.bias = M + D.off_b1;
   e1.gelu = true;
   e1.out_bf16 = W.h1.as<__nv_bfloat16>();
   e1.ld_bf16 = kMlpHid;
@@ -390,10 +398,10 @@ void forward(olpt_ctx* ctx, int64_t n, bool training) {
     e1.out_bf16_t = W.h1t.as<__nv_bfloat16>();
     e1.ld_t = lt;
   }
-  gemm_bf16(W.x.as<__nv_bfloat16>(), kMlpInPad, W.wb1.as<__nv_bfloat16>(), kMlpInPad, (int)n,
-            kMlpHid, kMlpInPad, e1, 1, err, s);
+  gemm_bf16(W.x.as<__nv_bfloat16>(), D.in_pad, W.wb1.as<__nv_bfloat16>(), D.in_pad, (int)n,
+            kMlpHid, D.in_pad, e1, 1, err, s);
   GemmEpilogue e2 = e1;
-  e2.bias = M + kOffB2;
+  e2.bias = M + D.off_b2;
   e2.out_bf16 = W.h2.as<__nv_bfloat16>();
   if (training) {
     e2.out_f32 = W.z2.as<float>();
@@ -402,7 +410,7 @@ void forward(olpt_ctx* ctx, int64_t n, bool training) {
   gemm_bf16(W.h1.as<__nv_bfloat16>(), kMlpHid, W.wb2.as<__nv_bfloat16>(), kMlpHid, (int)n, kMlpHid,
             kMlpHid, e2, 1, err, s);
   GemmEpilogue e3;
-  e3.bias = M + kOffB3;
+  e3.bias = M + D.off_b3;
   e3.gelu = true;
   e3.out_bf16 = W.h3.as<__nv_bfloat16>();
   e3.ld_bf16 = kMlpHid;
@@ -412,8 +420,8 @@ void forward(olpt_ctx* ctx, int64_t n, bool training) {
   }
   gemm_bf16(W.h2.as<__nv_bfloat16>(), kMlpHid, W.wb3.as<__nv_bfloat16>(), kMlpHid, (int)n, kMlpHid,
             kMlpHid, e3, 1, err, s);
-  head_fwd_kernel<<<OLPT_G(nblk(n * 32)), 256, 0, s>>>(W.h3.as<__nv_bfloat16>(), n, M,
-                                                      W.o.as<float>());
+  head_fwd_kernel<<<OLPT_G(nblk(n * 32)), 256, 0, s>>>(W.h3.as<__nv_bfloat16>(), n, M + D.off_w4,
+                                                      M + D.off_b4, W.o.as<float>());
   OLPT_CUDA(cudaGetLastError());
 }
 
@@ -451,30 +459,46 @@ void wgrad(olpt_ctx* ctx, const __nv_bfloat16* at, const __nv_bfloat16* bt, int6
 
 }  // namespace
 
+// The network's geometry follows the context's camera count (4 when no cameras are
+// uploaded yet); buffers are grown when it changes.
+void set_dims(olpt_ctx* ctx) {
+  MlpWork& W = ctx->mlp;
+  const int cams = ctx->n_cam >= 2 ? ctx->n_cam : 4;
+  OLPT_REQUIRE(cams <= kMlpMaxCams, OLPT_ERR_UNSUPPORTED,
+               "the learned proposal supports at most 8 cameras");
+  if (W.dims.cams != cams) {
+    W.dims = mlp_dims(cams);
+    W.ready = false;
+  }
+}
+
 void mlp_init(olpt_ctx* ctx, uint64_t seed) {
+  set_dims(ctx);
   alloc_params(ctx);
-  std::vector<float> p(kMlpParams, 0.0f);
+  const MlpDims& D = ctx->mlp.dims;
+  std::vector<float> p(D.params, 0.0f);
   std::mt19937_64 rng(seed);
   auto fill = [&](int64_t off, int fan_out, int fan_in) {
     const double lim = std::sqrt(6.0 / (double)fan_in);  // He-uniform for GELU layers
     std::uniform_real_distribution<double> U(-lim, lim);
     for (int64_t i = 0; i < (int64_t)fan_out * fan_in; ++i) p[off + i] = (float)U(rng);
   };
-  fill(kOffW1, kMlpHid, kMlpIn);
-  fill(kOffW2, kMlpHid, kMlpHid);
-  fill(kOffW3, kMlpHid, kMlpHid);
+  fill(D.off_w1, kMlpHid, D.in);
+  fill(D.off_w2, kMlpHid, kMlpHid);
+  fill(D.off_w3, kMlpHid, kMlpHid);
   {
     const double lim = std::sqrt(1.0 / (double)kMlpHid);
     std::uniform_real_distribution<double> U(-lim, lim);
-    for (int64_t i = 0; i < (int64_t)kMlpOut * kMlpHid; ++i) p[kOffW4 + i] = (float)U(rng);
+    for (int64_t i = 0; i < (int64_t)kMlpOut * kMlpHid; ++i) p[D.off_w4 + i] = (float)U(rng);
   }
   mlp_set_params(ctx, p.data());
 }
 
 void mlp_set_params(olpt_ctx* ctx, const float* host) {
   MlpWork& W = ctx->mlp;
+  set_dims(ctx);
   if (!W.ready) alloc_params(ctx);
-  OLPT_CUDA(cudaMemcpyAsync(W.master.p, host, (size_t)kMlpParams * 4, cudaMemcpyHostToDevice,
+  OLPT_CUDA(cudaMemcpyAsync(W.master.p, host, (size_t)W.dims.params * 4, cudaMemcpyHostToDevice,
                             ctx->stream));
   pack_weights(ctx);
   OLPT_CUDA(cudaStreamSynchronize(ctx->stream));
@@ -483,30 +507,34 @@ void mlp_set_params(olpt_ctx* ctx, const float* host) {
 
 void mlp_get_params(olpt_ctx* ctx, float* host) {
   OLPT_REQUIRE(ctx->mlp.ready, OLPT_ERR_INVALID_ARG, "network not initialised");
-  OLPT_CUDA(cudaMemcpyAsync(host, ctx->mlp.master.p, (size_t)kMlpParams * 4,
+  OLPT_CUDA(cudaMemcpyAsync(host, ctx->mlp.master.p, (size_t)ctx->mlp.dims.params * 4,
                             cudaMemcpyDeviceToHost, ctx->stream));
   OLPT_CUDA(cudaStreamSynchronize(ctx->stream));
 }
 
 void mlp_features_device(olpt_ctx* ctx, const ShakeParams& sp, __nv_bfloat16* x, float* f32) {
-  OLPT_REQUIRE(ctx->n_cam == kMlpCams, OLPT_ERR_UNSUPPORTED,
-               "the learned proposal is defined for 4 cameras");
+  if (!ctx->mlp.ready) set_dims(ctx);
+  OLPT_REQUIRE(ctx->n_cam == ctx->mlp.dims.cams, OLPT_ERR_UNSUPPORTED,
+               "learned proposal: the network was built for " +
+                   std::to_string(ctx->mlp.dims.cams) + " cameras, the rig has " +
+                   std::to_string(ctx->n_cam));
+  const MlpDims& D = ctx->mlp.dims;
   const int64_t n = ctx->obj.n;
   if (n == 0) return;
-  PlaneView pv[kMlpCams];
-  for (int c = 0; c < kMlpCams; ++c) {
+  PlaneSet pv{};
+  for (int c = 0; c < D.cams; ++c) {
     const ImagePlane& r = ctx->resid[c];
-    pv[c] = PlaneView{r.buf.as<unsigned char>(), r.pitch, r.H, r.W, r.dtype};
+    pv.p[c] = PlaneView{r.buf.as<unsigned char>(), r.pitch, r.H, r.W, r.dtype};
   }
   const OtfView ov = otf_view(ctx);
   cudaStream_t s = ctx->stream;
   if (sp.precision == 1)
     features_kernel<double><<<OLPT_G(nblk(n * 32)), 256, 0, s>>>(
-        ctx->cams_d.as<CamDev>(), ov, ctx->obj.xyz.as<double>(), n, pv[0], pv[1], pv[2], pv[3],
+        ctx->cams_d.as<CamDev>(), ov, ctx->obj.xyz.as<double>(), n, pv, D.cams, D.in, D.in_pad,
         sp.radius_obj, x, f32);
   else
     features_kernel<float><<<OLPT_G(nblk(n * 32)), 256, 0, s>>>(
-        ctx->cams_d.as<CamDev>(), ov, ctx->obj.xyz.as<double>(), n, pv[0], pv[1], pv[2], pv[3],
+        ctx->cams_d.as<CamDev>(), ov, ctx->obj.xyz.as<double>(), n, pv, D.cams, D.in, D.in_pad,
         sp.radius_obj, x, f32);
   OLPT_CUDA(cudaGetLastError());
 }
@@ -526,7 +554,8 @@ void gelu_inplace_device(float* p, int64_t n, cudaStream_t s) {
 
 void mlp_input_device(olpt_ctx* ctx, const float* x_f32, int64_t n, __nv_bfloat16* x) {
   if (n == 0) return;
-  input_kernel<<<OLPT_G(nblk(n * kMlpInPad)), 256, 0, ctx->stream>>>(x_f32, n, x);
+  const MlpDims& D = ctx->mlp.dims;
+  input_kernel<<<OLPT_G(nblk(n * D.in_pad)), 256, 0, ctx->stream>>>(x_f32, n, D.in, D.in_pad, x);
   OLPT_CUDA(cudaGetLastError());
 }
 
@@ -538,7 +567,8 @@ void mlp_infer_device(olpt_ctx* ctx, const __nv_bfloat16* x, int64_t n, float* o
   ensure_batch(ctx, n, false);
   OLPT_CUDA(cudaMemsetAsync(W.err.p, 0, 16, s));
   if (x != W.x.as<__nv_bfloat16>())
-    OLPT_CUDA(cudaMemcpyAsync(W.x.p, x, (size_t)n * kMlpInPad * 2, cudaMemcpyDeviceToDevice, s));
+    OLPT_CUDA(cudaMemcpyAsync(W.x.p, x, (size_t)n * W.dims.in_pad * 2, cudaMemcpyDeviceToDevice,
+                              s));
   forward(ctx, n, false);
   if (o != W.o.as<float>())
     OLPT_CUDA(cudaMemcpyAsync(o, W.o.p, (size_t)n * kMlpOut * 4, cudaMemcpyDeviceToDevice, s));
@@ -572,13 +602,15 @@ const double* train_enqueue(olpt_ctx* ctx, const float* x_f32, const float* tgt,
   OLPT_REQUIRE(W.ready, OLPT_ERR_INVALID_ARG, "network not initialised");
   OLPT_REQUIRE(n > 0, OLPT_ERR_INVALID_ARG, "empty batch");
   cudaStream_t s = ctx->stream;
+  const MlpDims& D = W.dims;
   ensure_batch(ctx, n, true);
   const int64_t lt = round8(n);
-  input_kernel<<<OLPT_G(nblk(n * kMlpInPad)), 256, 0, s>>>(x_f32, n, W.x.as<__nv_bfloat16>());
+  input_kernel<<<OLPT_G(nblk(n * D.in_pad)), 256, 0, s>>>(x_f32, n, D.in, D.in_pad,
+                                                          W.x.as<__nv_bfloat16>());
   {
-    dim3 g((unsigned)((n + 31) / 32), kMlpInPad / 32);
-    transpose_kernel<<<OLPT_G(g), dim3(32, 8), 0, s>>>(W.x.as<__nv_bfloat16>(), n, kMlpInPad,
-                                                       kMlpInPad, W.xt.as<__nv_bfloat16>(), lt);
+    dim3 g((unsigned)((n + 31) / 32), D.in_pad / 32);
+    transpose_kernel<<<OLPT_G(g), dim3(32, 8), 0, s>>>(W.x.as<__nv_bfloat16>(), n, D.in_pad,
+                                                       D.in_pad, W.xt.as<__nv_bfloat16>(), lt);
   }
   forward(ctx, n, true);
   float* G = W.grad.as<float>();
@@ -595,17 +627,18 @@ const double* train_enqueue(olpt_ctx* ctx, const float* x_f32, const float* tgt,
   W.hpart.ensure((size_t)hb * hlen * 4 + 64, s);
   head_wgrad_kernel<<<OLPT_G(hb), 256, 0, s>>>(W.dout.as<float>(), W.h3.as<__nv_bfloat16>(), n, rpb,
                                                W.hpart.as<float>());
-  sum_partials_kernel<<<OLPT_G(nblk(hlen)), 256, 0, s>>>(W.hpart.as<float>(), hb, hlen, G + kOffW4);
+  sum_partials_kernel<<<OLPT_G(nblk(hlen)), 256, 0, s>>>(W.hpart.as<float>(), hb, hlen,
+                                                         G + D.off_w4);
   // (hpart is reused by the bias gradients below, after these kernels in stream order)
   head_bwd_kernel<<<OLPT_G((unsigned)((n + 31) / 32)), 256, 0, s>>>(
-      W.dout.as<float>(), M, W.z3.as<float>(), n, W.dz3f.as<float>(), W.dz3b.as<__nv_bfloat16>(),
+      W.dout.as<float>(), M + D.off_w4, W.z3.as<float>(), n, W.dz3f.as<float>(), W.dz3b.as<__nv_bfloat16>(),
       W.dz3t.as<__nv_bfloat16>(), lt);
   OLPT_CUDA(cudaGetLastError());
   int* err = W.err.as<int>();
   // layer 3
   wgrad(ctx, W.dz3t.as<__nv_bfloat16>(), W.h2t.as<__nv_bfloat16>(), n, kMlpHid, kMlpHid, kMlpHid,
-        G + kOffW3, kMlpHid, kMlpHid);
-  bias_grad(ctx, W.dz3f.as<float>(), n, G + kOffB3);
+        G + D.off_w3, kMlpHid, kMlpHid);
+  bias_grad(ctx, W.dz3f.as<float>(), n, G + D.off_b3);
   GemmEpilogue d2;
   d2.gelu_pre = W.z2.as<float>();
   d2.ld_pre = kMlpHid;
@@ -619,8 +652,8 @@ const double* train_enqueue(olpt_ctx* ctx, const float* x_f32, const float* tgt,
             kMlpHid, kMlpHid, d2, 1, err, s);
   // layer 2
   wgrad(ctx, W.dz2t.as<__nv_bfloat16>(), W.h1t.as<__nv_bfloat16>(), n, kMlpHid, kMlpHid, kMlpHid,
-        G + kOffW2, kMlpHid, kMlpHid);
-  bias_grad(ctx, W.dz2f.as<float>(), n, G + kOffB2);
+        G + D.off_w2, kMlpHid, kMlpHid);
+  bias_grad(ctx, W.dz2f.as<float>(), n, G + D.off_b2);
   GemmEpilogue d1;
   d1.gelu_pre = W.z1.as<float>();
   d1.ld_pre = kMlpHid;
@@ -631,18 +664,18 @@ const double* train_enqueue(olpt_ctx* ctx, const float* x_f32, const float* tgt,
   gemm_bf16(W.dz2b.as<__nv_bfloat16>(), kMlpHid, W.wt2.as<__nv_bfloat16>(), kMlpHid, (int)n,
             kMlpHid, kMlpHid, d1, 1, err, s);
   // layer 1
-  wgrad(ctx, W.dz1t.as<__nv_bfloat16>(), W.xt.as<__nv_bfloat16>(), n, kMlpHid, kMlpInPad,
-        kMlpInPad, G + kOffW1, kMlpIn, kMlpIn);
-  bias_grad(ctx, W.dz1f.as<float>(), n, G + kOffB1);
+  wgrad(ctx, W.dz1t.as<__nv_bfloat16>(), W.xt.as<__nv_bfloat16>(), n, kMlpHid, D.in_pad,
+        D.in_pad, G + D.off_w1, D.in, D.in);
+  bias_grad(ctx, W.dz1f.as<float>(), n, G + D.off_b1);
   OLPT_CUDA(cudaGetLastError());
   if (update) {
     ++W.adam_t;
     const float b1 = 0.9f, b2 = 0.999f;
     const float bc1 = 1.0f - std::pow(b1, (float)W.adam_t);
     const float bc2 = 1.0f - std::pow(b2, (float)W.adam_t);
-    adam_kernel<<<OLPT_G(nblk(kMlpParams)), 256, 0, s>>>(W.master.as<float>(), G, W.am.as<float>(),
-                                                         W.av.as<float>(), kMlpParams, (float)lr, b1,
-                                                         b2, 1e-8f, bc1, bc2);
+    adam_kernel<<<OLPT_G(nblk(D.params)), 256, 0, s>>>(W.master.as<float>(), G, W.am.as<float>(),
+                                                       W.av.as<float>(), D.params, (float)lr, b1,
+                                                       b2, 1e-8f, bc1, bc2);
     OLPT_CUDA(cudaGetLastError());
     pack_weights(ctx);
   }
@@ -656,7 +689,8 @@ void mlp_train_many(olpt_ctx* ctx, const float* x, const float* t, int64_t n, in
   OLPT_REQUIRE(W.ready, OLPT_ERR_INVALID_ARG, "network not initialised");
   OLPT_REQUIRE(n > 0 && batch > 0 && steps >= 0, OLPT_ERR_INVALID_ARG, "mlp_train: bad sizes");
   cudaStream_t s = ctx->stream;
-  W.xin.ensure((size_t)batch * kMlpIn * 4, s);
+  const int in = W.dims.in;
+  W.xin.ensure((size_t)batch * in * 4, s);
   W.tgt.ensure((size_t)batch * kMlpOut * 4, s);
   // the steps are enqueued back to back; the losses stay on the device until the end
   W.loss_hist.ensure((size_t)(steps + 1) * sizeof(double), s);
@@ -664,8 +698,8 @@ void mlp_train_many(olpt_ctx* ctx, const float* x, const float* t, int64_t n, in
   OLPT_CUDA(cudaMemsetAsync(W.err.p, 0, 16, s));
   for (int it = 0; it < steps; ++it) {
     const double a = lr * (0.05 + 0.95 * 0.5 * (1.0 + std::cos(M_PI * it / (double)steps)));
-    sample_kernel<<<OLPT_G(nblk((int64_t)batch * kMlpIn)), 256, 0, s>>>(
-        x, t, n, batch, seed, it, W.xin.as<float>(), W.tgt.as<float>());
+    sample_kernel<<<OLPT_G(nblk((int64_t)batch * in)), 256, 0, s>>>(
+        x, t, n, in, batch, seed, it, W.xin.as<float>(), W.tgt.as<float>());
     OLPT_CUDA(cudaGetLastError());
     const double* d_loss = train_enqueue(ctx, W.xin.as<float>(), W.tgt.as<float>(), batch, a,
                                          ghost_weight, true);

@@ -153,7 +153,15 @@ struct StereoWork {
   DevBuf l2d_ptrs, cbp_ptrs, active_d, counters, scan_tmp;
   DevBuf path_a, path_b, term, pairs;
   DevBuf cand_ids, cand_e, cand_x;
+  // near-tolerance decision log: records (olpt_near_record) and a 64-bit counter of
+  // every near-tolerance test seen since the last reset (records beyond near_cap are
+  // counted, not stored)
+  DevBuf near_rec, near_count;
+  double near_band = 0.0;
+  int64_t near_cap = 0;
   void release(cudaStream_t s) {
+    near_rec.release(s);
+    near_count.release(s);
     for (int c = 0; c < OLPT_MAX_CAM; ++c) {
       cell_start[c].release(s);
       cell_cursor[c].release(s);
@@ -298,10 +306,11 @@ struct StbState {
 };
 
 // Device state of the learned proposal (mlp.cu): f32 master parameters, Adam moments
-// and gradients (flat, kMlpParams), bf16 weight copies for the GEMMs (row-major and
+// and gradients (flat, MlpDims::params), bf16 weight copies for the GEMMs (row-major and
 // transposed), and the activations of one batch.
 struct MlpWork {
   bool ready = false;
+  MlpDims dims = mlp_dims(4);  // network geometry (set from the camera count at init)
   int adam_t = 0;
   LearnedParams lp;
   int64_t n_learned = 0, n_fallback = 0;  // objects through the learned shake / its fallback
@@ -326,10 +335,10 @@ void mlp_init(olpt_ctx* ctx, uint64_t seed);
 void mlp_set_params(olpt_ctx* ctx, const float* host);
 void mlp_get_params(olpt_ctx* ctx, float* host);
 // features of the context's objects against residual planes computed with all of
-// them (FP32 or FP64 planes per sp.precision); x: n x kMlpInPad bf16 (device),
-// f32 (optional, device): n x kMlpIn
+// them (FP32 or FP64 planes per sp.precision); x: n x dims.in_pad bf16 (device),
+// f32 (optional, device): n x dims.in
 void mlp_features_device(olpt_ctx* ctx, const ShakeParams& sp, __nv_bfloat16* x, float* f32);
-// f32 rows of kMlpIn (device) -> bf16 rows of kMlpInPad
+// f32 rows of dims.in (device) -> bf16 rows of dims.in_pad
 void mlp_input_device(olpt_ctx* ctx, const float* x_f32, int64_t n, __nv_bfloat16* x);
 void gelu_inplace_device(float* p, int64_t n, cudaStream_t s);
 // residual planes of the current images with every object projected (the first step

@@ -982,17 +982,42 @@ static __device__ __align__(256) double g_noalloc_log_lut[65536];
 
 namespace {
 struct NoAllocDevice {
-  bool ready = false;
+  unsigned long long ctx_id = 0;     // CUDA context the table was filled in (0 = never)
   unsigned char* scratch = nullptr;  // device address of g_noalloc_scratch
   double* lut = nullptr;             // device address of g_noalloc_log_lut
 };
 std::mutex g_noalloc_mu;
 NoAllocDevice g_noalloc_dev[64];
+
+// Unique id of the calling thread's current CUDA context (cuCtxGetId, driver API
+// looked up through the runtime); a device reset gives the device a new context and
+// hence a new id, so the log table is filled again in it.
+cudaError_t current_context_id(unsigned long long* id) {
+  using GetCurrent = int (*)(void**);
+  using GetId = int (*)(void*, unsigned long long*);
+  static GetCurrent get_current = nullptr;
+  static GetId get_id = nullptr;
+  if (!get_current || !get_id) {
+    void* p = nullptr;
+    cudaDriverEntryPointQueryResult q;
+    cudaError_t e = cudaGetDriverEntryPoint("cuCtxGetCurrent", &p, cudaEnableDefault, &q);
+    if (e != cudaSuccess || q != cudaDriverEntryPointSuccess || !p) return cudaErrorNotSupported;
+    get_current = reinterpret_cast<GetCurrent>(p);
+    e = cudaGetDriverEntryPoint("cuCtxGetId", &p, cudaEnableDefault, &q);
+    if (e != cudaSuccess || q != cudaDriverEntryPointSuccess || !p) return cudaErrorNotSupported;
+    get_id = reinterpret_cast<GetId>(p);
+  }
+  void* ctx = nullptr;
+  if (get_current(&ctx) != 0 || !ctx) return cudaErrorDeviceUninitialized;
+  return get_id(ctx, id) == 0 ? cudaSuccess : cudaErrorDeviceUninitialized;
+}
 }  // namespace
 
-// Once per device, with that device current: resolve the arrays' device addresses
-// (in host code their names are host-side stand-ins, not device addresses) and fill
-// the log table.  Synchronous; must run before any stream capture.
+// Every call, with the device current: resolve the arrays' device addresses (in host
+// code their names are host-side stand-ins, not device addresses) and, the first time
+// in each CUDA context of the device (after a cudaDeviceReset too), fill the log
+// table.  The fill is a synchronous copy, so the first call in a context must come
+// before any stream capture.
 static olpt_status_t noalloc_setup(int dev, NoAllocDevice*& out, std::string& err) {
   std::lock_guard<std::mutex> lk(g_noalloc_mu);
   if (dev < 0 || dev >= 64) {
@@ -1000,13 +1025,19 @@ static olpt_status_t noalloc_setup(int dev, NoAllocDevice*& out, std::string& er
     return OLPT_ERR_INVALID_ARG;
   }
   NoAllocDevice& d = g_noalloc_dev[dev];
-  if (!d.ready) {
-    cudaError_t e = cudaGetSymbolAddress((void**)&d.scratch, g_noalloc_scratch);
-    if (e == cudaSuccess) e = cudaGetSymbolAddress((void**)&d.lut, g_noalloc_log_lut);
-    if (e != cudaSuccess) {
-      err = std::string("cudaGetSymbolAddress failed: ") + cudaGetErrorString(e);
-      return OLPT_ERR_CUDA;
-    }
+  cudaError_t e = cudaGetSymbolAddress((void**)&d.scratch, g_noalloc_scratch);
+  if (e == cudaSuccess) e = cudaGetSymbolAddress((void**)&d.lut, g_noalloc_log_lut);
+  if (e != cudaSuccess) {
+    err = std::string("cudaGetSymbolAddress failed: ") + cudaGetErrorString(e);
+    return OLPT_ERR_CUDA;
+  }
+  unsigned long long ctx_id = 0;
+  e = current_context_id(&ctx_id);
+  if (e != cudaSuccess) {
+    err = std::string("no current CUDA context: ") + cudaGetErrorString(e);
+    return OLPT_ERR_CUDA;
+  }
+  if (d.ctx_id != ctx_id) {
     std::vector<double> t(65536);
     for (int v = 0; v < 65536; ++v) {
       const double x = (double)v;
@@ -1017,7 +1048,7 @@ static olpt_status_t noalloc_setup(int dev, NoAllocDevice*& out, std::string& er
       err = std::string("log table upload failed: ") + cudaGetErrorString(e);
       return OLPT_ERR_CUDA;
     }
-    d.ready = true;
+    d.ctx_id = ctx_id;
   }
   out = &d;
   return OLPT_OK;

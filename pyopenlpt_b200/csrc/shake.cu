@@ -1133,7 +1133,7 @@ static void learned_impl(olpt_ctx* ctx, const ShakeParams& sp) {
   if (n > 0) {
     // 1. residual with every candidate at its stereo position, features, network
     residual_pass<Real>(ctx, v, nullptr, 0, 0);
-    M.x.ensure((size_t)n * kMlpInPad * 2, s);
+    M.x.ensure((size_t)n * M.dims.in_pad * 2, s);
     mlp_features_device(ctx, sp, M.x.as<__nv_bfloat16>(), nullptr);
     M.o.ensure((size_t)n * kMlpOut * 4, s);
     mlp_infer_device(ctx, M.x.as<__nv_bfloat16>(), n, M.o.as<float>());
@@ -1211,9 +1211,10 @@ void residual_all_device(olpt_ctx* ctx, const ShakeParams& sp) {
 }
 
 void learned_shake_device(olpt_ctx* ctx, const ShakeParams& sp) {
-  OLPT_REQUIRE(ctx->n_cam == kMlpCams, OLPT_ERR_UNSUPPORTED,
-               "the learned shake is defined for 4 cameras");
   OLPT_REQUIRE(ctx->mlp.ready, OLPT_ERR_INVALID_ARG, "learned shake: network not initialised");
+  OLPT_REQUIRE(ctx->n_cam == ctx->mlp.dims.cams, OLPT_ERR_UNSUPPORTED,
+               "learned shake: the network was built for " + std::to_string(ctx->mlp.dims.cams) +
+                   " cameras, the rig has " + std::to_string(ctx->n_cam));
   if (sp.precision == 1)
     learned_impl<double>(ctx, sp);
   else

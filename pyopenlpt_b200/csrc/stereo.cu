@@ -54,6 +54,12 @@ struct SmView {
   const double* cbp[OLPT_MAX_CAM][OLPT_MAX_CAM];    // [t][c]: n[t] x 4
   double tol2d, tol3d;
   double limit[6];
+  // near-tolerance log (off when near_band == 0): 2D tests whose distance lies within
+  // near_band px of tol2d are appended to near_rec
+  double near_band;
+  olpt_near_record* near_rec;
+  unsigned long long* near_count;
+  long long near_cap;
 };
 
 struct Path {
@@ -320,6 +326,23 @@ __device__ __forceinline__ int append_slot(int* counter) {
   return base + __popc(m & ((1u << lane) - 1u));
 }
 
+// Appends one near-tolerance 2D decision to the log (rare: only tests whose
+// distance is within near_band px of the tolerance).
+__device__ __noinline__ void near_append(const SmView& v, int kind, int k, int cam, int id,
+                                         int other_cam, int other_id, double margin) {
+  const unsigned long long slot = atomicAdd(v.near_count, 1ull);
+  if ((long long)slot >= v.near_cap) return;
+  olpt_near_record r;
+  r.kind = kind;
+  r.n_chosen = k;
+  r.cam = cam;
+  r.id = id;
+  r.other_cam = other_cam;
+  r.other_id = other_id;
+  r.margin_px = margin;
+  v.near_rec[slot] = r;
+}
+
 // Expand one level, first half: each path has K chosen cameras; its candidates on
 // the target camera are enumerated over rows of cells and kept when they pass the
 // strip test (IDMap::visitPointsInRowSpans) and the back-projection test.  WARP: one
@@ -445,6 +468,11 @@ __global__ void __launch_bounds__(256, 4) enum_kernel(const SmView v, const Path
         const double dx = xy.x - lp[i][0], dy = xy.y - lp[i][1];
         const double z = dy * lU[i][0] - dx * lU[i][1];
         ok = ok && !(z * z > tol2);
+        if (v.near_band > 0.0) {
+          const double m = fabs(z) - v.tol2d;
+          if (fabs(m) < v.near_band)
+            near_append(v, 0, K, t, citems[q], P.cams[i], P.ids[i], m);
+        }
       }
       if (!ok) continue;
       // checkBackProjection (StereoMatch.cpp:1206-1227)
@@ -456,6 +484,11 @@ __global__ void __launch_bounds__(256, 4) enum_kernel(const SmView v, const Path
         const double d0 = cpt[i][0] - a.x, d1 = cpt[i][1] - a.y;
         const double z = d1 * b.x - d0 * b.y;
         ok = !(z * z > tol2);
+        if (v.near_band > 0.0) {
+          const double m = fabs(z) - v.tol2d;
+          if (fabs(m) < v.near_band)
+            near_append(v, 1, K, t, citems[q], P.cams[i], P.ids[i], m);
+        }
       }
       if (!ok) continue;
       const int slot = append_slot(pair_count);
@@ -732,6 +765,12 @@ void stereo_match_device(olpt_ctx* ctx, const SmParams& prm, StereoResult& res) 
   v.cell = std::max(1, prm.idmap_cell_px);
   v.tol2d = prm.tol_2d_px;
   v.tol3d = prm.tol_3d_mm;
+  v.near_band = ctx->sm.near_band;
+  if (v.near_band > 0.0) {
+    v.near_rec = ctx->sm.near_rec.as<olpt_near_record>();
+    v.near_count = ctx->sm.near_count.as<unsigned long long>();
+    v.near_cap = ctx->sm.near_cap;
+  }
   for (int q = 0; q < 6; ++q) v.limit[q] = prm.limit[q];
 
   StereoWork& W = ctx->sm;

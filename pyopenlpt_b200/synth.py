@@ -69,7 +69,7 @@ class PinholeCam:
 def ring_rig(n_cam: int, n_row: int, n_col: int, focal: float, radius: float = 500.0,
              elevation_deg: float = 30.0, az_step_deg: float = 45.0) -> List[PinholeCam]:
     """Cameras on a horizontal ring, tilted down by ``elevation_deg``, all aimed at
-    the origin (the BASELINE rig: R=500 mm, 45 deg spacing, 30 deg tilt)."""
+    the origin (default: R=500 mm, 45 deg spacing, 30 deg tilt)."""
     cams = []
     el = math.radians(elevation_deg)
     for i in range(n_cam):
@@ -117,6 +117,8 @@ class Scene:
     volume: tuple                    # (xmin,xmax,ymin,ymax,zmin,zmax)
     otf_abc: tuple                   # (a, b, c)
     max_val: int
+    otf_table: Optional[np.ndarray] = None   # [4][n_cam][nx*ny*nz] when not uniform
+    otf_n: tuple = (2, 2, 2)
 
     @property
     def n_cam(self) -> int:
@@ -130,8 +132,8 @@ def make_scene(n_particles: int = 10000, n_cam: int = 4, size: int = 1024, focal
                require_all_views: bool = True) -> Scene:
     """A single frame: uniform particles in ``volume`` seen by a ring rig.
 
-    Defaults are the BASELINE single-frame IPR scene: 4 cams, 1024^2 uint8,
-    f = 5000 px, 10,000 particles in a 40x40x20 mm box, a=200, b=c=0.5, sigma=2.
+    Defaults are the single-frame IPR scene of 4 cams, 1024^2 uint8, f = 5000 px,
+    10,000 particles in a 40x40x20 mm box, a=200, b=c=0.5, sigma=2 (0.01 ppp).
     """
     rng = np.random.default_rng(seed)
     n_row = n_row or size
@@ -200,8 +202,8 @@ def make_sequence(n_particles: int = 51000, n_frames: int = 50, n_cam: int = 4,
                   with_images: bool = True) -> Sequence_:
     """Particles advected by a Burgers vortex plus drift (RK4, FP64); the time step
     gives at most `max_px_per_frame` pixels of image motion per frame; particles that
-    leave the volume are re-seeded uniformly.  Defaults: the BASELINE STB sequence
-    (51,000 particles, 4 x 1280x800 12-bit, 60x40x30 mm, 50 frames)."""
+    leave the volume are re-seeded uniformly.  Defaults: the STB sequence of 51,000
+    particles (0.05 ppp), 4 x 1280x800 12-bit, 60x40x30 mm, 50 frames."""
     rng = np.random.default_rng(seed)
     cams = ring_rig(n_cam, n_row, n_col, focal)
     lo = np.array(volume[0::2])
@@ -352,7 +354,10 @@ def write_stb_config(seq, folder: str, ipr: "IPRSettings", stb: STBSettings,
             f.write("\n".join(names) + "\n")
         lists.append(os.path.join(folder, lp))
     with open(os.path.join(folder, "otf.txt"), "w") as f:
-        f.write(otf_text(seq.n_cam, seq.volume, *seq.otf_abc))
+        if getattr(seq, "otf_table", None) is not None:
+            f.write(otf_text_table(seq.otf_table, seq.otf_n, seq.volume))
+        else:
+            f.write(otf_text(seq.n_cam, seq.volume, *seq.otf_abc))
     tracer = os.path.join(folder, "tracerConfig.txt")
     with open(tracer, "w") as f:
         f.write("\n".join(str(v) for v in [
@@ -381,5 +386,336 @@ def write_scene_files(scene: Scene, folder: str) -> List[str]:
             f.write(cm.to_text())
         paths.append(p)
     with open(os.path.join(folder, "otf.txt"), "w") as f:
-        f.write(otf_text(scene.n_cam, scene.volume, *scene.otf_abc))
+        if scene.otf_table is not None:
+            f.write(otf_text_table(scene.otf_table, scene.otf_n, scene.volume))
+        else:
+            f.write(otf_text(scene.n_cam, scene.volume, *scene.otf_abc))
     return paths
+
+
+# ----------------------------------------------------------------------------- polynomial rigs
+# Exponent rows (px, py, pz) of a full cubic in (X, Y, Z): 20 monomials, constant first.
+CUBIC_TERMS = [(i, j, k) for d in range(4) for i in range(d, -1, -1) for j in range(d - i, -1, -1)
+               for k in [d - i - j]]
+
+
+@dataclasses.dataclass
+class PolyCam:
+    """Camera of the reference's POLYNOMIAL model (Camera::polyProject,
+    src/srcMath/Camera.cpp:969-990): u = sum_i cu_i X^pu_i Y^qu_i Z^ru_i, same for v;
+    lines of sight by Newton inversion on the two reference planes (REF_Z here)."""
+    n_row: int
+    n_col: int
+    u_coeffs: np.ndarray           # (n, 4): coefficient, x power, y power, z power
+    v_coeffs: np.ndarray
+    plane: tuple                   # the two REF_Z planes (z values, mm)
+    ref_plane: int = 3
+
+    def project(self, xyz: np.ndarray) -> np.ndarray:
+        xyz = np.asarray(xyz, dtype=np.float64).reshape(-1, 3)
+        out = np.zeros((len(xyz), 2))
+        for k, co in enumerate((self.u_coeffs, self.v_coeffs)):
+            for c, px, py, pz in co:
+                out[:, k] += c * xyz[:, 0] ** px * xyz[:, 1] ** py * xyz[:, 2] ** pz
+        return out
+
+    def to_text(self) -> str:
+        """The POLYNOMIAL camera file (Camera::loadParameters, Camera.cpp:99-158)."""
+        ref = {1: "REF_X", 2: "REF_Y", 3: "REF_Z"}[self.ref_plane]
+
+        def rows(co):
+            return [",".join(repr(float(v)) for v in r) for r in co]
+        lines = ["# Camera Model: (PINHOLE/POLYNOMIAL)", "POLYNOMIAL",
+                 "# Camera Calibration Error: ", "None",
+                 "# Image Size: (n_row,n_col)", f"{self.n_row},{self.n_col}",
+                 "# Reference Plane: (REF_X/REF_Y/REF_Z,coordinate,coordinate)",
+                 f"{ref},{float(self.plane[0])!r},{float(self.plane[1])!r}",
+                 "# Number of Coefficients: ", str(len(self.u_coeffs)),
+                 "# U_Coeff (coefficient, x power, y power, z power)"] + rows(self.u_coeffs) + [
+                 "# V_Coeff (coefficient, x power, y power, z power)"] + rows(self.v_coeffs)
+        return "\n".join(lines) + "\n"
+
+
+def focal_for_volume(n_cam: int, size: int, volume, fill: float = 0.92, **rig) -> List[float]:
+    """Per camera of a ring rig, the focal length (px) at which the volume's corners
+    project inside ``fill`` of the image, so the particles cover as much of every
+    image as the box's outline allows."""
+    lo = np.array(volume[0::2], dtype=np.float64)
+    hi = np.array(volume[1::2], dtype=np.float64)
+    corners = np.array([[lo[0] if i & 1 else hi[0], lo[1] if i & 2 else hi[1],
+                         lo[2] if i & 4 else hi[2]] for i in range(8)])
+    out = []
+    for cm in ring_rig(n_cam, size, size, 1.0, **rig):
+        uv = cm.project(corners) - np.array([cm.cx, cm.cy])
+        out.append(fill * 0.5 * (size - 1) / float(np.max(np.abs(uv))))
+    return out
+
+
+def poly_rig(n_cam: int, size: int, volume, max_distortion_px: float = 2.0, seed: int = 0,
+             **rig) -> List[PolyCam]:
+    """Seeded cubic polynomial cameras: a ring rig of pinholes (focal sized to the
+    volume) plus a radial and decentring distortion of at most ``max_distortion_px``
+    at the image corners, fitted by least squares with the 20 monomials of a full cubic
+    in (X, Y, Z) over the slab of the viewing frustum between the two reference planes
+    (z = zmin and z = zmax of the volume), as a calibration with targets filling the
+    view on both planes would.  The fitted polynomials are the cameras: images are
+    rendered with them."""
+    rng = np.random.default_rng(seed)
+    focals = focal_for_volume(n_cam, size, volume, **rig)
+    pins = [ring_rig(n_cam, size, size, f, **rig)[i] for i, f in enumerate(focals)]
+    z0, z1 = float(volume[4]), float(volume[5])
+    g = np.linspace(-0.02 * size, 1.02 * size, 33)
+    pu, pv = [a.ravel() for a in np.meshgrid(g, g, indexing="ij")]
+    A_terms = np.array(CUBIC_TERMS, dtype=np.float64)
+    cams = []
+    for pc in pins:
+        # rays of the pixel grid, cut by 9 planes between the reference planes
+        d_cam = np.stack([(pu - pc.cx) / pc.fx, (pv - pc.cy) / pc.fy, np.ones_like(pu)], axis=1)
+        d_w = d_cam @ pc.R          # R^T d: directions in world coordinates
+        o_w = pc.Tinv
+        P = []
+        for z in np.linspace(z0, z1, 9):
+            s_ = (z - o_w[2]) / d_w[:, 2]
+            P.append(o_w + s_[:, None] * d_w)
+        P = np.concatenate(P)
+        A = np.stack([P[:, 0] ** i * P[:, 1] ** j * P[:, 2] ** k for i, j, k in CUBIC_TERMS],
+                     axis=1)
+        uv = pc.project(P)
+        d = uv - np.array([pc.cx, pc.cy])
+        r_corner = math.hypot(pc.cx, pc.cy)
+        r2 = (d * d).sum(axis=1) / (r_corner * r_corner)
+        k_rad = rng.uniform(0.5, 1.0) * max_distortion_px / r_corner * rng.choice([-1.0, 1.0])
+        t = rng.normal(0.0, 0.25 * max_distortion_px / r_corner, size=2)
+        uvd = uv + d * (k_rad * r2)[:, None] + np.outer(r2, t) * r_corner
+        cu, *_ = np.linalg.lstsq(A, uvd[:, 0], rcond=None)
+        cv, *_ = np.linalg.lstsq(A, uvd[:, 1], rcond=None)
+        cams.append(PolyCam(size, size, np.column_stack([cu, A_terms]),
+                            np.column_stack([cv, A_terms]), (z0, z1)))
+    return cams
+
+
+# ----------------------------------------------------------------------------- OTF grids
+def otf_grid(n_cam: int, n=(5, 5, 5), a_range=(2400.0, 3600.0), bc_range=(0.3, 0.9),
+             seed: int = 0) -> np.ndarray:
+    """Seeded spatially varying OTF table [4][n_cam][nx*ny*nz] (a, b, c, alpha = 0):
+    a, b and c drawn uniformly per grid node, interpolated trilinearly in between."""
+    rng = np.random.default_rng(seed)
+    ng = n[0] * n[1] * n[2]
+    t = np.zeros((4, n_cam, ng))
+    t[0] = rng.uniform(*a_range, size=(n_cam, ng))
+    t[1] = rng.uniform(*bc_range, size=(n_cam, ng))
+    t[2] = rng.uniform(*bc_range, size=(n_cam, ng))
+    return t
+
+
+def otf_eval(table: np.ndarray, n, volume, cam: int, xyz: np.ndarray) -> np.ndarray:
+    """(a, b, c) at each point: OTF::getOTFParam (src/srcSTB/OTF.cpp:273-338) --
+    clamp to the box, trilinear interpolation in the grid cell (index x*ny*nz+y*nz+z)."""
+    nx, ny, nz = n
+    lo = np.array(volume[0::2], dtype=np.float64)
+    hi = np.array(volume[1::2], dtype=np.float64)
+    p = np.clip(np.asarray(xyz, dtype=np.float64).reshape(-1, 3), lo, hi)
+    cells = np.array([nx, ny, nz]) - 1
+    f = (p - lo) / (hi - lo) * cells
+    i0 = np.clip(np.floor(f).astype(np.int64), 0, cells - 1)
+    w = f - i0
+    out = np.zeros((len(p), 3))
+    for dx in (0, 1):
+        for dy in (0, 1):
+            for dz in (0, 1):
+                idx = (i0[:, 0] + dx) * ny * nz + (i0[:, 1] + dy) * nz + (i0[:, 2] + dz)
+                wt = ((w[:, 0] if dx else 1 - w[:, 0]) * (w[:, 1] if dy else 1 - w[:, 1])
+                      * (w[:, 2] if dz else 1 - w[:, 2]))
+                out += wt[:, None] * table[:3, cam, idx].T
+    return out
+
+
+def otf_text_table(table: np.ndarray, n, volume) -> str:
+    """An OTF table [4][n_cam][n_grid] in the reference's OTF file layout
+    (OTF::loadParam, src/srcSTB/OTF.cpp:195-243)."""
+    n_cam, ng = table.shape[1], table.shape[2]
+
+    def block(q):
+        return "\n".join(",".join(repr(float(v)) for v in table[q, c]) for c in range(n_cam))
+    return "\n".join([
+        "# Size: (n_cam,nx,ny,nz,n_grid)", f"{n_cam},{n[0]},{n[1]},{n[2]},{ng}",
+        "# Boundary: (xmin,xmax,ymin,ymax,zmin,zmax)", ",".join(repr(float(v)) for v in volume),
+        "# a: (n_cam,n_grid)", block(0), "# b: (n_cam,n_grid)", block(1),
+        "# c: (n_cam,n_grid)", block(2), "# alpha: (n_cam,n_grid)", block(3),
+    ]) + "\n"
+
+
+# ----------------------------------------------------------------------------- flows
+def abc_velocity(xyz: np.ndarray, A: float = 1.0, B: float = 1.0, C_: float = 1.0,
+                 wavelength: float = 40.0) -> np.ndarray:
+    """Arnold-Beltrami-Childress flow, k = 2 pi / wavelength:
+    u = A sin kz + C cos ky, v = B sin kx + A cos kz, w = C sin ky + B cos kx."""
+    k = 2.0 * math.pi / wavelength
+    x, y, z = xyz[:, 0], xyz[:, 1], xyz[:, 2]
+    return np.stack([A * np.sin(k * z) + C_ * np.cos(k * y),
+                     B * np.sin(k * x) + A * np.cos(k * z),
+                     C_ * np.sin(k * y) + B * np.cos(k * x)], axis=1)
+
+
+# ----------------------------------------------------------------------------- torch rendering
+def _project_torch(cm, P):
+    """The camera's projection of torch points P (n, 3) float64 (pinhole without
+    distortion, or the cubic polynomial)."""
+    import torch
+    if isinstance(cm, PolyCam):
+        out = []
+        for co in (cm.u_coeffs, cm.v_coeffs):
+            acc = torch.zeros(len(P), dtype=torch.float64, device=P.device)
+            for c, px, py, pz in co:
+                acc = acc + float(c) * P[:, 0] ** int(px) * P[:, 1] ** int(py) * P[:, 2] ** int(pz)
+            out.append(acc)
+        return torch.stack(out, dim=1)
+    R = torch.as_tensor(cm.R, dtype=torch.float64, device=P.device)
+    T = torch.as_tensor(cm.T, dtype=torch.float64, device=P.device)
+    pc = P @ R.T + T
+    return torch.stack([pc[:, 0] / pc[:, 2] * cm.fx + cm.cx, pc[:, 1] / pc[:, 2] * cm.fy + cm.cy],
+                       dim=1)
+
+
+def _otf_torch(table, n, volume, cam, P):
+    """otf_eval on torch points."""
+    import torch
+    nx, ny, nz = n
+    lo = torch.tensor(volume[0::2], dtype=torch.float64, device=P.device)
+    hi = torch.tensor(volume[1::2], dtype=torch.float64, device=P.device)
+    p = torch.minimum(torch.maximum(P, lo), hi)
+    cells = torch.tensor([nx - 1, ny - 1, nz - 1], device=P.device)
+    f = (p - lo) / (hi - lo) * cells
+    i0 = torch.minimum(torch.clamp(torch.floor(f).long(), min=0), cells - 1)
+    w = f - i0
+    tab = torch.as_tensor(table[:3, cam], dtype=torch.float64, device=P.device)  # (3, ng)
+    out = torch.zeros((len(P), 3), dtype=torch.float64, device=P.device)
+    for dx in (0, 1):
+        for dy in (0, 1):
+            for dz in (0, 1):
+                idx = (i0[:, 0] + dx) * ny * nz + (i0[:, 1] + dy) * nz + (i0[:, 2] + dz)
+                wt = ((w[:, 0] if dx else 1 - w[:, 0]) * (w[:, 1] if dy else 1 - w[:, 1])
+                      * (w[:, 2] if dz else 1 - w[:, 2]))
+                out += wt[:, None] * tab[:, idx].T
+    return out
+
+
+def render_frame(cams, xyz: np.ndarray, otf_table: np.ndarray, otf_n, volume,
+                 noise: np.ndarray, max_val: int, dtype, device="cpu", half: int = 3):
+    """Render one frame of every camera with torch on ``device``: per particle its
+    projection by the camera's own model and its (a, b, c) from the OTF table,
+    a exp(-b dx^2 - c dy^2) over a (2 half + 1)^2 window, fused by max, plus the given
+    noise planes (n_cam, H, W), rounded and clipped.  Returns numpy (n_cam, H, W)
+    ``dtype``."""
+    import torch
+    P = torch.from_numpy(np.ascontiguousarray(xyz, dtype=np.float64)).to(device)
+    out = []
+    for ci, cm in enumerate(cams):
+        H, W = cm.n_row, cm.n_col
+        uv = _project_torch(cm, P)
+        abc = _otf_torch(otf_table, otf_n, volume, ci, P)
+        img = torch.zeros(H * W, dtype=torch.float64, device=device)
+        cu = torch.round(uv[:, 0]).long()
+        cv = torch.round(uv[:, 1]).long()
+        for dy in range(-half, half + 1):
+            for dx in range(-half, half + 1):
+                x = cu + dx
+                y = cv + dy
+                ok = (x >= 0) & (x < W) & (y >= 0) & (y < H)
+                ddx = x[ok].double() - uv[ok, 0]
+                ddy = y[ok].double() - uv[ok, 1]
+                val = abc[ok, 0] * torch.exp(-abc[ok, 1] * ddx * ddx - abc[ok, 2] * ddy * ddy)
+                img.scatter_reduce_(0, y[ok] * W + x[ok], val, reduce="amax")
+        img = img.view(H, W) + torch.from_numpy(noise[ci]).to(device, torch.float64)
+        img = torch.clamp(torch.round(img), 0, max_val)
+        out.append(img.to(torch.int32).cpu().numpy().astype(dtype))
+    return np.stack(out)
+
+
+@dataclasses.dataclass
+class PolySequence:
+    """A particle sequence seen by polynomial cameras with a spatially varying OTF."""
+    cams: List[PolyCam]
+    frames: List[np.ndarray]         # frames[t]: (n_cam, H, W) images
+    truth: List[np.ndarray]          # truth[t]: (N, 3) positions
+    ids: List[np.ndarray]
+    volume: tuple
+    otf_table: np.ndarray            # [4][n_cam][nx*ny*nz]
+    otf_n: tuple
+    max_val: int
+    dt: float
+
+    @property
+    def n_cam(self) -> int:
+        return len(self.cams)
+
+
+def px_per_mm(cam, at) -> float:
+    """Largest image motion (px) per mm of world motion at point ``at`` (the spectral
+    norm of the projection's Jacobian, central differences)."""
+    at = np.asarray(at, dtype=np.float64)
+    J = np.stack([(cam.project(at + e) - cam.project(at - e))[0] / 2e-3
+                  for e in np.eye(3) * 1e-3], axis=1)
+    return float(np.linalg.norm(J, 2))
+
+
+def make_poly_sequence(ppp: float = 0.1, n_frames: int = 100, n_cam: int = 6, size: int = 2048,
+                       volume=(-40.0, 40.0, -40.0, 40.0, -20.0, 20.0), bits: int = 16,
+                       noise_sigma: float = 20.0, otf_n=(5, 5, 5), a_range=(2400.0, 3600.0),
+                       bc_range=(0.3, 0.9), max_px_per_frame: float = 4.0,
+                       wavelength: float = 40.0, max_distortion_px: float = 2.0,
+                       seed: int = 1234, device="cpu", with_images: bool = True) -> PolySequence:
+    """Particles advected by ABC flow (A = B = C = 1, RK4 in FP64) seen by ``n_cam``
+    cubic polynomial cameras (seeded, at most ``max_distortion_px`` of distortion at
+    the corners), images of size^2 pixels with ppp * size^2 particles in ``volume``
+    (whose projection fills the images), a seeded 5x5x5 OTF grid (a in a_range, b and
+    c in bc_range), Gaussian noise, ``bits``-bit integer images.  The time step gives
+    at most ``max_px_per_frame`` of image motion; particles leaving the volume are
+    re-seeded uniformly.  Defaults: 6 cameras, 2048^2 uint16, 0.1 ppp (419,430
+    particles), 80x80x40 mm, 100 frames."""
+    rng = np.random.default_rng(seed)
+    cams = poly_rig(n_cam, size, volume, max_distortion_px, seed=seed + 1)
+    table = otf_grid(n_cam, otf_n, a_range, bc_range, seed=seed + 2)
+    n = int(round(ppp * size * size))
+    lo = np.array(volume[0::2], dtype=np.float64)
+    hi = np.array(volume[1::2], dtype=np.float64)
+    xyz = lo + (hi - lo) * rng.random((n, 3))
+    ids = np.arange(n)
+    next_id = n
+    vel = lambda p: abc_velocity(p, wavelength=wavelength)  # noqa: E731
+    probe = lo + (hi - lo) * rng.random((100000, 3))
+    vmax = float(np.max(np.linalg.norm(vel(probe), axis=1)))
+    # image motion per mm: the largest over the cameras at the volume's centre
+    c0 = 0.5 * (lo + hi)
+    ppm = max(px_per_mm(cm, c0) for cm in cams)
+    dt = max_px_per_frame / (ppm * max(vmax, 1e-9))
+    max_val = (1 << bits) - 1 if bits < 16 else 65535
+    dtype = np.uint8 if bits <= 8 else np.uint16
+    frames, truth, idl = [], [], []
+    for t in range(n_frames):
+        truth.append(xyz.copy())
+        idl.append(ids.copy())
+        if with_images:
+            nz = rng.standard_normal((n_cam, size, size), dtype=np.float32) * noise_sigma
+            frames.append(render_frame(cams, xyz, table, otf_n, volume, nz, max_val, dtype,
+                                       device))
+        xyz = rk4(vel, xyz, dt)
+        out = np.any((xyz < lo) | (xyz > hi), axis=1)
+        k = int(out.sum())
+        if k:
+            xyz[out] = lo + (hi - lo) * rng.random((k, 3))
+            ids[out] = np.arange(next_id, next_id + k)
+            next_id += k
+    return PolySequence(cams, frames, truth, idl, tuple(volume), table, tuple(otf_n), max_val, dt)
+
+
+def make_poly_scene(ppp: float = 0.02, size: int = 512, n_cam: int = 6,
+                    volume=(-10.0, 10.0, -10.0, 10.0, -5.0, 5.0), bits: int = 12,
+                    noise_sigma: float = 20.0, seed: int = 7, **kw) -> Scene:
+    """One frame of make_poly_sequence as a Scene (polynomial cameras, 5x5x5 OTF)."""
+    seq = make_poly_sequence(ppp=ppp, n_frames=1, n_cam=n_cam, size=size, volume=volume,
+                             bits=bits, noise_sigma=noise_sigma, seed=seed, **kw)
+    a_mid = float(np.mean(seq.otf_table[0]))
+    return Scene(seq.cams, seq.truth[0], list(seq.frames[0]), seq.volume,
+                 (a_mid, float(np.mean(seq.otf_table[1])), float(np.mean(seq.otf_table[2]))),
+                 seq.max_val, otf_table=seq.otf_table, otf_n=seq.otf_n)

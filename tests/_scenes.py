@@ -15,6 +15,8 @@ def scene(kind: str = "small"):
     if kind == "u16":       # 12-bit images, 3 cameras, non-square
         return synth.make_scene(n_particles=1500, n_cam=3, n_row=400, n_col=640, focal=2500.0,
                                 a=3000.0, noise=20.0, bits=12, seed=11)
+    if kind == "poly":      # 6 cubic polynomial cameras, 512^2 12-bit, 5x5x5 OTF, 0.01 ppp
+        return synth.make_poly_scene(ppp=0.01, size=512, n_cam=6, seed=7)
     raise KeyError(kind)
 
 
@@ -23,6 +25,11 @@ def settings(kind: str = "small") -> synth.IPRSettings:
     (src/srcSTB/Config.cpp:222-224)."""
     s = synth.IPRSettings()
     s.match_cam_count = min(s.match_cam_count, scene(kind).n_cam)
+    if kind == "poly":
+        # every camera in the build: with check cameras the reference's checkMatch
+        # leaves e_check NaN and match() throws (StereoMatch.cpp:120-127, 505-600)
+        s.min_obj_int, s.shake_width, s.tol_3d_mm = 300, 0.025, 0.03
+        s.match_cam_count = scene(kind).n_cam
     return s
 
 
@@ -35,7 +42,10 @@ def ref_oracle(kind: str = "small", threads: int = 0):
 def gpu_context(sc):
     from pyopenlpt_b200 import _ffi
     ctx = _ffi.Context(0)
-    ctx.upload_cameras([_ffi.camera_desc_from_pinhole(c) for c in sc.cams])
-    from oracle.ref import otf_table
-    ctx.upload_otf(2, 2, 2, sc.volume, otf_table(sc.n_cam, sc.otf_abc))
+    ctx.upload_cameras([_ffi.camera_desc(c) for c in sc.cams])
+    if sc.otf_table is not None:
+        ctx.upload_otf(*sc.otf_n, sc.volume, sc.otf_table)
+    else:
+        from oracle.ref import otf_table
+        ctx.upload_otf(2, 2, 2, sc.volume, otf_table(sc.n_cam, sc.otf_abc))
     return ctx

@@ -1,16 +1,19 @@
 """Regenerate tests/golden/*.json from the reference's own test fixtures.
 
 Reads (text only) the camera files under test/inputs/test_Camera and the expected
-values under test/solutions/test_Camera of the reference checkout (default
-/root/reference), as used by its test_Camera.cpp test_function_2/3/5, and writes
+values under test/solutions/test_Camera of the reference checkout (the argument,
+else $OLPT_REFERENCE_DIR, else the tree the oracle Makefile built from), as used by its test_Camera.cpp test_function_2/3/5, and writes
 camera_golden.json.  Run: python tests/golden/make_golden.py [reference_root]
 """
 import json
 import os
 import sys
 
-REF = sys.argv[1] if len(sys.argv) > 1 else "/root/reference"
 HERE = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, os.path.dirname(os.path.dirname(HERE)))
+from oracle.refdir import reference_dir  # noqa: E402
+
+REF = sys.argv[1] if len(sys.argv) > 1 else reference_dir()
 
 
 def numbers(path):

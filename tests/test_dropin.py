@@ -1,4 +1,4 @@
-"""The C++ drop-in classes and their Python module (pyopenlpt_b200.openlpt) without a
+"""The C++ drop-in classes and their Python module (pyopenlpt) without a
 GPU: module surface, the reference's config and camera formats, TIFF reading (against
 the reference's own image fixtures when the reference tree is mounted)."""
 import os
@@ -7,16 +7,19 @@ import tempfile
 import numpy as np
 import pytest
 
-from pyopenlpt_b200 import openlpt as lpt
+from oracle.refdir import reference_dir
+from pyopenlpt_b200 import openlpt  # noqa: F401  (puts the compiled module on sys.path)
 from pyopenlpt_b200 import synth
 
-REFERENCE = "/root/reference"
+import pyopenlpt as lpt  # noqa: E402  the reference's own import line
+
+REFERENCE = reference_dir()
 
 
 def test_module_surface():
     for name in ("Camera", "OTF", "Image", "ImageIO", "Pt2D", "Pt3D", "Tracer2D", "Tracer3D",
                  "ObjFlag", "BasicSetting", "TracerConfig", "STBParam", "ShakeParam", "PFParam",
-                 "SMParam", "IPRParam", "ObjectFinder2D", "StereoMatch", "Shake", "IPR", "STB",
+                 "SMParam", "IPRParam", "ObjectConfig", "ObjectFinder2D", "StereoMatch", "Shake", "IPR", "STB",
                  "Track", "run"):
         assert hasattr(lpt, name), name
 
@@ -75,7 +78,7 @@ def _load(path):
         return lpt.ImageIO("", lst).loadImg(0).to_numpy()
 
 
-@pytest.mark.skipif(not os.path.isdir(REFERENCE), reason="reference tree not mounted")
+@pytest.mark.skipif(REFERENCE is None, reason="reference tree not mounted")
 def test_tiff_reader_on_reference_fixtures():
     """PackBits and LZW+predictor TIFFs of the reference's tests: detections on the
     decoded images match the reference's known answers."""

@@ -130,14 +130,18 @@ def _roi(H, W, cx, cy, r):
     return max(rmin, 0), min(rmax, H), max(cmin, 0), min(cmax, W)
 
 
-def test_features_match_restatement(ctx):
-    sc = _scenes.scene("small")
-    s = _scenes.settings("small")
+@pytest.mark.parametrize("kind", ["small", "poly"])
+def test_features_match_restatement(ctx, kind):
+    """4 pinhole cameras with a uniform OTF, and 6 polynomial cameras with a 5x5x5 OTF."""
+    sc = _scenes.scene(kind)
+    s = _scenes.settings(kind)
     g = _scenes.gpu_context(sc)
+    n_c = sc.n_cam
+    base, one = 121 * n_c, 121 * n_c + 2 * n_c
     try:
         g.upload_images(sc.images)
         rng = np.random.default_rng(3)
-        xyz = sc.xyz[:300] + rng.normal(0, 0.03, (300, 3))
+        xyz = sc.xyz[:300] + rng.normal(0, 0.03 if kind == "small" else 0.01, (300, 3))
         g.upload_objects(xyz)
         sp = _ffi.shake_params(s, precision=0)
         feats = g.mlp_features(sp)
@@ -164,13 +168,14 @@ def test_features_match_restatement(ctx):
                             val = val + max(p, np.float32(0))
                         val = val / max(q[0], np.float32(1e-6)) if val > 0 else np.float32(0)
                     want[o, c * 121 + t] = val
-                want[o, 484 + 2 * c] = u - ru
-                want[o, 485 + 2 * c] = v - rv
-            want[o, 492] = 1.0
+                want[o, base + 2 * c] = u - ru
+                want[o, base + 1 + 2 * c] = v - rv
+            want[o, one] = 1.0
+        assert feats.shape == (len(xyz), one + 1)
         d = np.abs(feats - want)
-        print("features |diff| max", d.max())
+        print(f"{kind} features |diff| max", d.max())
         assert d.max() < 1e-4
-        assert feats[:, :484].max() > 0.5  # the particles are in the patches
+        assert feats[:, :base].max() > 0.5  # the particles are in the patches
     finally:
         g.close()
 
@@ -189,3 +194,39 @@ def test_resident_dataset_training(ctx):
     first = ctx.mlp_train_step(xs[:2048], ts[:2048], lr=0.0, update=False)
     print("resident-dataset training: loss", losses[0], "->", np.mean(losses[-20:]), "eval", first)
     assert np.mean(losses[-20:]) < 0.35 * losses[0]
+
+
+def test_six_camera_network_matches_oracle():
+    """The network of a 6-camera rig (n_in = 739, padded to 768): forward and the
+    gradients of one training step against the oracle."""
+    sc = _scenes.scene("poly")
+    g = _scenes.gpu_context(sc)
+    try:
+        n_in, n_params = g.mlp_dims()
+        assert (n_in, n_params) == (R.n_in(6), 256 * R.n_in(6) + 256 * 3 + 2 * 256 * 256 + 4 * 256 + 4)
+        rng = np.random.default_rng(21)
+        flat = R.init(9, n_in)
+        g.mlp_set_params(flat)
+        x = np.zeros((900, n_in), np.float32)
+        x[:, :726] = np.clip(rng.normal(0.2, 0.3, (900, 726)), 0, None)
+        x[:, 726:738] = rng.uniform(-0.5, 0.5, (900, 12))
+        x[:, 738] = 1.0
+        got = g.mlp_forward(x)
+        want, _ = R.forward(flat, x)
+        d = np.abs(got - want)
+        print("6-camera forward |diff| max", d.max(), "mean", d.mean())
+        assert d.max() < 3e-2 and d.mean() < 3e-3
+        t = _targets(rng, 900)
+        loss, gr = g.mlp_train_step(x, t, lr=0.0, update=False, want_grad=True)
+        loss_ref, g_ref = R.backward(flat, x, t, 1.0)
+        assert abs(loss - loss_ref) <= 2e-3 * abs(loss_ref)
+        off = 0
+        for name, shp in R.shapes(n_in):
+            k = int(np.prod(shp))
+            a, b = gr[off:off + k], g_ref[off:off + k]
+            rel = np.linalg.norm(a - b) / max(np.linalg.norm(b), 1e-12)
+            print(f"6-camera grad {name}: rel err {rel:.2e}")
+            assert rel < 2e-2, name
+            off += k
+    finally:
+        g.close()
