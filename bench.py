@@ -211,7 +211,7 @@ def reference_ipr_time(sc, s, threads: int, images=None):
     return len(out["xyz"]), dt
 
 
-REF_STB_BUDGET_S = 240.0  # convergence frames of the reference arm stop after this
+REF_STB_BUDGET_S = 400.0  # convergence frames of the reference arm stop after this
 
 
 def reference_stb(name, threads, warmup, steps, budget_s):
@@ -527,11 +527,38 @@ def frame_quality(xyz, truth):
 
 def mean_quality(qs):
     keys = ("recall_05", "ghost_05", "recall_10", "ghost_10")
-    return {k: round(float(np.mean([q[k] for q in qs])), 5) for k in keys}
+    out = {k: round(float(np.mean([q[k] for q in qs])), 5) for k in keys}
+    if qs and "ms" in qs[0]:
+        ms = float(np.sum([q["ms"] for q in qs]))
+        out.update(ms_per_frame=round(ms / len(qs), 3),
+                   particles_per_s=round(float(np.sum([q["parts"] for q in qs])) / (ms * 1e-3), 1))
+    return out
+
+
+def meets(m, plain, slack=0.005):
+    """Recall within slack of the plain form's and no higher ghost rate, at 0.05 and
+    0.1 mm."""
+    return all(m["recall_" + k] >= plain["recall_" + k] - slack and
+               m["ghost_" + k] <= plain["ghost_" + k] + 1e-9 for k in ("05", "10"))
+
+
+def timed_frame(o, stream, fn):
+    """Event-timed call on the library stream (L2 flushed first); milliseconds."""
+    torch = o.torch
+    with torch.cuda.stream(stream):
+        o.flush.zero_()
+        e0 = torch.cuda.Event(enable_timing=True)
+        e1 = torch.cuda.Event(enable_timing=True)
+        e0.record(stream)
+    fn()
+    e1.record(stream)
+    e1.synchronize()
+    return e0.elapsed_time(e1)
 
 
 def run_ours_stb(args, o: Ours, pre):
     from pyopenlpt_b200 import _ffi
+    from pyopenlpt_b200 import learned as L
     torch = o.torch
     nf = N_INIT + args.warmup + args.steps
     t_gen = time.perf_counter()
@@ -564,8 +591,15 @@ def run_ours_stb(args, o: Ours, pre):
         a = time.perf_counter()
         frame_device(ctx, t)
         init_ms.append(1e3 * (time.perf_counter() - a))
+    want_learned = (o.world == 1 and args.learn_frames > 0
+                    and WORKLOADS[args.workload].get("gen") == "poly")
+    state_init = L.stb_state(ctx) if want_learned else None
+    plain_warm = []
     for t in range(N_INIT, t0_frame):
-        frame_device(ctx, t)
+        ms = timed_frame(o, stream, lambda: frame_device(ctx, t))
+        plain_warm.append(dict(frame_quality(ctx.stb_frame_objects(), seq.truth[t]), ms=ms,
+                               parts=ctx.stb_frame_points(t)))
+    state_t0 = L.stb_state(ctx) if want_learned else None
     torch.cuda.synchronize()
 
     clocks = ClockSampler(o.local)
@@ -593,7 +627,8 @@ def run_ours_stb(args, o: Ours, pre):
         launches_q = _ffi.launch_count()
         xyz = ctx.stb_frame_objects()
         plain_objs[t] = xyz
-        quality.append(frame_quality(xyz, seq.truth[t]))
+        quality.append(dict(frame_quality(xyz, seq.truth[t]), ms=e0.elapsed_time(e1),
+                            parts=ctx.stb_frame_points(t)))
         launches0 += _ffi.launch_count() - launches_q
     torch.cuda.synchronize()
     o.barrier()
@@ -637,6 +672,10 @@ def run_ours_stb(args, o: Ours, pre):
                  "track_lists_after": dict(zip(_ffi.TRACK_LISTS, lists)),
                  "quality_vs_truth": mean_quality(quality),
                  "generation_s": round(t_gen, 1)}
+        if want_learned:
+            extra["learned"] = learned_stb(args, o, seq, s, st, nf, t0_frame, new_ctx,
+                                           frame_device, state_init, state_t0, plain_warm,
+                                           quality)
         if o.world == 1 and o.prec == 0 and not args.no_fp64_check:
             extra["fp64_check"] = fp64_check(args, o, seq, s, st, nf, t0_frame, new_ctx,
                                              frame_device, plain_objs, res32, H, W)
@@ -651,6 +690,122 @@ def run_ours_stb(args, o: Ours, pre):
         extra.update(pre)
         o.line(prof, dev_ms, parts, e2e_s, e2e_parts, bi, bo // max(1, args.steps), launches,
                clk, workload_config(args.workload, s, seq=seq, st=st), cpu, extra)
+
+
+def learned_stb(args, o, seq, s, st, nf, t0_frame, new_ctx, frame_device, state_init, state_t0,
+                plain_warm, plain_timed):
+    """The learned form on the same frames as the plain form.
+
+    1. Tuples from the plain GPU shake on a separate seeded sequence of the same
+       workload: prediction-like starts (true particles displaced by 0.3 and 1 px,
+       plus 10% uniform points) and the candidates of the first IPR loop.
+    2. Training on the device (olpt_mlp_train).
+    3. Calibration on the warm-up frames, from the plain tracker's tracks after the
+       initial phase: the fastest settings whose recall is within 0.5% of the plain
+       form's and whose ghost rate is not higher, at 0.05 and 0.1 mm.
+    4. Evaluation on the timed frames, from the plain tracker's tracks at the first
+       timed frame, device-timed like the plain form."""
+    import dataclasses
+    from pyopenlpt_b200 import learned as L
+    torch = o.torch
+    mm_px = 1.0 / max(synth.px_per_mm(c, np.zeros(3)) for c in seq.cams)
+    ls0 = L.LearnedSettings(out_scale_mm=0.5 * mm_px, ghost_tol_mm=1.5 * mm_px,
+                            refine_width_mm=0.4 * s.shake_width, ghost_logit=5.0,
+                            refine_loops=1, fallback_residual=1e9)
+    # 1. tuples
+    t_c = time.perf_counter()
+    tseq, _, _ = build_sequence(args.workload, 4321 + o.rank, args.learn_frames,
+                                device=f"cuda:{o.local}")
+    ctx = new_ctx()
+    xs, ts = [], []
+    per_frame = max(1, args.learn_tuples // max(1, args.learn_frames))
+    for f in range(args.learn_frames):
+        ctx.upload_images(list(tseq.frames[f]))
+        x, t = L.collect_predictions(ctx, tseq.truth[f], s, ls0, (0.3 * mm_px, 1.0 * mm_px),
+                                     tseq.volume, n_max=int(0.8 * per_frame), seed=f)
+        xs.append(x)
+        ts.append(t)
+        ctx.upload_images(list(tseq.frames[f]))
+        x, t = L.collect_ipr(ctx, tseq.truth[f], s, tseq.volume, ls0, loops=1)
+        room = max(0, per_frame - len(xs[-1]))
+        if len(x) > room:
+            keep = np.random.default_rng(f).choice(len(x), room, replace=False)
+            x, t = x[keep], t[keep]
+        xs.append(x)
+        ts.append(t)
+    x = np.concatenate(xs)
+    t = np.concatenate(ts)
+    del xs, ts, tseq
+    t_collect = time.perf_counter() - t_c
+    # 2. training
+    ctx.mlp_init(1)
+    t_t = time.perf_counter()
+    losses = L.train(ctx, x, t, steps=args.learn_steps, batch=8192, lr=2e-3)
+    t_train = time.perf_counter() - t_t
+    n_tuples, ghost_share = len(x), float(np.mean(t[:, 3]))
+    del x, t
+    params = ctx.mlp_get_params()
+    ctx.close()
+
+    def run(ls, state, frames):
+        c = new_ctx()
+        c.mlp_set_params(params)
+        c.learned_configure(ls.params(enable=True))
+        L.set_stb_state(c, state)
+        st_ = torch.cuda.ExternalStream(c.stream())
+        a0, b0 = c.learned_stats()
+        out = []
+        for f in frames:
+            ms = timed_frame(o, st_, lambda: frame_device(c, f))
+            out.append(dict(frame_quality(c.stb_frame_objects(), seq.truth[f]), ms=ms,
+                            parts=c.stb_frame_points(f)))
+        a1, b1 = c.learned_stats()
+        c.close()
+        return out, (b1 - b0) / max(1, a1 - a0)
+
+    # 3. calibration on the warm-up frames
+    warm = list(range(N_INIT, t0_frame))
+    pw = mean_quality(plain_warm)
+    sweep, chosen = [], None
+    grid = [dict(refine_loops=1, ghost_logit=5.0, fallback_residual=1e9),
+            dict(refine_loops=1, ghost_logit=5.0, fallback_residual=0.3),
+            dict(refine_loops=1, ghost_logit=5.0, fallback_residual=0.1),
+            dict(refine_loops=2, ghost_logit=5.0, fallback_residual=0.3),
+            dict(refine_loops=2, ghost_logit=8.0, fallback_residual=0.1),
+            dict(refine_loops=2, ghost_logit=8.0, fallback_residual=0.03)]
+    for g in grid:
+        ls = dataclasses.replace(ls0, **g)
+        res, fb = run(ls, state_init, warm)
+        m = mean_quality(res)
+        ok = meets(m, pw)
+        sweep.append(dict(g, **m, fallback_fraction=round(fb, 4), meets=ok))
+        if ok and (chosen is None or m["ms_per_frame"] < chosen[1]["ms_per_frame"]):
+            chosen = (ls, m)
+    ls = chosen[0] if chosen is not None else dataclasses.replace(ls0, **grid[-1])
+    # 4. evaluation on the timed frames
+    res, fb = run(ls, state_t0, list(range(t0_frame, nf)))
+    lm, pm = mean_quality(res), mean_quality(plain_timed)
+    return {
+        "form": "MLP proposal on every prediction and IPR candidate (ghosts dropped), "
+                "refine_loops plain shake iterations, plain-shake fallback above the "
+                "residual threshold",
+        "train": {"frames": args.learn_frames, "tuples": n_tuples,
+                  "ghost_share": round(ghost_share, 4), "steps": len(losses),
+                  "collect_s": round(t_collect, 1), "train_s": round(t_train, 1),
+                  "loss_first": round(losses[0], 4),
+                  "loss_last50": round(float(np.mean(losses[-50:])), 4)},
+        "calibration": {"frames": warm, "plain": pw, "sweep": sweep,
+                        "chosen": {"refine_loops": ls.refine_loops, "ghost_logit": ls.ghost_logit,
+                                   "fallback_residual": ls.fallback_residual,
+                                   "refine_width_mm": ls.refine_width_mm,
+                                   "out_scale_mm": ls.out_scale_mm},
+                        "met": chosen is not None},
+        "eval": {"frames": list(range(t0_frame, nf)), "plain": pm, "learned": lm,
+                 "fallback_fraction": round(fb, 4),
+                 "speedup_particles_per_s": round(lm["particles_per_s"] / pm["particles_per_s"], 3),
+                 "speedup_time": round(pm["ms_per_frame"] / lm["ms_per_frame"], 3),
+                 "meets_recall_and_ghost": meets(lm, pm)},
+    }
 
 
 def fp64_check(args, o, seq, s, st, nf, t0_frame, new_ctx, frame_device, objs32, res32, H, W):
@@ -707,7 +862,7 @@ def learned_comparison(args, o: Ours):
     ctx = _ffi.Context(o.local)
     t0 = time.perf_counter()
     xs, ts = [], []
-    for i in range(args.learn_frames):
+    for i in range(args.learn_ipr_frames):
         x, t = L.collect(ctx, L.scene(i, LEARN_PPP[i % len(LEARN_PPP)]), s, ls)
         xs.append(x)
         ts.append(t)
@@ -804,7 +959,7 @@ def learned_comparison(args, o: Ours):
                     "refine shake, calibrated loop count; eval: device time per IPR, L2 "
                     "flushed; batched: wall time, frames on concurrent contexts/streams",
         "batched": batched,
-        "train": {"frames": args.learn_frames, "tuples": n_tuples, "steps": len(losses),
+        "train": {"frames": args.learn_ipr_frames, "tuples": n_tuples, "steps": len(losses),
                   "collect_s": round(t_collect, 1), "train_s": round(t_train, 1),
                   "loss_first": round(losses[0], 4),
                   "loss_last50": round(float(np.mean(losses[-50:])), 4)},
@@ -862,24 +1017,35 @@ def detection_roofline(args, o: Ours):
     ctx.close()
     peak, peak_kind = measured_peak_hbm()
     dets = int(counts.sum())
-    algo = img_bytes / n + 24.0 * dets  # image read + detections written (x, y f64, row/col i32)
-    achieved = algo / (ms / n * 1e-3) / 1e9
+    # algorithmic bytes: the image read once + 8 B per detection (an FP32 x, y pair);
+    # the kernel writes FP64 x, y and the int32 peak pixel (24 B per detection), which
+    # is stated beside it
+    algo = img_bytes / n + 8.0 * dets
+    written = img_bytes / n + 24.0 * dets
+    sec = ms / n * 1e-3
+    achieved = algo / sec / 1e9
     return {"kernel": "detect_kernel<uint16_t> (staged single read)",
             "images": f"{DET_CAMS} x {DET_SIZE}x{DET_SIZE} uint16 (12-bit), {n_spots} spots "
                       f"each (0.1 ppp), noise sigma 20, threshold 300",
             "detections_per_launch": dets, "launch_us": round(ms / n * 1e3, 2),
-            "bytes_per_launch": algo, "achieved": achieved, "peak": peak, "unit": "GB/s",
+            "bytes_per_launch": algo,
+            "bytes_per_launch_note": "image + 8 B per detection (FP32 x, y)",
+            "achieved": achieved, "peak": peak, "unit": "GB/s",
             "frac": achieved / peak, "peak_source": peak_kind, "launches": n,
+            "bytes_moved_per_launch": written,
+            "bytes_moved_note": "image + 24 B per detection as written (FP64 x, y, int32 "
+                                "row/col)",
+            "achieved_moved": written / sec / 1e9,
             "timing": "CUDA events on the library stream, L2 flushed before each launch"}
 
 
 def run_ours(args):
     o = Ours(args)
     learned = None
-    if o.world == 1 and args.learn_frames > 0:
+    if o.world == 1 and args.learn_ipr_frames > 0:
         learned = learned_comparison(args, o)
         o.torch.cuda.synchronize()
-    pre = {} if learned is None else {"learned": learned}
+    pre = {} if learned is None else {"learned_ipr_1024_u8": learned}
     if o.world == 1 and not args.no_detection_roofline:
         pre["detection_roofline"] = detection_roofline(args, o)
         o.torch.cuda.synchronize()
@@ -905,9 +1071,15 @@ def main():
                     help="skip the FP32-vs-FP64 comparison of the STB workload")
     ap.add_argument("--no-detection-roofline", action="store_true",
                     help="skip the detection kernel's roofline measurement")
-    ap.add_argument("--learn-frames", type=int, default=24,
-                    help="frames of training tuples for the learned comparison (0 = skip)")
+    ap.add_argument("--learn-frames", type=int, default=3,
+                    help="frames of training tuples for the learned form of the STB "
+                         "workload (0 = skip)")
+    ap.add_argument("--learn-ipr-frames", type=int, default=24,
+                    help="frames of training tuples for the learned single-frame IPR "
+                         "comparison at 1024^2 (0 = skip)")
     ap.add_argument("--learn-steps", type=int, default=3000)
+    ap.add_argument("--learn-tuples", type=int, default=2_000_000,
+                    help="training tuples of the learned form on the STB workloads")
     ap.add_argument("--learn-reps", type=int, default=5)
     ap.add_argument("--learn-batch", type=int, default=4,
                     help="frames processed at once in the batched learned comparison")

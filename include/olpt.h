@@ -124,6 +124,13 @@ olpt_status_t olpt_find_peaks(olpt_ctx* ctx, double min_obj_int, int64_t* counts
 /* Download detections of one camera in raster order: xy (n x 2, x = col, y = row) and
  * the integer peak pixel rc (n x 2: row, col); either may be NULL. */
 olpt_status_t olpt_get_peaks(olpt_ctx* ctx, int cam, double* xy, int32_t* rc, int64_t cap);
+/* Failure-detection test hook (no reference counterpart): in the next olpt_find_peaks
+ * that uses the staged single-read kernel, the row band with this ticket (tickets
+ * number the bands of all cameras in launch order, camera 0 first) never publishes its
+ * detection count, and the bands after it give up their bounded look-back wait after
+ * wait_limit_ns (at most 2 s) instead of the default 2 s.  That olpt_find_peaks then
+ * returns OLPT_ERR_TIMEOUT with its results void, and the context stays usable. */
+olpt_status_t olpt_test_hold_detection_band(olpt_ctx* ctx, int ticket, int64_t wait_limit_ns);
 /* Replace the detections of every camera with host lists (n_cam arrays of n x 2). */
 olpt_status_t olpt_detections_upload(olpt_ctx* ctx, int n_cam, const int64_t* counts,
                                      const double* const* xy);

@@ -580,6 +580,15 @@ olpt_status_t olpt_stereo_match(olpt_ctx* ctx, const olpt_sm_params* p, int64_t*
   });
 }
 
+olpt_status_t olpt_test_hold_detection_band(olpt_ctx* ctx, int ticket, int64_t wait_limit_ns) {
+  return guard(ctx, [&] {
+    OLPT_REQUIRE(ticket >= 0 && wait_limit_ns > 0 && wait_limit_ns <= 2000000000ll,
+                 OLPT_ERR_INVALID_ARG, "ticket >= 0 and 0 < wait_limit_ns <= 2 s");
+    ctx->test_hold_ticket = ticket;
+    ctx->test_wait_limit_ns = (unsigned long long)wait_limit_ns;
+  });
+}
+
 olpt_status_t olpt_stereo_near_log_enable(olpt_ctx* ctx, double band_px, int64_t capacity) {
   return guard(ctx, [&] {
     OLPT_REQUIRE(band_px >= 0.0 && capacity >= 0, OLPT_ERR_INVALID_ARG,

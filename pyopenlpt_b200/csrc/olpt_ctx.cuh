@@ -318,12 +318,15 @@ struct MlpWork {
   DevBuf master, grad, am, av, wb1, wb2, wb3, wt2, wt3;
   DevBuf x, xt, xin, tgt, z1, z2, z3, h1, h2, h3, h1t, h2t, o, dout;
   DevBuf dz1f, dz2f, dz3f, dz2b, dz3b, dz1t, dz2t, dz3t, part, hpart, loss, err;
-  DevBuf keep, pos, start_xyz, act, nres, ds_x, ds_t, loss_hist;
+  // learned shake: keep[i] = 1 for the input objects the network did not drop (the
+  // objects left are the kept ones in input order), pos = their exclusive scan; fb =
+  // fallback counter
+  DevBuf keep, pos, start_xyz, act, nres, ds_x, ds_t, loss_hist, fb;
   void release(cudaStream_t s) {
     for (DevBuf* b : {&master, &grad, &am, &av, &wb1, &wb2, &wb3, &wt2, &wt3, &x, &xt, &xin, &tgt,
                       &z1, &z2, &z3, &h1, &h2, &h3, &h1t, &h2t, &o, &dout, &dz1f, &dz2f, &dz3f,
                       &dz2b, &dz3b, &dz1t, &dz2t, &dz3t, &part, &hpart, &loss, &err, &keep, &pos,
-                      &start_xyz, &act, &nres, &ds_x, &ds_t, &loss_hist})
+                      &start_xyz, &act, &nres, &ds_x, &ds_t, &loss_hist, &fb})
       b->release(s);
     ready = false;
     cap = 0;
@@ -394,6 +397,9 @@ struct olpt_ctx {
   } det_map[OLPT_MAX_CAM];
   olpt::DevBuf band_counts, band_offsets;
   olpt::DevBuf lut_u8, lut_u16;  // log(max(v, 1e-4)) of every integer level
+  // failure-detection test hook of the next staged detection launch (-1 = off)
+  int test_hold_ticket = -1;
+  unsigned long long test_wait_limit_ns = 0;
 
   // stereo matching
   olpt::StereoWork sm;

@@ -337,6 +337,11 @@ struct DetArgs {
   int min_level;            // integer images: v < min_level  <=>  (double)v < min_int
   const double* lut;        // integer images only
   unsigned long long* dc;   // det_counts words
+  // failure-detection tests only (olpt_test_hold_detection_band): the band with this
+  // ticket never publishes its count, and the look-back waits give up after
+  // wait_limit_ns; -1 / the default limit otherwise
+  int hold_ticket;
+  unsigned long long wait_limit_ns;
 };
 
 // A band state is read as one word (flag and count together), so a relaxed load is
@@ -603,7 +608,8 @@ __global__ void __launch_bounds__(kDetThreads, 3) detect_kernel(const __grid_con
     }
     const unsigned long long total = (unsigned long long)__shfl_sync(0xffffffffu, acc, 0);
     if (lane == 0) s_total = acc;
-    if (lane == 0) st_release_u64(state, (band == 0 ? kStPrefix : kStAggregate) | total);
+    const bool held = tk == a.hold_ticket;
+    if (lane == 0 && !held) st_release_u64(state, (band == 0 ? kStPrefix : kStAggregate) | total);
     // 3. look-back over windows of 32 earlier bands: sum the aggregates down to the
     //    nearest published prefix (bands before the camera's first count as an empty
     //    prefix); wait while a band above that prefix has published nothing yet
@@ -624,7 +630,7 @@ __global__ void __launch_bounds__(kDetThreads, 3) detect_kernel(const __grid_con
           if (lane == 0) {
             const uint64_t now = umma::global_timer();
             if (t0 == 0) t0 = now;
-            else if (now - t0 > umma::kWaitLimitNs) expired = 1;
+            else if (now - t0 > a.wait_limit_ns) expired = 1;
           }
           if (__shfl_sync(0xffffffffu, expired, 0)) {
             if (lane == 0) atomicOr(dc + kDcErr, 2ull);
@@ -641,8 +647,9 @@ __global__ void __launch_bounds__(kDetThreads, 3) detect_kernel(const __grid_con
         if (pmask) break;
         top -= 32;
       }
-      if (lane == 0) st_release_u64(state, kStPrefix | (prefix + total));
+      if (lane == 0 && !held) st_release_u64(state, kStPrefix | (prefix + total));
     }
+    if (held) ok = 0;
     if (lane == 0) {
       if (band == c.n_bands - 1) dc[cam] = prefix + total;
       s_prefix = (long long)prefix;
@@ -909,6 +916,9 @@ void find_peaks_device(olpt_ctx* ctx, double min_int, bool sync_counts) {
     const size_t words = (size_t)kDcState + blocks;
     ctx->det_counts.ensure(words * sizeof(int64_t), ctx->stream);
     a.dc = ctx->det_counts.as<unsigned long long>();
+    a.hold_ticket = ctx->test_hold_ticket;
+    a.wait_limit_ns = ctx->test_hold_ticket >= 0 ? ctx->test_wait_limit_ns : umma::kWaitLimitNs;
+    ctx->test_hold_ticket = -1;
     // totals, error word, ticket and band states start at zero
     OLPT_CUDA(cudaMemsetAsync(ctx->det_counts.p, 0, words * sizeof(int64_t), ctx->stream));
     if (blocks > 0) {

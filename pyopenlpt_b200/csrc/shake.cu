@@ -1175,8 +1175,8 @@ static void learned_impl(olpt_ctx* ctx, const ShakeParams& sp) {
                            M.nres.as<double>());
     // 4. fallback: the full plain shake for objects whose residue stays high
     M.act.ensure((size_t)n + 16, s);
-    M.keep.ensure(16, s);
-    int* cnt = M.keep.as<int>();
+    M.fb.ensure(16, s);
+    int* cnt = M.fb.as<int>();
     OLPT_CUDA(cudaMemsetAsync(cnt, 0, sizeof(int), s));
     fallback_kernel<Real><<<OLPT_G(nblk(n)), 256, 0, s>>>(
         M.nres.as<double>(), ctx->shk.otfp.as<Real>(), ctx->cams_d.as<CamDev>(), C, n,

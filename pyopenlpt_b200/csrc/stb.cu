@@ -1042,12 +1042,33 @@ void conv_phase(olpt_ctx* ctx, int frame) {
                               cudaMemcpyHostToDevice, s));
     init_pred_kernel<<<OLPT_G(nblk(n_la)), 256, 0, s>>>(ctx->obj.flags.as<uint8_t>(),
                                                        ctx->obj.score.as<double>(), n_la);
+    // with the learned proposal configured, the predictions go through the learned
+    // shake, which drops the network's ghosts (they end like ghost-flagged tracks)
+    const bool learned = ctx->mlp.lp.enable != 0;
     pause();
-    shake_device(ctx, S.ipr.shake);
+    if (learned)
+      learned_shake_device(ctx, S.ipr.shake);
+    else
+      shake_device(ctx, S.ipr.shake);
     residual_device(ctx, S.ipr.shake, true, true);
     resume();
-    const std::vector<double> sx = download(ctx->obj.xyz.as<double>(), 3 * (size_t)n_la, s);
-    const std::vector<uint8_t> fl = download(ctx->obj.flags.as<uint8_t>(), n_la, s);
+    const int64_t n_out = ctx->obj.n;
+    const std::vector<double> sx0 = download(ctx->obj.xyz.as<double>(), 3 * (size_t)n_out, s);
+    const std::vector<uint8_t> fl0 = download(ctx->obj.flags.as<uint8_t>(), (size_t)n_out, s);
+    std::vector<double> sx(3 * (size_t)n_la, 0.0);
+    std::vector<uint8_t> fl(n_la, 1);
+    if (learned) {
+      const std::vector<int> keep = download(ctx->mlp.keep.as<int>(), n_la, s);
+      int64_t j = 0;
+      for (int i = 0; i < n_la; ++i)
+        if (keep[i] && j < n_out) {
+          std::copy(&sx0[3 * j], &sx0[3 * j] + 3, &sx[3 * i]);
+          fl[i] = fl0[j++];
+        }
+    } else {
+      sx = sx0;
+      fl = fl0;
+    }
     TrackList kept;
     kept.reserve(n_la);
     for (int i = 0; i < n_la; ++i) {

@@ -199,3 +199,89 @@ def calibrate(ctx: _ffi.Context, sc: synth.Scene, s: synth.IPRSettings, ls: Lear
         if meets(m, plain, slack):
             return s.n_loop_ipr, cand, plain, sweep
     return s.n_loop_ipr, dataclasses.replace(ls, fallback_residual=0.0), plain, sweep
+
+
+# ----------------------------------------------------------------------------- STB rigs
+def bind_rig(ctx: _ffi.Context, rig) -> None:
+    """Cameras (pinhole or polynomial) and OTF (uniform or a grid) of a scene or
+    sequence into the context."""
+    ctx.upload_cameras([_ffi.camera_desc(c) for c in rig.cams])
+    if getattr(rig, "otf_table", None) is not None:
+        ctx.upload_otf(*rig.otf_n, rig.volume, rig.otf_table)
+    else:
+        ctx.upload_otf(2, 2, 2, rig.volume, synth.otf_table_array(len(rig.cams), rig.otf_abc))
+
+
+def collect_predictions(ctx: _ffi.Context, truth: np.ndarray, s: synth.IPRSettings,
+                        ls: LearnedSettings, sigma_mm: Sequence[float], volume,
+                        frac_random: float = 0.1, n_max: Optional[int] = None,
+                        seed: int = 0) -> Tuple[np.ndarray, np.ndarray]:
+    """Tuples at the starting points the STB frame loop shakes: true particles
+    displaced by Gaussian noise (the predictions of live tracks; the sigmas are used
+    in equal shares), plus ``frac_random`` of uniform points in the volume (the
+    predictions of lost tracks).  Features against the residual with all of them,
+    the converged plain-shake correction, and a ghost label (no true particle within
+    ghost_tol_mm of the converged position).  The context holds the frame's images."""
+    rng = np.random.default_rng(seed)
+    base = truth if n_max is None or n_max >= len(truth) else truth[
+        rng.choice(len(truth), n_max, replace=False)]
+    parts = np.array_split(base, len(sigma_mm))
+    starts = [p + rng.normal(0.0, sg, p.shape) for p, sg in zip(parts, sigma_mm)]
+    lo = np.array(volume[0::2], dtype=np.float64)
+    hi = np.array(volume[1::2], dtype=np.float64)
+    n_rand = int(frac_random * len(base))
+    starts.append(lo + (hi - lo) * rng.random((n_rand, 3)))
+    x0 = np.concatenate(starts)
+    sp = _ffi.shake_params(s, 0)
+    ctx.upload_objects(x0)
+    x = ctx.mlp_features(sp)
+    ctx.shake(sp)
+    o = ctx.objects()
+    d, _ = cKDTree(truth).query(o["xyz"])
+    t = np.zeros((len(x0), 4), np.float32)
+    t[:, :3] = (o["xyz"] - x0) / ls.out_scale_mm
+    t[:, 3] = (d > ls.ghost_tol_mm).astype(np.float32)
+    return x, t
+
+
+def collect_ipr(ctx: _ffi.Context, truth: np.ndarray, s: synth.IPRSettings, volume,
+                ls: LearnedSettings, loops: int = 1) -> Tuple[np.ndarray, np.ndarray]:
+    """IPR-candidate tuples of the frame in the context (the first ``loops`` IPR loops
+    run step by step, as ``collect`` does for a scene)."""
+    ctx.learned_configure(ls.params(enable=False))
+    sm = _ffi.sm_params(s, volume)
+    sp = _ffi.shake_params(s, 0)
+    tree = cKDTree(truth)
+    tol0 = sm.tol_2d_px
+    xs: List[np.ndarray] = []
+    ts: List[np.ndarray] = []
+    for loop in range(loops):
+        sm.tol_2d_px = tol0 * 1.5 ** loop
+        ctx.find_peaks(s.min_obj_int)
+        _, nm = ctx.stereo_match(sm)
+        if nm == 0:
+            break
+        x = ctx.mlp_features(sp)
+        x0 = ctx.objects()["xyz"]
+        ctx.shake(sp)
+        o = ctx.objects()
+        d, _ = tree.query(o["xyz"])
+        t = np.zeros((nm, 4), np.float32)
+        t[:, :3] = (o["xyz"] - x0) / ls.out_scale_mm
+        t[:, 3] = (d > ls.ghost_tol_mm).astype(np.float32)
+        xs.append(x)
+        ts.append(t)
+        ctx.residual(sp, use_flags=True, make_current=True)
+    if not xs:
+        return np.zeros((0, ctx.mlp_dims()[0]), np.float32), np.zeros((0, 4), np.float32)
+    return np.concatenate(xs), np.concatenate(ts)
+
+
+def stb_state(ctx: _ffi.Context):
+    """The four track lists of a tracker (rows of track id, frame, xyz)."""
+    return [ctx.stb_tracks(w) for w in range(4)]
+
+
+def set_stb_state(ctx: _ffi.Context, state) -> None:
+    for w, (tid, fr, xyz) in enumerate(state):
+        ctx.stb_set_tracks(w, tid, fr, xyz)

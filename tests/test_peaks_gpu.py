@@ -5,6 +5,7 @@ import dataclasses
 import numpy as np
 import pytest
 
+from pyopenlpt_b200 import _ffi
 from tests import _scenes
 
 pytestmark = pytest.mark.gpu
@@ -164,3 +165,23 @@ def test_peaks_inactive_camera():
         assert counts[c] == len(want)
         xy, _ = ctx.get_peaks(c, counts[c])
         assert np.array_equal(xy, want)
+
+
+def test_lookback_timeout_reports_and_context_recovers():
+    """A band that never publishes its count (the failure-detection hook) makes the
+    bands after it give up their bounded look-back wait (1 ms here): olpt_find_peaks
+    returns OLPT_ERR_TIMEOUT, and the same context then detects normally again."""
+    import ctypes as C
+    sc = _scenes.scene("small")
+    ctx = _scenes.gpu_context(sc)
+    ctx.upload_images(sc.images)
+    want = ctx.find_peaks(30)
+    L = _ffi.lib()
+    for ticket in (0, 3):
+        assert L.olpt_test_hold_detection_band(ctx.h, ticket, C.c_int64(1_000_000)) == 0
+        with pytest.raises(_ffi.OlptError) as e:
+            ctx.find_peaks(30)
+        assert e.value.code == 4  # OLPT_ERR_TIMEOUT
+        assert np.array_equal(ctx.find_peaks(30), want)
+    assert L.olpt_test_hold_detection_band(ctx.h, -1, C.c_int64(1000)) == 1
+    ctx.close()
