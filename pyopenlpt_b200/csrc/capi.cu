@@ -2,6 +2,8 @@
 // Declarations and reference citations: include/olpt.h.
 #include <cuda_runtime.h>
 
+#include <cstring>
+
 #include <algorithm>
 
 #include <cmath>
@@ -145,6 +147,7 @@ OtfView otf_view(olpt_ctx* ctx) {
     v.d[k] = ctx->otf.d[k];
   }
   v.table = ctx->otf_table.as<double>();
+  v.alpha_zero = ctx->otf.alpha_zero;
   return v;
 }
 
@@ -325,6 +328,15 @@ olpt_status_t olpt_cameras_upload(olpt_ctx* ctx, const olpt_camera_desc* cams, i
           DV2[d0] = V[d0];
           DV2[d1] = std::max(V[d1] - 1, 0.0);
         }
+        // exponents all in {0, 1, 2, 3}: the device evaluates the powers once per point
+        auto small = [](double e) { return e == 0.0 || e == 1.0 || e == 2.0 || e == 3.0; };
+        c.pow3 = 1;
+        for (int i2 = 0; i2 < n; ++i2)
+          for (int j = 1; j < 4; ++j)
+            if (!small(c.ucoef[4 * i2 + j]) || !small(c.vcoef[4 * i2 + j]) ||
+                !small(c.ducoef[4 * i2 + j]) || !small(c.dvcoef[4 * i2 + j]) ||
+                !small(c.ducoef[4 * (i2 + n) + j]) || !small(c.dvcoef[4 * (i2 + n) + j]))
+              c.pow3 = 0;
       }
     }
     ctx->cams_h = h;
@@ -426,6 +438,13 @@ olpt_status_t olpt_otf_upload(olpt_ctx* ctx, int nx, int ny, int nz, const doubl
       o.d[k] = (o.bmax[k] - o.bmin[k]) / (n[k] - 1);  // OTF::setGrid (OTF.cpp:146-157)
     }
     const size_t bytes = (size_t)4 * ctx->n_cam * o.n_grid * sizeof(double);
+    o.alpha_zero = 1;
+    const double* alpha = abca + (size_t)3 * ctx->n_cam * o.n_grid;
+    for (size_t i = 0; i < (size_t)ctx->n_cam * o.n_grid; ++i) {
+      uint64_t bits;
+      std::memcpy(&bits, alpha + i, sizeof(bits));
+      if (bits != 0) o.alpha_zero = 0;
+    }
     ctx->otf_table.ensure(bytes, ctx->stream);
     OLPT_CUDA(cudaMemcpyAsync(ctx->otf_table.p, abca, bytes, cudaMemcpyHostToDevice, ctx->stream));
     OLPT_CUDA(cudaStreamSynchronize(ctx->stream));

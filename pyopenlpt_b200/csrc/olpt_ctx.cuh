@@ -100,6 +100,7 @@ struct OtfDev {
   double bmin[3], bmax[3];
   double d[3];  // grid spacing
   double* table = nullptr;  // [4][n_cam][n_grid] a,b,c,alpha (device)
+  int alpha_zero = 0;       // every alpha entry is +0.0 (cos = 1, sin = +0 exactly)
 };
 
 // Per-camera 2D detection list (SoA, FP64 like the reference's Pt2D).

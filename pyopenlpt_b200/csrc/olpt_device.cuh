@@ -32,6 +32,7 @@ struct CamDev {
   // polynomial
   int ref_plane;  // 1 = REF_X, 2 = REF_Y, 3 = REF_Z
   int n_coeff;
+  int pow3;       // every exponent (of the model and its derivatives) is 0, 1, 2 or 3
   double plane[2];
   double ucoef[OLPT_MAX_POLY * 4];
   double vcoef[OLPT_MAX_POLY * 4];
@@ -191,20 +192,49 @@ __device__ __forceinline__ double poly_pow(double x, double e) {
   return pow(x, e);
 }
 
+// The powers 0..3 of a point's coordinates, each the value poly_pow returns, so that
+// a model whose exponents are all 0..3 (pow3) multiplies table entries instead of
+// evaluating one power per term: the same factors in the same order.
+__device__ __forceinline__ void poly_powers(const double P[3], double pw[3][4]) {
+#pragma unroll
+  for (int j = 0; j < 3; ++j) {
+    pw[j][0] = 1.0;
+    pw[j][1] = P[j];
+    pw[j][2] = poly_pow(P[j], 2.0);
+    pw[j][3] = poly_pow(P[j], 3.0);
+  }
+}
+
 // Camera::polyProject (Camera.cpp:969-990).
 __device__ __forceinline__ void poly_project(const CamDev& c, double X, double Y, double Z,
                                              double& u, double& v) {
   const double P[3] = {X, Y, Z};
   double su = 0, sv = 0;
-  for (int i = 0; i < c.n_coeff; ++i) {
-    double uv = c.ucoef[4 * i];
-    double vv = c.vcoef[4 * i];
-    for (int j = 1; j < 4; ++j) {
-      uv *= poly_pow(P[j - 1], c.ucoef[4 * i + j]);
-      vv *= poly_pow(P[j - 1], c.vcoef[4 * i + j]);
+  if (c.pow3) {
+    double pw[3][4];
+    poly_powers(P, pw);
+    for (int i = 0; i < c.n_coeff; ++i) {
+      double uv = c.ucoef[4 * i];
+      double vv = c.vcoef[4 * i];
+#pragma unroll
+      for (int j = 1; j < 4; ++j) {
+        uv *= pw[j - 1][(int)c.ucoef[4 * i + j]];
+        vv *= pw[j - 1][(int)c.vcoef[4 * i + j]];
+      }
+      su += uv;
+      sv += vv;
     }
-    su += uv;
-    sv += vv;
+  } else {
+    for (int i = 0; i < c.n_coeff; ++i) {
+      double uv = c.ucoef[4 * i];
+      double vv = c.vcoef[4 * i];
+      for (int j = 1; j < 4; ++j) {
+        uv *= poly_pow(P[j - 1], c.ucoef[4 * i + j]);
+        vv *= poly_pow(P[j - 1], c.vcoef[4 * i + j]);
+      }
+      su += uv;
+      sv += vv;
+    }
   }
   u = su;
   v = sv;
@@ -223,14 +253,23 @@ __device__ __forceinline__ void poly_img_to_world(const CamDev& c, double pu, do
   const int n = c.n_coeff;
   while (err > 1e-5 && iter < 50) {
     double j00 = 0, j01 = 0, j10 = 0, j11 = 0;
+    double pw[3][4];
+    if (c.pow3) poly_powers(P, pw);
     for (int i = 0; i < n; ++i) {
       double dudx = c.ducoef[4 * i], dudy = c.ducoef[4 * (i + n)];
       double dvdx = c.dvcoef[4 * i], dvdy = c.dvcoef[4 * (i + n)];
       for (int j = 1; j < 4; ++j) {
-        dudx *= poly_pow(P[j - 1], c.ducoef[4 * i + j]);
-        dudy *= poly_pow(P[j - 1], c.ducoef[4 * (i + n) + j]);
-        dvdx *= poly_pow(P[j - 1], c.dvcoef[4 * i + j]);
-        dvdy *= poly_pow(P[j - 1], c.dvcoef[4 * (i + n) + j]);
+        if (c.pow3) {
+          dudx *= pw[j - 1][(int)c.ducoef[4 * i + j]];
+          dudy *= pw[j - 1][(int)c.ducoef[4 * (i + n) + j]];
+          dvdx *= pw[j - 1][(int)c.dvcoef[4 * i + j]];
+          dvdy *= pw[j - 1][(int)c.dvcoef[4 * (i + n) + j]];
+        } else {
+          dudx *= poly_pow(P[j - 1], c.ducoef[4 * i + j]);
+          dudy *= poly_pow(P[j - 1], c.ducoef[4 * (i + n) + j]);
+          dvdx *= poly_pow(P[j - 1], c.dvcoef[4 * i + j]);
+          dvdy *= poly_pow(P[j - 1], c.dvcoef[4 * (i + n) + j]);
+        }
       }
       j00 += dudx;
       j01 += dudy;

@@ -10,6 +10,9 @@ struct OtfView {
   int nx, ny, nz, n_grid, n_cam;
   double bmin[3], bmax[3], d[3];
   const double* table;  // [4][n_cam][n_grid]
+  // every alpha entry is +0.0: the interpolated angle is then +0.0 and its cosine and
+  // sine are exactly 1 and +0 (the reference's values), so they are not evaluated
+  int alpha_zero;
 };
 
 __device__ __forceinline__ double otf_lerp8(const double* v, double xd, double yd, double zd) {
@@ -52,7 +55,8 @@ __device__ __forceinline__ void otf_param(const OtfView& o, int cam, double X, d
                     x0 * nyz + (y0 + 1) * o.nz + z0,       x0 * nyz + nyz + (y0 + 1) * o.nz + z0,
                     x0 * nyz + nyz + (y0 + 1) * o.nz + z0 + 1, x0 * nyz + (y0 + 1) * o.nz + z0 + 1};
   double res[4];
-  for (int q = 0; q < 4; ++q) {
+  const int nq = o.alpha_zero ? 3 : 4;
+  for (int q = 0; q < nq; ++q) {
     const double* tab = o.table + ((size_t)q * o.n_cam + cam) * o.n_grid;
     double v[8];
     for (int k = 0; k < 8; ++k) v[k] = tab[g[k]];
@@ -61,8 +65,13 @@ __device__ __forceinline__ void otf_param(const OtfView& o, int cam, double X, d
   out[0] = res[0];
   out[1] = res[1];
   out[2] = res[2];
-  out[3] = cos(res[3]);
-  out[4] = sin(res[3]);
+  if (o.alpha_zero) {
+    out[3] = 1.0;
+    out[4] = 0.0;
+  } else {
+    out[3] = cos(res[3]);
+    out[4] = sin(res[3]);
+  }
 }
 
 }  // namespace olpt

@@ -22,22 +22,45 @@ def _run(kind, precision, **over):
 
 
 def _ref(kind, s):
+    """The reference's runIPR; for polynomial cameras single-threaded with a fixed
+    srand (its Newton start points come from rand())."""
     from oracle.ref import RefOracle
     sc = _scenes.scene(kind)
+    if kind == "poly":
+        r = RefOracle(sc, s, threads=1)
+        r.srand(7)
+        return r.ipr(sc.images)
     return RefOracle(sc, s, threads=0).ipr(sc.images)
 
 
-@pytest.mark.parametrize("over", [{}, {"n_cam_reduced": 1, "n_loop_ipr": 2}])
-def test_ipr_fp64_matches_reference(over):
-    sc, s, xyz, uv = _run("small", 1, **over)
-    want = _ref("small", s)
+@pytest.mark.parametrize("kind,over", [("small", {}),
+                                       ("small", {"n_cam_reduced": 1, "n_loop_ipr": 2}),
+                                       ("cfg1", {}), ("poly", {})])
+def test_ipr_fp64_matches_reference(kind, over):
+    """IPR::runIPR in FP64 mode against the reference (10,000 particles on 4 x 1024^2
+    for cfg1; 6 polynomial cameras with a 5x5x5 OTF for poly): object counts and every
+    reference object reproduced within 1e-4 mm, with the near-tolerance stereo tests
+    of the run printed (polynomial lines of sight differ from the reference's by its
+    random Newton start, so decisions within 1e-6 px of the tolerance may flip)."""
+    sc = _scenes.scene(kind)
+    s = _scenes.settings(kind)
+    for k, v in over.items():
+        setattr(s, k, v)
+    ctx = _scenes.gpu_context(sc)
+    ctx.near_log_enable(1e-6)
+    ctx.upload_images(sc.images)
+    n = ctx.ipr_run(_ffi.ipr_params(s, sc.volume, 1))
+    xyz, uv = ctx.ipr_result(n)
+    _, n_near = ctx.near_log()
+    want = _ref(kind, s)
     n_ref = len(want["xyz"])
-    print(f"IPR fp64: gpu {len(xyz)} ref {n_ref}")
-    assert abs(len(xyz) - n_ref) <= max(3, 0.005 * n_ref)
     d = _metrics.match(want["xyz"], xyz)
-    frac = np.mean(d <= 1e-4)
-    print(f"  reference objects reproduced within 1e-4 mm: {frac:.4f}")
-    assert frac >= 0.99
+    miss = int(np.sum(d > 1e-4))
+    extra = int(np.sum(_metrics.match(xyz, want["xyz"]) > 1e-4))
+    print(f"IPR fp64 {kind} {over}: here {len(xyz)} reference {n_ref}; reference objects "
+          f"not reproduced within 1e-4 mm {miss}, extra objects {extra}; near-tolerance "
+          f"stereo tests {n_near}")
+    assert miss <= max(1, int(0.002 * n_ref)) and extra <= max(1, int(0.002 * n_ref))
 
 
 def test_ipr_fp32_recall_ghost():

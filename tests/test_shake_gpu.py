@@ -47,20 +47,36 @@ def _shake_cmp(kind, precision):
     return got, want, d
 
 
-def test_shake_fp64_matches_reference():
-    got, want, d = _shake_cmp("small", 1)
+@pytest.mark.parametrize("kind", ["small", "cfg1"])
+def test_shake_fp64_matches_reference(kind):
+    """FP64 mode against Shake::runShake: every object's position, flag and score.
+    exp() is the only operation whose rounding differs from glibc's, so a line-search
+    decision can flip only where two residues tie to rounding; each object beyond
+    1e-9 mm is printed, and at most 0.2% may differ beyond 1e-4 mm."""
+    got, want, d = _shake_cmp(kind, 1)
     n = len(d)
-    frac_exact = np.mean(d <= 1e-9)
-    frac_tol = np.mean(d <= 1e-4)
-    print(f"fp64 shake: n={n} <=1e-9mm {frac_exact:.4f} <=1e-4mm {frac_tol:.4f} max {d.max():.3g}")
-    assert frac_tol >= 0.995
-    assert np.mean(got["flags"] == want["flags"]) >= 0.995
+    n9, n4 = int(np.sum(d > 1e-9)), int(np.sum(d > 1e-4))
+    flags_diff = int(np.sum(got["flags"] != want["flags"]))
+    print(f"fp64 shake {kind}: {n} objects, beyond 1e-9 mm {n9}, beyond 1e-4 mm {n4}, "
+          f"flags differ {flags_diff}, max {d.max():.3g} mm")
+    for i in np.flatnonzero(d > 1e-9)[:10]:
+        print(f"  object {i}: |dxyz| {d[i]:.3e} mm, score {got['score'][i]:.9g} vs "
+              f"{want['score'][i]:.9g}, flag {got['flags'][i]} vs {want['flags'][i]}")
+    assert n4 <= max(1, int(0.002 * n))
+    assert flags_diff <= max(1, int(0.002 * n))
     ok = d <= 1e-9
     assert np.allclose(got["score"][ok], want["score"][ok], rtol=1e-9)
 
 
-def test_shake_fp32_position_tolerance():
-    got, want, d = _shake_cmp("small", 0)
-    frac = np.mean(d <= 1e-4)
-    print(f"fp32 shake: <=1e-4mm {frac:.4f} median {np.median(d):.3g} p99 {np.quantile(d, .99):.3g}")
-    assert frac >= 0.95
+@pytest.mark.parametrize("kind", ["small", "cfg1"])
+def test_shake_fp32_against_fp64_reference(kind):
+    """FP32 production shake (residual, OTF Gaussian and sums in FP32) against the
+    reference: the distribution of position errors and the count of objects beyond
+    1e-4 mm (decisions that FP32 rounding flips), printed; at most 2% beyond 1e-4 mm."""
+    got, want, d = _shake_cmp(kind, 0)
+    n = len(d)
+    n4 = int(np.sum(d > 1e-4))
+    print(f"fp32 shake {kind}: {n} objects, median {np.median(d):.3g} mm, p99 "
+          f"{np.quantile(d, .99):.3g} mm, max {d.max():.3g} mm, beyond 1e-4 mm {n4} "
+          f"({n4 / max(n, 1):.4f}), flags differ {int(np.sum(got['flags'] != want['flags']))}")
+    assert n4 <= max(2, int(0.02 * n))

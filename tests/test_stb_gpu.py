@@ -97,21 +97,34 @@ def _reproduced(ref_rows, gpu_rows, tol):
     return hit / len(rt)
 
 
-def test_stb_fp64_tracks_match_reference():
+def test_stb_fp64_track_lists_identical():
+    """FP64 mode: after every frame, the four track lists equal the reference's row for
+    row -- track ids (list positions) and frames exactly, positions within 1e-9 mm
+    (only exp() rounding may differ).  Every difference is printed with its size."""
+    from tests import _tracks
     ref, _ = _ref_run()
     _, gpu = _gpu_run(1)
+    bad, worst = [], 0.0
     for t in range(N_FRAMES):
         for name in _ffi.TRACK_LISTS:
-            a, b = ref[t][name], gpu[t][name]
-            na = len(_tracks(a))
-            nb = len(_tracks(b))
-            frac = _reproduced(a, b, 1e-6)
-            print(f"frame {t} {name:13s}: ref {na:5d} tracks gpu {nb:5d} reproduced {frac:.4f}")
-            assert abs(na - nb) <= max(2, 0.01 * na), (t, name, na, nb)
-            assert frac >= 0.98, (t, name, frac)
+            ok, dmax, msgs = _tracks.compare(ref[t][name], gpu[t][name], 1e-9,
+                                             f"frame {t} {name}")
+            worst = max(worst, dmax)
+            print(f"frame {t} {name:13s}: {len(ref[t][name]):6d} rows, ids and frames "
+                  f"{'equal' if ok else 'DIFFER'}, max |dxyz| {dmax:.2e} mm")
+            for m in msgs:
+                print("  " + m)
+            if not ok:
+                bad.append((t, name))
+    print(f"largest position difference over all frames and lists: {worst:.3e} mm")
+    assert not bad, bad
 
 
-def test_stb_fp32_track_counts_close():
+def test_stb_fp32_tracks_against_fp64():
+    """FP32 production path against the FP64 reference: the tracks it reproduces
+    within 1e-4 mm (same frames, every point), and the ones it does not, printed per
+    list; at most 2% of the long tracks may differ (a shake decision that FP32 rounding
+    flips changes a track from then on)."""
     ref, _ = _ref_run()
     _, gpu = _gpu_run(0)
     t = N_FRAMES - 1
@@ -119,9 +132,12 @@ def test_stb_fp32_track_counts_close():
         na = len(_tracks(ref[t][name]))
         nb = len(_tracks(gpu[t][name]))
         frac = _reproduced(ref[t][name], gpu[t][name], 1e-4)
-        print(f"fp32 frame {t} {name}: ref {na} gpu {nb} reproduced within 1e-4 mm {frac:.4f}")
-        assert abs(na - nb) <= max(5, 0.03 * na)
-        assert frac >= 0.9
+        n_diff = na - int(round(frac * na))
+        print(f"fp32 frame {t} {name}: reference {na} tracks, here {nb}; reproduced within "
+              f"1e-4 mm: {na - n_diff}, not reproduced: {n_diff}")
+        if name == "long_active":
+            assert n_diff <= max(2, int(0.02 * na))
+            assert abs(na - nb) <= max(2, int(0.02 * na))
 
 
 def _read_csv(path):
@@ -150,10 +166,11 @@ def test_stb_output_files_match_reference():
                 ha, ra = _read_csv(os.path.join(ref_dir, sub, f))
                 hb, rb = _read_csv(os.path.join(d, sub, f))
                 assert ha == hb
-                same = sum(x == y for x, y in zip(ra, rb)) / max(1, len(ra))
-                print(f"{sub}/{f}: {len(ra)} rows ref, {len(rb)} gpu, identical lines {same:.4f}")
-                assert abs(len(ra) - len(rb)) <= max(8, 0.01 * len(ra))
-                assert same >= 0.95 or len(ra) == 0
+                diff = [i for i, (x, y) in enumerate(zip(ra, rb)) if x != y]
+                print(f"{sub}/{f}: {len(ra)} rows, {len(diff)} lines differ")
+                for i in diff[:5]:
+                    print(f"  reference: {ra[i]}\n  here:      {rb[i]}")
+                assert len(ra) == len(rb) and not diff
 
 
 def test_stb_save_load_round_trip():
