@@ -849,7 +849,9 @@ LEARN_PPP = (0.01, 0.02, 0.03, 0.05, 0.08, 0.1)
 
 def learned_comparison(args, o: Ours):
     """The learned proposal against the plain GPU form on its own workload (4 cameras,
-    1024^2 uint8, OTF b, c uniform in [0.3, 0.8]): tuples from the plain pipeline on
+    1024^2 uint8, the 40 x 40 x 20 mm volume filling the images so that ppp counts the
+    illuminated area, OTF b, c uniform in [0.3, 0.8], settings in pixels of the rig:
+    shake width 0.25 px): tuples from the plain pipeline on
     seeded frames at 0.01-0.1 ppp, training on the device, calibration on a validation
     frame (fewest IPR loops whose recall is within 0.5% of the plain 4-loop IPR and
     whose ghost rate is not higher, at 0.05 and 0.1 mm), then device-timed IPR of both
@@ -857,8 +859,7 @@ def learned_comparison(args, o: Ours):
     from pyopenlpt_b200 import _ffi, learned as L
     import dataclasses
     torch = o.torch
-    s = synth.IPRSettings()
-    ls = L.LearnedSettings()
+    s, ls = L.rig_settings(L.scene(0, 0.01))
     ctx = _ffi.Context(o.local)
     t0 = time.perf_counter()
     xs, ts = [], []

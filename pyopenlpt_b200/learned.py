@@ -37,14 +37,33 @@ class LearnedSettings:
                                   fallback_residual=self.fallback_residual)
 
 
+VOLUME = (-20.0, 20.0, -20.0, 20.0, -10.0, 10.0)
+
+
 def scene(seed: int, ppp: float, size: int = 1024, n_cam: int = 4,
           bc: Optional[Tuple[float, float]] = None) -> synth.Scene:
-    """A learned-proposal frame: 4 cameras, size^2 uint8, ppp particles per pixel,
-    OTF b, c uniform in [0.3, 0.8] unless given."""
+    """A learned-proposal frame: 4 cameras, size^2 uint8, ppp * size^2 particles in the
+    40 x 40 x 20 mm volume, the focal length chosen so that the volume fills the
+    images (ppp then counts the illuminated area), OTF b, c uniform in [0.3, 0.8]
+    unless given."""
     rng = np.random.default_rng(10_000 + seed)
     b, c = bc if bc is not None else rng.uniform(0.3, 0.8, 2)
+    focal = min(synth.focal_for_volume(n_cam, size, VOLUME))
     return synth.make_scene(n_particles=int(ppp * size * size), n_cam=n_cam, size=size,
-                            focal=5000.0 * size / 1024.0, b=float(b), c=float(c), seed=seed)
+                            focal=focal, volume=VOLUME, b=float(b), c=float(c), seed=seed)
+
+
+def rig_settings(rig, **over) -> Tuple[synth.IPRSettings, LearnedSettings]:
+    """IPR and learned-shake knobs in pixels of the rig: shake width 0.25 px, tol_3d
+    0.6 px, network output unit 0.5 px, ghost label beyond 1.5 px, refinement width
+    0.1 px (mm per px from the largest image motion per mm at the volume's centre)."""
+    c0 = 0.5 * (np.array(rig.volume[0::2]) + np.array(rig.volume[1::2]))
+    mm_px = 1.0 / max(synth.px_per_mm(cm, c0) for cm in rig.cams)
+    s = synth.IPRSettings(shake_width=0.25 * mm_px, tol_3d_mm=0.6 * mm_px, **over)
+    s.match_cam_count = min(s.match_cam_count, len(rig.cams))
+    ls = LearnedSettings(out_scale_mm=0.5 * mm_px, ghost_tol_mm=1.5 * mm_px,
+                         refine_width_mm=0.1 * mm_px)
+    return s, ls
 
 
 def bind(ctx: _ffi.Context, sc: synth.Scene):

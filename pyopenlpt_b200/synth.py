@@ -653,7 +653,7 @@ class PolySequence:
 def px_per_mm(cam, at) -> float:
     """Largest image motion (px) per mm of world motion at point ``at`` (the spectral
     norm of the projection's Jacobian, central differences)."""
-    at = np.asarray(at, dtype=np.float64)
+    at = np.asarray(at, dtype=np.float64).reshape(1, 3)
     J = np.stack([(cam.project(at + e) - cam.project(at - e))[0] / 2e-3
                   for e in np.eye(3) * 1e-3], axis=1)
     return float(np.linalg.norm(J, 2))

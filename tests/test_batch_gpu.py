@@ -9,8 +9,8 @@ pytestmark = pytest.mark.gpu
 
 
 def test_batch_equals_one_at_a_time():
-    s = synth.IPRSettings()
     scenes = [L.scene(700 + i, 0.02, size=512) for i in range(3)]
+    s, _ = L.rig_settings(scenes[0])
     ctxs = [_ffi.Context(0) for _ in scenes]
     try:
         p = _ffi.ipr_params(s, scenes[0].volume)

@@ -6,6 +6,7 @@ stereo candidates toward the converged shake positions, (2) the ghost
 logit separates ghost candidates from real ones, and (3) IPR with the learned shake
 has at least the plain method's recall and a lower ghost rate against the ground
 truth."""
+import dataclasses
 import functools
 
 import numpy as np
@@ -31,8 +32,7 @@ def _auc(score, label):
 @functools.lru_cache(maxsize=None)
 def _trained():
     ctx = _ffi.Context(0)
-    s = synth.IPRSettings()
-    ls = L.LearnedSettings()
+    s, ls = L.rig_settings(L.scene(0, 0.01, size=SIZE))
     xs, ts = [], []
     for i in range(12):
         x, t = L.collect(ctx, L.scene(i, PPP[i % len(PPP)], size=SIZE), s, ls)
@@ -62,7 +62,7 @@ def test_learned_ipr_beats_plain_on_ground_truth():
     ctx, s, ls = _trained()
     sc = L.scene(501, 0.02, size=SIZE)
     plain = L.run_ipr(ctx, sc, s, None)
-    cfg = L.LearnedSettings(ghost_logit=4.0, fallback_residual=1e9)
+    cfg = dataclasses.replace(ls, ghost_logit=4.0, fallback_residual=1e9)
     a0, b0 = ctx.learned_stats()
     learned = L.run_ipr(ctx, sc, s, cfg)
     a1, b1 = ctx.learned_stats()
@@ -72,7 +72,7 @@ def test_learned_ipr_beats_plain_on_ground_truth():
     assert learned["recall_05"] >= plain["recall_05"] - 0.005
     assert learned["ghost_10"] < plain["ghost_10"]
     # the fallback path: every object back through the full plain shake
-    full = L.run_ipr(ctx, sc, s, L.LearnedSettings(ghost_logit=4.0, fallback_residual=0.0))
+    full = L.run_ipr(ctx, sc, s, dataclasses.replace(ls, ghost_logit=4.0, fallback_residual=0.0))
     a2, b2 = ctx.learned_stats()
     assert b2 - b1 == a2 - a1 > 0
     assert full["n"] > 0
