@@ -344,11 +344,6 @@ olpt_status_t olpt_cameras_upload(olpt_ctx* ctx, const olpt_camera_desc* cams, i
     ctx->cams_d.ensure(sizeof(CamDev) * OLPT_MAX_CAM, ctx->stream);
     OLPT_CUDA(cudaMemcpyAsync(ctx->cams_d.p, h.data(), sizeof(CamDev) * n_cam,
                               cudaMemcpyHostToDevice, ctx->stream));
-    std::vector<CamF> hf(n_cam);
-    for (int i = 0; i < n_cam; ++i) hf[i] = cam_to_f32(h[i]);
-    ctx->cams_f_d.ensure(sizeof(CamF) * OLPT_MAX_CAM, ctx->stream);
-    OLPT_CUDA(cudaMemcpyAsync(ctx->cams_f_d.p, hf.data(), sizeof(CamF) * n_cam,
-                              cudaMemcpyHostToDevice, ctx->stream));
     OLPT_CUDA(cudaStreamSynchronize(ctx->stream));
   });
 }

@@ -378,7 +378,6 @@ struct olpt_ctx {
   int n_cam = 0;
   std::vector<olpt::CamDev> cams_h;
   olpt::DevBuf cams_d;
-  olpt::DevBuf cams_f_d;  // FP32 copies of the cameras' geometry (CamF)
 
   olpt::OtfDev otf;
   olpt::DevBuf otf_table;

@@ -300,98 +300,6 @@ __device__ __forceinline__ void poly_img_to_world(const CamDev& c, double pu, do
   }
 }
 
-// ---------------------------------------------------------------- FP32 projection
-// The camera in FP32, for the production shake, whose line search projects in FP32
-// (the FP64 functions above are the reference's arithmetic, used everywhere else).
-struct CamF {
-  int type, n_dist, is_distorted, n_coeff, pow3;
-  float fx, fy, cx, cy;
-  float dist[12];
-  float R[9], T[3];
-  float ucoef[OLPT_MAX_POLY * 4];
-  float vcoef[OLPT_MAX_POLY * 4];
-};
-
-__host__ inline CamF cam_to_f32(const CamDev& c) {
-  CamF f{};
-  f.type = c.type;
-  f.n_dist = c.n_dist;
-  f.is_distorted = c.is_distorted;
-  f.n_coeff = c.n_coeff;
-  f.pow3 = c.pow3;
-  f.fx = (float)c.fx;
-  f.fy = (float)c.fy;
-  f.cx = (float)c.cx;
-  f.cy = (float)c.cy;
-  for (int k = 0; k < 12; ++k) f.dist[k] = (float)c.dist[k];
-  for (int k = 0; k < 9; ++k) f.R[k] = (float)c.R[k];
-  for (int k = 0; k < 3; ++k) f.T[k] = (float)c.T[k];
-  for (int k = 0; k < OLPT_MAX_POLY * 4; ++k) {
-    f.ucoef[k] = (float)c.ucoef[k];
-    f.vcoef[k] = (float)c.vcoef[k];
-  }
-  return f;
-}
-
-// Camera::project in FP32: pinhole with distortion (Camera.cpp:648-690, 913-966) or
-// the polynomial (Camera.cpp:969-990), powers by products (powf for other exponents).
-__device__ __forceinline__ void cam_project_f(const CamF& c, float X, float Y, float Z, float& u,
-                                              float& v) {
-  if (c.type == CAM_PINHOLE) {
-    const float t0 = fmaf(c.R[2], Z, fmaf(c.R[1], Y, c.R[0] * X)) + c.T[0];
-    const float t1 = fmaf(c.R[5], Z, fmaf(c.R[4], Y, c.R[3] * X)) + c.T[1];
-    const float t2 = fmaf(c.R[8], Z, fmaf(c.R[7], Y, c.R[6] * X)) + c.T[2];
-    const float inv = t2 != 0.0f ? 1.0f / t2 : 1.0f;
-    const float x = t0 * inv, y = t1 * inv;
-    float xd = x, yd = y;
-    if (c.is_distorted) {
-      const float* k = c.dist;
-      const float r2 = x * x + y * y, r4 = r2 * r2, r6 = r4 * r2;
-      const float a1 = 2 * x * y, a2 = r2 + 2 * x * x, a3 = r2 + 2 * y * y;
-      float cdist = 1 + k[0] * r2 + k[1] * r4;
-      if (c.n_dist > 4) cdist += k[4] * r6;
-      float icdist2 = 1.0f;
-      if (c.n_dist > 5) icdist2 = 1.0f / (1 + k[5] * r2 + k[6] * r4 + k[7] * r6);
-      xd = x * cdist * icdist2 + k[2] * a1 + k[3] * a2;
-      yd = y * cdist * icdist2 + k[2] * a3 + k[3] * a1;
-      if (c.n_dist > 8) {
-        xd += k[8] * r2 + k[9] * r4;
-        yd += k[10] * r2 + k[11] * r4;
-      }
-    }
-    u = fmaf(xd, c.fx, c.cx);
-    v = fmaf(yd, c.fy, c.cy);
-    return;
-  }
-  const float P[3] = {X, Y, Z};
-  float pw[3][4];
-#pragma unroll
-  for (int j = 0; j < 3; ++j) {
-    pw[j][0] = 1.0f;
-    pw[j][1] = P[j];
-    pw[j][2] = P[j] * P[j];
-    pw[j][3] = pw[j][2] * P[j];
-  }
-  float su = 0.0f, sv = 0.0f;
-  for (int i = 0; i < c.n_coeff; ++i) {
-    float a = c.ucoef[4 * i], b = c.vcoef[4 * i];
-#pragma unroll
-    for (int j = 1; j < 4; ++j) {
-      if (c.pow3) {
-        a *= pw[j - 1][(int)c.ucoef[4 * i + j]];
-        b *= pw[j - 1][(int)c.vcoef[4 * i + j]];
-      } else {
-        a *= powf(P[j - 1], c.ucoef[4 * i + j]);
-        b *= powf(P[j - 1], c.vcoef[4 * i + j]);
-      }
-    }
-    su += a;
-    sv += b;
-  }
-  u = su;
-  v = sv;
-}
-
 // ---------------------------------------------------------------- dispatch
 // Camera::project (Camera.cpp:648-677).
 __device__ __forceinline__ void cam_project(const CamDev& c, double X, double Y, double Z,

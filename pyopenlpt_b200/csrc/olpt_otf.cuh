@@ -74,48 +74,4 @@ __device__ __forceinline__ void otf_param(const OtfView& o, int cam, double X, d
   }
 }
 
-// OTF::getOTFParam in FP32 for the production shake: the same clamping, cell and
-// trilinear weights, evaluated in single precision.
-__device__ __forceinline__ void otf_param_f(const OtfView& o, int cam, float X, float Y, float Z,
-                                            float out[5]) {
-  const float P[3] = {X, Y, Z};
-  const int n[3] = {o.nx, o.ny, o.nz};
-  float t[3];
-  int id[3];
-  for (int k = 0; k < 3; ++k) {
-    const float lo = (float)o.bmin[k], hi = (float)o.bmax[k];
-    const float p = fminf(fmaxf(P[k], lo), hi);
-    const float f = (p - lo) / (float)o.d[k];
-    int i = (int)floorf(f);
-    i = i < 0 ? 0 : i;
-    i = i > n[k] - 2 ? n[k] - 2 : i;
-    id[k] = i;
-    t[k] = fmaxf(0.0f, fminf(1.0f, f - (float)i));
-  }
-  const int nyz = o.ny * o.nz;
-  const int base = id[0] * nyz + id[1] * o.nz + id[2];
-  const int nq = o.alpha_zero ? 3 : 4;
-  float res[4];
-  for (int q = 0; q < nq; ++q) {
-    const double* tab = o.table + ((size_t)q * o.n_cam + cam) * o.n_grid + base;
-    const float c000 = (float)tab[0], c001 = (float)tab[1];
-    const float c010 = (float)tab[o.nz], c011 = (float)tab[o.nz + 1];
-    const float c100 = (float)tab[nyz], c101 = (float)tab[nyz + 1];
-    const float c110 = (float)tab[nyz + o.nz], c111 = (float)tab[nyz + o.nz + 1];
-    const float c00 = c000 + (c100 - c000) * t[0], c01 = c001 + (c101 - c001) * t[0];
-    const float c10 = c010 + (c110 - c010) * t[0], c11 = c011 + (c111 - c011) * t[0];
-    const float c0 = c00 + (c10 - c00) * t[1], c1 = c01 + (c11 - c01) * t[1];
-    res[q] = c0 + (c1 - c0) * t[2];
-  }
-  out[0] = res[0];
-  out[1] = res[1];
-  out[2] = res[2];
-  if (o.alpha_zero) {
-    out[3] = 1.0f;
-    out[4] = 0.0f;
-  } else {
-    sincosf(res[3], &out[4], &out[3]);
-  }
-}
-
 }  // namespace olpt

@@ -28,7 +28,6 @@ struct PlaneView {
 struct ShakeView {
   int n_cam;
   const CamDev* cams;
-  const CamF* camsf;  // the same cameras in FP32 (the production line search)
   OtfView otf;
   double r_px, ratio;
   int roi_area;          // augmented ROI pixels (side^2)

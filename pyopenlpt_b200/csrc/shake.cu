@@ -19,11 +19,10 @@
 //     shared memory, then runs the reference's axis-wise line search.  Each residue
 //     evaluation spreads (camera, pixel) pairs over the lanes; the scalar control
 //     flow is executed identically by all lanes.
-// Precision: Real = float is the production path (projections, OTF lookup, residual,
-// Gaussian and MSE in FP32; the line search's trial positions, polyfit and decisions
-// in FP64); Real = double is the parity path with the reference's FP64 arithmetic,
-// which also sums every camera's squared error in the reference's row-major order so
-// that only exp() rounding differs.
+// Precision: Real = float is the production path (residual, OTF Gaussian and MSE in
+// FP32); Real = double is the parity path, which also sums every camera's squared
+// error in the reference's row-major order so that only exp() rounding differs.
+// Projections, polyfit and all decisions stay in FP64 in both.
 #include <cuda_runtime.h>
 
 #include <algorithm>
@@ -44,23 +43,6 @@ namespace {
 
 inline int nblk(int64_t n, int t = 256) { return (int)((n + t - 1) / t); }
 
-// Real = float (production): projection and OTF in FP32 (cam_project_f, otf_param_f);
-// Real = double (parity): the reference's FP64 arithmetic.
-template <typename Real>
-__device__ __forceinline__ void point_geom(const ShakeView& v, int c, double X, double Y,
-                                           double Z, double& u, double& w, Real q[5]) {
-  if constexpr (sizeof(Real) == 4) {
-    float uf, wf;
-    cam_project_f(v.camsf[c], (float)X, (float)Y, (float)Z, uf, wf);
-    u = uf;
-    w = wf;
-    otf_param_f(v.otf, c, (float)X, (float)Y, (float)Z, q);
-  } else {
-    cam_project(v.cams[c], X, Y, Z, u, w);
-    otf_param(v.otf, c, X, Y, Z, q);
-  }
-}
-
 // ---------------------------------------------------------------- 1. prep
 template <typename Real>
 __global__ void prep_kernel(ShakeView v, const double* xyz, int64_t n, double* uv, Real* otfp,
@@ -71,11 +53,12 @@ __global__ void prep_kernel(ShakeView v, const double* xyz, int64_t n, double* u
   const bool masked = flags && flags[o] != 0;
   for (int c = 0; c < v.n_cam; ++c) {
     double u, w;
-    Real q[5];
-    point_geom<Real>(v, c, X, Y, Z, u, w, q);
+    cam_project(v.cams[c], X, Y, Z, u, w);
     uv[(o * v.n_cam + c) * 2] = u;
     uv[(o * v.n_cam + c) * 2 + 1] = w;
-    for (int k = 0; k < 5; ++k) otfp[(o * v.n_cam + c) * 5 + k] = q[k];
+    double q[5];
+    otf_param(v.otf, c, X, Y, Z, q);
+    for (int k = 0; k < 5; ++k) otfp[(o * v.n_cam + c) * 5 + k] = (Real)q[k];
     int key = -1;
     if (!masked && (all_cams || v.cams[c].is_active)) {
       const Rect r = roi_bound(v.cams[c].n_row, v.cams[c].n_col, u, w, v.r_px, v.r_px);
@@ -181,11 +164,12 @@ __device__ void eval_geom(const ShakeView& v, const double P[3], Smem<Real>& S) 
   const int lane = threadIdx.x & 31;
   if (lane < NC) {
     double u, w;
-    Real q[5];
-    point_geom<Real>(v, lane, P[0], P[1], P[2], u, w, q);
+    cam_project(v.cams[lane], P[0], P[1], P[2], u, w);
     S.uvc[2 * lane] = u;
     S.uvc[2 * lane + 1] = w;
-    for (int k = 0; k < 5; ++k) S.otf[5 * lane + k] = q[k];
+    double q[5];
+    otf_param(v.otf, lane, P[0], P[1], P[2], q);
+    for (int k = 0; k < 5; ++k) S.otf[5 * lane + k] = (Real)q[k];
   }
   __syncwarp();
 }
@@ -276,11 +260,12 @@ __device__ void eval_geom3(const ShakeView& v, const double P[3], int ax, double
     double Q[3] = {P[0], P[1], P[2]};
     Q[ax] = x0 + rel[j];
     double u, w;
-    Real q[5];
-    point_geom<Real>(v, c, Q[0], Q[1], Q[2], u, w, q);
+    cam_project(v.cams[c], Q[0], Q[1], Q[2], u, w);
     S.uvc[2 * lane] = u;
     S.uvc[2 * lane + 1] = w;
-    for (int k = 0; k < 5; ++k) S.otf[5 * lane + k] = q[k];
+    double q[5];
+    otf_param(v.otf, c, Q[0], Q[1], Q[2], q);
+    for (int k = 0; k < 5; ++k) S.otf[5 * lane + k] = (Real)q[k];
   }
   __syncwarp();
 }
@@ -929,7 +914,6 @@ static ShakeView make_view(olpt_ctx* ctx, const ShakeParams& sp, bool fp64) {
   ShakeView v{};
   v.n_cam = ctx->n_cam;
   v.cams = ctx->cams_d.as<CamDev>();
-  v.camsf = ctx->cams_f_d.as<CamF>();
   v.otf = otf_view(ctx);
   v.r_px = sp.radius_obj;
   v.ratio = (double)sp.ratio_augimg;
