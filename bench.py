@@ -72,17 +72,31 @@ WORKLOADS = {
 # 12-bit images); every camera in the build (match_cam_count = 6: with check
 # cameras the reference's StereoMatch aborts, StereoMatch.cpp:120-127).
 POLY_PX = dict(shake_width=0.25, tol_3d=0.6, link=10.0, pf_r=30.0)
+# The reference's default cap of 200,000 detections per camera (limit2DObjectNumber,
+# IPR.cpp:19-38) drops each camera's detections independently at random; at 0.1 ppp on
+# 2048^2 (about 420,000 detections per camera) a particle would keep all six views
+# with probability 0.48^6 (about 1%), so these workloads raise the cap above the
+# detection count.  Six convergence-phase frames run untimed after the initial phase
+# (and before the warm-up frames) so that the timed frames see a converging tracker.
 WORKLOADS["stb_2048_u16_6cam_poly_419k"] = dict(
     kind="stb", gen="poly", seq=dict(ppp=0.1, n_cam=6, size=2048,
                                      volume=(-40.0, 40.0, -40.0, 40.0, -20.0, 20.0), bits=12),
-    settings=dict(min_obj_int=300), stb=dict(pf_nx=11, pf_ny=11, pf_nz=6))
+    settings=dict(min_obj_int=300, n_obj2d_process_max=1_000_000),
+    stb=dict(pf_nx=11, pf_ny=11, pf_nz=6), converge=6)
 WORKLOADS["stb_256_u16_6cam_poly_6.5k"] = dict(
     kind="stb", gen="poly", seq=dict(ppp=0.1, n_cam=6, size=256,
                                      volume=(-5.0, 5.0, -5.0, 5.0, -2.5, 2.5), bits=12),
-    settings=dict(min_obj_int=300), stb=dict(pf_nx=11, pf_ny=11, pf_nz=6))
+    settings=dict(min_obj_int=300, n_obj2d_process_max=1_000_000),
+    stb=dict(pf_nx=11, pf_ny=11, pf_nz=6), converge=6)
 # the reference arm's sample of each workload (a workload the CPU path finishes)
 REFERENCE_SAMPLE = {"stb_2048_u16_6cam_poly_419k": "stb_256_u16_6cam_poly_6.5k"}
 DEFAULT_WORKLOAD = "stb_2048_u16_6cam_poly_419k"
+
+
+def pre_frames(name: str) -> int:
+    """Frames processed before the warm-up frames: the initial phase plus the
+    workload's untimed convergence-phase frames."""
+    return N_INIT + WORKLOADS[name].get("converge", 0)
 
 
 def ipr_settings(name: str, n_cam: int):
@@ -211,7 +225,7 @@ def reference_ipr_time(sc, s, threads: int, images=None):
     return len(out["xyz"]), dt
 
 
-REF_STB_BUDGET_S = 400.0  # convergence frames of the reference arm stop after this
+REF_STB_BUDGET_S = 420.0  # convergence frames of the reference arm stop after this
 
 
 def reference_stb(name, threads, warmup, steps, budget_s):
@@ -221,7 +235,8 @@ def reference_stb(name, threads, warmup, steps, budget_s):
     passed.  Particles per frame = track points the frame adds over the four lists."""
     from oracle.ref import RefSTB
     sample_name = REFERENCE_SAMPLE.get(name, name)
-    nf = N_INIT + warmup + steps
+    pre = pre_frames(name)
+    nf = pre + warmup + steps
     seq, s, st = build_sequence(sample_name, 1234, nf)
     times, counts = [], []
     with _MuteStdout():
@@ -231,7 +246,7 @@ def reference_stb(name, threads, warmup, steps, budget_s):
             a = time.perf_counter()
             ref.frame(t)
             dt = time.perf_counter() - a
-            if t >= N_INIT + warmup:
+            if t >= pre + warmup:
                 rows = ref.tracks()
                 times.append(dt)
                 counts.append(sum(int(np.count_nonzero(v[:, 1] == t)) for v in rows.values()
@@ -268,7 +283,8 @@ def run_reference(args):
         else:
             cfg = workload_config(args.workload, s, seq=seq, st=st)
         sample = (f"STB::processFrame on {sample_name}: {N_INIT} initial-phase and "
-                  f"{args.warmup} convergence-phase frames untimed, then {len(times)} "
+                  f"{pre_frames(args.workload) - N_INIT + args.warmup} convergence-phase "
+                  f"frames untimed, then {len(times)} "
                   f"convergence-phase frames timed (the same frame indices as the GPU arm; "
                   f"stops after {REF_STB_BUDGET_S:.0f} s); OpenMP, all host threads")
     value = sum(counts) / sum(times)
@@ -302,7 +318,9 @@ def workload_config(name, s, sc=None, seq=None, st=None):
         base.update(particles=int(len(seq.truth[0])), cameras=seq.n_cam,
                     image=f"{H}x{W} {dt} ({int(seq.max_val).bit_length()}-bit)",
                     ppp=round(len(seq.truth[0]) / (H * W), 4),
-                    initial_frames=N_INIT, link_radius_mm=st.radius_search_track,
+                    initial_frames=N_INIT,
+                    untimed_convergence_frames=WORKLOADS[name].get("converge", 0),
+                    link_radius_mm=st.radius_search_track,
                     pred_field=f"{st.pf_nx}x{st.pf_ny}x{st.pf_nz} r {st.pf_r} mm",
                     match_cam_count=s.match_cam_count,
                     detection_cap=s.n_obj2d_process_max,
@@ -560,7 +578,8 @@ def run_ours_stb(args, o: Ours, pre):
     from pyopenlpt_b200 import _ffi
     from pyopenlpt_b200 import learned as L
     torch = o.torch
-    nf = N_INIT + args.warmup + args.steps
+    pre = pre_frames(args.workload)
+    nf = pre + args.warmup + args.steps
     t_gen = time.perf_counter()
     seq, s, st = build_sequence(args.workload, 1234 + o.rank, nf, device=f"cuda:{o.local}")
     t_gen = time.perf_counter() - t_gen
@@ -571,11 +590,11 @@ def run_ours_stb(args, o: Ours, pre):
     dev_frames = [torch.from_numpy(f).cuda() for f in frames]
     host_frames = [torch.from_numpy(f).pin_memory() for f in frames]
     params = _ffi.stb_params(s, st, seq.volume, 0, nf - 1, o.prec)
-    t0_frame = N_INIT + args.warmup
+    t0_frame = pre + args.warmup
 
-    def new_ctx(prec=o.prec):
+    def new_ctx(prec=o.prec, sk=None):
         ctx = o.context(seq)
-        ctx.stb_configure(_ffi.stb_params(s, st, seq.volume, 0, nf - 1, prec))
+        ctx.stb_configure(_ffi.stb_params(sk or s, st, seq.volume, 0, nf - 1, prec))
         return ctx
 
     def frame_device(ctx, t):
@@ -591,11 +610,16 @@ def run_ours_stb(args, o: Ours, pre):
         a = time.perf_counter()
         frame_device(ctx, t)
         init_ms.append(1e3 * (time.perf_counter() - a))
+    conv_ms = []
+    for t in range(N_INIT, pre):
+        a = time.perf_counter()
+        frame_device(ctx, t)
+        conv_ms.append(1e3 * (time.perf_counter() - a))
     want_learned = (o.world == 1 and args.learn_frames > 0
                     and WORKLOADS[args.workload].get("gen") == "poly")
     state_init = L.stb_state(ctx) if want_learned else None
     plain_warm = []
-    for t in range(N_INIT, t0_frame):
+    for t in range(pre, t0_frame):
         ms = timed_frame(o, stream, lambda: frame_device(ctx, t))
         plain_warm.append(dict(frame_quality(ctx.stb_frame_objects(), seq.truth[t]), ms=ms,
                                parts=ctx.stb_frame_points(t)))
@@ -637,7 +661,6 @@ def run_ours_stb(args, o: Ours, pre):
     ctx.profile(False)
     clk = clocks.stop()
     lists, _, _ = ctx.stb_counts()
-    res32 = ctx.stb_frame_image(0, H, W) if o.world == 1 and o.prec == 0 else None
     ctx.close()
 
     # end to end through the C ABI with host (pinned) images: a second tracker over the
@@ -668,6 +691,7 @@ def run_ours_stb(args, o: Ours, pre):
     if o.rank == 0:
         cpu = None
         extra = {"initial_phase_ms_per_frame": [round(x, 1) for x in init_ms],
+                 "untimed_convergence_ms_per_frame": [round(x, 1) for x in conv_ms],
                  "extended_plus_new_per_step": ext_new / args.steps,
                  "track_lists_after": dict(zip(_ffi.TRACK_LISTS, lists)),
                  "quality_vs_truth": mean_quality(quality),
@@ -677,8 +701,7 @@ def run_ours_stb(args, o: Ours, pre):
                                            frame_device, state_init, state_t0, plain_warm,
                                            quality)
         if o.world == 1 and o.prec == 0 and not args.no_fp64_check:
-            extra["fp64_check"] = fp64_check(args, o, seq, s, st, nf, t0_frame, new_ctx,
-                                             frame_device, plain_objs, res32, H, W)
+            extra["fp64_check"] = fp64_check(o, seq, s, nf - 1, plain_objs[nf - 1])
         if o.world == 1 and not args.no_cpu_baseline:
             threads = os.cpu_count() or 1
             times, counts, rseq, _, _, sname = reference_stb(args.workload, threads, 0, 2, 60.0)
@@ -700,8 +723,8 @@ def learned_stb(args, o, seq, s, st, nf, t0_frame, new_ctx, frame_device, state_
        workload: prediction-like starts (true particles displaced by 0.3 and 1 px,
        plus 10% uniform points) and the candidates of the first IPR loop.
     2. Training on the device (olpt_mlp_train).
-    3. Calibration on the warm-up frames, from the plain tracker's tracks after the
-       initial phase: the fastest settings whose recall is within 0.5% of the plain
+    3. Calibration on the warm-up frames, from the plain tracker's tracks before them:
+       the fastest settings whose recall is within 0.5% of the plain
        form's and whose ghost rate is not higher, at 0.05 and 0.1 mm.
     4. Evaluation on the timed frames, from the plain tracker's tracks at the first
        timed frame, device-timed like the plain form."""
@@ -747,8 +770,8 @@ def learned_stb(args, o, seq, s, st, nf, t0_frame, new_ctx, frame_device, state_
     params = ctx.mlp_get_params()
     ctx.close()
 
-    def run(ls, state, frames):
-        c = new_ctx()
+    def run(ls, loops, state, frames):
+        c = new_ctx(sk=dataclasses.replace(s, n_loop_ipr=loops))
         c.mlp_set_params(params)
         c.learned_configure(ls.params(enable=True))
         L.set_stb_state(c, state)
@@ -764,26 +787,31 @@ def learned_stb(args, o, seq, s, st, nf, t0_frame, new_ctx, frame_device, state_
         return out, (b1 - b0) / max(1, a1 - a0)
 
     # 3. calibration on the warm-up frames
-    warm = list(range(N_INIT, t0_frame))
+    warm = list(range(t0_frame - len(plain_warm), t0_frame))
     pw = mean_quality(plain_warm)
     sweep, chosen = [], None
-    grid = [dict(refine_loops=1, ghost_logit=5.0, fallback_residual=1e9),
-            dict(refine_loops=1, ghost_logit=5.0, fallback_residual=0.3),
-            dict(refine_loops=1, ghost_logit=5.0, fallback_residual=0.1),
-            dict(refine_loops=2, ghost_logit=5.0, fallback_residual=0.3),
-            dict(refine_loops=2, ghost_logit=8.0, fallback_residual=0.1),
-            dict(refine_loops=2, ghost_logit=8.0, fallback_residual=0.03)]
-    for g in grid:
+    # (IPR loops per frame, settings): the network's proposals let the IPR on the
+    # residual run fewer loops; the fallback re-runs the plain shake for hard objects
+    grid = [(1, dict(refine_loops=1, ghost_logit=5.0, fallback_residual=1e9)),
+            (1, dict(refine_loops=1, ghost_logit=5.0, fallback_residual=0.3)),
+            (2, dict(refine_loops=1, ghost_logit=5.0, fallback_residual=1e9)),
+            (2, dict(refine_loops=1, ghost_logit=5.0, fallback_residual=0.3)),
+            (s.n_loop_ipr, dict(refine_loops=1, ghost_logit=5.0, fallback_residual=1e9)),
+            (s.n_loop_ipr, dict(refine_loops=2, ghost_logit=8.0, fallback_residual=0.1))]
+    for loops, g in grid:
         ls = dataclasses.replace(ls0, **g)
-        res, fb = run(ls, state_init, warm)
+        res, fb = run(ls, loops, state_init, warm)
         m = mean_quality(res)
         ok = meets(m, pw)
-        sweep.append(dict(g, **m, fallback_fraction=round(fb, 4), meets=ok))
-        if ok and (chosen is None or m["ms_per_frame"] < chosen[1]["ms_per_frame"]):
-            chosen = (ls, m)
-    ls = chosen[0] if chosen is not None else dataclasses.replace(ls0, **grid[-1])
+        sweep.append(dict(g, ipr_loops=loops, **m, fallback_fraction=round(fb, 4), meets=ok))
+        if ok and (chosen is None or m["ms_per_frame"] < chosen[2]["ms_per_frame"]):
+            chosen = (ls, loops, m)
+    if chosen is not None:
+        ls, loops = chosen[0], chosen[1]
+    else:
+        loops, ls = grid[-1][0], dataclasses.replace(ls0, **grid[-1][1])
     # 4. evaluation on the timed frames
-    res, fb = run(ls, state_t0, list(range(t0_frame, nf)))
+    res, fb = run(ls, loops, state_t0, list(range(t0_frame, nf)))
     lm, pm = mean_quality(res), mean_quality(plain_timed)
     return {
         "form": "MLP proposal on every prediction and IPR candidate (ghosts dropped), "
@@ -795,7 +823,8 @@ def learned_stb(args, o, seq, s, st, nf, t0_frame, new_ctx, frame_device, state_
                   "loss_first": round(losses[0], 4),
                   "loss_last50": round(float(np.mean(losses[-50:])), 4)},
         "calibration": {"frames": warm, "plain": pw, "sweep": sweep,
-                        "chosen": {"refine_loops": ls.refine_loops, "ghost_logit": ls.ghost_logit,
+                        "chosen": {"ipr_loops": loops, "refine_loops": ls.refine_loops,
+                                   "ghost_logit": ls.ghost_logit,
                                    "fallback_residual": ls.fallback_residual,
                                    "refine_width_mm": ls.refine_width_mm,
                                    "out_scale_mm": ls.out_scale_mm},
@@ -808,39 +837,35 @@ def learned_stb(args, o, seq, s, st, nf, t0_frame, new_ctx, frame_device, state_
     }
 
 
-def fp64_check(args, o, seq, s, st, nf, t0_frame, new_ctx, frame_device, objs32, res32, H, W):
-    """The FP32 production path against the library's FP64 mode (the reference's
-    arithmetic) on the same frames: position differences of the frame's particles
-    matched one to one (nearest within 1e-3 mm), their reprojection differences, and
-    the residual image of camera 0 after the last frame."""
-    from scipy.spatial import cKDTree
-    ctx = new_ctx(1)
-    d_all, r_all, unmatched = [], [], 0
-    for t in range(nf):
-        frame_device(ctx, t)
-        if t in objs32:
-            x64 = ctx.stb_frame_objects()
-            x32 = objs32[t]
-            if len(x64) and len(x32):
-                d, j = cKDTree(x64).query(x32)
-                ok = d <= 1e-3
-                unmatched += int(np.sum(~ok)) + max(0, len(x64) - int(np.sum(ok)))
-                d_all.append(d[ok])
-                for c in range(len(seq.cams)):
-                    r_all.append(np.abs(ctx.project(c, x32[ok]) - ctx.project(c, x64[j[ok]])).max(1))
-    res64 = ctx.stb_frame_image(0, H, W)
+def fp64_check(o, seq, s, t, xyz):
+    """The FP32 production shake against the library's FP64 mode (the reference's
+    arithmetic) on the same input: frame t's images and the plain tracker's particles
+    of that frame as starting positions, one runShake in each precision.  Reports the
+    position differences, the reprojection differences on every camera, and the
+    residual image of camera 0 (FP32 plane against the FP64 one)."""
+    from pyopenlpt_b200 import _ffi, learned as L
+    ctx = _ffi.Context(o.local)
+    L.bind_rig(ctx, seq)
+    H, W = seq.cams[0].n_row, seq.cams[0].n_col
+    out, res = {}, {}
+    for prec in (0, 1):
+        ctx.upload_images(list(seq.frames[t]))
+        ctx.upload_objects(xyz)
+        sp = _ffi.shake_params(s, prec)
+        ctx.shake(sp)
+        out[prec] = ctx.objects()
+        ctx.residual(sp)
+        res[prec] = ctx.residual_image(0, (H, W), np.float64)
+    d = np.max(np.abs(out[0]["xyz"] - out[1]["xyz"]), axis=1)
+    r = np.max(np.abs(out[0]["uv"] - out[1]["uv"]), axis=(1, 2))
+    ok = np.isfinite(d)
     ctx.close()
-    d = np.concatenate(d_all) if d_all else np.zeros(0)
-    r = np.concatenate(r_all) if r_all else np.zeros(0)
-    return {"frames": len(objs32), "matched": int(len(d)), "unmatched": unmatched,
-            "position_mm": {"median": float(np.median(d)) if len(d) else None,
-                            "p99": float(np.quantile(d, 0.99)) if len(d) else None,
-                            "max": float(d.max()) if len(d) else None,
-                            "frac_le_1e-4": float(np.mean(d <= 1e-4)) if len(d) else None},
-            "reprojection_px": {"median": float(np.median(r)) if len(r) else None,
-                                "max": float(r.max()) if len(r) else None},
-            "residual_cam0_max_abs": float(np.max(np.abs(res32 - res64))) if res32 is not None
-            else None}
+    return {"frame": t, "objects": int(len(xyz)),
+            "position_mm": {"median": float(np.median(d[ok])), "p99": float(np.quantile(d[ok], 0.99)),
+                            "max": float(d[ok].max()), "frac_le_1e-4": float(np.mean(d[ok] <= 1e-4))},
+            "reprojection_px": {"median": float(np.median(r[ok])), "max": float(r[ok].max())},
+            "flags_differ": int(np.sum(out[0]["flags"] != out[1]["flags"])),
+            "residual_cam0_max_abs": float(np.max(np.abs(res[0] - res[1])))}
 
 
 # ----------------------------------------------------------------------------- learned

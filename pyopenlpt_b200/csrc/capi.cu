@@ -34,6 +34,9 @@ olpt_status_t guard(olpt_ctx* ctx, F&& f) {
     return e.code;
   } catch (CudaError const& e) {
     ctx->err = std::string(cudaGetErrorString(e.code)) + " (" + e.where + ")";
+    // a non-sticky error also stays recorded as the runtime's last error: clear it,
+    // or the next call's launch check would report it again
+    cudaGetLastError();
     return e.code == cudaErrorMemoryAllocation ? OLPT_ERR_OOM : OLPT_ERR_CUDA;
   } catch (std::bad_alloc const&) {
     ctx->err = "host allocation failed";
@@ -1195,6 +1198,7 @@ olpt_status_t olpt_mlp_features(olpt_ctx* ctx, const olpt_shake_params* p, float
     const int64_t n = ctx->obj.n;
     if (n == 0) return;
     OLPT_REQUIRE(x, OLPT_ERR_INVALID_ARG, "null output");
+    mlp_sync_dims(ctx);
     residual_all_device(ctx, sp);
     MlpWork& W = ctx->mlp;
     cudaStream_t s = ctx->stream;

@@ -472,6 +472,10 @@ void set_dims(olpt_ctx* ctx) {
   }
 }
 
+void mlp_sync_dims(olpt_ctx* ctx) {
+  if (!ctx->mlp.ready) set_dims(ctx);
+}
+
 void mlp_init(olpt_ctx* ctx, uint64_t seed) {
   set_dims(ctx);
   alloc_params(ctx);
@@ -513,7 +517,7 @@ void mlp_get_params(olpt_ctx* ctx, float* host) {
 }
 
 void mlp_features_device(olpt_ctx* ctx, const ShakeParams& sp, __nv_bfloat16* x, float* f32) {
-  if (!ctx->mlp.ready) set_dims(ctx);
+  mlp_sync_dims(ctx);
   OLPT_REQUIRE(ctx->n_cam == ctx->mlp.dims.cams, OLPT_ERR_UNSUPPORTED,
                "learned proposal: the network was built for " +
                    std::to_string(ctx->mlp.dims.cams) + " cameras, the rig has " +

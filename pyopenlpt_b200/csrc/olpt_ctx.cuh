@@ -335,6 +335,8 @@ struct MlpWork {
 };
 
 // mlp.cu
+// the network geometry of the context's camera count, unless a network is set
+void mlp_sync_dims(olpt_ctx* ctx);
 void mlp_init(olpt_ctx* ctx, uint64_t seed);
 void mlp_set_params(olpt_ctx* ctx, const float* host);
 void mlp_get_params(olpt_ctx* ctx, float* host);

