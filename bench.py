@@ -228,14 +228,14 @@ def reference_ipr_time(sc, s, threads: int, images=None):
 REF_STB_BUDGET_S = 420.0  # convergence frames of the reference arm stop after this
 
 
-def reference_stb(name, threads, warmup, steps, budget_s):
+def reference_stb(name, threads, warmup, steps, budget_s, converge=None):
     """The reference STB (compiled from its sources) on the workload's CPU sample:
     N_INIT initial-phase and ``warmup`` convergence-phase frames untimed, then up to
     ``steps`` convergence frames timed (wall clock), stopping once ``budget_s`` has
     passed.  Particles per frame = track points the frame adds over the four lists."""
     from oracle.ref import RefSTB
     sample_name = REFERENCE_SAMPLE.get(name, name)
-    pre = pre_frames(name)
+    pre = pre_frames(name) if converge is None else N_INIT + converge
     nf = pre + warmup + steps
     seq, s, st = build_sequence(sample_name, 1234, nf)
     times, counts = [], []
@@ -574,12 +574,12 @@ def timed_frame(o, stream, fn):
     return e0.elapsed_time(e1)
 
 
-def run_ours_stb(args, o: Ours, pre):
+def run_ours_stb(args, o: Ours, pre_lines):
     from pyopenlpt_b200 import _ffi
     from pyopenlpt_b200 import learned as L
     torch = o.torch
-    pre = pre_frames(args.workload)
-    nf = pre + args.warmup + args.steps
+    n_pre = pre_frames(args.workload)
+    nf = n_pre + args.warmup + args.steps
     t_gen = time.perf_counter()
     seq, s, st = build_sequence(args.workload, 1234 + o.rank, nf, device=f"cuda:{o.local}")
     t_gen = time.perf_counter() - t_gen
@@ -590,7 +590,7 @@ def run_ours_stb(args, o: Ours, pre):
     dev_frames = [torch.from_numpy(f).cuda() for f in frames]
     host_frames = [torch.from_numpy(f).pin_memory() for f in frames]
     params = _ffi.stb_params(s, st, seq.volume, 0, nf - 1, o.prec)
-    t0_frame = pre + args.warmup
+    t0_frame = n_pre + args.warmup
 
     def new_ctx(prec=o.prec, sk=None):
         ctx = o.context(seq)
@@ -611,7 +611,7 @@ def run_ours_stb(args, o: Ours, pre):
         frame_device(ctx, t)
         init_ms.append(1e3 * (time.perf_counter() - a))
     conv_ms = []
-    for t in range(N_INIT, pre):
+    for t in range(N_INIT, n_pre):
         a = time.perf_counter()
         frame_device(ctx, t)
         conv_ms.append(1e3 * (time.perf_counter() - a))
@@ -619,7 +619,7 @@ def run_ours_stb(args, o: Ours, pre):
                     and WORKLOADS[args.workload].get("gen") == "poly")
     state_init = L.stb_state(ctx) if want_learned else None
     plain_warm = []
-    for t in range(pre, t0_frame):
+    for t in range(n_pre, t0_frame):
         ms = timed_frame(o, stream, lambda: frame_device(ctx, t))
         plain_warm.append(dict(frame_quality(ctx.stb_frame_objects(), seq.truth[t]), ms=ms,
                                parts=ctx.stb_frame_points(t)))
@@ -696,21 +696,29 @@ def run_ours_stb(args, o: Ours, pre):
                  "track_lists_after": dict(zip(_ffi.TRACK_LISTS, lists)),
                  "quality_vs_truth": mean_quality(quality),
                  "generation_s": round(t_gen, 1)}
+        # the secondary measurements: a failure is recorded in the line, not fatal
+        def guarded(key, fn):
+            try:
+                extra[key] = fn()
+            except Exception as e:  # noqa: BLE001
+                extra[key] = {"error": f"{type(e).__name__}: {e}"}
+
         if want_learned:
-            extra["learned"] = learned_stb(args, o, seq, s, st, nf, t0_frame, new_ctx,
-                                           frame_device, state_init, state_t0, plain_warm,
-                                           quality)
+            guarded("learned", lambda: learned_stb(args, o, seq, s, st, nf, t0_frame, new_ctx,
+                                                   frame_device, state_init, state_t0,
+                                                   plain_warm, quality))
         if o.world == 1 and o.prec == 0 and not args.no_fp64_check:
-            extra["fp64_check"] = fp64_check(o, seq, s, nf - 1, plain_objs[nf - 1])
+            guarded("fp64_check", lambda: fp64_check(o, seq, s, nf - 1, plain_objs[nf - 1]))
         if o.world == 1 and not args.no_cpu_baseline:
             threads = os.cpu_count() or 1
-            times, counts, rseq, _, _, sname = reference_stb(args.workload, threads, 0, 2, 60.0)
+            times, counts, rseq, _, _, sname = reference_stb(args.workload, threads, 0, 2, 60.0,
+                                                             converge=0)
             cpu = {"value": sum(counts) / sum(times), "unit": "particles/s", "cores": threads,
                    "kind": "reference",
                    "sample": f"STB::processFrame compiled from the reference sources (OpenMP) "
                              f"on {sname}: {N_INIT} initial-phase frames untimed, then "
                              f"{len(times)} convergence-phase frames timed"}
-        extra.update(pre)
+        extra.update(pre_lines)
         o.line(prof, dev_ms, parts, e2e_s, e2e_parts, bi, bo // max(1, args.steps), launches,
                clk, workload_config(args.workload, s, seq=seq, st=st), cpu, extra)
 
