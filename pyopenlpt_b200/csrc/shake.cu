@@ -45,7 +45,7 @@ inline int nblk(int64_t n, int t = 256) { return (int)((n + t - 1) / t); }
 
 // ---------------------------------------------------------------- 1. prep
 template <typename Real>
-__global__ void prep_kernel(ShakeView v, const double* xyz, int64_t n, double* uv, Real* otfp,
+__global__ void prep_kernel(const __grid_constant__ ShakeView v, const double* xyz, int64_t n, double* uv, Real* otfp,
                             int* pair_key, const uint8_t* flags, int all_cams) {
   int64_t o = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
   if (o >= n) return;
@@ -82,7 +82,7 @@ __device__ __forceinline__ void smem_max(double* p, double v) {
 // Window tiles are keyed by the tile of the window's top-left pixel, so a CTA
 // gathers bins of its own tile and the tiles up/left of it (windows < 32 px).
 template <typename Real>
-__global__ void __launch_bounds__(256) residual_kernel(ShakeView v, const double* uv,
+__global__ void __launch_bounds__(256) residual_kernel(const __grid_constant__ ShakeView v, const double* uv,
                                                        const Real* otfp, const int* bin_start,
                                                        const int* bin_items, int clamp,
                                                        int all_cams) {
@@ -392,7 +392,7 @@ __device__ __forceinline__ bool in_roi(const Rect& R, double u, double w) {
 }
 
 template <typename Real, int NC>
-__global__ void __launch_bounds__(128, 8) shake_kernel(ShakeView v, int64_t n, double* xyz,
+__global__ void __launch_bounds__(128, 8) shake_kernel(const __grid_constant__ ShakeView v, int64_t n, double* xyz,
                                                     double* uv, const Real* otfp, double* score,
                                                     double delta, const uint8_t* active,
                                                     double* resid_out) {

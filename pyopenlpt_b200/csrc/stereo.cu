@@ -224,7 +224,7 @@ __device__ double seg_len(const double* L, double W, double H) {
 }
 
 // seed level: one path per reference detection with its second build camera
-__global__ void seed_kernel(const SmView v, int ref, Path* out, int* out_count, int cap) {
+__global__ void seed_kernel(const __grid_constant__ SmView v, int ref, Path* out, int* out_count, int cap) {
   int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
   if (i >= v.n[ref]) return;
   int best = -1;
@@ -349,12 +349,11 @@ __device__ __noinline__ void near_append(const SmView& v, int kind, int k, int c
 // warp per path, lanes take rows (the single long strip of K = 1); otherwise one
 // thread per path (K >= 2, where the strips intersect in a few rows).
 template <int K, bool WARP>
-__global__ void __launch_bounds__(256, 4) enum_kernel(const SmView v, const Path* in, int n_in,
+__global__ void __launch_bounds__(256, 4) enum_kernel(const __grid_constant__ SmView v, const Path* in, int n_in,
                                                    Pair* pairs, int* pair_count, int pair_cap) {
   const int gtid = blockIdx.x * blockDim.x + threadIdx.x;
   const int pidx = WARP ? (gtid >> 5) : gtid;
   const int r0 = WARP ? (threadIdx.x & 31) : 0;
-  const int rstep = WARP ? 32 : 1;
   if (pidx >= n_in) return;
   const Path P = in[pidx];
   const int t = P.target;
@@ -415,9 +414,11 @@ __global__ void __launch_bounds__(256, 4) enum_kernel(const SmView v, const Path
     }
   }
 
-  for (int cy = row_lo + r0; cy <= row_hi; cy += rstep) {
-    // IDMap::computeStripIntersection, one row
-    int xmin = 0, xmax = cols - 1;
+  // IDMap::computeStripIntersection, one row: the cell range [xmin, xmax] (empty when
+  // xmin > xmax)
+  auto row_span = [&](int cy, int& xmin, int& xmax) {
+    xmin = 0;
+    xmax = cols - 1;
 #pragma unroll
     for (int i = 0; i < K; ++i) {
       if (xmin > xmax) break;
@@ -455,44 +456,97 @@ __global__ void __launch_bounds__(256, 4) enum_kernel(const SmView v, const Path
       xmin = xmin > a ? xmin : a;
       xmax = xmax < b ? xmax : b;
     }
-    if (xmin > xmax) continue;
-    // the cells xmin..xmax of this row are adjacent in cell order: one item range,
-    // visited in the same order as cell by cell
-    const int q1 = cstart[cy * cols + xmax + 1];
-    for (int q = cstart[cy * cols + xmin]; q < q1; ++q) {
-      const double2 xy = cxy[q];
-      bool ok = true;
-      // IDMap::visitPointsInRowSpans precise test
+  };
+  // IDMap::visitPointsInRowSpans precise test and checkBackProjection of the item at
+  // cell-ordered position q; true when the pair passes both
+  auto item_ok = [&](int q) -> bool {
+    const double2 xy = cxy[q];
+    bool ok = true;
+    // IDMap::visitPointsInRowSpans precise test
 #pragma unroll
-      for (int i = 0; i < K; ++i) {
-        const double dx = xy.x - lp[i][0], dy = xy.y - lp[i][1];
-        const double z = dy * lU[i][0] - dx * lU[i][1];
-        ok = ok && !(z * z > tol2);
-        if (v.near_band > 0.0) {
-          const double m = fabs(z) - v.tol2d;
-          if (fabs(m) < v.near_band)
-            near_append(v, 0, K, t, citems[q], P.cams[i], P.ids[i], m);
+    for (int i = 0; i < K; ++i) {
+      const double dx = xy.x - lp[i][0], dy = xy.y - lp[i][1];
+      const double z = dy * lU[i][0] - dx * lU[i][1];
+      ok = ok && !(z * z > tol2);
+      if (v.near_band > 0.0) {
+        const double m = fabs(z) - v.tol2d;
+        if (fabs(m) < v.near_band)
+          near_append(v, 0, K, t, citems[q], P.cams[i], P.ids[i], m);
+      }
+    }
+    if (!ok) return false;
+    // checkBackProjection (StereoMatch.cpp:1206-1227)
+#pragma unroll
+    for (int i = 0; i < K; ++i) {
+      if (!ok) break;
+      const double2 a = reinterpret_cast<const double2*>(cbp[i])[2 * q];
+      const double2 b = reinterpret_cast<const double2*>(cbp[i])[2 * q + 1];
+      const double d0 = cpt[i][0] - a.x, d1 = cpt[i][1] - a.y;
+      const double z = d1 * b.x - d0 * b.y;
+      ok = !(z * z > tol2);
+      if (v.near_band > 0.0) {
+        const double m = fabs(z) - v.tol2d;
+        if (fabs(m) < v.near_band)
+          near_append(v, 1, K, t, citems[q], P.cams[i], P.ids[i], m);
+      }
+    }
+    return ok;
+  };
+
+  if constexpr (WARP) {
+    // one warp per path: 32 rows at a time (lane = row), then the rows' item ranges
+    // flattened over the lanes (consecutive items of a row are adjacent in memory, so
+    // the loads coalesce and no lane idles on a short row)
+    for (int base = row_lo; base <= row_hi; base += 32) {
+      const int cy = base + r0;
+      int q0 = 0, cnt = 0;
+      if (cy <= row_hi) {
+        int xmin, xmax;
+        row_span(cy, xmin, xmax);
+        if (xmin <= xmax) {
+          q0 = cstart[cy * cols + xmin];
+          cnt = cstart[cy * cols + xmax + 1] - q0;
         }
       }
-      if (!ok) continue;
-      // checkBackProjection (StereoMatch.cpp:1206-1227)
+      int incl = cnt;
 #pragma unroll
-      for (int i = 0; i < K; ++i) {
-        if (!ok) break;
-        const double2 a = reinterpret_cast<const double2*>(cbp[i])[2 * q];
-        const double2 b = reinterpret_cast<const double2*>(cbp[i])[2 * q + 1];
-        const double d0 = cpt[i][0] - a.x, d1 = cpt[i][1] - a.y;
-        const double z = d1 * b.x - d0 * b.y;
-        ok = !(z * z > tol2);
-        if (v.near_band > 0.0) {
-          const double m = fabs(z) - v.tol2d;
-          if (fabs(m) < v.near_band)
-            near_append(v, 1, K, t, citems[q], P.cams[i], P.ids[i], m);
-        }
+      for (int o = 1; o < 32; o <<= 1) {
+        const int t_ = __shfl_up_sync(0xffffffffu, incl, o);
+        if (r0 >= o) incl += t_;
       }
-      if (!ok) continue;
-      const int slot = append_slot(pair_count);
-      if (slot < pair_cap) pairs[slot] = Pair{pidx, citems[q]};
+      const int excl = incl - cnt;
+      const int total = __shfl_sync(0xffffffffu, incl, 31);
+      for (int k0 = 0; k0 < total; k0 += 32) {
+        const int k = k0 + r0;
+        // the row holding item k: the largest lane r with excl[r] <= k
+        int r = 0;
+#pragma unroll
+        for (int step = 16; step > 0; step >>= 1) {
+          const int e = __shfl_sync(0xffffffffu, excl, r + step);
+          if (e <= k) r += step;
+        }
+        const int qr = __shfl_sync(0xffffffffu, q0, r);
+        const int er = __shfl_sync(0xffffffffu, excl, r);
+        if (k >= total) continue;
+        const int q = qr + (k - er);
+        if (!item_ok(q)) continue;
+        const int slot = append_slot(pair_count);
+        if (slot < pair_cap) pairs[slot] = Pair{pidx, citems[q]};
+      }
+    }
+  } else {
+    for (int cy = row_lo; cy <= row_hi; ++cy) {
+      int xmin, xmax;
+      row_span(cy, xmin, xmax);
+      if (xmin > xmax) continue;
+      // the cells xmin..xmax of this row are adjacent in cell order: one item range,
+      // visited in the same order as cell by cell
+      const int q1 = cstart[cy * cols + xmax + 1];
+      for (int q = cstart[cy * cols + xmin]; q < q1; ++q) {
+        if (!item_ok(q)) continue;
+        const int slot = append_slot(pair_count);
+        if (slot < pair_cap) pairs[slot] = Pair{pidx, citems[q]};
+      }
     }
   }
 }
@@ -502,7 +556,7 @@ __global__ void __launch_bounds__(256, 4) enum_kernel(const SmView v, const Path
 // TriangulationCheckWithTol: StereoMatch.cpp:1072-1141) on the path's lines plus the
 // candidate's, then the child path (terminal, or with its next target camera).
 template <int K>
-__global__ void __launch_bounds__(256, 2) tri_kernel(const SmView v, const Path* in,
+__global__ void __launch_bounds__(256, 2) tri_kernel(const __grid_constant__ SmView v, const Path* in,
                                                      const Pair* pairs, int n_pairs, Path* out,
                                                      int* out_count, int out_cap, Path* term,
                                                      int* term_count, int term_cap) {
@@ -657,7 +711,7 @@ __global__ void __launch_bounds__(256, 2) tri_kernel(const SmView v, const Path*
 
 // StereoMatch::checkMatch, case "every active camera was used to build"
 // (StereoMatch.cpp:520-540): triangulate in camera order, gate on tol_3d and limit.
-__global__ void check_kernel(const SmView v, const Path* term, int n_term, int* cand_ids,
+__global__ void check_kernel(const __grid_constant__ SmView v, const Path* term, int n_term, int* cand_ids,
                              double* cand_e, double* cand_x, int* cand_count, int cap) {
   int i = blockIdx.x * blockDim.x + threadIdx.x;
   if (i >= n_term) return;
