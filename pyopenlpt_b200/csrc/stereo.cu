@@ -349,7 +349,7 @@ __device__ __noinline__ void near_append(const SmView& v, int kind, int k, int c
 // warp per path, lanes take rows (the single long strip of K = 1); otherwise one
 // thread per path (K >= 2, where the strips intersect in a few rows).
 template <int K, bool WARP>
-__global__ void __launch_bounds__(256, 4) enum_kernel(const __grid_constant__ SmView v, const Path* in, int n_in,
+__global__ void __launch_bounds__(256, K == 1 ? 4 : 3) enum_kernel(const __grid_constant__ SmView v, const Path* in, int n_in,
                                                    Pair* pairs, int* pair_count, int pair_cap) {
   const int gtid = blockIdx.x * blockDim.x + threadIdx.x;
   const int pidx = WARP ? (gtid >> 5) : gtid;
@@ -374,7 +374,6 @@ __global__ void __launch_bounds__(256, 4) enum_kernel(const __grid_constant__ Sm
   const int rows = v.rows[t], cols = v.cols[t];
   const double cellp = (double)v.cell;
   const double hw = 0.5 * v.cell, hh = 0.5 * v.cell;
-  const double to_index = 1.0 / v.cell;
   const double tol_grow = v.tol2d + 1e-6;
   const double tol2 = v.tol2d * v.tol2d;
   const int* cstart = v.cell_start[t];
@@ -414,44 +413,51 @@ __global__ void __launch_bounds__(256, 4) enum_kernel(const __grid_constant__ Sm
     }
   }
 
-  // IDMap::computeStripIntersection, one row: the cell range [xmin, xmax] (empty when
-  // xmin > xmax)
+  // IDMap::computeStripIntersection, one row: a cell range [xmin, xmax] (empty when
+  // xmin > xmax) that contains the reference's.  The range only selects the items that
+  // the exact FP64 tests below then decide, and every item that passes them lies in a
+  // cell of the reference's range, so any superset of that range gives the same
+  // accepted set.  It is evaluated in FP32 with the strip widened by 0.01 px and the
+  // cell bounds widened by 1e-3 cells (FP32 errors here stay below 1e-3 px), and the
+  // division by n0 folded into one reciprocal per strip.
+  float sn0[K], sn1[K], sd[K], sT[K], sinv[K];
+  bool shz[K];
+#pragma unroll
+  for (int i = 0; i < K; ++i) {
+    const double n0 = -lU[i][1], n1 = lU[i][0];
+    sn0[i] = (float)n0;
+    sn1[i] = (float)n1;
+    sd[i] = (float)(-(n0 * lp[i][0] + n1 * lp[i][1]));
+    sT[i] = (float)(tol_grow + fabs(n0) * hw + fabs(n1) * hh) + 0.01f;
+    shz[i] = fabs(n0) < 1e-12;
+    sinv[i] = shz[i] ? 0.0f : 1.0f / (float)n0;
+  }
+  const float cellf = (float)cellp, to_index_f = 1.0f / cellf;
   auto row_span = [&](int cy, int& xmin, int& xmax) {
     xmin = 0;
     xmax = cols - 1;
+    const float y_c = ((float)cy + 0.5f) * cellf;
 #pragma unroll
     for (int i = 0; i < K; ++i) {
-      if (xmin > xmax) break;
-      const double n0 = -lU[i][1], n1 = lU[i][0];
-      const double d = -(n0 * lp[i][0] + n1 * lp[i][1]);
-      const double y_c = (cy + 0.5) * cellp;
-      const double C = n1 * y_c + d;
-      const double proj_extent = fabs(n0) * hw + fabs(n1) * hh;
-      const double T = tol_grow + proj_extent;
+      const float C = fmaf(sn1[i], y_c, sd[i]);
       int a = 0, b = cols - 1;
-      if (fabs(n0) < 1e-12) {
-        if (fabs(C) > T) {
+      if (shz[i]) {
+        if (fabsf(C) > sT[i]) {
           xmin = 1;
           xmax = 0;
-          break;
         }
       } else {
-        double xl = (-T - C) / n0;
-        double xr = (T - C) / n0;
+        float xl = (-sT[i] - C) * sinv[i];
+        float xr = (sT[i] - C) * sinv[i];
         if (xl > xr) {
-          double s = xl;
+          const float s_ = xl;
           xl = xr;
-          xr = s;
+          xr = s_;
         }
-        a = (int)ceil(xl * to_index - 0.5 - 1e-9);
-        b = (int)floor(xr * to_index - 0.5 + 1e-9);
+        a = (int)ceilf(xl * to_index_f - 0.5f - 1e-3f);
+        b = (int)floorf(xr * to_index_f - 0.5f + 1e-3f);
         a = a > 0 ? a : 0;
         b = b < cols - 1 ? b : cols - 1;
-        if (a > b) {
-          xmin = 1;
-          xmax = 0;
-          break;
-        }
       }
       xmin = xmin > a ? xmin : a;
       xmax = xmax < b ? xmax : b;
