@@ -349,19 +349,26 @@ __device__ __noinline__ void near_append(const SmView& v, int kind, int k, int c
 // warp per path, lanes take rows (the single long strip of K = 1); otherwise one
 // thread per path (K >= 2, where the strips intersect in a few rows).
 template <int K, bool WARP>
-__global__ void __launch_bounds__(256, K == 1 ? 4 : 3) enum_kernel(const __grid_constant__ SmView v, const Path* in, int n_in,
+__global__ void __launch_bounds__(256, K == 1 ? 4 : 2) enum_kernel(const __grid_constant__ SmView v, const Path* in, int n_in,
                                                    Pair* pairs, int* pair_count, int pair_cap) {
   const int gtid = blockIdx.x * blockDim.x + threadIdx.x;
   const int pidx = WARP ? (gtid >> 5) : gtid;
   const int r0 = WARP ? (threadIdx.x & 31) : 0;
-  if (pidx >= n_in) return;
-  const Path P = in[pidx];
+  // thread-per-path levels keep every lane of a warp to the end (the items of the
+  // warp's paths are shared out over all lanes); a lane without a path has no rows
+  const bool live = pidx < n_in;
+  if (WARP && !live) return;
+  Path P{};
+  if (live) P = in[pidx];
   const int t = P.target;
   // image lines of the chosen points on the target camera
   double lp[K][2], lU[K][2];
   double cpt[K][2];
 #pragma unroll
   for (int i = 0; i < K; ++i) {
+    lp[i][0] = lp[i][1] = lU[i][0] = cpt[i][0] = cpt[i][1] = 0.0;
+    lU[i][1] = 1.0;
+    if (!live) continue;
     const int c = P.cams[i];
     const double* L = v.l2d[c][t] + 6 * (int64_t)P.ids[i];
     lp[i][0] = L[0];
@@ -381,14 +388,14 @@ __global__ void __launch_bounds__(256, K == 1 ? 4 : 3) enum_kernel(const __grid_
   const double2* cxy = v.cxy[t];
   const double* cbp[K];
 #pragma unroll
-  for (int i = 0; i < K; ++i) cbp[i] = v.cbp[t][P.cams[i]];
+  for (int i = 0; i < K; ++i) cbp[i] = live ? v.cbp[t][P.cams[i]] : nullptr;
 
   // Rows that can hold a non-empty span: with two or more strips, the cell-centre rows
   // inside the y-extent of the first two strips' intersection parallelogram (plus one
   // row each side).  Rows outside it have an empty exact span, so skipping them leaves
   // the visited set unchanged.
-  int row_lo = 0, row_hi = rows - 1;
-  if (K >= 2) {
+  int row_lo = 0, row_hi = live ? rows - 1 : -1;
+  if (K >= 2 && live) {
     const double n00 = -lU[0][1], n01 = lU[0][0], n10 = -lU[1][1], n11 = lU[1][0];
     const double d0 = -(n00 * lp[0][0] + n01 * lp[0][1]);
     const double d1 = -(n10 * lp[1][0] + n11 * lp[1][1]);
@@ -541,17 +548,91 @@ __global__ void __launch_bounds__(256, K == 1 ? 4 : 3) enum_kernel(const __grid_
       }
     }
   } else {
-    for (int cy = row_lo; cy <= row_hi; ++cy) {
-      int xmin, xmax;
-      row_span(cy, xmin, xmax);
-      if (xmin > xmax) continue;
-      // the cells xmin..xmax of this row are adjacent in cell order: one item range,
-      // visited in the same order as cell by cell
-      const int q1 = cstart[cy * cols + xmax + 1];
-      for (int q = cstart[cy * cols + xmin]; q < q1; ++q) {
-        if (!item_ok(q)) continue;
+    // K >= 2, one path per lane: row j of every lane's path at a time, the 32 rows'
+    // item ranges flattened over the warp; an item is tested against its owner lane's
+    // lines and points (fetched by shuffles), so no lane waits on another's long row
+    const int lane = threadIdx.x & 31;
+    const int nrow = row_hi >= row_lo ? row_hi - row_lo + 1 : 0;
+    const int maxrow = __reduce_max_sync(0xffffffffu, nrow);
+    for (int j = 0; j < maxrow; ++j) {
+      int q0 = 0, cnt = 0;
+      if (j < nrow) {
+        const int cy = row_lo + j;
+        int xmin, xmax;
+        row_span(cy, xmin, xmax);
+        if (xmin <= xmax) {
+          q0 = cstart[cy * cols + xmin];
+          cnt = cstart[cy * cols + xmax + 1] - q0;
+        }
+      }
+      int incl = cnt;
+#pragma unroll
+      for (int o = 1; o < 32; o <<= 1) {
+        const int t_ = __shfl_up_sync(0xffffffffu, incl, o);
+        if (lane >= o) incl += t_;
+      }
+      const int excl = incl - cnt;
+      const int total = __shfl_sync(0xffffffffu, incl, 31);
+      for (int k0 = 0; k0 < total; k0 += 32) {
+        const int k = k0 + lane;
+        int r = 0;
+#pragma unroll
+        for (int step = 16; step > 0; step >>= 1) {
+          const int e = __shfl_sync(0xffffffffu, excl, r + step);
+          if (e <= k) r += step;
+        }
+        const int qr = __shfl_sync(0xffffffffu, q0, r);
+        const int er = __shfl_sync(0xffffffffu, excl, r);
+        const int ot = __shfl_sync(0xffffffffu, t, r);
+        const int opidx = __shfl_sync(0xffffffffu, pidx, r);
+        double Lp[K][2], LU[K][2], Cp[K][2];
+        const double* Cb[K];
+#pragma unroll
+        for (int i = 0; i < K; ++i) {
+          Lp[i][0] = __shfl_sync(0xffffffffu, lp[i][0], r);
+          Lp[i][1] = __shfl_sync(0xffffffffu, lp[i][1], r);
+          LU[i][0] = __shfl_sync(0xffffffffu, lU[i][0], r);
+          LU[i][1] = __shfl_sync(0xffffffffu, lU[i][1], r);
+          Cp[i][0] = __shfl_sync(0xffffffffu, cpt[i][0], r);
+          Cp[i][1] = __shfl_sync(0xffffffffu, cpt[i][1], r);
+          Cb[i] = reinterpret_cast<const double*>(__shfl_sync(
+              0xffffffffu, reinterpret_cast<unsigned long long>(cbp[i]), r));
+        }
+        if (k >= total) continue;
+        const int q = qr + (k - er);
+        const double2 xy = v.cxy[ot][q];
+        bool ok = true;
+        // IDMap::visitPointsInRowSpans precise test
+#pragma unroll
+        for (int i = 0; i < K; ++i) {
+          const double dx = xy.x - Lp[i][0], dy = xy.y - Lp[i][1];
+          const double z = dy * LU[i][0] - dx * LU[i][1];
+          ok = ok && !(z * z > tol2);
+          if (v.near_band > 0.0) {
+            const double m = fabs(z) - v.tol2d;
+            if (fabs(m) < v.near_band)
+              near_append(v, 0, K, ot, v.cell_items[ot][q], in[opidx].cams[i], in[opidx].ids[i], m);
+          }
+        }
+        if (!ok) continue;
+        // checkBackProjection (StereoMatch.cpp:1206-1227)
+#pragma unroll
+        for (int i = 0; i < K; ++i) {
+          if (!ok) break;
+          const double2 a = reinterpret_cast<const double2*>(Cb[i])[2 * q];
+          const double2 b = reinterpret_cast<const double2*>(Cb[i])[2 * q + 1];
+          const double d0 = Cp[i][0] - a.x, d1 = Cp[i][1] - a.y;
+          const double z = d1 * b.x - d0 * b.y;
+          ok = !(z * z > tol2);
+          if (v.near_band > 0.0) {
+            const double m = fabs(z) - v.tol2d;
+            if (fabs(m) < v.near_band)
+              near_append(v, 1, K, ot, v.cell_items[ot][q], in[opidx].cams[i], in[opidx].ids[i], m);
+          }
+        }
+        if (!ok) continue;
         const int slot = append_slot(pair_count);
-        if (slot < pair_cap) pairs[slot] = Pair{pidx, citems[q]};
+        if (slot < pair_cap) pairs[slot] = Pair{opidx, v.cell_items[ot][q]};
       }
     }
   }
