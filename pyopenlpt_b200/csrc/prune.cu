@@ -116,6 +116,22 @@ __global__ void id_keys_kernel(const int* ids, int M, int n, int bits, uint64_t*
   val[j] = j;
 }
 
+// Word w of the candidates' id keys, for a lexicographic sort in several 64-bit
+// passes: the ids of cameras [w * per, (w + 1) * per) of candidate perm[i] (i when perm
+// is null), packed most significant first; val[i] = the candidate.
+__global__ void word_keys_kernel(const int* ids, int M, int n, int bits, int per, int w,
+                                 const int* perm, uint64_t* key, int* val) {
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= M) return;
+  const int j = perm ? perm[i] : i;
+  const int c1 = min(n, (w + 1) * per);
+  uint64_t k = 0;
+  for (int c = w * per; c < c1; ++c)
+    k = (k << bits) | (uint64_t)(uint32_t)(ids[(int64_t)j * n + c] + 1);
+  key[i] = k;
+  val[i] = j;
+}
+
 __global__ void gather_cand_kernel(const int* perm, int M, int n, const int* ids, const double* e,
                                    const double* X, int* ids_s, double* e_s, double* X_s) {
   const int i = blockIdx.x * blockDim.x + threadIdx.x;
@@ -563,21 +579,39 @@ void radix_sort_device(DevBuf& key, DevBuf& val, DevBuf& key2, DevBuf& val2, Dev
   OLPT_CUDA(cudaGetLastError());
 }
 
-// Sort the device candidates (ids, e, X) by ids into the `_s` buffers; false when
-// the packed key does not fit in 64 bits.
+// Sort the device candidates (ids, e, X) by ids into the `_s` buffers.  The ids of all
+// cameras form one lexicographic key; when it does not fit in 64 bits it is split into
+// words sorted least significant first, each pass stable, so the order is the same.
 bool sort_candidates_device(PruneWork& W, const int* ids, const double* e, const double* X, int M,
                             int n, int max_id, cudaStream_t s) {
   const int bits = bit_width((uint64_t)(max_id + 1));
-  if (bits * n > 64) return false;
+  if (bits > 32) return false;
   W.key.ensure((size_t)(M + 1) * sizeof(uint64_t), s);
   W.val.ensure((size_t)(M + 1) * sizeof(int), s);
+  W.key2.ensure((size_t)(M + 1) * sizeof(uint64_t), s);
+  W.val2.ensure((size_t)(M + 1) * sizeof(int), s);
   W.ids_s.ensure((size_t)(M + 1) * n * sizeof(int), s);
   W.e_s.ensure((size_t)(M + 1) * sizeof(double), s);
   W.X_s.ensure((size_t)(M + 1) * 3 * sizeof(double), s);
   if (M == 0) return true;
-  id_keys_kernel<<<OLPT_G(nblk(M)), 256, 0, s>>>(ids, M, n, bits, W.key.as<uint64_t>(),
-                                                W.val.as<int>());
-  radix_sort_device(W.key, W.val, W.key2, W.val2, W.hist, W.scan_tmp, M, bits * n, s);
+  if (bits * n <= 64) {
+    id_keys_kernel<<<OLPT_G(nblk(M)), 256, 0, s>>>(ids, M, n, bits, W.key.as<uint64_t>(),
+                                                  W.val.as<int>());
+    radix_sort_device(W.key, W.val, W.key2, W.val2, W.hist, W.scan_tmp, M, bits * n, s);
+  } else {
+    const int per = 64 / bits;
+    const int words = (n + per - 1) / per;
+    for (int w = words - 1; w >= 0; --w) {
+      const bool first = w == words - 1;
+      word_keys_kernel<<<OLPT_G(nblk(M)), 256, 0, s>>>(
+          ids, M, n, bits, per, w, first ? nullptr : W.val.as<int>(), W.key2.as<uint64_t>(),
+          W.val2.as<int>());
+      std::swap(W.key, W.key2);
+      std::swap(W.val, W.val2);
+      const int in_word = std::min(n, (w + 1) * per) - w * per;
+      radix_sort_device(W.key, W.val, W.key2, W.val2, W.hist, W.scan_tmp, M, bits * in_word, s);
+    }
+  }
   gather_cand_kernel<<<OLPT_G(nblk(M)), 256, 0, s>>>(W.val.as<int>(), M, n, ids, e, X,
                                                     W.ids_s.as<int>(), W.e_s.as<double>(),
                                                     W.X_s.as<double>());

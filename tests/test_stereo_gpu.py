@@ -39,14 +39,26 @@ def _run(kind, dets=None, tol_2d=None, active=None):
     return (ids, e, x, mids, mx), want
 
 
-@pytest.mark.parametrize("kind", ["small", "cfg1", "u16"])
+@pytest.mark.parametrize("kind", ["small", "cfg1", "u16", "poly"])
 def test_candidate_set_and_matches_bit_exact(kind):
+    """Also 6 polynomial cameras, whose candidate id keys (6 x 12 bits) need the
+    two-word device sort."""
     (ids, e, x, mids, mx), want = _run(kind)
     assert len(ids) == len(want["cand"]), (len(ids), len(want["cand"]))
     assert np.array_equal(ids, want["cand"])
-    assert np.array_equal(e, want["e_check"])
     assert np.array_equal(mids, want["sel"])
-    assert np.array_equal(mx, want["xyz"])
+    if kind == "poly":
+        # the reference's polynomial lines of sight start their Newton solve at rand()
+        # draws, so e_check and positions agree to rounding, not bit for bit; e_check
+        # (an RMS distance from a difference of squares) to 1e-9 mm absolute
+        print(f"poly: {len(ids)} candidates, {len(mids)} matches; max |de| "
+              f"{np.max(np.abs(e - want['e_check'])):.3g}, max |dxyz| "
+              f"{np.max(np.abs(mx - want['xyz'])):.3g} mm")
+        assert np.max(np.abs(e - want["e_check"])) <= 1e-9
+        assert np.max(np.abs(mx - want["xyz"])) <= 1e-9
+    else:
+        assert np.array_equal(e, want["e_check"])
+        assert np.array_equal(mx, want["xyz"])
 
 
 def test_wider_tolerance_and_camera_subset():
