@@ -355,6 +355,32 @@ olpt_status_t olpt_stb_set_tracks(olpt_ctx* ctx, int which, const int32_t* track
  * reference's CSV format. */
 olpt_status_t olpt_stb_save_tracks(olpt_ctx* ctx, int which, const char* path);
 olpt_status_t olpt_stb_load_tracks(olpt_ctx* ctx, int which, const char* path);
+/* OTF::estimateUniformOTFFromImage (src/srcSTB/OTF.cpp:17-144) for one camera, on
+ * the device: the context's planes are that camera's images (one plane per image, with
+ * one camera description per plane for the sizes); tracer detections above
+ * min_obj_int, at most max_per_image of them per image (the reference: 1000, chosen by
+ * std::shuffle with std::default_random_engine(123)), the window of radius
+ * radius_obj_px around each, and the reference's a = min(mean + 2 std, max) of the
+ * centre pixels and least squares for b, c.  abc = (a, b, c), uniform over the grid
+ * with alpha = 0; n_samples = window pixels used, 0 when an image has no detection
+ * (the reference then leaves the OTF unchanged). */
+olpt_status_t olpt_otf_estimate(olpt_ctx* ctx, double min_obj_int, double radius_obj_px,
+                                int max_per_image, double abc[3], int64_t* n_samples);
+/* Track files (olpt_stb_save_tracks and the per-frame files of olpt_stb_process_frame
+ * under output_path, STB::saveTracksAll, src/srcSTB/STB.cpp:926-965) are formatted on
+ * the device and written by a writer thread of the context.  enable = 0 (default):
+ * each call returns after its files are written.  enable = 1: the calls return once
+ * the rows are formatted and the files are written while later frames run, in call
+ * order; olpt_track_files_flush waits for them and reports the first write error (a
+ * later save reports it too), olpt_stb_load_tracks and olpt_ctx_destroy wait for them
+ * first.  The numbers are those of the reference's std::fixed, precision 6 output
+ * ("%.6f": the exact binary value rounded to six decimals, ties to even). */
+olpt_status_t olpt_track_files_async(olpt_ctx* ctx, int enable);
+olpt_status_t olpt_track_files_flush(olpt_ctx* ctx);
+/* The device formatter on n host doubles: "%.6f" of each, one per line, into out
+ * (capacity bytes; out = NULL: length only).  |v| >= 2^63 gives OLPT_ERR_UNSUPPORTED. */
+olpt_status_t olpt_format_fixed6(olpt_ctx* ctx, const double* values, int64_t n, char* out,
+                                 int64_t capacity, int64_t* length);
 
 /* ------------------------------------------------------------------ learned proposal */
 /* No reference counterpart: a small MLP that reads, for each candidate after stereo

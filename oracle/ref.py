@@ -207,6 +207,16 @@ class RefOracle:
         r = self._take(h, [f"img{c}" for c in range(self.n_cam)])
         return [r[f"img{c}"].reshape(d[c].shape) for c in range(self.n_cam)]
 
+    def otf_estimate(self, cam: int, imgs):
+        """OTF::estimateUniformOTFFromImage of camera `cam` on its images: (a, b, c, alpha)
+        of the estimate, or None when the reference skipped it."""
+        d, p, H, W = self._imgs(imgs)
+        out = np.zeros(4)
+        rc = self.lib.oref_otf_estimate(C.c_void_p(self.cfg), cam, len(d), p, H, W, _as_dp(out))
+        if rc < 0:
+            raise RuntimeError(self.lib.oref_last_error().decode())
+        return None if rc == 1 else out
+
     def ipr(self, imgs):
         d, p, H, W = self._imgs(imgs)
         h = self.lib.oref_ipr(C.c_void_p(self.cams), C.c_void_p(self.cfg), self.n_cam, p, H, W)

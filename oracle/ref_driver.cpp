@@ -452,6 +452,30 @@ void* oref_ipr(void* cams_h, void* cfg_h, int n_cam, const double* const* imgs, 
 }  // extern "C"
 
 extern "C" {
+// OTF::estimateUniformOTFFromImage (OTF.cpp:17-144) of camera `cam` on n_img in-memory
+// images of that camera; out: a, b, c, alpha of grid node 0.  Returns 1 when the
+// reference skipped the estimation (an image without detections), -1 on a throw.
+int oref_otf_estimate(void* cfg_h, int cam, int n_img, const double* const* imgs, const int* H,
+                      const int* W, double* out4) {
+  auto& cfg = *static_cast<TracerConfig*>(cfg_h);
+  try {
+    auto images = make_images(n_img, imgs, H, W);
+    const double before = cfg._otf._param.a(cam, 0);
+    cfg._otf._param.a(cam, 0) = std::nan("");
+    cfg._otf.estimateUniformOTFFromImage(cam, cfg, images);
+    const bool skipped = std::isnan(cfg._otf._param.a(cam, 0));
+    if (skipped) cfg._otf._param.a(cam, 0) = before;
+    out4[0] = cfg._otf._param.a(cam, 0);
+    out4[1] = cfg._otf._param.b(cam, 0);
+    out4[2] = cfg._otf._param.c(cam, 0);
+    out4[3] = cfg._otf._param.alpha(cam, 0);
+    return skipped ? 1 : 0;
+  } catch (std::exception const& e) {
+    g_last_error = e.what();
+    return -1;
+  }
+}
+
 // OTF::getOTFParam (OTF.cpp:273-338) of the config's OTF for n points.
 int oref_otf_param(void* cfg_h, int cam, long long n, const double* xyz, double* out5) {
   auto& cfg = *static_cast<TracerConfig*>(cfg_h);

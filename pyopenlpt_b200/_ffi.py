@@ -266,6 +266,15 @@ class Context:
         self._check(self.L.olpt_find_peaks(self.h, C.c_double(min_int), _p(counts, _i64p)))
         return counts
 
+    def otf_estimate(self, min_int: float, radius_obj: float, max_per_image: int = 1000):
+        """olpt_otf_estimate on the context's planes: (a, b, c), or None when an image
+        has no detection; and the number of window samples used."""
+        abc = np.zeros(3)
+        n = C.c_int64()
+        self._check(self.L.olpt_otf_estimate(self.h, C.c_double(min_int), C.c_double(radius_obj),
+                                             int(max_per_image), _p(abc), C.byref(n)))
+        return (abc if n.value > 0 else None), n.value
+
     def get_peaks(self, cam: int, n: int):
         xy = np.empty((n, 2))
         rc = np.empty((n, 2), dtype=np.int32)
@@ -435,6 +444,24 @@ class Context:
 
     def stb_load_tracks(self, which: int, path: str):
         self._check(self.L.olpt_stb_load_tracks(self.h, which, str(path).encode()))
+
+    def track_files_async(self, enable: bool = True):
+        """Track files written by the context's writer thread while later calls run."""
+        self._check(self.L.olpt_track_files_async(self.h, int(bool(enable))))
+
+    def flush_track_files(self):
+        self._check(self.L.olpt_track_files_flush(self.h))
+
+    def format_fixed6(self, values) -> str:
+        """The device formatter: '%.6f' of each value, one per line."""
+        v = np.ascontiguousarray(values, dtype=np.float64).ravel()
+        n = C.c_int64()
+        self._check(self.L.olpt_format_fixed6(self.h, _p(v), C.c_int64(v.size), None,
+                                              C.c_int64(0), C.byref(n)))
+        buf = C.create_string_buffer(max(n.value, 1))
+        self._check(self.L.olpt_format_fixed6(self.h, _p(v), C.c_int64(v.size), buf,
+                                              C.c_int64(n.value), C.byref(n)))
+        return buf.raw[:n.value].decode()
 
     # ---------------------------------------------------------------- profiling
     def stream(self) -> int:

@@ -603,116 +603,25 @@ bool BasicSetting::readConfig(const std::string& config_path) {
 
 namespace {
 // myMATH::inverse with the Gauss method for a 2 x 2 matrix (inc/libMath/myMATH.h:182-255).
-void gauss_inverse2(const double A[4], double inv[4]) {
-  double u[4] = {A[0], A[1], A[2], A[3]};
-  int idx[2] = {0, 1};
-  const double maxrow[2] = {std::max(u[0], u[1]), std::max(u[2], u[3])};
-  double mp = 0;
-  int t = 0;
-  for (int x = 0; x < 2; ++x) {
-    const double piv = std::fabs(u[2 * idx[x]] / maxrow[idx[x]]);
-    if (piv > mp) {
-      mp = piv;
-      t = x;
-    }
-  }
-  std::swap(idx[t], idx[0]);
-  const double m = u[2 * idx[1]] / u[2 * idx[0]];
-  u[2 * idx[1]] = m;
-  u[2 * idx[1] + 1] -= m * u[2 * idx[0] + 1];
-  double bm[4] = {1, 0, 0, 1};
-  for (int it = 0; it < 2; ++it) {
-    bm[2 * idx[1] + it] -= u[2 * idx[1]] * bm[2 * idx[0] + it];
-    inv[2 + it] = bm[2 * idx[1] + it] / u[2 * idx[1] + 1];
-    double z = bm[2 * idx[0] + it];
-    z -= u[2 * idx[0] + 1] * inv[2 + it];
-    inv[it] = z / u[2 * idx[0]];
-  }
-}
-
-// OTF::estimateUniformOTFFromImage (src/srcSTB/OTF.cpp:17-144): tracer detections on
-// the device, at most 1000 per image (std::shuffle with default_random_engine(123)),
-// then the reference's least squares for b, c and the peak statistics for a.
+// OTF::estimateUniformOTFFromImage (src/srcSTB/OTF.cpp:17-144) through
+// olpt_otf_estimate: the camera's images as the context's planes, detections, the
+// reference's selection of at most 1000 per image and its least squares on the device.
 void estimate_otf(OTF& otf, int cam_id, const TracerConfig& cfg, const std::vector<Image>& imgs) {
   olpt_ctx* ctx = default_context();
-  std::vector<std::vector<Pt2D>> det_all;
-  for (const Image& im : imgs) {
-    olpt_camera_desc d = dummy_camera(im.getDimRow(), im.getDimCol());
-    check(ctx, olpt_cameras_upload(ctx, &d, 1));
-    upload_images(ctx, {im});
-    int64_t cnt = 0;
-    check(ctx, olpt_find_peaks(ctx, (double)cfg._min_obj_int, &cnt));
-    std::vector<double> xy(2 * (size_t)cnt + 2);
-    check(ctx, olpt_get_peaks(ctx, 0, xy.data(), nullptr, cnt));
-    std::vector<Pt2D> det(cnt);
-    for (int64_t i = 0; i < cnt; ++i) det[i] = Pt2D(xy[2 * i], xy[2 * i + 1]);
-    if (det.size() > 1000) {
-      std::shuffle(det.begin(), det.end(), std::default_random_engine(123));
-      det.erase(det.begin() + 1000, det.end());
-    } else if (det.empty()) {
-      std::cerr << "[WARN] OTF calibration skipped: no tracer found | ctx: cam_id=" << cam_id
-                << std::endl;
-      return;
-    }
-    det_all.push_back(std::move(det));
+  std::vector<olpt_camera_desc> d;
+  for (const Image& im : imgs) d.push_back(dummy_camera(im.getDimRow(), im.getDimCol()));
+  check(ctx, olpt_cameras_upload(ctx, d.data(), (int)d.size()));
+  upload_images(ctx, imgs);
+  double abc[3];
+  int64_t n = 0;
+  check(ctx, olpt_otf_estimate(ctx, (double)cfg._min_obj_int, cfg._radius_obj, 1000, abc, &n));
+  if (n == 0) {
+    std::cerr << "[WARN] OTF calibration skipped: no tracer found | ctx: cam_id=" << cam_id
+              << std::endl;
+    return;
   }
-  std::vector<double> I_list, a_list, cx, cy;
-  const double r_pt = cfg._radius_obj;
-  for (size_t i = 0; i < imgs.size(); ++i) {
-    const Image& im = imgs[i];
-    const int n_row = im.getDimRow(), n_col = im.getDimCol();
-    for (const Pt2D& p : det_all[i]) {
-      const double xc = p[0], yc = p[1];
-      const int yc0 = std::clamp<int>(int(std::round(yc)), 0, n_row - 1);
-      const int xc0 = std::clamp<int>(int(std::round(xc)), 0, n_col - 1);
-      a_list.push_back(im(yc0, xc0));
-      const int row_min = std::max(0, int(std::floor(yc - r_pt)));
-      const int row_max = std::min(n_row, int(std::ceil(yc + r_pt + 1)));
-      const int col_min = std::max(0, int(std::floor(xc - r_pt)));
-      const int col_max = std::min(n_col, int(std::ceil(xc + r_pt + 1)));
-      for (int row = row_min; row < row_max; ++row)
-        for (int col = col_min; col < col_max; ++col) {
-          I_list.push_back(im(row, col));
-          cx.push_back(std::pow(col - xc, 2));
-          cy.push_back(std::pow(row - yc, 2));
-        }
-    }
-  }
-  const double a_max = *std::max_element(a_list.begin(), a_list.end());
-  const int n_a = (int)a_list.size();
-  double a_mean = 0, a_std = 0;
-  for (int i = 0; i < n_a; ++i) a_mean += a_list[i];
-  a_mean /= n_a;
-  for (int i = 0; i < n_a; ++i) a_std += std::pow(a_list[i] - a_mean, 2);
-  a_std = std::sqrt(a_std / n_a);
-  const double a = std::min(a_mean + 2 * a_std, a_max);
-  // inverse(C^T C) C^T L, Matrix products accumulated from 0 in index order
-  const size_t n = I_list.size();
-  std::vector<double> L(n);
-  for (size_t i = 0; i < n; ++i) {
-    const double logI = I_list[i] < 1e-4 ? std::log(1e-4) : std::log(I_list[i]);
-    L[i] = -logI + std::log(a);
-  }
-  double A[4];
-  for (int r = 0; r < 2; ++r)
-    for (int c = 0; c < 2; ++c) {
-      double s = 0;
-      for (size_t i = 0; i < n; ++i) s += (r ? cy[i] : cx[i]) * (c ? cy[i] : cx[i]);
-      A[2 * r + c] = s;
-    }
-  double inv[4];
-  gauss_inverse2(A, inv);
-  double coef[2];
-  for (int r = 0; r < 2; ++r) {
-    double s = 0;
-    for (size_t i = 0; i < n; ++i) {
-      double k = 0;
-      k += inv[2 * r] * cx[i];
-      k += inv[2 * r + 1] * cy[i];
-      s += k * L[i];
-    }
-    coef[r] = s;
-  }
+  const double a = abc[0];
+  const double coef[2] = {abc[1], abc[2]};
   OTFParam& p = otf._param;
   for (int g = 0; g < p.n_grid; ++g) {
     p.a[(size_t)cam_id * p.n_grid + g] = a;

@@ -204,6 +204,8 @@ void olpt_ctx_destroy(olpt_ctx* ctx) {
   for (int c = 0; c < OLPT_MAX_CAM; ++c) ctx->stb.frame_img[c].buf.release(ctx->stream);
   ctx->prune.release(ctx->stream);
   ctx->mlp.release(ctx->stream);
+  ctx->tio.writer.stop();  // writes what is still queued
+  ctx->tio.release(ctx->stream);
   ctx->prof.release();
   cudaStreamSynchronize(ctx->stream);
   if (ctx->own_stream) cudaStreamDestroy(ctx->stream);
@@ -1082,7 +1084,49 @@ olpt_status_t olpt_stb_save_tracks(olpt_ctx* ctx, int which, const char* path) {
 olpt_status_t olpt_stb_load_tracks(olpt_ctx* ctx, int which, const char* path) {
   return guard(ctx, [&] {
     OLPT_REQUIRE(path, OLPT_ERR_INVALID_ARG, "null path");
+    flush_files(ctx);  // the file may still be queued for writing
     stb_load_tracks(ctx, which, path);
+  });
+}
+
+olpt_status_t olpt_otf_estimate(olpt_ctx* ctx, double min_obj_int, double radius_obj_px,
+                                int max_per_image, double abc[3], int64_t* n_samples) {
+  return guard(ctx, [&] {
+    OLPT_REQUIRE(abc && n_samples && max_per_image > 0 && radius_obj_px >= 0,
+                 OLPT_ERR_INVALID_ARG, "bad arguments");
+    *n_samples = 0;
+    otf_estimate_device(ctx, min_obj_int, radius_obj_px, max_per_image, abc, n_samples);
+  });
+}
+
+olpt_status_t olpt_track_files_async(olpt_ctx* ctx, int enable) {
+  return guard(ctx, [&] {
+    if (!enable) flush_files(ctx);
+    ctx->tio.async = enable != 0;
+  });
+}
+
+olpt_status_t olpt_track_files_flush(olpt_ctx* ctx) {
+  return guard(ctx, [&] { flush_files(ctx); });
+}
+
+olpt_status_t olpt_format_fixed6(olpt_ctx* ctx, const double* values, int64_t n, char* out,
+                                 int64_t capacity, int64_t* length) {
+  return guard(ctx, [&] {
+    OLPT_REQUIRE(n >= 0 && (n == 0 || values) && length, OLPT_ERR_INVALID_ARG, "bad arguments");
+    std::string o;
+    TrackIoWork& W = ctx->tio;
+    for (int64_t at = 0; at < n; at += kMaxRowsPerPass) {
+      const int64_t m = std::min<int64_t>(kMaxRowsPerPass, n - at);
+      W.xyz.ensure((size_t)m * sizeof(double) + 16, ctx->stream);
+      OLPT_CUDA(cudaMemcpyAsync(W.xyz.p, values + at, (size_t)m * sizeof(double),
+                                cudaMemcpyHostToDevice, ctx->stream));
+      format_rows_device(ctx, nullptr, 0, W.xyz.as<double>(), 1, nullptr, 0, m, o);
+    }
+    *length = (int64_t)o.size();
+    OLPT_REQUIRE(!out || capacity >= (int64_t)o.size(), OLPT_ERR_INVALID_ARG,
+                 "output capacity too small");
+    if (out) std::memcpy(out, o.data(), o.size());
   });
 }
 

@@ -16,6 +16,7 @@
 #include "olpt_shake.h"
 #include "olpt_stb.h"
 #include "olpt_stereo.h"
+#include "olpt_trackio.h"
 
 namespace olpt {
 
@@ -278,6 +279,30 @@ OtfView otf_view(olpt_ctx* ctx);
 void shake_device(olpt_ctx* ctx, const ShakeParams& sp);
 void residual_device(olpt_ctx* ctx, const ShakeParams& sp, bool use_flags, bool make_current);
 
+// Track files (trackio.cu): device buffers of the row formatter and the writer thread.
+// async: the frame loop's track files are written while later frames run (flush_files
+// waits for them); otherwise every save returns after its file is written.
+constexpr int64_t kMaxRowsPerPass = 1 << 20;
+struct TrackIoWork {
+  DevBuf ints, xyz, uv, len, off, bad, bytes, tmp;
+  bool async = false;
+  FileWriter writer;
+  void release(cudaStream_t s) {
+    for (DevBuf* x : {&ints, &xyz, &uv, &len, &off, &bad, &bytes, &tmp}) x->release(s);
+  }
+};
+// rows of n_int ints, then n1 + n2 doubles from two arrays (device), "%.6f" numbers,
+// comma separated, one per line; n <= kMaxRowsPerPass; appended to out
+void format_rows_device(olpt_ctx* ctx, const int* ints, int n_int, const double* d1, int n1,
+                        const double* d2, int n2, int64_t n, std::string& out);
+// bytes -> file on the writer thread (waits for it unless the context writes async)
+void write_file(olpt_ctx* ctx, const std::string& file, std::string&& bytes);
+// waits for every posted file; throws the first write error
+void flush_files(olpt_ctx* ctx);
+// OTF estimation from the context's planes (otf_est.cu); false: an image without detections
+bool otf_estimate_device(olpt_ctx* ctx, double min_int, double r_pt, int max_det, double abc[3],
+                         int64_t* n_samples);
+
 // Device workspace of the STB frame loop (grown on demand, reused across frames).
 struct StbWork {
   DevBuf a, b, c, d, ia, link, flag, field, field2, kern, k1, k2;
@@ -421,6 +446,7 @@ struct olpt_ctx {
 
   // Shake-the-Box frame loop
   olpt::StbState stb;
+  olpt::TrackIoWork tio;
 
   // learned proposal
   olpt::MlpWork mlp;

@@ -733,70 +733,49 @@ std::vector<double> run_ipr_host(olpt_ctx* ctx) {
   return download(ctx->ipr.out_xyz.as<double>(), (size_t)ctx->ipr.n_out * 3, ctx->stream);
 }
 
-// "%.6f" equals std::ostream fixed with precision 6 (libstdc++ formats through
-// the C library).
-void put_f6(std::string& o, double v) {
-  char b[64];
-  const int n = std::snprintf(b, sizeof b, "%.6f", v);
-  o.append(b, n);
-}
-
 // STB::saveTracks (STB.cpp:967-1004) + Track::saveTrack + Tracer3D::saveObject3D
 // (ObjectInfo.cpp:76-94).  The 2D columns are each point's projection on every
 // camera: the reference's objects always hold projectObject2D of their centre
-// (end of Shake::shakeOneObject, buildTrackFromPredField, loadTrack).
+// (end of Shake::shakeOneObject, buildTrackFromPredField, loadTrack).  The points go
+// to the device in passes of at most kMaxRowsPerPass rows, are projected and
+// formatted there (trackio.cu), and the file is written by the context's writer.
 void save_tracks_file(olpt_ctx* ctx, const TrackList& tracks, const std::string& file) {
-  int64_t n = 0;
-  for (const TrackH& t : tracks) n += (int64_t)t.size();
-  std::vector<double> xyz;
-  xyz.reserve(3 * n);
-  for (const TrackH& t : tracks) xyz.insert(xyz.end(), t.xyz.begin(), t.xyz.end());
   const int C = ctx->n_cam;
-  std::vector<double> uv;
-  if (n > 0) {
-    cudaStream_t s = ctx->stream;
-    StbWork& W = ctx->stb.w;
-    const double* d_x = upload(W.a, xyz, s);
-    W.b.ensure((size_t)(n * C * 2 + 1) * sizeof(double), s);
-    project_all_kernel<<<OLPT_G(nblk(n)), 256, 0, s>>>(ctx->cams_d.as<CamDev>(), C, d_x, n,
-                                                      W.b.as<double>());
-    OLPT_CUDA(cudaGetLastError());
-    uv = download(W.b.as<double>(), (size_t)n * C * 2, s);
-  }
-  std::FILE* f = std::fopen(file.c_str(), "w");
-  OLPT_REQUIRE(f, OLPT_ERR_INVALID_ARG, "Cannot open file: " + file);
   std::string o = "TrackID,FrameID,WorldX,WorldY,WorldZ";
   for (int i = 0; i < C; ++i)
     o += ",cam" + std::to_string(i) + "_x(col),cam" + std::to_string(i) + "_y(row)";
   o += "\n";
-  int64_t pt = 0;
-  for (size_t i = 0; i < tracks.size(); ++i) {
-    const TrackH& tr = tracks[i];
-    for (size_t k = 0; k < tr.size(); ++k, ++pt) {
-      o += std::to_string(i);
-      o += ',';
-      o += std::to_string(tr.t[k]);
-      o += ',';
-      put_f6(o, tr.xyz[3 * k]);
-      o += ',';
-      put_f6(o, tr.xyz[3 * k + 1]);
-      o += ',';
-      put_f6(o, tr.xyz[3 * k + 2]);
-      for (int c = 0; c < C; ++c) {
-        o += ',';
-        put_f6(o, uv[(pt * C + c) * 2]);
-        o += ',';
-        put_f6(o, uv[(pt * C + c) * 2 + 1]);
+  cudaStream_t s = ctx->stream;
+  TrackIoWork& W = ctx->tio;
+  std::vector<int> ids;
+  std::vector<double> xyz;
+  size_t tr_i = 0, pt_k = 0;  // next point to pack: track tr_i, its point pt_k
+  for (;;) {
+    ids.clear();
+    xyz.clear();
+    while (tr_i < tracks.size() && (int64_t)ids.size() < 2 * kMaxRowsPerPass) {
+      const TrackH& tr = tracks[tr_i];
+      if (pt_k >= tr.size()) {
+        ++tr_i;
+        pt_k = 0;
+        continue;
       }
-      o += '\n';
+      ids.push_back((int)tr_i);  // static_cast<int>(i) of the list index
+      ids.push_back(tr.t[pt_k]);
+      xyz.insert(xyz.end(), tr.xyz.begin() + 3 * pt_k, tr.xyz.begin() + 3 * pt_k + 3);
+      ++pt_k;
     }
-    if (o.size() > (1u << 20)) {
-      std::fwrite(o.data(), 1, o.size(), f);
-      o.clear();
-    }
+    const int64_t n = (int64_t)ids.size() / 2;
+    if (n == 0) break;
+    const int* d_ids = upload(W.ints, ids, s);
+    const double* d_x = upload(W.xyz, xyz, s);
+    W.uv.ensure((size_t)(n * C * 2 + 1) * sizeof(double), s);
+    project_all_kernel<<<OLPT_G(nblk(n)), 256, 0, s>>>(ctx->cams_d.as<CamDev>(), C, d_x, n,
+                                                      W.uv.as<double>());
+    OLPT_CUDA(cudaGetLastError());
+    format_rows_device(ctx, d_ids, 2, d_x, 3, W.uv.as<double>(), 2 * C, n, o);
   }
-  std::fwrite(o.data(), 1, o.size(), f);
-  std::fclose(f);
+  write_file(ctx, file, std::move(o));
 }
 
 // STB::saveTracksAll (STB.cpp:926-965).
@@ -805,7 +784,12 @@ void save_tracks_all(olpt_ctx* ctx, const std::string& folder, int frame) {
   StbState& S = ctx->stb;
   const fs::path dir(folder);
   const std::string s = std::to_string(frame);
-  auto remove_with_prefix = [&](const std::string& prefix) {
+  // the reference's saveTracks fails on a folder it cannot write into; here before
+  // anything is queued
+  OLPT_REQUIRE(fs::is_directory(dir), OLPT_ERR_INVALID_ARG,
+               "Cannot open file: " + (dir / ("LongTrackActive_" + s + ".csv")).string());
+  // runs on the writer thread, after the files posted before it
+  auto remove_with_prefix = [dir](const std::string& prefix) {
     if (!fs::exists(dir)) return;
     for (const auto& e : fs::directory_iterator(dir)) {
       if (!e.is_regular_file()) continue;
@@ -817,8 +801,10 @@ void save_tracks_all(olpt_ctx* ctx, const std::string& folder, int frame) {
       }
     }
   };
-  remove_with_prefix("LongTrackActive_");
-  remove_with_prefix("ShortTrackActive_");
+  ctx->tio.writer.post([remove_with_prefix] {
+    remove_with_prefix("LongTrackActive_");
+    remove_with_prefix("ShortTrackActive_");
+  });
   save_tracks_file(ctx, S.long_active, (dir / ("LongTrackActive_" + s + ".csv")).string());
   save_tracks_file(ctx, S.short_active, (dir / ("ShortTrackActive_" + s + ".csv")).string());
   save_tracks_file(ctx, S.exited, (dir / ("ExitTrack_" + s + ".csv")).string());

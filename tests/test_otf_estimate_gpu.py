@@ -1,0 +1,64 @@
+"""OTF estimation on the device (olpt_otf_estimate) against the reference's own
+OTF::estimateUniformOTFFromImage compiled from its sources: equal to the last bit on
+8-bit and 12-bit images with more than the 1000 detections per image the reference
+samples, on float images with non-integer samples, and skipped where the reference
+skips (an image without detections)."""
+import numpy as np
+import pytest
+
+from pyopenlpt_b200 import _ffi
+from tests import _scenes
+
+pytestmark = pytest.mark.gpu
+
+
+def _device(sc, imgs, min_int, r):
+    ctx = _ffi.Context(0)
+    try:
+        descs = []
+        for im in imgs:
+            e = _ffi.camera_desc(sc.cams[0])
+            e.n_row, e.n_col = im.shape
+            descs.append(e)
+        ctx.upload_cameras(descs)
+        ctx.upload_images(imgs)
+        return ctx.otf_estimate(min_int, r)
+    finally:
+        ctx.close()
+
+
+@pytest.mark.parametrize("kind", ["small", "u16", "float"])
+def test_otf_estimate_equals_reference(kind):
+    from oracle.ref import RefOracle
+    sc = _scenes.scene("small" if kind == "float" else kind)
+    s = _scenes.settings("small" if kind == "float" else kind)
+    imgs = [np.ascontiguousarray(im) for im in sc.images]
+    if kind == "float":  # non-integer samples: the C library's log path
+        rng = np.random.default_rng(3)
+        imgs = [im.astype(np.float64) + rng.uniform(0, 1, im.shape) for im in imgs]
+    ref = RefOracle(sc, s, threads=1)
+    try:
+        want = ref.otf_estimate(0, imgs)
+    finally:
+        ref.close()
+    got, n = _device(sc, imgs, s.min_obj_int, s.radius_obj)
+    counts = [int(np.count_nonzero(im > s.min_obj_int)) for im in imgs]
+    print(f"{kind}: reference (a, b, c) = {want[:3]}, device = {got}, {n} samples, "
+          f"pixels above threshold {counts}")
+    assert want is not None and got is not None and n > 0
+    assert np.array_equal(got, want[:3])
+    assert want[3] == 0.0
+
+
+def test_otf_estimate_skips_like_reference():
+    from oracle.ref import RefOracle
+    sc = _scenes.scene("small")
+    s = _scenes.settings("small")
+    imgs = [np.ascontiguousarray(sc.images[0]), np.zeros_like(sc.images[1])]
+    ref = RefOracle(sc, s, threads=1)
+    try:
+        assert ref.otf_estimate(0, imgs) is None
+    finally:
+        ref.close()
+    got, n = _device(sc, imgs, s.min_obj_int, s.radius_obj)
+    assert got is None and n == 0

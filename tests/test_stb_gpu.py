@@ -48,11 +48,12 @@ def _ref_run():
     return out, os.path.join(r._tmp, "out")
 
 
-def _gpu_run(precision, out_dir=None):
+def _gpu_run(precision, out_dir=None, async_files=False):
     from oracle.ref import otf_table
     seq = _seq()
     ipr, stb = _settings(seq)
     ctx = _ffi.Context(0)
+    ctx.track_files_async(async_files)
     ctx.upload_cameras([_ffi.camera_desc_from_pinhole(c) for c in seq.cams])
     ctx.upload_otf(2, 2, 2, seq.volume, otf_table(seq.n_cam, seq.otf_abc))
     ctx.stb_configure(_ffi.stb_params(ipr, stb, seq.volume, 0, N_FRAMES - 1, precision,
@@ -66,6 +67,7 @@ def _gpu_run(precision, out_dir=None):
             tid, fr, xyz = ctx.stb_tracks(w)
             lists[name] = np.column_stack([tid, fr, xyz]).astype(np.float64).reshape(-1, 5)
         out.append(lists)
+    ctx.flush_track_files()
     return ctx, out
 
 
@@ -149,7 +151,8 @@ def _read_csv(path):
 def test_stb_output_files_match_reference():
     _, ref_dir = _ref_run()
     with tempfile.TemporaryDirectory() as d:
-        _gpu_run(1, out_dir=d)
+        # the track files written by the writer thread while later frames run
+        _gpu_run(1, out_dir=d, async_files=True)
         # predictive fields of the initial phase
         pf = sorted(f for f in os.listdir(ref_dir) if f.startswith("PredField_"))
         assert pf and pf == sorted(f for f in os.listdir(d) if f.startswith("PredField_"))
