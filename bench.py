@@ -88,8 +88,23 @@ WORKLOADS["stb_256_u16_6cam_poly_6.5k"] = dict(
                                      volume=(-5.0, 5.0, -5.0, 5.0, -2.5, 2.5), bits=12),
     settings=dict(min_obj_int=300, n_obj2d_process_max=1_000_000),
     stb=dict(pf_nx=11, pf_ny=11, pf_nz=6), converge=6)
+# Many independent sequences on one GPU: 64 seeded sequences (synth.batch_plan:
+# particles log-uniform in [2,000, 80,000], 4-6 pinhole cameras, 512/1024/2048^2 uint8
+# (a = 200, b = c = 0.5, noise 2), 20 frames of Taylor-Green flow with wavelength in
+# [20, 60] mm at <= 3 px/frame); settings in pixels of each rig as above, threshold 30.
+# One step = one convergence-phase frame of every sequence (olpt_stb_process_frame_batch).
+WORKLOADS["stb_batch64_tg_u8"] = dict(
+    kind="batch", n_seq=64, n_frames=20,
+    settings=dict(min_obj_int=30, n_obj2d_process_max=1_000_000),
+    stb=dict(pf_nx=11, pf_ny=11, pf_nz=6))
+# one sequence of the batch's shapes that the CPU path finishes (its reference sample)
+WORKLOADS["stb_tg_512_u8_4cam_2k"] = dict(
+    kind="stb", gen="tg", seq=dict(n_particles=2000, n_cam=4, size=512, wavelength=40.0),
+    settings=dict(min_obj_int=30, n_obj2d_process_max=1_000_000),
+    stb=dict(pf_nx=11, pf_ny=11, pf_nz=6))
 # the reference arm's sample of each workload (a workload the CPU path finishes)
-REFERENCE_SAMPLE = {"stb_2048_u16_6cam_poly_419k": "stb_256_u16_6cam_poly_6.5k"}
+REFERENCE_SAMPLE = {"stb_2048_u16_6cam_poly_419k": "stb_256_u16_6cam_poly_6.5k",
+                    "stb_batch64_tg_u8": "stb_tg_512_u8_4cam_2k"}
 DEFAULT_WORKLOAD = "stb_2048_u16_6cam_poly_419k"
 
 
@@ -110,20 +125,29 @@ def build_scene(name: str, seed: int):
     return sc, ipr_settings(name, sc.n_cam)
 
 
+def px_settings(seq, w):
+    """IPR / STB knobs of a workload whose lengths are given in pixels of the rig
+    (POLY_PX), every camera in the build."""
+    mm_px = 1.0 / max(synth.px_per_mm(c, np.zeros(3)) for c in seq.cams)
+    s = synth.IPRSettings(**w["settings"])
+    s.match_cam_count = seq.n_cam
+    s.shake_width = POLY_PX["shake_width"] * mm_px
+    s.tol_3d_mm = POLY_PX["tol_3d"] * mm_px
+    st = synth.STBSettings(radius_search_obj=POLY_PX["link"] * mm_px,
+                           radius_search_track=POLY_PX["link"] * mm_px,
+                           pf_r=POLY_PX["pf_r"] * mm_px, **w["stb"])
+    return s, st
+
+
 def build_sequence(name: str, seed: int, n_frames: int, device="cpu", with_images=True):
     w = WORKLOADS[name]
     if w.get("gen") == "poly":
         seq = synth.make_poly_sequence(n_frames=n_frames, seed=seed, device=device,
                                        with_images=with_images, **w["seq"])
-        mm_px = 1.0 / max(synth.px_per_mm(c, np.zeros(3)) for c in seq.cams)
-        s = synth.IPRSettings(**w["settings"])
-        s.match_cam_count = seq.n_cam
-        s.shake_width = POLY_PX["shake_width"] * mm_px
-        s.tol_3d_mm = POLY_PX["tol_3d"] * mm_px
-        st = synth.STBSettings(radius_search_obj=POLY_PX["link"] * mm_px,
-                               radius_search_track=POLY_PX["link"] * mm_px,
-                               pf_r=POLY_PX["pf_r"] * mm_px, **w["stb"])
-        return seq, s, st
+        return (seq, *px_settings(seq, w))
+    if w.get("gen") == "tg":
+        seq = synth.make_tg_sequence(n_frames=n_frames, seed=seed, device=device, **w["seq"])
+        return (seq, *px_settings(seq, w))
     seq = synth.make_sequence(n_frames=n_frames, seed=seed, with_images=with_images, **w["seq"])
     return seq, ipr_settings(name, seq.n_cam), synth.STBSettings(**w["stb"])
 
@@ -276,7 +300,10 @@ def run_reference(args):
     else:
         times, counts, seq, s, st, sample_name = reference_stb(
             args.workload, threads, args.warmup, args.steps, REF_STB_BUDGET_S)
-        if sample_name != args.workload:
+        if kind == "batch":
+            cfg = {"workload": args.workload, "sequences": WORKLOADS[args.workload]["n_seq"],
+                   "reference_sample": workload_config(sample_name, s, seq=seq, st=st)}
+        elif sample_name != args.workload:
             main = build_sequence(args.workload, 1234, 1, with_images=False)
             cfg = workload_config(args.workload, main[1], seq=main[0], st=main[2])
             cfg["reference_sample"] = workload_config(sample_name, s, seq=seq, st=st)
@@ -325,7 +352,11 @@ def workload_config(name, s, sc=None, seq=None, st=None):
                     match_cam_count=s.match_cam_count,
                     detection_cap=s.n_obj2d_process_max,
                     step="one convergence-phase frame")
-        if isinstance(seq, synth.PolySequence):
+        if WORKLOADS[name].get("gen") == "tg":
+            base.update(camera_model="pinhole ring rig", otf="uniform (a, b, c) = "
+                        f"{tuple(float(x) for x in seq.otf_table[:3, 0, 0])}",
+                        flow="Taylor-Green cells (random phase), <= 3 px/frame")
+        elif isinstance(seq, synth.PolySequence):
             base.update(camera_model="cubic polynomial (20 terms), <= 2 px corner distortion",
                         otf=f"{'x'.join(map(str, seq.otf_n))} grid, a in [2400, 3600], "
                             "b, c in [0.3, 0.9]",
@@ -723,6 +754,164 @@ def run_ours_stb(args, o: Ours, pre_lines):
                clk, workload_config(args.workload, s, seq=seq, st=st), cpu, extra)
 
 
+def run_ours_batch(args, o: Ours, pre_lines):
+    """Many independent sequences at once: every sequence's frame t in one
+    olpt_stb_process_frame_batch call (one step).  `value`: frames resident in HBM;
+    `e2e`: a second pass whose steps upload every sequence's frame from pinned host
+    memory and read back its particles.  The same sequences run one at a time on one
+    context each give the batching gain and the per-sequence equality check (track
+    lists identical to the batched run's after the last frame)."""
+    from pyopenlpt_b200 import _ffi
+    torch = o.torch
+    w = WORKLOADS[args.workload]
+    plan = synth.batch_plan(w["n_seq"], seed=2024 + 1000 * o.rank)
+    nf = max(w["n_frames"], N_INIT + args.warmup + args.steps)
+    t0_frame = N_INIT + args.warmup
+    t_gen = time.perf_counter()
+    seqs, sets = [], []
+    for p in plan:
+        seq = synth.make_tg_sequence(n_frames=nf, device=f"cuda:{o.local}", **p)
+        seqs.append(seq)
+        sets.append(px_settings(seq, w))
+    t_gen = time.perf_counter() - t_gen
+    dev = [[torch.from_numpy(np.ascontiguousarray(f)).cuda() for f in q.frames] for q in seqs]
+    host = [[torch.from_numpy(np.ascontiguousarray(f)).pin_memory() for f in q.frames]
+            for q in seqs]
+
+    def make(i):
+        q = seqs[i]
+        s, st = sets[i]
+        ctx = o.context(q)
+        ctx.stb_configure(_ffi.stb_params(s, st, q.volume, 0, nf - 1, o.prec))
+        return ctx
+
+    def put_device(ctx, i, t):
+        q = seqs[i]
+        H, W = q.cams[0].n_row, q.cams[0].n_col
+        d = dev[i][t]
+        ctx.upload_images_device([d[c].data_ptr() for c in range(q.n_cam)], _ffi.OLPT_U8,
+                                 [H] * q.n_cam, [W] * q.n_cam)
+
+    def lists(ctx):
+        return [ctx.stb_tracks(k) for k in range(4)]
+
+    # batched pass, device-resident frames
+    ctxs = [make(i) for i in range(len(seqs))]
+    for t in range(t0_frame):
+        for i, c in enumerate(ctxs):
+            put_device(c, i, t)
+        _ffi.stb_process_frame_batch(ctxs, [t] * len(ctxs))
+    for c in ctxs:
+        c.profile(True)
+    clocks = ClockSampler(o.local)
+    clocks.start()
+    torch.cuda.synchronize()
+    launches0 = _ffi.launch_count()
+    step_ms, parts = [], 0
+    for t in range(t0_frame, t0_frame + args.steps):
+        o.flush.zero_()
+        torch.cuda.synchronize()
+        a = time.perf_counter()
+        for i, c in enumerate(ctxs):
+            put_device(c, i, t)
+        _ffi.stb_process_frame_batch(ctxs, [t] * len(ctxs))
+        torch.cuda.synchronize()
+        step_ms.append(1e3 * (time.perf_counter() - a))
+        parts += sum(c.stb_frame_points(t) for c in ctxs)
+    launches = _ffi.launch_count() - launches0
+    clk = clocks.stop()
+    prof = {}
+    for k in list(PROF_NAMES) + list(PHASE_NAMES):
+        vals = [c.profile_read(k) for c in ctxs]
+        prof[k] = (sum(v[0] for v in vals), sum(v[1] for v in vals), sum(v[2] for v in vals))
+    batched_lists = [lists(c) for c in ctxs]
+    for c in ctxs:
+        c.close()
+
+    # end to end: pinned host frames uploaded through the C ABI, particles read back
+    ctxs = [make(i) for i in range(len(seqs))]
+    for t in range(t0_frame):
+        for i, c in enumerate(ctxs):
+            c.upload_images(list(host[i][t].numpy()))
+        _ffi.stb_process_frame_batch(ctxs, [t] * len(ctxs))
+    e2e_s, e2e_parts, bi, bo = 0.0, 0, 0, 0
+    for t in range(t0_frame, t0_frame + args.steps):
+        o.flush.zero_()
+        torch.cuda.synchronize()
+        a = time.perf_counter()
+        for i, c in enumerate(ctxs):
+            c.upload_images(list(host[i][t].numpy()))
+        _ffi.stb_process_frame_batch(ctxs, [t] * len(ctxs))
+        outs = [c.stb_frame_objects() for c in ctxs]
+        e2e_s += time.perf_counter() - a
+        e2e_parts += sum(c.stb_frame_points(t) for c in ctxs)
+        bo += sum(x.nbytes for x in outs)
+    bi = sum(q.n_cam * q.cams[0].n_row * q.cams[0].n_col for q in seqs)
+    for c in ctxs:
+        c.close()
+
+    # one sequence at a time, same frames: the batching gain and the equality check
+    solo_ms, equal = 0.0, 0
+    mism = []
+    for i in range(len(seqs)):
+        ctx = make(i)
+        stream = torch.cuda.ExternalStream(ctx.stream())
+        for t in range(t0_frame + args.steps):
+            put_device(ctx, i, t)
+            if t < t0_frame:
+                ctx.stb_process_frame(t)
+            else:
+                solo_ms += timed_frame(o, stream, lambda: ctx.stb_process_frame(t))
+        same = all(all(np.array_equal(x, y) for x, y in zip(a_, b_))
+                   for a_, b_ in zip(lists(ctx), batched_lists[i]))
+        equal += int(same)
+        if not same:
+            mism.append(i)
+        ctx.close()
+
+    dev_ms = sum(step_ms)
+    dev_ms, parts, e2e_s, e2e_parts = o.reduce(dev_ms, parts, e2e_s, e2e_parts)
+    if o.rank != 0:
+        return
+    cpu = None
+    if o.world == 1 and not args.no_cpu_baseline:
+        threads = os.cpu_count() or 1
+        times, counts, _, _, _, sname = reference_stb(args.workload, threads, 0, 2, 60.0,
+                                                      converge=0)
+        cpu = {"value": sum(counts) / sum(times), "unit": "particles/s", "cores": threads,
+               "kind": "reference",
+               "sample": f"STB::processFrame compiled from the reference sources (OpenMP) on "
+                         f"{sname} (one sequence of the batch's shapes): {N_INIT} initial-phase "
+                         f"frames untimed, then {len(times)} convergence-phase frames timed"}
+    sizes = {}
+    for p in plan:
+        key = f"{p['n_cam']}cam_{p['size']}"
+        sizes[key] = sizes.get(key, 0) + 1
+    cfg = {"workload": args.workload, "sequences": len(plan),
+           "particles_total": int(sum(p["n_particles"] for p in plan)),
+           "particles_range": [min(p["n_particles"] for p in plan),
+                               max(p["n_particles"] for p in plan)],
+           "rigs": sizes, "frames": nf, "initial_frames": N_INIT,
+           "step": "one convergence-phase frame of every sequence",
+           "settings": "threshold 30, shake width 0.25 px, tol_2d 1 px, tol_3d 0.6 px, "
+                       "link radii 10 px, field 11x11x6 r 30 px, 4 IPR loops x 4 shakes, "
+                       "match_cam_count = cameras",
+           "parallelism": "one context per sequence, persistent host workers, one stream each",
+           "timing": "wall clock around each batched step with device synchronisation on both "
+                     "sides (the step spans one stream per sequence)",
+           "l2": "flushed (256 MiB write) before every timed step; the step's frames "
+                 f"({bi / 2**20:.0f} MiB) exceed L2"}
+    extra = {"generation_s": round(t_gen, 1),
+             "one_at_a_time": {"value": parts / (solo_ms * 1e-3) if solo_ms else None,
+                               "unit": "particles/s", "ms_per_step": solo_ms / args.steps,
+                               "batching_gain": solo_ms / dev_ms if dev_ms else None},
+             "per_sequence_equal_to_one_at_a_time": f"{equal}/{len(seqs)}",
+             "mismatched_sequences": mism}
+    extra.update(pre_lines)
+    o.line(prof, dev_ms, parts, e2e_s, e2e_parts, bi, bo // max(1, args.steps), launches, clk,
+           cfg, cpu, extra)
+
+
 def learned_stb(args, o, seq, s, st, nf, t0_frame, new_ctx, frame_device, state_init, state_t0,
                 plain_warm, plain_timed):
     """The learned form on the same frames as the plain form.
@@ -1083,8 +1272,11 @@ def run_ours(args):
     if o.world == 1 and not args.no_detection_roofline:
         pre["detection_roofline"] = detection_roofline(args, o)
         o.torch.cuda.synchronize()
-    if WORKLOADS[args.workload]["kind"] == "ipr":
+    kind = WORKLOADS[args.workload]["kind"]
+    if kind == "ipr":
         run_ours_ipr(args, o, pre)
+    elif kind == "batch":
+        run_ours_batch(args, o, pre)
     else:
         run_ours_stb(args, o, pre)
     if o.world > 1:

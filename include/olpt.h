@@ -278,6 +278,22 @@ typedef struct olpt_ipr_params {
  * tolerance growing x1.5 per loop.  The current images end as the final residual.
  * n_objects receives the number of reconstructed objects. */
 olpt_status_t olpt_ipr_run(olpt_ctx* ctx, const olpt_ipr_params* p, int64_t* n_objects);
+/* Launch shapes of the shake (warps per block: 1, 2 or 4) and of the residual image
+ * (threads per 32x32 tile block: 128 or 256).  They change only the speed: every
+ * result is the same for every choice.  Default {4, 256}. */
+typedef struct olpt_tuning {
+  int shake_warps_per_block;
+  int residual_threads;
+} olpt_tuning;
+olpt_status_t olpt_tuning_get(olpt_ctx* ctx, olpt_tuning* out);
+olpt_status_t olpt_tuning_set(olpt_ctx* ctx, const olpt_tuning* t);
+/* Autotuner: times olpt_ipr_run on the context's current images (restored before every
+ * trial) with each candidate launch shape, `reps` runs each, keeps the fastest in the
+ * context and returns it with its mean time.  Every candidate must reproduce the first
+ * candidate's objects bit for bit (OLPT_ERR_INTERNAL otherwise).  The images are left
+ * as they were before the call. */
+olpt_status_t olpt_autotune_ipr(olpt_ctx* ctx, const olpt_ipr_params* p, int reps,
+                                olpt_tuning* best, double* best_ms);
 /* Independent frames at once (no reference counterpart): olpt_ipr_run on every
  * context, each from its own host thread on its own stream, so the frames' kernels
  * overlap on the device.  n_objects[i] receives context i's count; the first failing
@@ -326,6 +342,12 @@ olpt_status_t olpt_stb_configure(olpt_ctx* ctx, const olpt_stb_params* p);
  * repeat check, short-track linking, linear-fit pruning.  The current images end as
  * residuals. */
 olpt_status_t olpt_stb_process_frame(olpt_ctx* ctx, int frame);
+/* Independent sequences at once (no reference counterpart): olpt_stb_process_frame
+ * (ctxs[i], frames[i]) for every context, each on a persistent host worker and the
+ * context's own stream, so the sequences' kernels overlap on the device.  Each
+ * sequence's results are those of running it alone.  The first failing context's
+ * status is returned (its message in that context's olpt_last_error). */
+olpt_status_t olpt_stb_process_frame_batch(olpt_ctx* const* ctxs, int n_ctx, const int* frames);
 /* Sizes of the four track lists (indexed by OLPT_TRACK_*), and the particles of the
  * last frame: predictions extended and new IPR objects (either pointer may be NULL). */
 olpt_status_t olpt_stb_counts(olpt_ctx* ctx, int64_t counts[4], int64_t* n_extended,

@@ -48,6 +48,10 @@ class CameraDesc(C.Structure):
     ]
 
 
+class Tuning(C.Structure):
+    _fields_ = [("shake_warps_per_block", C.c_int), ("residual_threads", C.c_int)]
+
+
 class SmParams(C.Structure):
     _fields_ = [("match_cam_count", C.c_int), ("idmap_cell_px", C.c_int),
                 ("tol_2d_px", C.c_double), ("tol_3d_mm", C.c_double), ("limit", C.c_double * 6)]
@@ -376,6 +380,24 @@ class Context:
         self._check(self.L.olpt_ipr_run(self.h, C.byref(params), C.byref(n)))
         return n.value
 
+    def tuning(self):
+        """(shake warps per block, residual threads per block) of the context."""
+        t = Tuning()
+        self._check(self.L.olpt_tuning_get(self.h, C.byref(t)))
+        return t.shake_warps_per_block, t.residual_threads
+
+    def set_tuning(self, shake_warps: int, residual_threads: int):
+        self._check(self.L.olpt_tuning_set(self.h, C.byref(Tuning(shake_warps, residual_threads))))
+
+    def autotune_ipr(self, params: "IprParams", reps: int = 2):
+        """olpt_autotune_ipr on the current images: the fastest launch shapes (kept in the
+        context) and their mean IPR time in ms."""
+        t = Tuning()
+        ms = C.c_double()
+        self._check(self.L.olpt_autotune_ipr(self.h, C.byref(params), int(reps), C.byref(t),
+                                             C.byref(ms)))
+        return (t.shake_warps_per_block, t.residual_threads), ms.value
+
     def ipr_result(self, n: int):
         xyz = np.empty((n, 3))
         uv = np.empty((n, self.n_cam, 2))
@@ -588,6 +610,21 @@ def ipr_params(settings, limit, precision: int = 0) -> IprParams:
                      shake=shake_params(settings, precision), n_cam_reduced=settings.n_cam_reduced,
                      n_loop_ipr=settings.n_loop_ipr, n_loop_ipr_reduced=settings.n_loop_ipr_reduced,
                      n_obj2d_process_max=settings.n_obj2d_process_max)
+
+
+def stb_process_frame_batch(ctxs: Sequence["Context"], frames: Sequence[int]):
+    """olpt_stb_process_frame_batch: frame frames[i] of every context's sequence at once
+    (persistent host workers, one stream per context)."""
+    L = lib()
+    arr = (C.c_void_p * len(ctxs))(*[c.h for c in ctxs])
+    fr = (C.c_int * len(ctxs))(*[int(f) for f in frames])
+    rc = L.olpt_stb_process_frame_batch(arr, len(ctxs), fr)
+    if rc != 0:
+        for c in ctxs:
+            msg = L.olpt_last_error(c.h)
+            if msg:
+                raise OlptError(rc, msg.decode())
+        raise OlptError(rc, "olpt_stb_process_frame_batch failed")
 
 
 def ipr_run_batch(ctxs: Sequence["Context"], params: IprParams):

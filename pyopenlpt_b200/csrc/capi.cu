@@ -9,6 +9,10 @@
 #include <cmath>
 #include <new>
 #include <string>
+#include <chrono>
+#include <condition_variable>
+#include <functional>
+#include <mutex>
 #include <thread>
 #include <vector>
 
@@ -889,24 +893,192 @@ olpt_status_t olpt_ipr_run(olpt_ctx* ctx, const olpt_ipr_params* p, int64_t* n_o
   });
 }
 
-olpt_status_t olpt_ipr_run_batch(olpt_ctx* const* ctxs, int n_ctx, const olpt_ipr_params* p,
-                                 int64_t* n_objects) {
-  if (!ctxs || n_ctx <= 0 || !p) return OLPT_ERR_INVALID_ARG;
+// Persistent host workers for the batch entry points: job i of a batch runs on worker
+// i, which keeps its thread across batches (no thread start-up per frame).
+class BatchPool {
+ public:
+  ~BatchPool() {
+    {
+      std::lock_guard<std::mutex> lk(mu_);
+      quit_ = true;
+      gen_++;
+    }
+    cv_.notify_all();
+    for (auto& t : th_) t.join();
+  }
+  // runs fn(0 .. n-1) on n workers and waits for all of them; one batch at a time
+  void run(int n, const std::function<void(int)>& fn) {
+    std::lock_guard<std::mutex> one(batch_mu_);
+    std::unique_lock<std::mutex> lk(mu_);
+    while ((int)th_.size() < n) {
+      const int id = (int)th_.size();
+      th_.emplace_back([this, id] { loop(id); });
+    }
+    fn_ = &fn;
+    n_ = n;
+    left_ = n;
+    gen_++;
+    cv_.notify_all();
+    done_cv_.wait(lk, [this] { return left_ == 0; });
+    fn_ = nullptr;
+  }
+
+ private:
+  void loop(int id) {
+    std::unique_lock<std::mutex> lk(mu_);
+    uint64_t seen = gen_;
+    for (;;) {
+      cv_.wait(lk, [&] { return gen_ != seen; });
+      seen = gen_;
+      if (quit_) return;
+      if (id >= n_) continue;
+      const std::function<void(int)>* f = fn_;
+      lk.unlock();
+      (*f)(id);
+      lk.lock();
+      if (--left_ == 0) done_cv_.notify_all();
+    }
+  }
+  std::mutex mu_, batch_mu_;
+  std::condition_variable cv_, done_cv_;
+  std::vector<std::thread> th_;
+  const std::function<void(int)>* fn_ = nullptr;
+  int n_ = 0, left_ = 0;
+  uint64_t gen_ = 0;
+  bool quit_ = false;
+};
+
+static BatchPool& batch_pool() {
+  static BatchPool pool;
+  return pool;
+}
+
+static bool distinct_contexts(olpt_ctx* const* ctxs, int n_ctx) {
   for (int i = 0; i < n_ctx; ++i)
     for (int j = 0; j < i; ++j)
-      if (!ctxs[i] || ctxs[i] == ctxs[j]) return OLPT_ERR_INVALID_ARG;
+      if (!ctxs[i] || ctxs[i] == ctxs[j]) return false;
+  return n_ctx > 0 && ctxs[0];
+}
+
+olpt_status_t olpt_ipr_run_batch(olpt_ctx* const* ctxs, int n_ctx, const olpt_ipr_params* p,
+                                 int64_t* n_objects) {
+  if (!ctxs || n_ctx <= 0 || !p || !distinct_contexts(ctxs, n_ctx)) return OLPT_ERR_INVALID_ARG;
   std::vector<olpt_status_t> st(n_ctx, OLPT_OK);
   std::vector<int64_t> cnt(n_ctx, 0);
-  std::vector<std::thread> th;
-  th.reserve(n_ctx);
-  for (int i = 0; i < n_ctx; ++i)
-    th.emplace_back([&, i] {
-      cudaSetDevice(ctxs[i]->device);
-      st[i] = olpt_ipr_run(ctxs[i], p, &cnt[i]);
-    });
-  for (auto& t : th) t.join();
+  batch_pool().run(n_ctx, [&](int i) {
+    cudaSetDevice(ctxs[i]->device);
+    st[i] = olpt_ipr_run(ctxs[i], p, &cnt[i]);
+  });
   for (int i = 0; i < n_ctx; ++i)
     if (n_objects) n_objects[i] = cnt[i];
+  for (int i = 0; i < n_ctx; ++i)
+    if (st[i] != OLPT_OK) return st[i];
+  return OLPT_OK;
+}
+
+olpt_status_t olpt_tuning_get(olpt_ctx* ctx, olpt_tuning* out) {
+  return guard(ctx, [&] {
+    OLPT_REQUIRE(out, OLPT_ERR_INVALID_ARG, "null output");
+    *out = ctx->tune;
+  });
+}
+
+olpt_status_t olpt_tuning_set(olpt_ctx* ctx, const olpt_tuning* t) {
+  return guard(ctx, [&] {
+    OLPT_REQUIRE(t, OLPT_ERR_INVALID_ARG, "null tuning");
+    const int w = t->shake_warps_per_block, r = t->residual_threads;
+    OLPT_REQUIRE(w == 1 || w == 2 || w == 4, OLPT_ERR_INVALID_ARG,
+                 "shake warps per block must be 1, 2 or 4");
+    OLPT_REQUIRE(r == 128 || r == 256, OLPT_ERR_INVALID_ARG,
+                 "residual threads per block must be 128 or 256");
+    ctx->tune = *t;
+  });
+}
+
+olpt_status_t olpt_autotune_ipr(olpt_ctx* ctx, const olpt_ipr_params* p, int reps,
+                                olpt_tuning* best, double* best_ms) {
+  return guard(ctx, [&] {
+    OLPT_REQUIRE(p && reps > 0, OLPT_ERR_INVALID_ARG, "bad arguments");
+    OLPT_REQUIRE(ctx->n_cam > 0 && ctx->img[0].buf.p, OLPT_ERR_INVALID_ARG, "no images uploaded");
+    cudaStream_t s = ctx->stream;
+    // the images as uploaded: every trial starts from them, and they are put back
+    std::vector<DevBuf> keep(ctx->n_cam);
+    std::vector<size_t> bytes(ctx->n_cam);
+    for (int c = 0; c < ctx->n_cam; ++c) {
+      bytes[c] = (size_t)ctx->img[c].pitch * ctx->img[c].H;
+      keep[c].ensure(bytes[c] + 16, s);
+      OLPT_CUDA(cudaMemcpyAsync(keep[c].p, ctx->img[c].buf.p, bytes[c], cudaMemcpyDeviceToDevice, s));
+    }
+    auto restore = [&] {
+      for (int c = 0; c < ctx->n_cam; ++c)
+        OLPT_CUDA(cudaMemcpyAsync(ctx->img[c].buf.p, keep[c].p, bytes[c], cudaMemcpyDeviceToDevice,
+                                  s));
+    };
+    auto run = [&](std::vector<double>* xyz) {
+      int64_t n = 0;
+      const olpt_status_t st = olpt_ipr_run(ctx, p, &n);
+      if (st != OLPT_OK) throw ApiError{st, ctx->err};
+      if (xyz) {
+        xyz->resize((size_t)n * 3);
+        if (n > 0)
+          OLPT_CUDA(cudaMemcpyAsync(xyz->data(), ctx->ipr.out_xyz.p, n * 3 * sizeof(double),
+                                    cudaMemcpyDeviceToHost, s));
+        OLPT_CUDA(cudaStreamSynchronize(s));
+      }
+    };
+    const olpt_tuning start = ctx->tune;
+    const olpt_tuning cand[] = {{4, 256}, {2, 256}, {1, 256}, {4, 128}, {2, 128}, {1, 128}};
+    std::vector<double> first, got;
+    double best_t = 0;
+    olpt_tuning pick = start;
+    try {
+      for (size_t k = 0; k < sizeof cand / sizeof cand[0]; ++k) {
+        ctx->tune = cand[k];
+        restore();
+        run(&got);  // untimed: warms the launch shape, and its objects are checked
+        if (k == 0)
+          first = got;
+        else
+          OLPT_REQUIRE(got == first, OLPT_ERR_INTERNAL,
+                       "autotune: a launch shape changed the reconstructed objects");
+        double total = 0;
+        for (int r = 0; r < reps; ++r) {
+          restore();
+          OLPT_CUDA(cudaStreamSynchronize(s));
+          const auto a = std::chrono::steady_clock::now();
+          run(nullptr);
+          OLPT_CUDA(cudaStreamSynchronize(s));
+          total += std::chrono::duration<double, std::milli>(std::chrono::steady_clock::now() - a)
+                       .count();
+        }
+        const double t = total / reps;
+        if (k == 0 || t < best_t) {
+          best_t = t;
+          pick = cand[k];
+        }
+      }
+    } catch (...) {
+      ctx->tune = start;
+      restore();
+      for (auto& b : keep) b.release(s);
+      throw;
+    }
+    ctx->tune = pick;
+    restore();
+    OLPT_CUDA(cudaStreamSynchronize(s));
+    for (auto& b : keep) b.release(s);
+    if (best) *best = pick;
+    if (best_ms) *best_ms = best_t;
+  });
+}
+
+olpt_status_t olpt_stb_process_frame_batch(olpt_ctx* const* ctxs, int n_ctx, const int* frames) {
+  if (!ctxs || n_ctx <= 0 || !frames || !distinct_contexts(ctxs, n_ctx)) return OLPT_ERR_INVALID_ARG;
+  std::vector<olpt_status_t> st(n_ctx, OLPT_OK);
+  batch_pool().run(n_ctx, [&](int i) {
+    cudaSetDevice(ctxs[i]->device);
+    st[i] = olpt_stb_process_frame(ctxs[i], frames[i]);
+  });
   for (int i = 0; i < n_ctx; ++i)
     if (st[i] != OLPT_OK) return st[i];
   return OLPT_OK;

@@ -993,7 +993,7 @@ static void residual_pass(olpt_ctx* ctx, ShakeView& v, const uint8_t* flags, int
     bytes += (double)v.orig[c].H * v.orig[c].W * (esz + sizeof(Real));
   }
   const int pid = ctx->prof.begin(PROF_RESIDUAL, s);
-  residual_kernel<Real><<<OLPT_G(v.n_tiles), 256, 0, s>>>(v, ctx->obj.uv.as<double>(), W.otfp.as<Real>(),
+  residual_kernel<Real><<<OLPT_G(v.n_tiles), ctx->tune.residual_threads, 0, s>>>(v, ctx->obj.uv.as<double>(), W.otfp.as<Real>(),
                                                   W.bins.start.as<int>(), W.bins.items.as<int>(),
                                                   clamp, all_cams);
   ctx->prof.end(PROF_RESIDUAL, pid, s, bytes);
@@ -1037,7 +1037,7 @@ static void shake_iterations(olpt_ctx* ctx, const ShakeParams& sp, ShakeView& v,
   ShakeWork& W = ctx->shk;
   double dmin = sp.shakewidth_min;
   dmin = (dmin > 0) ? dmin : sp.shake_width / 20;
-  const int warps_per_blk = 4;
+  const int warps_per_blk = ctx->tune.shake_warps_per_block;  // 1, 2 or 4 (bound: 128 threads)
   const size_t smem = v.smem_per_warp * warps_per_blk;
 
   for (int it = 0; it < n_loop; ++it) {

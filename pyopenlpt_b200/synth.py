@@ -719,3 +719,68 @@ def make_poly_scene(ppp: float = 0.02, size: int = 512, n_cam: int = 6,
     return Scene(seq.cams, seq.truth[0], list(seq.frames[0]), seq.volume,
                  (a_mid, float(np.mean(seq.otf_table[1])), float(np.mean(seq.otf_table[2]))),
                  seq.max_val, otf_table=seq.otf_table, otf_n=seq.otf_n)
+
+
+# ----------------------------------------------------------------------------- many sequences
+def taylor_green_velocity(xyz: np.ndarray, wavelength: float, phase=(0.0, 0.0, 0.0)) -> np.ndarray:
+    """Taylor-Green cells (u = sin kx cos ky cos kz, v = -cos kx sin ky cos kz, w = 0,
+    k = 2 pi / wavelength, shifted by ``phase`` in mm): divergence-free, unit peak speed."""
+    k = 2.0 * math.pi / wavelength
+    x = k * (xyz[:, 0] + phase[0])
+    y = k * (xyz[:, 1] + phase[1])
+    z = k * (xyz[:, 2] + phase[2])
+    return np.stack([np.sin(x) * np.cos(y) * np.cos(z), -np.cos(x) * np.sin(y) * np.cos(z),
+                     np.zeros_like(x)], axis=1)
+
+
+def make_tg_sequence(n_particles: int, n_cam: int, size: int, n_frames: int = 20,
+                     wavelength: float = 40.0, volume=(-20.0, 20.0, -20.0, 20.0, -10.0, 10.0),
+                     a: float = 200.0, b: float = 0.5, c: float = 0.5, noise: float = 2.0,
+                     max_px_per_frame: float = 3.0, seed: int = 0,
+                     device="cpu") -> PolySequence:
+    """One sequence of the many-sequence batch: ``n_cam`` pinhole cameras on the ring
+    rig (focal sized so the volume fills the size^2 images), 8-bit images with a uniform
+    Gaussian OTF (a, b, c) and noise, particles advected by Taylor-Green cells of the
+    given wavelength (random phase; RK4 in FP64; at most ``max_px_per_frame`` of image
+    motion), re-seeded uniformly when they leave the volume."""
+    rng = np.random.default_rng(seed)
+    focal = min(focal_for_volume(n_cam, size, volume))
+    cams = ring_rig(n_cam, size, size, focal)
+    table = otf_table_array(n_cam, (a, b, c))
+    lo = np.array(volume[0::2], dtype=np.float64)
+    hi = np.array(volume[1::2], dtype=np.float64)
+    phase = tuple(rng.uniform(0.0, wavelength, 3))
+    vel = lambda p: taylor_green_velocity(p, wavelength, phase)  # noqa: E731
+    ppm = max(px_per_mm(cm, 0.5 * (lo + hi)) for cm in cams)
+    dt = max_px_per_frame / ppm  # unit peak speed
+    xyz = lo + (hi - lo) * rng.random((n_particles, 3))
+    ids = np.arange(n_particles)
+    next_id = n_particles
+    frames, truth, idl = [], [], []
+    for t in range(n_frames):
+        truth.append(xyz.copy())
+        idl.append(ids.copy())
+        nz = rng.standard_normal((n_cam, size, size), dtype=np.float32) * noise
+        frames.append(render_frame(cams, xyz, table, (2, 2, 2), volume, nz, 255, np.uint8, device))
+        xyz = rk4(vel, xyz, dt)
+        out = np.any((xyz < lo) | (xyz > hi), axis=1)
+        k = int(out.sum())
+        if k:
+            xyz[out] = lo + (hi - lo) * rng.random((k, 3))
+            ids[out] = np.arange(next_id, next_id + k)
+            next_id += k
+    return PolySequence(cams, frames, truth, idl, tuple(volume), table, (2, 2, 2), 255, dt)
+
+
+def batch_plan(n_seq: int = 64, seed: int = 2024, n_min: int = 2000, n_max: int = 80000):
+    """Seeded shapes of the many-sequence batch: per sequence (particles log-uniform in
+    [n_min, n_max], cameras in 4..6, image size in {512, 1024, 2048}, wavelength
+    uniform in [20, 60] mm, seed)."""
+    rng = np.random.default_rng(seed)
+    plan = []
+    for i in range(n_seq):
+        n = int(round(math.exp(rng.uniform(math.log(n_min), math.log(n_max)))))
+        plan.append(dict(n_particles=n, n_cam=int(rng.integers(4, 7)),
+                         size=int(rng.choice([512, 1024, 2048])),
+                         wavelength=float(rng.uniform(20.0, 60.0)), seed=seed + 1 + i))
+    return plan
