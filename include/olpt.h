@@ -278,22 +278,28 @@ typedef struct olpt_ipr_params {
  * tolerance growing x1.5 per loop.  The current images end as the final residual.
  * n_objects receives the number of reconstructed objects. */
 olpt_status_t olpt_ipr_run(olpt_ctx* ctx, const olpt_ipr_params* p, int64_t* n_objects);
-/* Launch shapes of the shake (warps per block: 1, 2 or 4) and of the residual image
- * (threads per 32x32 tile block: 128 or 256).  They change only the speed: every
- * result is the same for every choice.  Default {4, 256}. */
+/* Launch shapes of the shake (warps per block: 1, 2 or 4; registers a thread: 64, with
+ * 8 resident blocks per SM, or 128, with 4) and of the residual image (threads per
+ * 32x32 tile block: 128 or 256).  They change only the speed: every result is the same
+ * for every choice.  Default {4, 256, 128}. */
 typedef struct olpt_tuning {
   int shake_warps_per_block;
   int residual_threads;
+  int shake_regs;
 } olpt_tuning;
 olpt_status_t olpt_tuning_get(olpt_ctx* ctx, olpt_tuning* out);
 olpt_status_t olpt_tuning_set(olpt_ctx* ctx, const olpt_tuning* t);
+/* The autotuner's candidates (at most OLPT_TUNING_CANDIDATES), in trial order. */
+#define OLPT_TUNING_CANDIDATES 8
+olpt_status_t olpt_tuning_candidates(olpt_tuning* out, int* n);
 /* Autotuner: times olpt_ipr_run on the context's current images (restored before every
  * trial) with each candidate launch shape, `reps` runs each, keeps the fastest in the
- * context and returns it with its mean time.  Every candidate must reproduce the first
- * candidate's objects bit for bit (OLPT_ERR_INTERNAL otherwise).  The images are left
- * as they were before the call. */
+ * context and returns it with its mean time (cand_ms, optional: every candidate's mean
+ * time in trial order).  Every candidate must reproduce the first candidate's objects
+ * bit for bit (OLPT_ERR_INTERNAL otherwise).  The images are left as they were before
+ * the call. */
 olpt_status_t olpt_autotune_ipr(olpt_ctx* ctx, const olpt_ipr_params* p, int reps,
-                                olpt_tuning* best, double* best_ms);
+                                olpt_tuning* best, double* best_ms, double* cand_ms);
 /* Independent frames at once (no reference counterpart): olpt_ipr_run on every
  * context, each from its own host thread on its own stream, so the frames' kernels
  * overlap on the device.  n_objects[i] receives context i's count; the first failing

@@ -49,7 +49,8 @@ class CameraDesc(C.Structure):
 
 
 class Tuning(C.Structure):
-    _fields_ = [("shake_warps_per_block", C.c_int), ("residual_threads", C.c_int)]
+    _fields_ = [("shake_warps_per_block", C.c_int), ("residual_threads", C.c_int),
+                ("shake_regs", C.c_int)]
 
 
 class SmParams(C.Structure):
@@ -381,22 +382,25 @@ class Context:
         return n.value
 
     def tuning(self):
-        """(shake warps per block, residual threads per block) of the context."""
+        """(shake warps per block, residual threads per block, shake registers a thread)."""
         t = Tuning()
         self._check(self.L.olpt_tuning_get(self.h, C.byref(t)))
-        return t.shake_warps_per_block, t.residual_threads
+        return t.shake_warps_per_block, t.residual_threads, t.shake_regs
 
-    def set_tuning(self, shake_warps: int, residual_threads: int):
-        self._check(self.L.olpt_tuning_set(self.h, C.byref(Tuning(shake_warps, residual_threads))))
+    def set_tuning(self, shake_warps: int, residual_threads: int, shake_regs: int = 128):
+        self._check(self.L.olpt_tuning_set(
+            self.h, C.byref(Tuning(shake_warps, residual_threads, shake_regs))))
 
     def autotune_ipr(self, params: "IprParams", reps: int = 2):
         """olpt_autotune_ipr on the current images: the fastest launch shapes (kept in the
         context) and their mean IPR time in ms."""
         t = Tuning()
         ms = C.c_double()
+        cand = np.zeros(8)
         self._check(self.L.olpt_autotune_ipr(self.h, C.byref(params), int(reps), C.byref(t),
-                                             C.byref(ms)))
-        return (t.shake_warps_per_block, t.residual_threads), ms.value
+                                             C.byref(ms), _p(cand)))
+        self.autotune_trials = dict(zip(tuning_candidates(), cand.tolist()))
+        return (t.shake_warps_per_block, t.residual_threads, t.shake_regs), ms.value
 
     def ipr_result(self, n: int):
         xyz = np.empty((n, 3))
@@ -610,6 +614,17 @@ def ipr_params(settings, limit, precision: int = 0) -> IprParams:
                      shake=shake_params(settings, precision), n_cam_reduced=settings.n_cam_reduced,
                      n_loop_ipr=settings.n_loop_ipr, n_loop_ipr_reduced=settings.n_loop_ipr_reduced,
                      n_obj2d_process_max=settings.n_obj2d_process_max)
+
+
+def tuning_candidates():
+    """The autotuner's launch-shape candidates in trial order."""
+    L = lib()
+    n = C.c_int()
+    arr = (Tuning * 8)()
+    rc = L.olpt_tuning_candidates(arr, C.byref(n))
+    if rc != 0:
+        raise OlptError(rc, "olpt_tuning_candidates")
+    return [(t.shake_warps_per_block, t.residual_threads, t.shake_regs) for t in arr[:n.value]]
 
 
 def stb_process_frame_batch(ctxs: Sequence["Context"], frames: Sequence[int]):

@@ -986,17 +986,31 @@ olpt_status_t olpt_tuning_get(olpt_ctx* ctx, olpt_tuning* out) {
 olpt_status_t olpt_tuning_set(olpt_ctx* ctx, const olpt_tuning* t) {
   return guard(ctx, [&] {
     OLPT_REQUIRE(t, OLPT_ERR_INVALID_ARG, "null tuning");
-    const int w = t->shake_warps_per_block, r = t->residual_threads;
+    const int w = t->shake_warps_per_block, r = t->residual_threads, g = t->shake_regs;
     OLPT_REQUIRE(w == 1 || w == 2 || w == 4, OLPT_ERR_INVALID_ARG,
                  "shake warps per block must be 1, 2 or 4");
     OLPT_REQUIRE(r == 128 || r == 256, OLPT_ERR_INVALID_ARG,
                  "residual threads per block must be 128 or 256");
+    OLPT_REQUIRE(g == 64 || g == 128, OLPT_ERR_INVALID_ARG,
+                 "shake registers per thread must be 64 or 128");
     ctx->tune = *t;
   });
 }
 
+static const olpt_tuning kTuneCand[OLPT_TUNING_CANDIDATES] = {
+    {4, 256, 128}, {2, 256, 128}, {1, 256, 128}, {4, 256, 64},
+    {2, 256, 64},  {4, 128, 128}, {2, 128, 128}, {4, 128, 64}};
+
+olpt_status_t olpt_tuning_candidates(olpt_tuning* out, int* n) {
+  if (!n) return OLPT_ERR_INVALID_ARG;
+  *n = OLPT_TUNING_CANDIDATES;
+  if (out)
+    for (int i = 0; i < OLPT_TUNING_CANDIDATES; ++i) out[i] = kTuneCand[i];
+  return OLPT_OK;
+}
+
 olpt_status_t olpt_autotune_ipr(olpt_ctx* ctx, const olpt_ipr_params* p, int reps,
-                                olpt_tuning* best, double* best_ms) {
+                                olpt_tuning* best, double* best_ms, double* cand_ms) {
   return guard(ctx, [&] {
     OLPT_REQUIRE(p && reps > 0, OLPT_ERR_INVALID_ARG, "bad arguments");
     OLPT_REQUIRE(ctx->n_cam > 0 && ctx->img[0].buf.p, OLPT_ERR_INVALID_ARG, "no images uploaded");
@@ -1027,12 +1041,12 @@ olpt_status_t olpt_autotune_ipr(olpt_ctx* ctx, const olpt_ipr_params* p, int rep
       }
     };
     const olpt_tuning start = ctx->tune;
-    const olpt_tuning cand[] = {{4, 256}, {2, 256}, {1, 256}, {4, 128}, {2, 128}, {1, 128}};
+    const olpt_tuning* cand = kTuneCand;
     std::vector<double> first, got;
     double best_t = 0;
     olpt_tuning pick = start;
     try {
-      for (size_t k = 0; k < sizeof cand / sizeof cand[0]; ++k) {
+      for (int k = 0; k < OLPT_TUNING_CANDIDATES; ++k) {
         ctx->tune = cand[k];
         restore();
         run(&got);  // untimed: warms the launch shape, and its objects are checked
@@ -1052,6 +1066,7 @@ olpt_status_t olpt_autotune_ipr(olpt_ctx* ctx, const olpt_ipr_params* p, int rep
                        .count();
         }
         const double t = total / reps;
+        if (cand_ms) cand_ms[k] = t;
         if (k == 0 || t < best_t) {
           best_t = t;
           pick = cand[k];

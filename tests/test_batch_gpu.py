@@ -89,17 +89,18 @@ def test_autotune_keeps_results_and_images():
         p = _ffi.ipr_params(s, sc.volume)
         before = [ctx.image(c) for c in range(ctx.n_cam)]
         objs = {}
-        for shape in [(4, 256), (1, 128), (2, 256)]:
+        for shape in [(4, 256, 128), (1, 128, 64), (2, 256, 64), (4, 128, 128)]:
             L.bind(ctx, sc)
             ctx.set_tuning(*shape)
             n = ctx.ipr_run(p)
             objs[shape] = ctx.ipr_result(n)[0]
-        ref = objs[(4, 256)]
+        ref = objs[(4, 256, 128)]
         assert all(np.array_equal(v, ref) for v in objs.values())
         L.bind(ctx, sc)
         shape, ms = ctx.autotune_ipr(p, reps=1)
         print(f"autotuned launch shapes {shape}: {ms:.2f} ms per IPR")
-        assert shape in {(w, r) for w in (1, 2, 4) for r in (128, 256)} and ms > 0
+        assert shape in {(w, r, g) for w in (1, 2, 4) for r in (128, 256) for g in (64, 128)}
+        assert ms > 0
         assert ctx.tuning() == shape
         for c in range(ctx.n_cam):
             assert np.array_equal(ctx.image(c), before[c])
