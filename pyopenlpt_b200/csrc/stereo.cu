@@ -69,6 +69,18 @@ struct Path {
   int target;
 };
 
+// A partial path of exactly N chosen points, as the level kernels pass it on: the
+// chosen detection ids, their cameras packed 4 bits each (point i in bits 4i..4i+3)
+// and the next camera.  16 bytes for N = 2 (the 30 M first-level children of a 2048^2
+// frame) instead of the 48 of a full Path.
+template <int N>
+struct alignas(16) PathN {
+  int ids[N];
+  unsigned cams;
+  int target;
+  __host__ __device__ int cam(int i) const { return (int)((cams >> (4 * i)) & 15u); }
+};
+
 namespace {
 
 inline int nblk(int64_t n, int t = 256) { return (int)((n + t - 1) / t); }
@@ -224,7 +236,8 @@ __device__ double seg_len(const double* L, double W, double H) {
 }
 
 // seed level: one path per reference detection with its second build camera
-__global__ void seed_kernel(const __grid_constant__ SmView v, int ref, Path* out, int* out_count, int cap) {
+__global__ void seed_kernel(const __grid_constant__ SmView v, int ref, PathN<1>* out, int* out_count,
+                            int cap) {
   int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
   if (i >= v.n[ref]) return;
   int best = -1;
@@ -240,10 +253,9 @@ __global__ void seed_kernel(const __grid_constant__ SmView v, int ref, Path* out
   if (best < 0) return;
   int slot = atomicAdd(out_count, 1);
   if (slot >= cap) return;
-  Path p;
+  PathN<1> p;
   p.ids[0] = (int)i;
-  p.cams[0] = (signed char)ref;
-  p.k = 1;
+  p.cams = (unsigned)ref;
   p.target = best;
   out[slot] = p;
 }
@@ -349,7 +361,7 @@ __device__ __noinline__ void near_append(const SmView& v, int kind, int k, int c
 // warp per path, lanes take rows (the single long strip of K = 1); otherwise one
 // thread per path (K >= 2, where the strips intersect in a few rows).
 template <int K, bool WARP>
-__global__ void __launch_bounds__(256, K == 1 ? 4 : 2) enum_kernel(const __grid_constant__ SmView v, const Path* in, int n_in,
+__global__ void __launch_bounds__(256, K == 1 ? 4 : 2) enum_kernel(const __grid_constant__ SmView v, const void* in_v, int n_in,
                                                    Pair* pairs, int* pair_count, int pair_cap) {
   const int gtid = blockIdx.x * blockDim.x + threadIdx.x;
   const int pidx = WARP ? (gtid >> 5) : gtid;
@@ -358,7 +370,8 @@ __global__ void __launch_bounds__(256, K == 1 ? 4 : 2) enum_kernel(const __grid_
   // warp's paths are shared out over all lanes); a lane without a path has no rows
   const bool live = pidx < n_in;
   if (WARP && !live) return;
-  Path P{};
+  const PathN<K>* in = static_cast<const PathN<K>*>(in_v);
+  PathN<K> P{};
   if (live) P = in[pidx];
   const int t = P.target;
   // image lines of the chosen points on the target camera
@@ -369,7 +382,7 @@ __global__ void __launch_bounds__(256, K == 1 ? 4 : 2) enum_kernel(const __grid_
     lp[i][0] = lp[i][1] = lU[i][0] = cpt[i][0] = cpt[i][1] = 0.0;
     lU[i][1] = 1.0;
     if (!live) continue;
-    const int c = P.cams[i];
+    const int c = P.cam(i);
     const double* L = v.l2d[c][t] + 6 * (int64_t)P.ids[i];
     lp[i][0] = L[0];
     lp[i][1] = L[1];
@@ -388,7 +401,7 @@ __global__ void __launch_bounds__(256, K == 1 ? 4 : 2) enum_kernel(const __grid_
   const double2* cxy = v.cxy[t];
   const double* cbp[K];
 #pragma unroll
-  for (int i = 0; i < K; ++i) cbp[i] = live ? v.cbp[t][P.cams[i]] : nullptr;
+  for (int i = 0; i < K; ++i) cbp[i] = live ? v.cbp[t][P.cam(i)] : nullptr;
 
   // Rows that can hold a non-empty span: with two or more strips, the cell-centre rows
   // inside the y-extent of the first two strips' intersection parallelogram (plus one
@@ -484,7 +497,7 @@ __global__ void __launch_bounds__(256, K == 1 ? 4 : 2) enum_kernel(const __grid_
       if (v.near_band > 0.0) {
         const double m = fabs(z) - v.tol2d;
         if (fabs(m) < v.near_band)
-          near_append(v, 0, K, t, citems[q], P.cams[i], P.ids[i], m);
+          near_append(v, 0, K, t, citems[q], P.cam(i), P.ids[i], m);
       }
     }
     if (!ok) return false;
@@ -500,7 +513,7 @@ __global__ void __launch_bounds__(256, K == 1 ? 4 : 2) enum_kernel(const __grid_
       if (v.near_band > 0.0) {
         const double m = fabs(z) - v.tol2d;
         if (fabs(m) < v.near_band)
-          near_append(v, 1, K, t, citems[q], P.cams[i], P.ids[i], m);
+          near_append(v, 1, K, t, citems[q], P.cam(i), P.ids[i], m);
       }
     }
     return ok;
@@ -611,7 +624,7 @@ __global__ void __launch_bounds__(256, K == 1 ? 4 : 2) enum_kernel(const __grid_
           if (v.near_band > 0.0) {
             const double m = fabs(z) - v.tol2d;
             if (fabs(m) < v.near_band)
-              near_append(v, 0, K, ot, v.cell_items[ot][q], in[opidx].cams[i], in[opidx].ids[i], m);
+              near_append(v, 0, K, ot, v.cell_items[ot][q], in[opidx].cam(i), in[opidx].ids[i], m);
           }
         }
         if (!ok) continue;
@@ -627,7 +640,7 @@ __global__ void __launch_bounds__(256, K == 1 ? 4 : 2) enum_kernel(const __grid_
           if (v.near_band > 0.0) {
             const double m = fabs(z) - v.tol2d;
             if (fabs(m) < v.near_band)
-              near_append(v, 1, K, ot, v.cell_items[ot][q], in[opidx].cams[i], in[opidx].ids[i], m);
+              near_append(v, 1, K, ot, v.cell_items[ot][q], in[opidx].cam(i), in[opidx].ids[i], m);
           }
         }
         if (!ok) continue;
@@ -643,20 +656,20 @@ __global__ void __launch_bounds__(256, K == 1 ? 4 : 2) enum_kernel(const __grid_
 // TriangulationCheckWithTol: StereoMatch.cpp:1072-1141) on the path's lines plus the
 // candidate's, then the child path (terminal, or with its next target camera).
 template <int K>
-__global__ void __launch_bounds__(256, 2) tri_kernel(const __grid_constant__ SmView v, const Path* in,
-                                                     const Pair* pairs, int n_pairs, Path* out,
+__global__ void __launch_bounds__(256, 2) tri_kernel(const __grid_constant__ SmView v, const void* in_v,
+                                                     const Pair* pairs, int n_pairs, void* out_v,
                                                      int* out_count, int out_cap, Path* term,
                                                      int* term_count, int term_cap) {
   const int gi = blockIdx.x * blockDim.x + threadIdx.x;
   if (gi >= n_pairs) return;
   const Pair pr = pairs[gi];
-  const Path P = in[pr.path];
+  const PathN<K> P = static_cast<const PathN<K>*>(in_v)[pr.path];
   const int t = P.target;
   const int pid = pr.pid;
   double cp[K][3], cu[K][3];  // chosen lines of sight (build order)
 #pragma unroll
   for (int i = 0; i < K; ++i) {
-    const double* S = v.los[P.cams[i]] + 6 * (int64_t)P.ids[i];
+    const double* S = v.los[P.cam(i)] + 6 * (int64_t)P.ids[i];
 #pragma unroll
     for (int q = 0; q < 3; ++q) {
       cp[i][q] = S[q];
@@ -745,14 +758,27 @@ __global__ void __launch_bounds__(256, 2) tri_kernel(const __grid_constant__ SmV
         if (thrown) return;  // the reference's triangulation throws; the check fails
         const double err = sqrt(e / k1);
         if (!(err <= tq)) return;
-        Path ch = P;
+        PathN<K + 1> ch;
+#pragma unroll
+        for (int i = 0; i < K; ++i) ch.ids[i] = P.ids[i];
         ch.ids[K] = pid;
-        ch.cams[K] = (signed char)t;
-        ch.k = k1;
+        ch.cams = P.cams | ((unsigned)t << (4 * K));
         if (k1 == v.m) {
-          ch.target = -1;
+          Path full;
+#pragma unroll
+          for (int i = 0; i < OLPT_MAX_CAM; ++i) {
+            full.ids[i] = 0;
+            full.cams[i] = 0;
+          }
+#pragma unroll
+          for (int i = 0; i < K + 1; ++i) {
+            full.ids[i] = ch.ids[i];
+            full.cams[i] = (signed char)ch.cam(i);
+          }
+          full.k = k1;
+          full.target = -1;
           const int slot = append_slot(term_count);
-          if (slot < term_cap) term[slot] = ch;
+          if (slot < term_cap) term[slot] = full;
           return;
         }
         if (k1 >= OLPT_MAX_CAM) return;
@@ -762,18 +788,22 @@ __global__ void __launch_bounds__(256, 2) tri_kernel(const __grid_constant__ SmV
         for (int cam = 0; cam < v.n_cam; ++cam) {
           if (!v.active[cam]) continue;
           bool used = false;
-          for (int i = 0; i < k1; ++i) used |= (ch.cams[i] == cam);
+#pragma unroll
+          for (int i = 0; i < K + 1; ++i) used |= (ch.cam(i) == cam);
           if (used) continue;
-          double ux[OLPT_MAX_CAM], uy[OLPT_MAX_CAM];
-          for (int i = 0; i < k1; ++i) {
-            const double* L = v.l2d[ch.cams[i]][cam] + 6 * (int64_t)ch.ids[i];
+          double ux[K + 1], uy[K + 1];
+#pragma unroll
+          for (int i = 0; i < K + 1; ++i) {
+            const double* L = v.l2d[ch.cam(i)][cam] + 6 * (int64_t)ch.ids[i];
             ux[i] = L[2];
             uy[i] = L[3];
           }
           double score = 0.0;
           if (k1 >= 2) {
-            for (int i = 0; i < k1; ++i) {
-              for (int j = i + 1; j < k1; ++j) {
+#pragma unroll
+            for (int i = 0; i < K + 1; ++i) {
+#pragma unroll
+              for (int j = i + 1; j < K + 1; ++j) {
                 const double s = fabs(ux[i] * uy[j] - uy[i] * ux[j]);
                 if (s > score) score = s;
                 if (score >= 1.0 - 1e-12) break;
@@ -789,7 +819,7 @@ __global__ void __launch_bounds__(256, 2) tri_kernel(const __grid_constant__ SmV
         if (best < 0) return;
         ch.target = best;
         const int slot = append_slot(out_count);
-        if (slot < out_cap) out[slot] = ch;
+        if (slot < out_cap) static_cast<PathN<K + 1>*>(out_v)[slot] = ch;
       }
     }
   }
@@ -1035,7 +1065,8 @@ void stereo_match_device(olpt_ctx* ctx, const SmParams& prm, StereoResult& res) 
   int cap_a = (int)std::max<int64_t>(n_ref, 1024);
   W.path_a.ensure(cap_a * sizeof(Path), s);
   OLPT_CUDA(cudaMemsetAsync(cnt, 0, 8 * sizeof(int), s));
-  if (n_ref > 0) seed_kernel<<<OLPT_G(nblk(n_ref)), 256, 0, s>>>(v, ref, W.path_a.as<Path>(), cnt, cap_a);
+  if (n_ref > 0)
+    seed_kernel<<<OLPT_G(nblk(n_ref)), 256, 0, s>>>(v, ref, W.path_a.as<PathN<1>>(), cnt, cap_a);
   OLPT_CUDA(cudaGetLastError());
   int n_in = read_count(0);
   int term_cap = (int)std::max<int64_t>(4 * n_ref, 4096);
@@ -1065,8 +1096,8 @@ void stereo_match_device(olpt_ctx* ctx, const SmParams& prm, StereoResult& res) 
         default: kern = enum_kernel<7, false>; break;
       }
       const int64_t work = level == 1 ? (int64_t)n_in * 32 : (int64_t)n_in;
-      kern<<<OLPT_G(nblk(work)), 256, 0, s>>>(v, in_buf->as<Path>(), n_in, W.pairs.as<Pair>(),
-                                                cnt + 4, pair_cap);
+      kern<<<OLPT_G(nblk(work)), 256, 0, s>>>(v, in_buf->p, n_in, W.pairs.as<Pair>(), cnt + 4,
+                                                pair_cap);
       ctx->prof.end(PROF_STEREO, pid, s, 0.0);
       OLPT_CUDA(cudaGetLastError());
       n_pairs = read_count(4);
@@ -1097,8 +1128,8 @@ void stereo_match_device(olpt_ctx* ctx, const SmParams& prm, StereoResult& res) 
         default: kern = tri_kernel<7>; break;
       }
       if (n_pairs > 0)
-        kern<<<OLPT_G(nblk(n_pairs)), 256, 0, s>>>(v, in_buf->as<Path>(), W.pairs.as<Pair>(),
-                                                   n_pairs, out_buf->as<Path>(), cnt + 1, out_cap,
+        kern<<<OLPT_G(nblk(n_pairs)), 256, 0, s>>>(v, in_buf->p, W.pairs.as<Pair>(), n_pairs,
+                                                   out_buf->p, cnt + 1, out_cap,
                                                    W.term.as<Path>(), cnt + 2, term_cap);
       ctx->prof.end(PROF_STEREO, pid, s, 0.0);
       OLPT_CUDA(cudaGetLastError());
