@@ -369,7 +369,9 @@ PROF_NAMES = {0: "peak detection", 1: "stereo level expansion", 2: "residual ima
               3: "shake (warp per particle)", 4: "predictive field"}
 PHASE_NAMES = {5: "detection", 6: "stereo matching (all)", 7: "candidate sort + prune + greedy",
                8: "shake (all)", 9: "output + residual", 10: "STB track work",
-               11: "sequential greedy (replacement fallback)"}
+               11: "sequential greedy (replacement fallback)", 12: "track work: prediction",
+               13: "track work: extension", 14: "track work: linking and new tracks",
+               15: "track work: linear-fit pruning"}
 
 
 # DRAM bytes per shaken object (dram__bytes_read.sum + dram__bytes_write.sum of three

@@ -28,7 +28,12 @@ enum ProfPhase : int {
   PH_OUTPUT = 4,   // compaction of kept objects + final residual
   PH_TRACK = 5,    // STB track bookkeeping, prediction, linking and pruning
   PH_GREEDY_HOST = 6,  // sequential greedy, run when the device greedy meets a replacement
-  PH_N = 7
+  // parts of PH_TRACK
+  PH_TR_PREDICT = 7,   // packing, prediction kernel, range check
+  PH_TR_EXTEND = 8,    // extension of the long tracks by their shaken predictions
+  PH_TR_LINK = 9,      // new objects: repeat removal, short-track linking, new tracks
+  PH_TR_PRUNE = 10,    // linear-fit pruning of the long tracks
+  PH_N = 11
 };
 
 struct Prof {

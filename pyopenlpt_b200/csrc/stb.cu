@@ -972,6 +972,13 @@ void conv_phase(olpt_ctx* ctx, int frame) {
                     .count();
   };
   auto resume = [&] { t_track = std::chrono::steady_clock::now(); };
+  // the parts of the track work (the shake and the IPR excluded)
+  auto t_part = std::chrono::steady_clock::now();
+  auto part = [&](int ph) {
+    const auto now = std::chrono::steady_clock::now();
+    ctx->prof.add_phase(ph, std::chrono::duration<double, std::milli>(now - t_part).count());
+    t_part = now;
+  };
 
   // 1. prediction of the active long tracks
   int n_la = (int)S.long_active.size();
@@ -1018,6 +1025,7 @@ void conv_phase(olpt_ctx* ctx, int frame) {
     pred.resize(3 * w);
   }
 
+  part(PH_TR_PREDICT);
   // 2. shake the predictions; residual without the ghost / repeated ones; extend
   int64_t extended = 0;
   S.last_xyz.clear();
@@ -1032,12 +1040,14 @@ void conv_phase(olpt_ctx* ctx, int frame) {
     // shake, which drops the network's ghosts (they end like ghost-flagged tracks)
     const bool learned = ctx->mlp.lp.enable != 0;
     pause();
+    part(PH_TR_EXTEND);
     if (learned)
       learned_shake_device(ctx, S.ipr.shake);
     else
       shake_device(ctx, S.ipr.shake);
     residual_device(ctx, S.ipr.shake, true, true);
     resume();
+    t_part = std::chrono::steady_clock::now();
     const int64_t n_out = ctx->obj.n;
     const std::vector<double> sx0 = download(ctx->obj.xyz.as<double>(), 3 * (size_t)n_out, s);
     const std::vector<uint8_t> fl0 = download(ctx->obj.flags.as<uint8_t>(), (size_t)n_out, s);
@@ -1076,8 +1086,10 @@ void conv_phase(olpt_ctx* ctx, int frame) {
   // 3. IPR on the residual images
   snapshot_images(ctx);
   pause();
+  part(PH_TR_EXTEND);
   std::vector<double> oxyz = run_ipr_host(ctx);
   resume();
+  t_part = std::chrono::steady_clock::now();
   int n_obj = (int)(oxyz.size() / 3);
 
   // 4. drop the objects close to an active long track's last point
@@ -1175,6 +1187,7 @@ void conv_phase(olpt_ctx* ctx, int frame) {
     }
   }
 
+  part(PH_TR_LINK);
   // 6. linear-fit pruning of the active long tracks
   n_la = (int)S.long_active.size();
   if (n_la > 0) {
@@ -1217,6 +1230,7 @@ void conv_phase(olpt_ctx* ctx, int frame) {
     S.exited.clear();
   }
   pause();
+  part(PH_TR_PRUNE);
   ctx->prof.add_phase(PH_TRACK, track_ms);
 }
 
