@@ -911,8 +911,10 @@ class BatchPool {
     std::lock_guard<std::mutex> one(batch_mu_);
     std::unique_lock<std::mutex> lk(mu_);
     while ((int)th_.size() < n) {
+      // a new worker starts from the generation before this batch, so that it takes
+      // this batch however late it first acquires the lock
       const int id = (int)th_.size();
-      th_.emplace_back([this, id] { loop(id); });
+      th_.emplace_back([this, id, g = gen_] { loop(id, g); });
     }
     fn_ = &fn;
     n_ = n;
@@ -924,9 +926,8 @@ class BatchPool {
   }
 
  private:
-  void loop(int id) {
+  void loop(int id, uint64_t seen) {
     std::unique_lock<std::mutex> lk(mu_);
-    uint64_t seen = gen_;
     for (;;) {
       cv_.wait(lk, [&] { return gen_ != seen; });
       seen = gen_;
