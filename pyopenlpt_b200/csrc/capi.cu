@@ -1017,17 +1017,28 @@ olpt_status_t olpt_autotune_ipr(olpt_ctx* ctx, const olpt_ipr_params* p, int rep
     OLPT_REQUIRE(ctx->n_cam > 0 && ctx->img[0].buf.p, OLPT_ERR_INVALID_ARG, "no images uploaded");
     cudaStream_t s = ctx->stream;
     // the images as uploaded: every trial starts from them, and they are put back
+    // (the IPR leaves its residual in the planes, as F32 or F64: the planes' type and
+    // geometry are put back with their contents)
     std::vector<DevBuf> keep(ctx->n_cam);
-    std::vector<size_t> bytes(ctx->n_cam);
+    std::vector<ImagePlane> meta(ctx->n_cam);
     for (int c = 0; c < ctx->n_cam; ++c) {
-      bytes[c] = (size_t)ctx->img[c].pitch * ctx->img[c].H;
-      keep[c].ensure(bytes[c] + 16, s);
-      OLPT_CUDA(cudaMemcpyAsync(keep[c].p, ctx->img[c].buf.p, bytes[c], cudaMemcpyDeviceToDevice, s));
+      const ImagePlane& im = ctx->img[c];
+      meta[c].dtype = im.dtype;
+      meta[c].H = im.H;
+      meta[c].W = im.W;
+      meta[c].pitch = im.pitch;
+      const size_t bytes = (size_t)im.pitch * im.H;
+      keep[c].ensure(bytes + 16, s);
+      OLPT_CUDA(cudaMemcpyAsync(keep[c].p, im.buf.p, bytes, cudaMemcpyDeviceToDevice, s));
     }
     auto restore = [&] {
-      for (int c = 0; c < ctx->n_cam; ++c)
-        OLPT_CUDA(cudaMemcpyAsync(ctx->img[c].buf.p, keep[c].p, bytes[c], cudaMemcpyDeviceToDevice,
-                                  s));
+      for (int c = 0; c < ctx->n_cam; ++c) {
+        const ImagePlane& m = meta[c];
+        ensure_plane(ctx, c, m.dtype, m.H, m.W);
+        OLPT_CUDA(cudaMemcpy2DAsync(ctx->img[c].buf.p, ctx->img[c].pitch, keep[c].p, m.pitch,
+                                    (size_t)m.W * esize(m.dtype), m.H,
+                                    cudaMemcpyDeviceToDevice, s));
+      }
     };
     auto run = [&](std::vector<double>* xyz) {
       int64_t n = 0;
