@@ -281,7 +281,7 @@ olpt_status_t olpt_ipr_run(olpt_ctx* ctx, const olpt_ipr_params* p, int64_t* n_o
 /* Launch shapes of the shake (warps per block: 1, 2 or 4; registers a thread: 64, with
  * 8 resident blocks per SM, or 128, with 4) and of the residual image (threads per
  * 32x32 tile block: 128 or 256).  They change only the speed: every result is the same
- * for every choice.  Default {4, 256, 128}. */
+ * for every choice.  Default {4, 256, 64}. */
 typedef struct olpt_tuning {
   int shake_warps_per_block;
   int residual_threads;

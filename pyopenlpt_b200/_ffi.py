@@ -387,7 +387,7 @@ class Context:
         self._check(self.L.olpt_tuning_get(self.h, C.byref(t)))
         return t.shake_warps_per_block, t.residual_threads, t.shake_regs
 
-    def set_tuning(self, shake_warps: int, residual_threads: int, shake_regs: int = 128):
+    def set_tuning(self, shake_warps: int, residual_threads: int, shake_regs: int = 64):
         self._check(self.L.olpt_tuning_set(
             self.h, C.byref(Tuning(shake_warps, residual_threads, shake_regs))))
 

@@ -999,8 +999,8 @@ olpt_status_t olpt_tuning_set(olpt_ctx* ctx, const olpt_tuning* t) {
 }
 
 static const olpt_tuning kTuneCand[OLPT_TUNING_CANDIDATES] = {
-    {4, 256, 128}, {2, 256, 128}, {1, 256, 128}, {4, 256, 64},
-    {2, 256, 64},  {4, 128, 128}, {2, 128, 128}, {4, 128, 64}};
+    {4, 256, 64},  {2, 256, 64},  {1, 256, 64},  {4, 256, 128},
+    {2, 256, 128}, {4, 128, 64},  {2, 128, 64},  {4, 128, 128}};
 
 olpt_status_t olpt_tuning_candidates(olpt_tuning* out, int* n) {
   if (!n) return OLPT_ERR_INVALID_ARG;

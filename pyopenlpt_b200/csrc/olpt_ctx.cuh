@@ -399,7 +399,7 @@ void stb_load_tracks(olpt_ctx* ctx, int which, const std::string& path);
 struct olpt_ctx {
   int device = 0;
   // launch shapes chosen by olpt_autotune_ipr (they never change results)
-  olpt_tuning tune{4, 256, 128};
+  olpt_tuning tune{4, 256, 64};
   cudaStream_t stream = nullptr;
   bool own_stream = false;
   std::string err;

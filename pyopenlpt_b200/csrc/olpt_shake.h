@@ -37,7 +37,7 @@ struct ShakeView {
   int n_tiles;
   PlaneView orig[OLPT_MAX_CAM];  // current images (u8/u16/f32/f64)
   PlaneView res[OLPT_MAX_CAM];   // residual planes (Real)
-  size_t smem_per_warp, off_dd, off_otf, off_uv, off_roi;
+  size_t smem_per_warp, off_dd, off_otf, off_uv;
 };
 
 }  // namespace olpt

@@ -252,14 +252,13 @@ __device__ double residue(const ShakeView& v, const Rect* roi, Smem<Real>& S) {
 // the geometry arrays receives it (slot 0 is the one eval_geom uses).
 template <typename Real, int NC>
 __device__ void eval_geom3(const ShakeView& v, const double P[3], int ax, double x0,
-                           double delta, Smem<Real>& S) {
+                           const double rel[3], Smem<Real>& S) {
   const int lane = threadIdx.x & 31;
   constexpr int C = NC;
   if (lane < 3 * C) {
     const int j = lane / C, c = lane % C;
-    const double rel = j == 0 ? -delta : (j == 1 ? 0.0 : delta);
-    const double xt = x0 + rel;  // trial j of the axis
-    const double Q[3] = {ax == 0 ? xt : P[0], ax == 1 ? xt : P[1], ax == 2 ? xt : P[2]};
+    double Q[3] = {P[0], P[1], P[2]};
+    Q[ax] = x0 + rel[j];
     double u, w;
     cam_project(v.cams[c], Q[0], Q[1], Q[2], u, w);
     S.uvc[2 * lane] = u;
@@ -340,82 +339,60 @@ __device__ void residueK(const ShakeView& v, const Rect* roi, Smem<Real>& S, dou
 }
 
 // myMATH::polyfit order 2 (myMATH.cpp:490-534): (X^T X)^-1 X^T y with the
-// reference's operation order, for n <= 5 points.  Fixed-size loops with the points
-// i >= n skipped, so every array stays in registers (the sums are those of loops to n).
-__device__ __forceinline__ void polyfit2(const double (&x)[5], const double (&y)[5], int n,
-                                         double coef[3]) {
+// reference's operation order.
+__device__ void polyfit2(const double* x, const double* y, int n, double coef[3]) {
   double X[5][3];
-#pragma unroll
-  for (int i = 0; i < 5; ++i) {
+  for (int i = 0; i < n; ++i) {
     X[i][0] = 1.0;
     X[i][1] = x[i];
     X[i][2] = x[i] * x[i];
   }
   double A[9];
-#pragma unroll
   for (int r = 0; r < 3; ++r)
-#pragma unroll
     for (int c = 0; c < 3; ++c) {
       double s = 0;
-#pragma unroll
-      for (int i = 0; i < 5; ++i)
-        if (i < n) s += X[i][r] * X[i][c];
+      for (int i = 0; i < n; ++i) s += X[i][r] * X[i][c];
       A[3 * r + c] = s;
     }
   double Ai[9];
   gauss_inverse3(A, Ai);
-#pragma unroll
-  for (int r = 0; r < 3; ++r) {
-    double acc = 0;
-#pragma unroll
-    for (int i = 0; i < 5; ++i) {
-      if (i >= n) continue;
+  double B[3][5];
+  for (int r = 0; r < 3; ++r)
+    for (int i = 0; i < n; ++i) {
       double s = 0;
-#pragma unroll
       for (int k = 0; k < 3; ++k) s += Ai[3 * r + k] * X[i][k];
-      acc += s * y[i];  // B[r][i] * y[i], summed over i in order
+      B[r][i] = s;
     }
-    coef[r] = acc;
+  for (int r = 0; r < 3; ++r) {
+    double s = 0;
+    for (int i = 0; i < n; ++i) s += B[r][i] * y[i];
+    coef[r] = s;
   }
 }
 
-// The median of a[0 .. n) as the reference computes it (sort ascending, middle element,
-// mean of the two middle ones for even n), by ranks over a fixed-size register array:
-// the element of stable rank k is the sorted array's element k.
-template <int N>
-__device__ __forceinline__ double median_reg(const double (&a)[N], int n) {
+__device__ double median_small(double* a, int n) {
   if (n == 0) return 0.0;
-  const int mid = n / 2;
-  double hi = 0.0, lo = 0.0;
-#pragma unroll
-  for (int i = 0; i < N; ++i) {
-    if (i >= n) continue;
-    int pos = 0;
-#pragma unroll
-    for (int j = 0; j < N; ++j) {
-      if (j >= n) continue;
-      pos += (a[j] < a[i]) || (a[j] == a[i] && j < i);
+  for (int i = 1; i < n; ++i) {
+    double t = a[i];
+    int j = i - 1;
+    while (j >= 0 && a[j] > t) {
+      a[j + 1] = a[j];
+      --j;
     }
-    if (pos == mid) hi = a[i];
-    if (pos == mid - 1) lo = a[i];
+    a[j + 1] = t;
   }
-  return (n & 1) ? hi : 0.5 * (hi + lo);
-}
-
-// a[k] = v for the runtime index k < N, without indexing the array at run time
-template <int N>
-__device__ __forceinline__ void put_at(double (&a)[N], int k, double v) {
-#pragma unroll
-  for (int i = 0; i < N; ++i)
-    if (i == k) a[i] = v;
+  const int mid = n / 2;
+  double m = a[mid];
+  if ((n & 1) == 0) m = 0.5 * (m + a[mid - 1]);
+  return m;
 }
 
 __device__ __forceinline__ bool in_roi(const Rect& R, double u, double w) {
   return R.cmin <= u && u < R.cmax && R.rmin <= w && w < R.rmax;
 }
 
-// MINB: resident blocks per SM the kernel is compiled for -- 8 (64 registers a thread,
-// the line-search state partly in local memory) or 4 (128 registers, none spilled)
+// MINB: resident blocks per SM the kernel is compiled for -- 8 (64 registers a thread)
+// or 4 (128 registers)
 template <typename Real, int NC, int MINB>
 __global__ void __launch_bounds__(128, MINB) shake_kernel(const __grid_constant__ ShakeView v, int64_t n, double* xyz,
                                                     double* uv, const Real* otfp, double* score,
@@ -440,9 +417,7 @@ __global__ void __launch_bounds__(128, MINB) shake_kernel(const __grid_constant_
   double P[3] = {xyz[3 * o], xyz[3 * o + 1], xyz[3 * o + 2]};
   double f_final = 0.0;
   // ---- buildROIInfo (Shake.cpp:279-328)
-  // the ROIs in the warp's shared slot (every lane writes the same values): the rolled
-  // camera loops index them at run time
-  Rect* roi = reinterpret_cast<Rect*>(base + v.off_roi);
+  Rect roi[NC];
   const double* uvo = uv + o * C * 2;
   for (int c = 0; c < C; ++c) {
     roi[c] = Rect{0, 0, 0, 0};  // default-constructed PixelRange for skipped cameras
@@ -473,29 +448,27 @@ __global__ void __launch_bounds__(128, MINB) shake_kernel(const __grid_constant_
   __syncwarp();
 
   // ---- shakeOneObject (Shake.cpp:409-665)
-  // P, tmp and the trial offsets are read and written through selects on the axis, so
-  // that they stay in registers (the axis loop is not unrolled)
   double tmp[3] = {P[0], P[1], P[2]};
   for (int ax = 0; ax < 3; ++ax) {
-    const double x0 = ax == 0 ? P[0] : (ax == 1 ? P[1] : P[2]);
+    const double x0 = P[ax];
+    const double rel[3] = {-delta, 0.0, delta};
     double f[3];
     // the projections of the three trial points stay in the warp's shared slots
     // (slot j = trial j) instead of per-lane copies
     if ((sizeof(Real) == 8 && v.exact_sums)) {
-#pragma unroll
       for (int j = 2; j >= 0; --j) {  // slot 0 last: single evaluations write slot 0
-        put_at(tmp, ax, x0 + (j == 0 ? -delta : (j == 1 ? 0.0 : delta)));
+        tmp[ax] = x0 + rel[j];
         eval_geom<Real, NC>(v, tmp, S);
         f[j] = residue<Real, NC>(v, roi, S);
         if (j > 0 && lane < 2 * C) S.uvc[2 * j * C + lane] = S.uvc[lane];
         __syncwarp();
       }
     } else {
-      eval_geom3<Real, NC>(v, tmp, ax, x0, delta, S);
+      eval_geom3<Real, NC>(v, tmp, ax, x0, rel, S);
       residueK<Real, NC, 3>(v, roi, S, f);
       __syncwarp();
     }
-    put_at(tmp, ax, x0 + delta);  // as left by the last single evaluation
+    tmp[ax] = x0 + rel[2];  // as left by the last single evaluation
     auto su = [&](int j, int c) { return S.uvc[2 * (j * C + c)]; };
     auto sv = [&](int j, int c) { return S.uvc[2 * (j * C + c) + 1]; };
     auto sok = [&](int j, int c) { return in_roi(roi[c], su(j, c), sv(j, c)); };
@@ -527,17 +500,17 @@ __global__ void __launch_bounds__(128, MINB) shake_kernel(const __grid_constant_
       for (int c = 0; c < C; ++c) {
         if (sok(0, c) && sok(2, c)) {
           const double du = su(2, c) - su(0, c), dv = sv(2, c) - sv(0, c);
-          put_at(J, nJ++, hypot(du, dv) / fmax(2.0 * delta, 1e-12));
+          J[nJ++] = hypot(du, dv) / fmax(2.0 * delta, 1e-12);
         }
         if (sok(1, c)) {
           const Rect& R = roi[c];
           const double mu = fmin(su(1, c) - R.cmin, R.cmax - 1.0 - su(1, c));
           const double mv = fmin(sv(1, c) - R.rmin, R.rmax - 1.0 - sv(1, c));
-          put_at(M, nM++, fmin(mu, mv));
+          M[nM++] = fmin(mu, mv);
         }
       }
-      const double Jx = median_reg(J, nJ);
-      const double mpx = median_reg(M, nM);
+      const double Jx = median_small(J, nJ);
+      const double mpx = median_small(M, nM);
       const double Delta_roi = (Jx > 0.0 && mpx > 0.0) ? (0.5 * mpx / Jx) : 0.0;
       double Delta_try = 0.0;
       if (kappa > 0.0) {
@@ -554,7 +527,7 @@ __global__ void __launch_bounds__(128, MINB) shake_kernel(const __grid_constant_
       const double Dp = (Delta_try > 0.0 && Delta_roi > 0.0) ? fmin(Delta_try, Delta_roi) : 0.0;
       if (Dp > 0.0) {
         const double dx_exp = (s >= 0 ? +Dp : -Dp);
-        put_at(tmp, ax, x0 + dx_exp);
+        tmp[ax] = x0 + dx_exp;
         eval_geom<Real, NC>(v, tmp, S);
         bool out = false;
         for (int c = 0; c < C; ++c)
@@ -564,9 +537,9 @@ __global__ void __launch_bounds__(128, MINB) shake_kernel(const __grid_constant_
           }
         if (!out) {
           const double fexp = residue<Real, NC>(v, roi, S);
-          put_at(cx, nc, dx_exp);
-          put_at(cf, nc, fexp);
-          put_at(ca, nc, x0 + dx_exp);
+          cx[nc] = dx_exp;
+          cf[nc] = fexp;
+          ca[nc] = x0 + dx_exp;
           ++nc;
         }
         __syncwarp();
@@ -577,14 +550,12 @@ __global__ void __launch_bounds__(128, MINB) shake_kernel(const __grid_constant_
     if (allow_xhat && coef[2] > 0.0) {
       const double x_hat = -coef[1] / (2.0 * coef[2]);
       double xmin = cx[0], xmax = cx[0];
-#pragma unroll
-      for (int t = 0; t < 5; ++t) {
-        if (t >= nc) continue;
+      for (int t = 0; t < nc; ++t) {
         xmin = fmin(xmin, cx[t]);
         xmax = fmax(xmax, cx[t]);
       }
       if (x_hat >= xmin && x_hat <= xmax) {
-        put_at(tmp, ax, x0 + x_hat);
+        tmp[ax] = x0 + x_hat;
         eval_geom<Real, NC>(v, tmp, S);
         bool out = false;
         for (int c = 0; c < C; ++c)
@@ -594,39 +565,49 @@ __global__ void __launch_bounds__(128, MINB) shake_kernel(const __grid_constant_
           }
         if (!out) {
           const double fhat = residue<Real, NC>(v, roi, S);
-          put_at(cx, nc, x_hat);
-          put_at(cf, nc, fhat);
-          put_at(ca, nc, x0 + x_hat);
+          cx[nc] = x_hat;
+          cf[nc] = fhat;
+          ca[nc] = x0 + x_hat;
           ++nc;
         }
         __syncwarp();
       }
     }
-    double bf = cf[0], pa = ca[0];
-#pragma unroll
-    for (int t = 1; t < 5; ++t)
-      if (t < nc && cf[t] < bf) {
+    int best = 0;
+    double bf = cf[0];
+    for (int t = 1; t < nc; ++t)
+      if (cf[t] < bf) {
         bf = cf[t];
-        pa = ca[t];
+        best = t;
       }
-    put_at(P, ax, pa);
+    P[ax] = ca[best];
     f_final = bf;  // after the last axis: the residue at the final position
   }
 
   // ---- final projection + calObjectScore (Shake.cpp:668-782)
   eval_geom<Real, NC>(v, P, S);
-  // lane c < C: camera c's score rect and its sums (peak over the rect, sum of
-  // max(0, meas), sum of predictions, row-major); the flags and sums then reach every
-  // lane by ballot and shuffles (no run-time indexed per-lane arrays)
-  double pk = 0.0, nu = 0.0, de = 0.0;
-  bool my_use = false;
-  if (lane < C && v.cams[lane].is_active) {
+  double numer_c[NC], denom_c[NC], peak_c[NC];
+  Rect sr[NC];
+  int use[NC];
+  int n_used = 0;
+  for (int c = 0; c < C; ++c) {
+    use[c] = 0;
+    sr[c] = Rect{1, 0, 1, 0};
+    if (!v.cams[c].is_active) continue;
+    sr[c] = roi_bound(v.cams[c].n_row, v.cams[c].n_col, S.uvc[2 * c], S.uvc[2 * c + 1], v.r_px,
+                      v.r_px);
+    if (rect_empty(sr[c])) continue;
+    use[c] = 1;
+    ++n_used;
+  }
+  // per camera: peak over the rect, sum of max(0, meas), sum of predictions (in
+  // row-major order, one lane per camera)
+  if (lane < C) {
     const int c = lane;
-    const Rect R = roi_bound(v.cams[c].n_row, v.cams[c].n_col, S.uvc[2 * c], S.uvc[2 * c + 1],
-                             v.r_px, v.r_px);
-    my_use = !rect_empty(R);
-    if (my_use) {
-      const Rect Q = roi[c];
+    double pk = 0.0, nu = 0.0, de = 0.0;
+    if (use[c]) {
+      const Rect& R = sr[c];
+      const Rect& Q = roi[c];
       const bool qv = (Q.rmax - Q.rmin) > 0 && (Q.cmax - Q.cmin) > 0;
       const Real* res = reinterpret_cast<const Real*>(v.res[c].p);
       const int64_t rp = v.res[c].pitch / (int64_t)sizeof(Real);
@@ -641,15 +622,17 @@ __global__ void __launch_bounds__(128, MINB) shake_kernel(const __grid_constant_
           de += (double)gauss<Real>(cc, r, S.uvc[2 * c], S.uvc[2 * c + 1], S.otf + 5 * c);
         }
     }
+    peak_c[0] = pk;
+    numer_c[0] = nu;
+    denom_c[0] = de;
   }
-  unsigned use_bits = __ballot_sync(0xffffffffu, my_use) & ((1u << C) - 1u);
-  const int n_used = __popc(use_bits);
-  double numer_c[NC], denom_c[NC], peak_c[NC];
-#pragma unroll
-  for (int c = 0; c < C; ++c) {
-    peak_c[c] = __shfl_sync(0xffffffffu, pk, c);
-    numer_c[c] = __shfl_sync(0xffffffffu, nu, c);
-    denom_c[c] = __shfl_sync(0xffffffffu, de, c);
+  {
+    const double pk = peak_c[0], nu = numer_c[0], de = denom_c[0];
+    for (int c = 0; c < C; ++c) {
+      peak_c[c] = __shfl_sync(0xffffffffu, pk, c);
+      numer_c[c] = __shfl_sync(0xffffffffu, nu, c);
+      denom_c[c] = __shfl_sync(0xffffffffu, de, c);
+    }
   }
   double sc;
   if (n_used < 2) {
@@ -658,18 +641,16 @@ __global__ void __launch_bounds__(128, MINB) shake_kernel(const __grid_constant_
     if (n_used > 2) {
       int max_id = -1;
       double max_v = -__longlong_as_double(0x7ff0000000000000LL);
-#pragma unroll
       for (int c = 0; c < C; ++c)
-        if (((use_bits >> c) & 1u) && peak_c[c] > max_v) {
+        if (use[c] && peak_c[c] > max_v) {
           max_v = peak_c[c];
           max_id = c;
         }
-      if (max_id >= 0) use_bits &= ~(1u << max_id);
+      if (max_id >= 0) use[max_id] = 0;
     }
     double tn = 0.0, td = 0.0;
-#pragma unroll
     for (int c = 0; c < C; ++c) {
-      if (!((use_bits >> c) & 1u)) continue;
+      if (!use[c]) continue;
       tn += numer_c[c];
       td += denom_c[c];
     }
@@ -970,9 +951,6 @@ static ShakeView make_view(olpt_ctx* ctx, const ShakeParams& sp, bool fp64) {
   off = (off + 15) / 16 * 16;
   v.off_uv = off;
   off += 3 * (size_t)v.n_cam * 2 * 8;
-  off = (off + 15) / 16 * 16;
-  v.off_roi = off;
-  off += (size_t)v.n_cam * sizeof(Rect);
   v.smem_per_warp = (off + 15) / 16 * 16;
   return v;
 }

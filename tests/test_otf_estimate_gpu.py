@@ -1,8 +1,9 @@
 """OTF estimation on the device (olpt_otf_estimate) against the reference's own
 OTF::estimateUniformOTFFromImage compiled from its sources: equal to the last bit on
 8-bit and 12-bit images with more than the 1000 detections per image the reference
-samples, on float images with non-integer samples, and skipped where the reference
-skips (an image without detections)."""
+samples, within 1e-10 relative on float images with non-integer samples (their
+detections' sub-pixel fits use CUDA's log), and skipped where the reference skips (an
+image without detections)."""
 import numpy as np
 import pytest
 
@@ -46,7 +47,14 @@ def test_otf_estimate_equals_reference(kind):
     print(f"{kind}: reference (a, b, c) = {want[:3]}, device = {got}, {n} samples, "
           f"pixels above threshold {counts}")
     assert want is not None and got is not None and n > 0
-    assert np.array_equal(got, want[:3])
+    if kind == "float":
+        # the detections' sub-pixel centres on non-integer float images are fitted with
+        # CUDA's log (integer levels use the C library's values), so the centres, and with
+        # them the window squares, can differ from the reference's in the last bit
+        print(f"max relative difference {np.max(np.abs(got - want[:3]) / np.abs(want[:3])):.2e}")
+        assert np.allclose(got, want[:3], rtol=1e-10, atol=0)
+    else:
+        assert np.array_equal(got, want[:3])
     assert want[3] == 0.0
 
 
