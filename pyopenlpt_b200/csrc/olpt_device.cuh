@@ -205,12 +205,6 @@ __device__ __forceinline__ void poly_powers(const double P[3], double pw[3][4]) 
   }
 }
 
-// Entry e (0..3) of a power row, by selects: a table indexed at run time would live
-// in local memory, the selects keep it in registers.
-__device__ __forceinline__ double pick4(const double (&p)[4], int e) {
-  return e == 0 ? p[0] : (e == 1 ? p[1] : (e == 2 ? p[2] : p[3]));
-}
-
 // Camera::polyProject (Camera.cpp:969-990).
 __device__ __forceinline__ void poly_project(const CamDev& c, double X, double Y, double Z,
                                              double& u, double& v) {
@@ -224,8 +218,8 @@ __device__ __forceinline__ void poly_project(const CamDev& c, double X, double Y
       double vv = c.vcoef[4 * i];
 #pragma unroll
       for (int j = 1; j < 4; ++j) {
-        uv *= pick4(pw[j - 1], (int)c.ucoef[4 * i + j]);
-        vv *= pick4(pw[j - 1], (int)c.vcoef[4 * i + j]);
+        uv *= pw[j - 1][(int)c.ucoef[4 * i + j]];
+        vv *= pw[j - 1][(int)c.vcoef[4 * i + j]];
       }
       su += uv;
       sv += vv;
@@ -264,13 +258,12 @@ __device__ __forceinline__ void poly_img_to_world(const CamDev& c, double pu, do
     for (int i = 0; i < n; ++i) {
       double dudx = c.ducoef[4 * i], dudy = c.ducoef[4 * (i + n)];
       double dvdx = c.dvcoef[4 * i], dvdy = c.dvcoef[4 * (i + n)];
-#pragma unroll
       for (int j = 1; j < 4; ++j) {
         if (c.pow3) {
-          dudx *= pick4(pw[j - 1], (int)c.ducoef[4 * i + j]);
-          dudy *= pick4(pw[j - 1], (int)c.ducoef[4 * (i + n) + j]);
-          dvdx *= pick4(pw[j - 1], (int)c.dvcoef[4 * i + j]);
-          dvdy *= pick4(pw[j - 1], (int)c.dvcoef[4 * (i + n) + j]);
+          dudx *= pw[j - 1][(int)c.ducoef[4 * i + j]];
+          dudy *= pw[j - 1][(int)c.ducoef[4 * (i + n) + j]];
+          dvdx *= pw[j - 1][(int)c.dvcoef[4 * i + j]];
+          dvdy *= pw[j - 1][(int)c.dvcoef[4 * (i + n) + j]];
         } else {
           dudx *= poly_pow(P[j - 1], c.ducoef[4 * i + j]);
           dudy *= poly_pow(P[j - 1], c.ducoef[4 * (i + n) + j]);
