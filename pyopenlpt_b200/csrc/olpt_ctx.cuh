@@ -322,6 +322,9 @@ struct StbState {
   IprParams ipr;
   bool configured = false;
   TrackList short_active, long_active, long_inactive, exited;
+  // capacity kept for the frame loop's temporary lists: one spare per role, so that the
+  // long-track and short-track buffers each circulate between their list and its spare
+  TrackList spare_long, spare_short;
   std::vector<std::vector<double>> ipr_xyz;   // initial phase, per frame
   std::vector<std::vector<char>> ipr_tracked;
   std::vector<double> linfit_kernel;          // 2 x n_pts

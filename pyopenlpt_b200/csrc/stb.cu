@@ -708,6 +708,22 @@ void last_points(const TrackH& tr, int k, double* dst) {
   std::copy(tr.xyz.end() - 3 * k, tr.xyz.end(), dst);
 }
 
+// The frame loop's temporary track lists reuse the capacity of earlier frames' lists:
+// a list of 10^5 tracks is tens of MB, and an allocation that size is fresh pages (and
+// their faults) on every frame.
+TrackList take_list(TrackList& spare, size_t n) {
+  TrackList t;
+  t.swap(spare);
+  t.clear();
+  t.reserve(n);
+  return t;
+}
+
+void give_list(TrackList& spare, TrackList& t) {
+  t.clear();
+  if (t.capacity() > spare.capacity()) spare.swap(t);
+}
+
 // Copy of the current images: what STB::processFrame leaves in img_list (the input
 // in the initial phase, the residual of the shaken predictions in the convergence
 // phase; the IPR works on its own copy).
@@ -1007,8 +1023,7 @@ void conv_phase(olpt_ctx* ctx, int frame) {
     OLPT_CUDA(cudaGetLastError());
     pred = download(W.b.as<double>(), 3 * (size_t)n_la, s);
     const std::vector<int> in_range = download(W.link.as<int>(), n_la, s);
-    TrackList kept;
-    kept.reserve(n_la);
+    TrackList kept = take_list(S.spare_long, n_la);
     size_t w = 0;
     for (int i = 0; i < n_la; ++i) {
       if (!in_range[i]) {
@@ -1021,6 +1036,7 @@ void conv_phase(olpt_ctx* ctx, int frame) {
       }
     }
     S.long_active.swap(kept);
+    give_list(S.spare_long, kept);
     n_la = (int)w;
     pred.resize(3 * w);
   }
@@ -1065,8 +1081,7 @@ void conv_phase(olpt_ctx* ctx, int frame) {
       sx = sx0;
       fl = fl0;
     }
-    TrackList kept;
-    kept.reserve(n_la);
+    TrackList kept = take_list(S.spare_long, n_la);
     for (int i = 0; i < n_la; ++i) {
       TrackH& tr = S.long_active[i];
       if (fl[i] == 0) {
@@ -1080,6 +1095,7 @@ void conv_phase(olpt_ctx* ctx, int frame) {
       }
     }
     S.long_active.swap(kept);
+    give_list(S.spare_long, kept);
     n_la = (int)S.long_active.size();
   }
 
@@ -1162,8 +1178,7 @@ void conv_phase(olpt_ctx* ctx, int frame) {
         link[j] = -1;
     }
     std::vector<char> used(n_obj, 0);
-    TrackList keep;
-    keep.reserve(n_sa + n_obj);
+    TrackList keep = take_list(S.spare_short, (size_t)n_sa + n_obj);
     for (int i = 0; i < n_sa; ++i) {
       const int lid = link[i];
       if (lid < 0 || lid >= n_obj) continue;
@@ -1177,6 +1192,7 @@ void conv_phase(olpt_ctx* ctx, int frame) {
         keep.push_back(std::move(tr));
     }
     S.short_active.swap(keep);
+    give_list(S.spare_short, keep);
     S.short_active.reserve(S.short_active.size() + n_obj);
     for (int i = 0; i < n_obj; ++i) {
       if (used[i]) continue;
@@ -1207,8 +1223,7 @@ void conv_phase(olpt_ctx* ctx, int frame) {
                                                     W.link.as<int>());
     OLPT_CUDA(cudaGetLastError());
     const std::vector<int> ok = download(W.link.as<int>(), n_la, s);
-    TrackList kept;
-    kept.reserve(n_la);
+    TrackList kept = take_list(S.spare_long, n_la);
     for (int i = 0; i < n_la; ++i) {
       TrackH& tr = S.long_active[i];
       if (ok[i])
@@ -1217,6 +1232,7 @@ void conv_phase(olpt_ctx* ctx, int frame) {
         S.long_inactive.push_back(std::move(tr));
     }
     S.long_active.swap(kept);
+    give_list(S.spare_long, kept);
   }
   S.last_extended = extended;
   S.last_new = n_obj;
