@@ -374,20 +374,24 @@ PHASE_NAMES = {5: "detection", 6: "stereo matching (all)", 7: "candidate sort + 
                15: "track work: linear-fit pruning"}
 
 
-# DRAM bytes per shaken object (dram__bytes_read.sum + dram__bytes_write.sum of three
-# shake_kernel launches of the STB convergence frames, 16-19 k objects each, divided by
-# their objects), and the kernel's algorithmic bytes per object for 4 cameras in FP32:
-# 4 x 64 ROI pixels x 4 B + 2 x (24 + 4 x 16 + 8) B of state + 4 x 5 x 4 B of OTF.
-SHAKE_DRAM_BYTES_PER_OBJECT = 7_300.0
-SHAKE_ALGO_BYTES_PER_OBJECT = 1_296.0
+# Per camera count: DRAM bytes per shaken object measured with ncu, and the kernel's
+# algorithmic bytes per object in FP32 (C x 64 ROI pixels x 4 B + 2 x (24 + C x 16 + 8) B
+# of state + C x 5 x 4 B of OTF).  4 cameras: dram__bytes_read.sum + dram__bytes_write.sum
+# of three shake_kernel launches of the 1280x800 STB convergence frames (16-19 k objects
+# each) over their objects.  6 cameras: two launches of the first IPR of a 2048^2 headline
+# frame (14,840 objects each), dram__bytes.sum.per_second x duration over the objects.
+SHAKE_TRAFFIC = {4: (7_300.0, 1_296.0), 6: (22_440.0, 1_912.0)}
 
 
-def shake_traffic(args, prec, dom, bytes_per_launch):
+def shake_traffic(args, prec, dom, bytes_per_launch, cams):
     """DRAM traffic of an average shake launch of the STB workload, scaled from the
     per-object figure by the objects the launch processes; None elsewhere."""
     if dom != 3 or prec != 0 or WORKLOADS[args.workload]["kind"] != "stb":
         return None
-    return bytes_per_launch / SHAKE_ALGO_BYTES_PER_OBJECT * SHAKE_DRAM_BYTES_PER_OBJECT
+    if cams not in SHAKE_TRAFFIC:
+        return None
+    dram, algo = SHAKE_TRAFFIC[cams]
+    return bytes_per_launch / algo * dram
 
 
 def reduce_replicas(dist, values, device):
@@ -473,7 +477,8 @@ class Ours:
                          "peak_source": peak_kind,
                          "bytes_per_launch": by / nl if nl else 0.0,
                          "launch_ms": ms / nl if nl else 0.0,
-                         "traffic": shake_traffic(args, self.prec, dom, by / nl if nl else 0.0)},
+                         "traffic": shake_traffic(args, self.prec, dom, by / nl if nl else 0.0,
+                                                  cfg.get("cameras"))},
             "cpu_baseline": cpu,
             "clocks": clk,
         }
